@@ -1,0 +1,196 @@
+/*
+ * cgx.h -- B200 (sm_100a) compressible-LES right-hand side and RK3 step for
+ * periodic Voronoi meshes: the C ABI that a host solver calls in place of the
+ * reference's IdealGasSolver hot path.
+ *
+ * Reference interface replaced (paths relative to the reference source tree):
+ *   IdealGasSolver::calcRhs                 src/charles/ideal_gas/IdealGasSolver.hpp:697-705
+ *     -> calcRhsBase                        src/charles/ideal_gas/IdealGasSolver.cpp:257-535
+ *   IdealGasSolver::rk3Step                 src/charles/ideal_gas/IdealGasSolver.hpp:692,
+ *                                           IdealGasSolver.cpp:840-872
+ *   updateConservativeAndPrimitiveData      src/charles/ideal_gas/IdealGasSolver.hpp:732-759
+ *   calcSgsAndMaterialProperties            src/charles/ideal_gas/IdealGasSolver.cpp:182-255
+ *     (computeSgsVreman IdealGasSolverSgs.cpp:207-296, setFgrCvs IdealGasSolver.cpp:894-984)
+ *   calcCfl                                 src/charles/ideal_gas/IdealGasSolver.cpp:1048-1095
+ *   setDt (TIMESTEP DT|CFL|CFL_DT)          src/charles/FlowSolver.hpp:2274-2328
+ *   advanceSolution                         src/charles/ideal_gas/IdealGasSolver.hpp:414-594
+ *   checkForNans / storeData / restoreData  src/charles/ideal_gas/IdealGasSolver.hpp:303-405,596-611
+ *   report() conservation totals            src/charles/ideal_gas/IdealGasSolver.hpp:825-838
+ *
+ * Conventions
+ *   - Every function returns CGX_OK (0) or a negative CGX_E_* code and never
+ *     throws; cgx_last_error() gives the text of the last failure on the
+ *     calling thread.
+ *   - Host arrays are in the caller's (reference) cell numbering and layout:
+ *     rho[ncv], u[ncv][3], rhoE[ncv], rhs[ncv][5] = {rho, rhou[3], rhoE}.
+ *     The library renumbers cells internally on a space-filling curve and
+ *     keeps the permutation.
+ *   - The library owns all device memory.  A solver handle is not
+ *     thread-safe; all of its work is ordered on one CUDA stream.
+ *   - Ghost cells are translated copies of owned cells (periodic boxes); the
+ *     library resolves them to their owners and stores no ghost data.
+ */
+#ifndef CGX_H
+#define CGX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGX_OK          0
+#define CGX_E_ARG      -1   /* invalid argument or inconsistent mesh */
+#define CGX_E_OOM      -2   /* host or device allocation failed */
+#define CGX_E_CUDA     -3   /* a CUDA call failed */
+#define CGX_E_NAN      -4   /* NaN detected; state restored (advanceSolution -1) */
+#define CGX_E_TIMEOUT  -5   /* a bounded device wait gave up */
+#define CGX_E_STATE    -6   /* call out of order (e.g. step before set_state) */
+
+typedef enum cgx_precision {
+  CGX_FP64  = 0,   /* all arithmetic in FP64 */
+  CGX_MIXED = 1    /* FP32 flux/gradient/SGS arithmetic, FP64 face sums,
+                      FP64 state, pressure recovery, dt and reductions */
+} cgx_precision;
+
+/* TIMESTEP modes (FlowSolver.hpp:2274-2328) */
+#define CGX_DT_CONST   0   /* TIMESTEP DT <dt>              */
+#define CGX_DT_CFL     1   /* TIMESTEP CFL <cfl>            */
+#define CGX_DT_CFL_DT  2   /* TIMESTEP CFL_DT <cfl> <dtmax> */
+
+/* SGS_MODEL */
+#define CGX_SGS_NONE    0
+#define CGX_SGS_VREMAN  1
+
+/* NO_DISS / ALL_DISS switches of setFgrCvs */
+#define CGX_DISS_SENSOR 0
+#define CGX_DISS_NONE   1
+#define CGX_DISS_ALL    2
+
+/* Solver parameters; names follow the reference's input-file keys. */
+typedef struct cgx_params {
+  double gamma;            /* GAMMA 1.4 */
+  double p_ref;            /* P_REF */
+  double rho_ref;          /* RHO_REF */
+  double T_ref;            /* T_REF */
+  double mu_ref;           /* MU_REF */
+  double mu_power_law;     /* MU_POWER_LAW 0.75 */
+  double Pr_lam;           /* PR_LAM 0.7 */
+  int    sgs_model;        /* SGS_MODEL (CGX_SGS_*) */
+  double vreman_coeff;     /* VREMAN_COEFF 0.07 */
+  double a_sgs_coeff;      /* A_SGS_COEFF 0.05 */
+  double a_sgs_coeff2;     /* A_SGS_COEFF2 0.0015 */
+  double lambda_dil_coeff; /* LAMBDA_DIL_COEFF 0 */
+  double Pr_t;             /* PR_T 0.9 */
+  double coeff_p;          /* COEFF_P 0.5 */
+  double coeff_h;          /* COEFF_H 0.1 */
+  double gr_nrm;           /* GR_NRM 0.03 */
+  int    diss_mode;        /* CGX_DISS_* */
+  int    dt_mode;          /* CGX_DT_* */
+  double dt_data[2];       /* DT: {dt}; CFL: {cfl}; CFL_DT: {cfl, dt_max} */
+  int    check_interval;   /* CHECK_INTERVAL (NaN store cadence) */
+} cgx_params;
+
+/* Fill with the reference's defaults (P_REF, RHO_REF, T_REF, MU_REF = 1). */
+void cgx_params_default(cgx_params* p);
+
+/*
+ * Mesh in the reference's single-rank layout (StaticSolver.hpp:416-481):
+ * owned cells [0,ncv), ghosts [ncv,ncv_g2) with icv_owner_g[ig-ncv] their
+ * owners; compact faces cvofa/n_fa/area_over_delta_fa (a face whose second
+ * cell is a ghost updates only its first cell); compact CSR cvocv_i/v (the
+ * diagonal first) with cvocv_grad_coeff; extended faces cvoef/n_ef/c_ef with
+ * c_ef NOT halved (as StaticSolver stores it); dcmag_hat_cv and
+ * sa_to_vol_ratio as FlowSolver::init() computes them.  x_cv[ncv][3] is
+ * optional: when given, cells are renumbered on a space-filling curve of x_cv.
+ */
+typedef struct cgx_mesh_desc {
+  int ncv, ncv_g2;
+  int nfa, nef;
+  const int*    cvofa;              /* [nfa][2] */
+  const double* n_fa;               /* [nfa][3] */
+  const double* area_over_delta_fa; /* [nfa] */
+  const double* vol_cv;             /* [ncv] */
+  const int*    cvocv_i;            /* [ncv+1] */
+  const int*    cvocv_v;            /* [cvocv_i[ncv]] */
+  const double* cvocv_grad_coeff;   /* [cvocv_i[ncv]][3] */
+  const int*    cvoef;              /* [nef][2] */
+  const double* n_ef;               /* [nef][3] */
+  const double* c_ef;               /* [nef][3] */
+  const double* dcmag_hat_cv;       /* [ncv] */
+  const double* sa_to_vol_ratio;    /* [ncv] */
+  const int*    icv_owner_g;        /* [ncv_g2-ncv] */
+  const double* x_cv;               /* [ncv][3] or NULL */
+} cgx_mesh_desc;
+
+typedef struct cgx_mesh cgx_mesh;
+typedef struct cgx_solver cgx_solver;
+
+typedef struct cgx_mesh_stats {
+  int    ncv;
+  long long n_ef_dir;      /* directed extended-face entries (2 per internal face) */
+  long long n_cf_dir;      /* directed compact-face entries */
+  double e_per_cell;       /* extended faces per cell, each face once */
+  double f_per_cell;       /* compact faces per cell, each face once */
+  size_t device_bytes;     /* device memory held by the mesh */
+} cgx_mesh_stats;
+
+/* Copy the mesh to device `device`, renumber it and build the CSR layouts. */
+int cgx_mesh_create(const cgx_mesh_desc* desc, int device, cgx_mesh** out);
+int cgx_mesh_stats_get(const cgx_mesh* m, cgx_mesh_stats* out);
+int cgx_mesh_destroy(cgx_mesh* m);
+
+int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision prec,
+                      cgx_solver** out);
+int cgx_solver_destroy(cgx_solver* s);
+
+/* Conserved state in reference order (host arrays). */
+int cgx_set_state(cgx_solver* s, const double* rho, const double* u, const double* rhoE);
+/* rho, u, p; rhoE = p/(gamma-1) + 0.5 rho |u|^2 (IdealGasSolver.hpp:275-301). */
+int cgx_set_state_primitive(cgx_solver* s, const double* rho, const double* u,
+                            const double* p);
+int cgx_get_state(cgx_solver* s, double* rho, double* u, double* rhoE);
+
+/* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
+ * then stores the state for NaN recovery (initialHookBcs -> storeData). */
+int cgx_init_complete(cgx_solver* s);
+int cgx_update_primitive(cgx_solver* s);
+int cgx_calc_sgs_props(cgx_solver* s);
+
+/* calcRhs into the solver's rhs buffer of rk_stage (1..3), which is zeroed
+ * first; if rhs_out != NULL the result is also copied out in reference order
+ * as [ncv][5] (unscaled face sums, as the reference stores them). */
+int cgx_calc_rhs(cgx_solver* s, double* rhs_out, double time, int rk_stage);
+/* rk3Step with weights w over the rhs buffers of stages 1..rk_stage. */
+int cgx_rk3_step(cgx_solver* s, const double w[3], double dt, int rk_stage);
+/* calcCfl(cfl, dt): rank-local max; cfl[ncv] optional (reference order). */
+int cgx_calc_cfl(cgx_solver* s, double dt, double* cfl_max, double* cfl);
+
+/* One advanceSolution with the current dt (setDt not included).  Returns
+ * CGX_E_NAN after restoring the stored state and scaling dt_data[0] by 0.8. */
+int cgx_advance_solution(cgx_solver* s);
+/* nsteps of {setDt; advanceSolution}, dt and time kept on the device, the
+ * step replayed from a CUDA graph.  NaNs are checked every check_interval
+ * steps and after the last one (CGX_E_NAN as above). */
+int cgx_step(cgx_solver* s, int nsteps);
+
+int cgx_get_time(cgx_solver* s, double* time, double* dt, int* step);
+/* report(): {sum rho V, sum rho u V (3), sum rhoE V}, fixed-order reduction. */
+int cgx_totals(cgx_solver* s, double out[5]);
+
+/* Diagnostics in reference order: p, T, sos [ncv]; dudx [ncv][3][3];
+ * aux [ncv][6] = {mu_total, loc_total, a_sgs, fgr, symh_fax, symp_fax}. */
+int cgx_get_primitive(cgx_solver* s, double* p, double* T, double* sos);
+int cgx_get_grad(cgx_solver* s, double* dudx);
+int cgx_get_aux(cgx_solver* s, double* aux);
+
+int cgx_synchronize(cgx_solver* s);
+/* Number of this library's kernels launched by the handle so far. */
+long long cgx_launch_count(const cgx_solver* s);
+
+const char* cgx_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

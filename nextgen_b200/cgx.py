@@ -1,0 +1,334 @@
+"""Host-side mirror of the reference solver interface over the C ABI
+(include/cgx.h).
+
+`Solver` exposes the reference's IdealGasSolver hot-path calls under their
+reference names (calcRhs, rk3Step, updateConservativeAndPrimitiveData,
+calcSgsAndMaterialProperties, calcCfl, advanceSolution, setDt-driven stepping,
+report() totals) on top of libcgx.so, with host numpy arrays in the caller's
+cell order.  Errors from the library raise `CgxError` carrying the library's
+message; there is no fallback path: without libcgx.so or a GPU the calls fail.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_dbl_p = ctypes.POINTER(ctypes.c_double)
+
+CGX_FP64 = 0
+CGX_MIXED = 1
+
+ERRORS = {-1: "CGX_E_ARG", -2: "CGX_E_OOM", -3: "CGX_E_CUDA", -4: "CGX_E_NAN",
+          -5: "CGX_E_TIMEOUT", -6: "CGX_E_STATE"}
+
+
+class CgxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "?"), code, msg))
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    """cgx_params: solver parameters named after the reference's input keys."""
+    _fields_ = [
+        ("gamma", ctypes.c_double), ("p_ref", ctypes.c_double), ("rho_ref", ctypes.c_double),
+        ("T_ref", ctypes.c_double), ("mu_ref", ctypes.c_double),
+        ("mu_power_law", ctypes.c_double), ("Pr_lam", ctypes.c_double),
+        ("sgs_model", ctypes.c_int),
+        ("vreman_coeff", ctypes.c_double), ("a_sgs_coeff", ctypes.c_double),
+        ("a_sgs_coeff2", ctypes.c_double), ("lambda_dil_coeff", ctypes.c_double),
+        ("Pr_t", ctypes.c_double),
+        ("coeff_p", ctypes.c_double), ("coeff_h", ctypes.c_double), ("gr_nrm", ctypes.c_double),
+        ("diss_mode", ctypes.c_int), ("dt_mode", ctypes.c_int),
+        ("dt_data", ctypes.c_double * 2), ("check_interval", ctypes.c_int),
+    ]
+
+    def __init__(self, **kw):
+        super().__init__()
+        # reference defaults (IdealGasSolver.hpp:147-155, IdealGasSolverSgs.cpp:209-213,
+        # IdealGasSolver.cpp:202-203,904)
+        self.gamma = 1.4
+        self.p_ref = 1.0
+        self.rho_ref = 1.0
+        self.T_ref = 1.0
+        self.mu_ref = 1.0
+        self.mu_power_law = 0.75
+        self.Pr_lam = 0.7
+        self.sgs_model = 0
+        self.vreman_coeff = 0.07
+        self.a_sgs_coeff = 0.05
+        self.a_sgs_coeff2 = 0.0015
+        self.lambda_dil_coeff = 0.0
+        self.Pr_t = 0.9
+        self.coeff_p = 0.5
+        self.coeff_h = 0.1
+        self.gr_nrm = 0.03
+        self.diss_mode = 0
+        self.dt_mode = 1
+        self.dt_data[0] = 0.8
+        self.dt_data[1] = 0.0
+        self.check_interval = 1
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+    def copy(self):
+        p = Params()
+        ctypes.pointer(p)[0] = self
+        return p
+
+
+class MeshDesc(ctypes.Structure):
+    """cgx_mesh_desc: the reference's single-rank mesh arrays."""
+    _fields_ = [
+        ("ncv", ctypes.c_int), ("ncv_g2", ctypes.c_int), ("nfa", ctypes.c_int), ("nef", ctypes.c_int),
+        ("cvofa", c_int_p), ("n_fa", c_dbl_p), ("area_over_delta_fa", c_dbl_p),
+        ("vol_cv", c_dbl_p), ("cvocv_i", c_int_p), ("cvocv_v", c_int_p),
+        ("cvocv_grad_coeff", c_dbl_p), ("cvoef", c_int_p), ("n_ef", c_dbl_p), ("c_ef", c_dbl_p),
+        ("dcmag_hat_cv", c_dbl_p), ("sa_to_vol_ratio", c_dbl_p), ("icv_owner_g", c_int_p),
+        ("x_cv", c_dbl_p),
+    ]
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+def mesh_desc(mesh, with_x=True):
+    """cgx_mesh_desc over the arrays of a PeriodicBoxMesh (or any object with
+    the same attribute names).  The arrays must outlive the descriptor."""
+    d = MeshDesc()
+    d.ncv, d.ncv_g2, d.nfa, d.nef = mesh.ncv, mesh.ncv_g2, mesh.nfa, mesh.nef
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a
+    d.cvofa = _p(arr(mesh.cvofa, np.int32), ctypes.c_int)
+    d.n_fa = _p(arr(mesh.n_fa, np.float64), ctypes.c_double)
+    d.area_over_delta_fa = _p(arr(mesh.area_over_delta_fa, np.float64), ctypes.c_double)
+    d.vol_cv = _p(arr(mesh.vol_cv, np.float64), ctypes.c_double)
+    d.cvocv_i = _p(arr(mesh.cvocv_i, np.int32), ctypes.c_int)
+    d.cvocv_v = _p(arr(mesh.cvocv_v, np.int32), ctypes.c_int)
+    d.cvocv_grad_coeff = _p(arr(mesh.cvocv_grad_coeff, np.float64), ctypes.c_double)
+    d.cvoef = _p(arr(mesh.cvoef, np.int32), ctypes.c_int)
+    d.n_ef = _p(arr(mesh.n_ef, np.float64), ctypes.c_double)
+    d.c_ef = _p(arr(mesh.c_ef, np.float64), ctypes.c_double)
+    d.dcmag_hat_cv = _p(arr(mesh.dcmag_hat_cv, np.float64), ctypes.c_double)
+    d.sa_to_vol_ratio = _p(arr(mesh.sa_to_vol_ratio, np.float64), ctypes.c_double)
+    d.icv_owner_g = _p(arr(mesh.icv_owner_g, np.int32), ctypes.c_int)
+    d.x_cv = _p(arr(mesh.x_cv[: mesh.ncv], np.float64), ctypes.c_double) if with_x else None
+    d._keep = keep
+    return d
+
+
+class MeshStats(ctypes.Structure):
+    _fields_ = [("ncv", ctypes.c_int), ("n_ef_dir", ctypes.c_longlong),
+                ("n_cf_dir", ctypes.c_longlong), ("e_per_cell", ctypes.c_double),
+                ("f_per_cell", ctypes.c_double), ("device_bytes", ctypes.c_size_t)]
+
+
+EXPORTS = [
+    "cgx_params_default", "cgx_mesh_create", "cgx_mesh_stats_get", "cgx_mesh_destroy",
+    "cgx_solver_create", "cgx_solver_destroy", "cgx_set_state", "cgx_set_state_primitive",
+    "cgx_get_state", "cgx_init_complete", "cgx_update_primitive", "cgx_calc_sgs_props",
+    "cgx_calc_rhs", "cgx_rk3_step", "cgx_calc_cfl", "cgx_advance_solution", "cgx_step",
+    "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
+    "cgx_synchronize", "cgx_launch_count", "cgx_last_error",
+]
+
+_LIB = None
+
+
+def lib():
+    """libcgx.so with argument types declared."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    L = _lib.load("libcgx.so")
+    vp = ctypes.c_void_p
+    sig = {
+        "cgx_params_default": (None, [ctypes.POINTER(Params)]),
+        "cgx_mesh_create": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.POINTER(vp)]),
+        "cgx_mesh_stats_get": (ctypes.c_int, [vp, ctypes.POINTER(MeshStats)]),
+        "cgx_mesh_destroy": (ctypes.c_int, [vp]),
+        "cgx_solver_create": (ctypes.c_int, [vp, ctypes.POINTER(Params), ctypes.c_int, ctypes.POINTER(vp)]),
+        "cgx_solver_destroy": (ctypes.c_int, [vp]),
+        "cgx_set_state": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "cgx_set_state_primitive": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "cgx_get_state": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "cgx_init_complete": (ctypes.c_int, [vp]),
+        "cgx_update_primitive": (ctypes.c_int, [vp]),
+        "cgx_calc_sgs_props": (ctypes.c_int, [vp]),
+        "cgx_calc_rhs": (ctypes.c_int, [vp, c_dbl_p, ctypes.c_double, ctypes.c_int]),
+        "cgx_rk3_step": (ctypes.c_int, [vp, c_dbl_p, ctypes.c_double, ctypes.c_int]),
+        "cgx_calc_cfl": (ctypes.c_int, [vp, ctypes.c_double, c_dbl_p, c_dbl_p]),
+        "cgx_advance_solution": (ctypes.c_int, [vp]),
+        "cgx_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "cgx_get_time": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_int_p]),
+        "cgx_totals": (ctypes.c_int, [vp, c_dbl_p]),
+        "cgx_get_primitive": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "cgx_get_grad": (ctypes.c_int, [vp, c_dbl_p]),
+        "cgx_get_aux": (ctypes.c_int, [vp, c_dbl_p]),
+        "cgx_synchronize": (ctypes.c_int, [vp]),
+        "cgx_launch_count": (ctypes.c_longlong, [vp]),
+        "cgx_last_error": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise CgxError(rc, lib().cgx_last_error().decode())
+    return rc
+
+
+def _out(n, *shape):
+    return np.empty((n,) + shape, dtype=np.float64)
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(c_dbl_p)
+
+
+class Mesh:
+    """Device copy of a mesh (cgx_mesh_create)."""
+
+    def __init__(self, mesh, device=0, sfc=True):
+        self.desc = mesh_desc(mesh, with_x=sfc)
+        self.ncv = mesh.ncv
+        h = ctypes.c_void_p()
+        _check(lib().cgx_mesh_create(ctypes.byref(self.desc), int(device), ctypes.byref(h)))
+        self.h = h
+
+    def stats(self):
+        st = MeshStats()
+        _check(lib().cgx_mesh_stats_get(self.h, ctypes.byref(st)))
+        return st
+
+    def close(self):
+        if self.h:
+            lib().cgx_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """IdealGasSolver hot path on the GPU (cgx_solver_*)."""
+
+    def __init__(self, mesh, params, precision=CGX_FP64):
+        self.mesh = mesh
+        self.ncv = mesh.ncv
+        self.params = params
+        h = ctypes.c_void_p()
+        _check(lib().cgx_solver_create(mesh.h, ctypes.byref(params), int(precision), ctypes.byref(h)))
+        self.h = h
+
+    # -- state ------------------------------------------------------------
+    def set_state(self, rho, u, rhoE):
+        rho, u, rhoE = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, rhoE))
+        _check(lib().cgx_set_state(self.h, _dp(rho), _dp(u), _dp(rhoE)))
+
+    def set_state_primitive(self, rho, u, p):
+        rho, u, p = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, p))
+        _check(lib().cgx_set_state_primitive(self.h, _dp(rho), _dp(u), _dp(p)))
+
+    def get_state(self):
+        rho, u, rhoE = _out(self.ncv), _out(self.ncv, 3), _out(self.ncv)
+        _check(lib().cgx_get_state(self.h, _dp(rho), _dp(u), _dp(rhoE)))
+        return rho, u, rhoE
+
+    # -- reference calls ----------------------------------------------------
+    def initComplete(self):
+        _check(lib().cgx_init_complete(self.h))
+
+    def updateConservativeAndPrimitiveData(self):
+        _check(lib().cgx_update_primitive(self.h))
+
+    def calcSgsAndMaterialProperties(self):
+        _check(lib().cgx_calc_sgs_props(self.h))
+
+    def calcRhs(self, rk_stage=1, time=0.0, copy_out=True):
+        out = _out(self.ncv, 5) if copy_out else None
+        _check(lib().cgx_calc_rhs(self.h, _dp(out), float(time), int(rk_stage)))
+        return out
+
+    def rk3Step(self, rk_wgt, dt, rk_stage):
+        w = np.ascontiguousarray(rk_wgt, dtype=np.float64)
+        _check(lib().cgx_rk3_step(self.h, _dp(w), float(dt), int(rk_stage)))
+
+    def calcCfl(self, dt=1.0, want_cells=False):
+        mx = ctypes.c_double()
+        cfl = _out(self.ncv) if want_cells else None
+        _check(lib().cgx_calc_cfl(self.h, float(dt), ctypes.byref(mx), _dp(cfl)))
+        return (mx.value, cfl) if want_cells else mx.value
+
+    def advanceSolution(self):
+        """0, or -1 after a NaN (state restored, dt_data[0] scaled by 0.8)."""
+        rc = lib().cgx_advance_solution(self.h)
+        if rc == -4:
+            return -1
+        _check(rc)
+        return 0
+
+    def step(self, nsteps):
+        """nsteps of setDt + advanceSolution; 0 or -1 after a NaN."""
+        rc = lib().cgx_step(self.h, int(nsteps))
+        if rc == -4:
+            return -1
+        _check(rc)
+        return 0
+
+    def time(self):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().cgx_get_time(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))
+        return t.value, dt.value, st.value
+
+    def totals(self):
+        out = np.empty(5)
+        _check(lib().cgx_totals(self.h, _dp(out)))
+        return out
+
+    def primitive(self):
+        p, T, sos = _out(self.ncv), _out(self.ncv), _out(self.ncv)
+        _check(lib().cgx_get_primitive(self.h, _dp(p), _dp(T), _dp(sos)))
+        return p, T, sos
+
+    def grad(self):
+        g = _out(self.ncv, 3, 3)
+        _check(lib().cgx_get_grad(self.h, _dp(g)))
+        return g
+
+    def aux(self):
+        a = _out(self.ncv, 6)
+        _check(lib().cgx_get_aux(self.h, _dp(a)))
+        return a
+
+    def synchronize(self):
+        _check(lib().cgx_synchronize(self.h))
+
+    def launch_count(self):
+        return int(lib().cgx_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().cgx_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

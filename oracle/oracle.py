@@ -1,0 +1,170 @@
+"""ctypes access to the CPU oracle (oracle.h).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the package.
+
+`Oracle(mesh, params, nparts, reference=False)` wraps liboracle.so (restated
+face fluxes); reference=True wraps _ref/libref.so (the reference's own
+IdealGasSolverFlux.hpp compiled in place), when it has been built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libref.so")
+
+c_dbl_p = ctypes.POINTER(ctypes.c_double)
+c_int_p = ctypes.POINTER(ctypes.c_int)
+
+_libs = {}
+
+
+def ref_available():
+    return os.path.exists(REF_LIB_PATH)
+
+
+def _load(path):
+    if path in _libs:
+        return _libs[path]
+    from nextgen_b200.cgx import MeshDesc, Params
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sig = {
+        "orc_create": (vp, [ctypes.POINTER(MeshDesc), ctypes.POINTER(Params), ctypes.c_int]),
+        "orc_destroy": (None, [vp]),
+        "orc_set_state": (None, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "orc_set_state_primitive": (None, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "orc_get_state": (None, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "orc_init_complete": (None, [vp]),
+        "orc_update_primitive": (None, [vp]),
+        "orc_calc_sgs_props": (None, [vp]),
+        "orc_calc_rhs": (None, [vp, ctypes.c_int, c_dbl_p, c_dbl_p]),
+        "orc_rk3_step": (None, [vp, c_dbl_p, ctypes.c_double, ctypes.c_int]),
+        "orc_calc_cfl": (ctypes.c_double, [vp, ctypes.c_double, c_dbl_p]),
+        "orc_set_dt": (ctypes.c_double, [vp]),
+        "orc_advance_solution": (ctypes.c_int, [vp]),
+        "orc_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "orc_totals": (None, [vp, c_dbl_p]),
+        "orc_get_time": (None, [vp, c_dbl_p, c_dbl_p, c_int_p]),
+        "orc_get_primitive": (None, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "orc_get_grad": (None, [vp, c_dbl_p]),
+        "orc_get_aux": (None, [vp, c_dbl_p]),
+        "orc_poison": (None, [vp, ctypes.c_int]),
+        "orc_uses_reference_flux": (ctypes.c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _libs[path] = L
+    return L
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(c_dbl_p)
+
+
+class Oracle:
+    def __init__(self, mesh, params, nparts=1, reference=False):
+        from nextgen_b200.cgx import mesh_desc
+        path = REF_LIB_PATH if reference else LIB_PATH
+        if not os.path.exists(path):
+            raise OSError("%s not built (make -C oracle%s)" % (path, " ref" if reference else ""))
+        self.L = _load(path)
+        self.desc = mesh_desc(mesh, with_x=False)
+        self.params = params
+        self.ncv = mesh.ncv
+        self.h = self.L.orc_create(ctypes.byref(self.desc), ctypes.byref(params), int(nparts))
+        if not self.h:
+            raise RuntimeError("orc_create failed")
+        self.uses_reference_flux = bool(self.L.orc_uses_reference_flux())
+
+    def set_state(self, rho, u, rhoE):
+        rho, u, rhoE = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, rhoE))
+        self.L.orc_set_state(self.h, _dp(rho), _dp(u), _dp(rhoE))
+
+    def set_state_primitive(self, rho, u, p):
+        rho, u, p = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, p))
+        self.L.orc_set_state_primitive(self.h, _dp(rho), _dp(u), _dp(p))
+
+    def get_state(self):
+        n = self.ncv
+        rho, u, rhoE = np.empty(n), np.empty((n, 3)), np.empty(n)
+        self.L.orc_get_state(self.h, _dp(rho), _dp(u), _dp(rhoE))
+        return rho, u, rhoE
+
+    def init_complete(self):
+        self.L.orc_init_complete(self.h)
+
+    def update_primitive(self):
+        self.L.orc_update_primitive(self.h)
+
+    def calc_sgs_props(self):
+        self.L.orc_calc_sgs_props(self.h)
+
+    def calc_rhs(self, rk_stage=1, want_scale=True):
+        rhs = np.empty((self.ncv, 5))
+        scale = np.empty((self.ncv, 5)) if want_scale else None
+        self.L.orc_calc_rhs(self.h, int(rk_stage), _dp(rhs), _dp(scale))
+        return (rhs, scale) if want_scale else rhs
+
+    def rk3_step(self, w, dt, stage):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        self.L.orc_rk3_step(self.h, _dp(w), float(dt), int(stage))
+
+    def calc_cfl(self, dt=1.0):
+        cfl = np.empty(self.ncv)
+        mx = self.L.orc_calc_cfl(self.h, float(dt), _dp(cfl))
+        return mx, cfl
+
+    def set_dt(self):
+        return self.L.orc_set_dt(self.h)
+
+    def advance_solution(self):
+        return self.L.orc_advance_solution(self.h)
+
+    def step(self, n):
+        return self.L.orc_step(self.h, int(n))
+
+    def totals(self):
+        out = np.empty(5)
+        self.L.orc_totals(self.h, _dp(out))
+        return out
+
+    def time(self):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self.L.orc_get_time(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st))
+        return t.value, dt.value, st.value
+
+    def primitive(self):
+        n = self.ncv
+        p, T, sos = np.empty(n), np.empty(n), np.empty(n)
+        self.L.orc_get_primitive(self.h, _dp(p), _dp(T), _dp(sos))
+        return p, T, sos
+
+    def grad(self):
+        g = np.empty((self.ncv, 3, 3))
+        self.L.orc_get_grad(self.h, _dp(g))
+        return g
+
+    def aux(self):
+        a = np.empty((self.ncv, 6))
+        self.L.orc_get_aux(self.h, _dp(a))
+        return a
+
+    def poison(self, icv):
+        self.L.orc_poison(self.h, int(icv))
+
+    def close(self):
+        if self.h:
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
