@@ -1,0 +1,324 @@
+"""Benchmark: RK3 cell-steps/s of the compressible-LES right-hand side on a
+jittered-lattice periodic Voronoi mesh (200^3 = 8M cells by default), FP64,
+one replica per GPU.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cgx|reference]
+
+Prints one JSON line (rank 0).  value = whole-job cell-steps/s from CUDA
+events on the solver's stream around K graph-replayed steps (max over ranks);
+e2e = the same metric through the C ABI with host buffers (pinned host state
+copied in and read back every step); roofline = the face-flux kernel's
+algorithmic bytes per launch over its measured launch time against the
+measured HBM copy bandwidth; cpu_baseline = the CPU oracle on the host cores
+on a bounded sample.  `--impl reference` times the reference's CPU path (the
+oracle built on the reference's own flux header when available) instead.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 cell-steps/s @8M cells FP64 vs mixed; served solves/s, p50/p99 latency"
+UNIT = "cell-steps/s"
+JITTER = 0.25
+SEED = 1234
+
+
+def bytes_model(e, f):
+    """Algorithmic bytes per cell: whole RK3 step (3 stages + once-per-step
+    work) and one face-flux (calcRhs) launch.  Each array element counted
+    once per kernel pass, neighbour gathers assumed cached:
+      per stage  504 + 56e + 96f   (state/RK 208, packed state 80,
+                                    gradient 168 + 56f, extended faces 56e,
+                                    compact extras 40f + 48)
+      per step   320 + 8e + 32f    (SGS/properties 200, Gibbs sensor 40 + 8e,
+                                    CFL 40 + 32f, totals 40)
+      calcRhs    56e + 40f + 200   (extended faces 56e, compact geometry 40f,
+                                    lagged properties 48, packed state 40,
+                                    dudx 72, rhs write 40)"""
+    step = 3 * (504 + 56 * e + 96 * f) + (320 + 8 * e + 32 * f)
+    rhs = 56 * e + 40 * f + 200
+    return step, rhs
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.f:
+            return None
+        try:
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        finally:
+            try:
+                os.unlink(self.f.name)
+            except Exception:
+                pass
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(seconds=12.0, n=48, lib_kind="reference"):
+    """The CPU oracle on a jittered n^3 box with all host threads: RK3 steps
+    until `seconds` of CPU work have run.  Returns the cpu_baseline object."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, ref_available
+    from nextgen_b200 import cases
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    cores = os.cpu_count() or 1
+    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED)
+    prm = cases.tgv_params()
+    rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
+    use_ref = lib_kind == "reference" and ref_available()
+    o = Oracle(m, prm, nparts=cores, reference=use_ref)
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    o.step(1)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    what = ("the oracle built on the reference's own IdealGasSolverFlux.hpp/States.hpp/RkWeights.hpp "
+            "(compiled in place) with the reference's rank-parallel face loops restated"
+            if use_ref else "the oracle (restated reference hot path)")
+    return {"value": m.ncv * steps / el, "unit": UNIT, "cores": cores,
+            "kind": "reference" if use_ref else "port",
+            "sample": "%d RK3 steps of %s on a jittered %d^3 periodic Voronoi box (%d cells, TGV Ma 0.1), "
+                      "%d OpenMP ranks over contiguous cell ranges" % (steps, what, n, m.ncv, cores)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, ref_available
+    from nextgen_b200 import cases
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    cores = os.cpu_count() or 1
+    n = args.ref_n
+    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED)
+    prm = cases.tgv_params()
+    rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
+    use_ref = ref_available()
+    o = Oracle(m, prm, nparts=cores, reference=use_ref)
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    if args.warmup:
+        o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    el = time.perf_counter() - t0
+    v = m.ncv * args.steps / el
+    what = ("oracle built on the reference's own IdealGasSolverFlux.hpp/States.hpp/RkWeights.hpp compiled in place"
+            if use_ref else "oracle port of the reference hot path")
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic",
+           "config": {"workload": "jittered-lattice periodic Voronoi %d^3 sample of the %d^3 (%d-cell) case, "
+                                  "TGV Ma 0.1 Re 1600, FP64 RK3 CFL 0.8" % (n, args.n, args.n ** 3),
+                      "cells": m.ncv, "e_per_cell": m.e_per_cell, "f_per_cell": m.f_per_cell,
+                      "parallelism": "cpu %d threads" % cores},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference" if use_ref else "port",
+                            "sample": "%d RK3 steps of the %s on a jittered %d^3 box (%d cells) per run, "
+                                      "%d OpenMP ranks" % (args.steps, what, n, m.ncv, cores)},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_cgx(args):
+    import torch
+    from nextgen_b200 import cases, cgx, dist
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+
+    rank, world, local = dist.env_rank()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init("nccl")
+    device = local
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    m = PeriodicBoxMesh(args.n, jitter=JITTER, seed=SEED, nthreads=max(1, cores // world))
+    t_mesh = time.perf_counter() - t0
+    prm = cases.tgv_params()
+    rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
+    t0 = time.perf_counter()
+    gm = cgx.Mesh(m, device=device)
+    t_up = time.perf_counter() - t0
+    st = gm.stats()
+    e, f = st.e_per_cell, st.f_per_cell
+    N = m.ncv
+    x_cv = np.array(m.x_cv[:N])
+    m.close()
+
+    solvers = {}
+    res = {}
+    for prec_name, prec in (("fp64", cgx.CGX_FP64),):
+        s = cgx.Solver(gm, prm, prec)
+        s.set_state_primitive(rho, u, p)
+        s.initComplete()
+        if args.warmup:
+            s.step(args.warmup)
+        dist.barrier()
+        s.synchronize()
+        n0 = s.launch_count()
+        with ClockSampler(device) as clk:
+            ms = s.step_timed(args.steps)
+        s.synchronize()
+        dist.barrier()
+        launches = s.launch_count() - n0
+        ms_max = dist.max_over_ranks(ms)
+        res[prec_name] = {"ms": ms_max, "launches": launches, "clocks": clk.summary()}
+        solvers[prec_name] = s
+
+    s = solvers["fp64"]
+    ktimes = s.kernel_times(reps=3)
+    step_bytes, rhs_bytes = bytes_model(e, f)
+    peak, peak_kind = measured_peaks()
+    ms_step = res["fp64"]["ms"] / args.steps
+    value = world * N * args.steps / (res["fp64"]["ms"] * 1e-3)
+    achieved = rhs_bytes * N / (ktimes["rhs"] * 1e-3) / 1e9
+
+    # e2e: the C-ABI calls a host solver makes each step, with host buffers
+    r_h = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    u_h = torch.empty(3 * N, dtype=torch.float64, pin_memory=True)
+    e_h = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    s.get_state_ptr(r_h.data_ptr(), u_h.data_ptr(), e_h.data_ptr())
+    ke = max(1, min(args.steps, args.e2e_steps))
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        s.set_state_ptr(r_h.data_ptr(), u_h.data_ptr(), e_h.data_ptr())
+        s.step(1)
+        s.get_state_ptr(r_h.data_ptr(), u_h.data_ptr(), e_h.data_ptr())
+    el = time.perf_counter() - t0
+    el = dist.max_over_ranks(el)
+    e2e = world * N * ke / el
+
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "rhs_dram_bytes_per_cell.json")
+    if os.path.exists(tp):
+        try:
+            traffic = float(json.load(open(tp))["dram_bytes_per_cell"]) * N
+        except Exception:
+            traffic = None
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3 = %d cells per GPU, "
+                               "Taylor-Green Ma 0.1 Re 1600 Pr 0.71, Vreman SGS, FP64 RK3 at CFL 0.8"
+                               % (args.n, N),
+                   "cells": N, "e_per_cell": e, "f_per_cell": f,
+                   "l2": "inputs larger than L2 (%.1f GB mesh on device)" % (st.device_bytes / 1e9),
+                   "parallelism": "replicas x%d" % world, "precision": "fp64",
+                   "mesh_build_s": round(t_mesh, 2), "mesh_upload_s": round(t_up, 2)},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 40 * N, "d2h_bytes_per_step": 40 * N,
+                "steps": ke, "how": "per step: cgx_set_state (pinned host -> device), cgx_step(1), "
+                                    "cgx_get_state (device -> pinned host); host wall clock"},
+        "gpu_launches": res["fp64"]["launches"],
+        "clocks": res["fp64"]["clocks"],
+        "roofline": {"bound": "hbm", "kernel": "k_rhs (calcRhsBase)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_cell": rhs_bytes,
+                     "launch_ms": ktimes["rhs"]},
+        "step_roofline": {"bytes_per_cell_step": step_bytes, "achieved": value / world * step_bytes / 1e9,
+                          "frac": value / world * step_bytes / 1e9 / peak, "unit": "GB/s"},
+        "kernel_ms": ktimes,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds, n=args.cpu_n)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    for k in list(solvers):
+        solvers[k].close()
+    gm.close()
+    dist.finalize()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cgx", choices=["cgx", "reference"])
+    ap.add_argument("--n", type=int, default=200, help="lattice edge (cells = n^3)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-n", type=int, default=48)
+    ap.add_argument("--ref-n", type=int, default=48)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 0 or args.steps < 1:
+        sys.exit("steps >= 1, warmup >= 0")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_cgx(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -174,6 +174,7 @@ int cgx_advance_solution(cgx_solver* s);
  * steps and after the last one (CGX_E_NAN as above). */
 int cgx_step(cgx_solver* s, int nsteps);
 
+/* time, dt of the last completed step (0 before the first) and step count */
 int cgx_get_time(cgx_solver* s, double* time, double* dt, int* step);
 /* report(): {sum rho V, sum rho u V (3), sum rhoE V}, fixed-order reduction. */
 int cgx_totals(cgx_solver* s, double out[5]);
@@ -185,6 +186,16 @@ int cgx_get_grad(cgx_solver* s, double* dudx);
 int cgx_get_aux(cgx_solver* s, double* aux);
 
 int cgx_synchronize(cgx_solver* s);
+
+/* Timing hooks (no counterpart in the reference, which prints wall time per
+ * step, FlowSolver.hpp:2596-2605): run nsteps as cgx_step does and return
+ * their device time from CUDA events on the solver's stream. */
+int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms);
+/* Average device time of one launch of each step kernel, measured with CUDA
+ * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs),
+ * ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is kept),
+ * ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/CFL. */
+int cgx_kernel_times(cgx_solver* s, int reps, double ms[4]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
 

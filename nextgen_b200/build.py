@@ -1,0 +1,83 @@
+"""Build the package's native libraries in-tree (nextgen_b200/lib/).
+
+  libcgx.so          CUDA kernels + C ABI (include/cgx.h), sm_100a only
+  libcgx_meshgen.so  host mesh/operator generator (include/cgx_meshgen.h)
+
+`python -m nextgen_b200.build` rebuilds whatever is out of date.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "lib")
+INC = os.path.join(ROOT, "include")
+
+NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _cxx():
+    # the system g++ (an environment CXX may lack libgomp)
+    for c in ("/usr/bin/g++", "g++"):
+        if shutil.which(c):
+            return c
+    raise RuntimeError("no g++ found")
+
+
+def _nvcc():
+    for c in ("/usr/local/cuda/bin/nvcc", "nvcc"):
+        if shutil.which(c):
+            return c
+    raise RuntimeError("no nvcc found")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout)
+        raise RuntimeError("build failed: %s" % " ".join(cmd))
+    return r.stdout
+
+
+def build_meshgen(force=False):
+    out = os.path.join(LIB, "libcgx_meshgen.so")
+    src = os.path.join(CSRC, "meshgen.cpp")
+    if force or _stale(out, [src, os.path.join(INC, "cgx_meshgen.h")]):
+        os.makedirs(LIB, exist_ok=True)
+        _run([_cxx(), "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out, src])
+    return out
+
+
+def build_cgx(force=False, verbose=False):
+    out = os.path.join(LIB, "libcgx.so")
+    srcs = [os.path.join(CSRC, f) for f in ("cgx.cu", "cgx_kernels.cuh")] + [os.path.join(INC, "cgx.h")]
+    if force or _stale(out, srcs):
+        os.makedirs(LIB, exist_ok=True)
+        cmd = [_nvcc(), "-O3", "-std=c++17"] + NVCC_ARCH + [
+            "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", _cxx(),
+            "-shared", "-o", out, os.path.join(CSRC, "cgx.cu"), "-lgomp"]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        log = _run(cmd)
+        if verbose:
+            sys.stdout.write(log)
+    return out
+
+
+def build_all(force=False, verbose=False):
+    return [build_meshgen(force), build_cgx(force, verbose)]
+
+
+if __name__ == "__main__":
+    for p in build_all(force="--force" in sys.argv, verbose="-v" in sys.argv):
+        print(p)

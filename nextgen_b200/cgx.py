@@ -136,7 +136,7 @@ EXPORTS = [
     "cgx_get_state", "cgx_init_complete", "cgx_update_primitive", "cgx_calc_sgs_props",
     "cgx_calc_rhs", "cgx_rk3_step", "cgx_calc_cfl", "cgx_advance_solution", "cgx_step",
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
-    "cgx_synchronize", "cgx_launch_count", "cgx_last_error",
+    "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times",
 ]
 
 _LIB = None
@@ -175,6 +175,8 @@ def lib():
         "cgx_synchronize": (ctypes.c_int, [vp]),
         "cgx_launch_count": (ctypes.c_longlong, [vp]),
         "cgx_last_error": (ctypes.c_char_p, []),
+        "cgx_step_timed": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+        "cgx_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -315,6 +317,28 @@ class Solver:
         a = _out(self.ncv, 6)
         _check(lib().cgx_get_aux(self.h, _dp(a)))
         return a
+
+    def step_timed(self, nsteps):
+        """Run nsteps; return their device time in ms (CUDA events on the
+        solver's stream)."""
+        ms = ctypes.c_float()
+        _check(lib().cgx_step_timed(self.h, int(nsteps), ctypes.byref(ms)))
+        return float(ms.value)
+
+    def kernel_times(self, reps=5):
+        """Average ms per launch of {rhs, rk+prim, grad, step_end}."""
+        ms = np.zeros(4)
+        _check(lib().cgx_kernel_times(self.h, int(reps), _dp(ms)))
+        return dict(zip(("rhs", "rk_prim", "grad", "step_end"), ms.tolist()))
+
+    def set_state_ptr(self, rho_ptr, u_ptr, rhoE_ptr):
+        """cgx_set_state from raw host pointers (e.g. pinned buffers)."""
+        _check(lib().cgx_set_state(self.h, ctypes.cast(rho_ptr, c_dbl_p), ctypes.cast(u_ptr, c_dbl_p),
+                                   ctypes.cast(rhoE_ptr, c_dbl_p)))
+
+    def get_state_ptr(self, rho_ptr, u_ptr, rhoE_ptr):
+        _check(lib().cgx_get_state(self.h, ctypes.cast(rho_ptr, c_dbl_p), ctypes.cast(u_ptr, c_dbl_p),
+                                   ctypes.cast(rhoE_ptr, c_dbl_p)))
 
     def synchronize(self):
         _check(lib().cgx_synchronize(self.h))

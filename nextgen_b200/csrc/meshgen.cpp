@@ -31,6 +31,9 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -39,6 +42,17 @@
 namespace {
 
 thread_local std::string g_err;
+
+struct PhaseTimer {
+  bool on = std::getenv("CGX_MESHGEN_VERBOSE") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char* what) {
+    if (!on) return;
+    auto n = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "meshgen %-22s %8.3f s\n", what, std::chrono::duration<double>(n - t).count());
+    t = n;
+  }
+};
 
 struct V3 {
   double x, y, z;
@@ -415,6 +429,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
   (void)nthreads;
 #endif
   try {
+    PhaseTimer PT;
     const int ncv = nx * ny * nz;
     const double hx = Lx / nx, hy = Ly / ny, hz = Lz / nz;
     const double hmax = std::max(hx, std::max(hy, hz));
@@ -431,6 +446,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
       xvv[c] = {(i + 0.5 + rx) * hx, (j + 0.5 + ry) * hy, (k + 0.5 + rz) * hz};
     }
 
+    PT.mark("seeds");
     // ---------------- Voronoi cells ----------------
     std::vector<std::vector<RawFace>> raw(ncv);
     std::vector<double> vol(ncv);
@@ -539,6 +555,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
       return CGX_MG_E_GEOM;
     }
 
+    PT.mark("voronoi");
     // ---------------- compact faces ----------------
     // A face between cell a and image (b,s) is owned by min(a,b); its
     // geometry is the owner's.  Internal faces (s == 0): one face, icv0 = a <
@@ -655,6 +672,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
     perf.shrink_to_fit();
     raw.clear();
     raw.shrink_to_fit();
+    PT.mark("compact faces");
     const int ncv_g = ncv + int(g_owner.size());
 
     auto image_pos = [&](int cell, int sx, int sy, int sz) -> V3 {
@@ -709,6 +727,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
       }
     }
 
+    PT.mark("faocv/local");
     // ---------------- cvocv (StaticSolver.cpp:6659-6726) ----------------
     std::vector<int> cvocv_i(ncv + 1);
     for (int a = 0; a <= ncv; ++a) cvocv_i[a] = faocv_i[a] + a;
@@ -781,6 +800,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
       }
     }
 
+    PT.mark("grad coeff");
     // ---------------- extended operator rows (StripedMesh.hpp:6014-6130) ----
     // Row r of D gathers (i) the terms r adds itself for each of its compact
     // faces and (ii) the terms each compact neighbour k adds to row r (the
@@ -892,6 +912,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
       return nullptr;
     };
 
+    PT.mark("D rows");
     // ---------------- extended faces (StripedMesh.hpp:6589-6866) ----------
     // canonical pair (a,b,s) with a < b: n = D(a,(b,s)) - D(b,(a,-s)),
     //                                    c = D(a,(b,s)) + D(b,(a,-s)).
@@ -899,7 +920,6 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
       int a, b, sx, sy, sz;
       double n[3], c[3];
     };
-    std::vector<int64_t> ef_cnt(ncv + 1, 0);
     auto for_row_faces = [&](int r, auto&& emit) {
       for (int64_t e = drow_i[r]; e < drow_i[r + 1]; ++e) {
         int j, sx, sy, sz;
@@ -937,39 +957,62 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
     int n_self = 0;
 #pragma omp parallel for schedule(dynamic, 1024) reduction(+ : n_self)
     for (int r = 0; r < ncv; ++r) {
-      int64_t cnt = 0;
       for (int64_t e = drow_i[r]; e < drow_i[r + 1]; ++e) {
         int j, sx, sy, sz;
         img_unkey(dent[e].key, j, sx, sy, sz);
         if (j == r) ++n_self;
       }
-      for_row_faces(r, [&](const EFace&) { ++cnt; });
-      ef_cnt[r + 1] = cnt;
     }
     if (n_self > 0) {
       g_err = "cgx_meshgen_periodic_box: box too thin (extended stencil reaches a cell's own image)";
       return CGX_MG_E_GEOM;
     }
-    for (int a = 0; a < ncv; ++a) ef_cnt[a + 1] += ef_cnt[a];
-    std::vector<EFace> efs(size_t(ef_cnt[ncv]));
+    // bucket the faces by their first cell a (the smaller index), then order
+    // each bucket by (b, shift): the order of a global sort by (a, b, shift)
+    std::vector<int> ocnt(ncv, 0);
 #pragma omp parallel for schedule(dynamic, 1024)
-    for (int r = 0; r < ncv; ++r) {
-      int64_t pos = ef_cnt[r];
-      for_row_faces(r, [&](const EFace& f) { efs[pos++] = f; });
-    }
+    for (int r = 0; r < ncv; ++r)
+      for_row_faces(r, [&](const EFace& f) {
+#pragma omp atomic
+        ocnt[f.a]++;
+      });
+    std::vector<int64_t> ooff(ncv + 1, 0);
+    for (int a = 0; a < ncv; ++a) ooff[a + 1] = ooff[a] + ocnt[a];
+    std::vector<EFace> efs(size_t(ooff[ncv]));
+    std::fill(ocnt.begin(), ocnt.end(), 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int r = 0; r < ncv; ++r)
+      for_row_faces(r, [&](const EFace& f) {
+        int pos;
+#pragma omp atomic capture
+        pos = ocnt[f.a]++;
+        efs[size_t(ooff[f.a] + pos)] = f;
+      });
     std::vector<DEnt>().swap(dent);
-    // sort by (a, b, shift)
-    std::sort(efs.begin(), efs.end(), [](const EFace& p, const EFace& q) {
-      if (p.a != q.a) return p.a < q.a;
-      return img_key(p.b, p.sx, p.sy, p.sz) < img_key(q.b, q.sx, q.sy, q.sz);
-    });
-    int64_t nef_i64 = 0, nper_ef = 0;
-    for (const EFace& f : efs) {
-      if (f.sx == 0 && f.sy == 0 && f.sz == 0)
-        ++nef_i64;
-      else
-        nper_ef += 2;
+    auto efkey = [](const EFace& p) { return img_key(p.b, p.sx, p.sy, p.sz); };
+    std::vector<int> ni(ncv + 1, 0), np(ncv, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int a = 0; a < ncv; ++a) {
+      std::sort(efs.begin() + ooff[a], efs.begin() + ooff[a + 1],
+                [&](const EFace& p, const EFace& q) { return efkey(p) < efkey(q); });
+      int c = 0;
+      for (int64_t k = ooff[a]; k < ooff[a + 1]; ++k) c += (efs[k].sx == 0 && efs[k].sy == 0 && efs[k].sz == 0);
+      ni[a + 1] = c;
     }
+    // per-side periodic entries: both cells of a periodic pair
+    for (int a = 0; a < ncv; ++a) {
+      for (int64_t k = ooff[a]; k < ooff[a + 1]; ++k) {
+        const EFace& f = efs[k];
+        if (f.sx || f.sy || f.sz) {
+          ++np[f.a];
+          ++np[f.b];
+        }
+      }
+    }
+    for (int a = 0; a < ncv; ++a) ni[a + 1] += ni[a];
+    std::vector<int64_t> poff(ncv + 1, 0);
+    for (int a = 0; a < ncv; ++a) poff[a + 1] = poff[a] + np[a];
+    const int64_t nef_i64 = ni[ncv], nper_ef = poff[ncv];
     if (nef_i64 + nper_ef > int64_t(2147483647)) {
       g_err = "cgx_meshgen_periodic_box: too many extended faces";
       return CGX_MG_E_ARG;
@@ -979,49 +1022,60 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
     std::vector<int> cvoef(2 * size_t(nef));
     std::vector<double> n_ef(3 * size_t(nef)), c_ef(3 * size_t(nef));
     {
-      int ii = 0;
-      for (const EFace& f : efs) {
-        if (f.sx || f.sy || f.sz) continue;
-        cvoef[2 * size_t(ii)] = f.a;
-        cvoef[2 * size_t(ii) + 1] = f.b;
-        for (int i = 0; i < 3; ++i) {
-          n_ef[3 * size_t(ii) + i] = f.n[i];
-          c_ef[3 * size_t(ii) + i] = f.c[i];
+#pragma omp parallel for schedule(dynamic, 1024)
+      for (int a = 0; a < ncv; ++a) {
+        int ii = ni[a];
+        for (int64_t k = ooff[a]; k < ooff[a + 1]; ++k) {
+          const EFace& f = efs[k];
+          if (f.sx || f.sy || f.sz) continue;
+          cvoef[2 * size_t(ii)] = f.a;
+          cvoef[2 * size_t(ii) + 1] = f.b;
+          for (int i = 0; i < 3; ++i) {
+            n_ef[3 * size_t(ii) + i] = f.n[i];
+            c_ef[3 * size_t(ii) + i] = f.c[i];
+          }
+          ++ii;
         }
-        ++ii;
       }
-      // periodic pairs: one face per owning side, grouped by icv0
+      // periodic pairs: one face per owning side, grouped by icv0, each
+      // group ordered by the image key
       struct PSide {
-        int a;
         int64_t key;
         double n[3], c[3];
       };
-      std::vector<PSide> ps;
-      ps.reserve(size_t(nper_ef));
-      for (const EFace& f : efs) {
-        if (!(f.sx || f.sy || f.sz)) continue;
-        PSide p0{f.a, img_key(f.b, f.sx, f.sy, f.sz), {f.n[0], f.n[1], f.n[2]}, {f.c[0], f.c[1], f.c[2]}};
-        PSide p1{f.b, img_key(f.a, -f.sx, -f.sy, -f.sz), {-f.n[0], -f.n[1], -f.n[2]}, {f.c[0], f.c[1], f.c[2]}};
-        ps.push_back(p0);
-        ps.push_back(p1);
-      }
-      std::sort(ps.begin(), ps.end(), [](const PSide& p, const PSide& q) {
-        if (p.a != q.a) return p.a < q.a;
-        return p.key < q.key;
-      });
-      // level-2 ghosts are those images not already ghosts
-      for (const PSide& p : ps) {
-        int b, sx, sy, sz;
-        img_unkey(p.key, b, sx, sy, sz);
-        cvoef[2 * size_t(ii)] = p.a;
-        cvoef[2 * size_t(ii) + 1] = ghost_index(b, sx, sy, sz);
-        for (int i = 0; i < 3; ++i) {
-          n_ef[3 * size_t(ii) + i] = p.n[i];
-          c_ef[3 * size_t(ii) + i] = p.c[i];
+      std::vector<PSide> ps(static_cast<size_t>(nper_ef));
+      std::fill(np.begin(), np.end(), 0);
+      for (int a = 0; a < ncv; ++a) {
+        for (int64_t k = ooff[a]; k < ooff[a + 1]; ++k) {
+          const EFace& f = efs[k];
+          if (!(f.sx || f.sy || f.sz)) continue;
+          PSide p0{img_key(f.b, f.sx, f.sy, f.sz), {f.n[0], f.n[1], f.n[2]}, {f.c[0], f.c[1], f.c[2]}};
+          PSide p1{img_key(f.a, -f.sx, -f.sy, -f.sz), {-f.n[0], -f.n[1], -f.n[2]}, {f.c[0], f.c[1], f.c[2]}};
+          ps[size_t(poff[f.a] + np[f.a]++)] = p0;
+          ps[size_t(poff[f.b] + np[f.b]++)] = p1;
         }
-        ++ii;
+      }
+#pragma omp parallel for schedule(dynamic, 1024)
+      for (int a = 0; a < ncv; ++a)
+        std::sort(ps.begin() + poff[a], ps.begin() + poff[a + 1],
+                  [](const PSide& p, const PSide& q) { return p.key < q.key; });
+      // level-2 ghosts are those images not already ghosts
+      for (int a = 0; a < ncv; ++a) {
+        for (int64_t k = poff[a]; k < poff[a + 1]; ++k) {
+          const PSide& p = ps[size_t(k)];
+          const size_t ii = size_t(nef_i64 + k);
+          int b, sx, sy, sz;
+          img_unkey(p.key, b, sx, sy, sz);
+          cvoef[2 * ii] = a;
+          cvoef[2 * ii + 1] = ghost_index(b, sx, sy, sz);
+          for (int i = 0; i < 3; ++i) {
+            n_ef[3 * ii + i] = p.n[i];
+            c_ef[3 * ii + i] = p.c[i];
+          }
+        }
       }
     }
+    PT.mark("ef assembly");
     std::vector<EFace>().swap(efs);
     const int ncv_g2 = ncv + int(g_owner.size());
     // ghosts reachable by compact faces were numbered first
@@ -1093,6 +1147,7 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
     }
     for (int a = 0; a < ncv; ++a) sav[a] = sav[a] / vol[a];
 
+    PT.mark("factors");
     // ---------------- output ----------------
     cgx_meshgen_out* m = static_cast<cgx_meshgen_out*>(std::calloc(1, sizeof(cgx_meshgen_out)));
     if (!m) throw std::bad_alloc();

@@ -530,6 +530,17 @@ void zero_rhs(orc_solver* o, int k) {
 
 }  // namespace
 
+#ifdef CGX_ORACLE_REFERENCE_FLUX
+#include "SvdNew.hpp"
+// The reference's own 3x3 SVD (src/core/common/SvdNew.hpp:24), exposed so the
+// tests can rebuild the gradient coefficients with it.
+extern "C" int orc_ref_svd33(const double* A, double* U, double* V, double* sigma) {
+  double max_err = 0.0;
+  calcSvd33(U, V, sigma, A, max_err);
+  return 0;
+}
+#endif
+
 extern "C" int orc_uses_reference_flux(void) {
 #ifdef CGX_ORACLE_REFERENCE_FLUX
   return 1;

@@ -1,0 +1,76 @@
+"""The C-ABI libraries load and export every symbol their headers declare.
+
+CPU only: loads the libraries, calls nothing that needs a GPU.
+"""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    src = open(os.path.join(ROOT, header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(\w+)\s*\([^;{]*\)\s*;", src, flags=re.M)
+    return sorted(set(n for n in names if n.startswith(("cgx_", "orc_"))))
+
+
+def test_cgx_exports_every_declared_symbol(built):
+    from nextgen_b200 import _lib, cgx
+    names = declared("include/cgx.h")
+    assert len(names) >= 25
+    L = ctypes.CDLL(_lib.path("libcgx.so"))
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(cgx.EXPORTS) <= set(names)
+
+
+def test_meshgen_exports_every_declared_symbol(built):
+    from nextgen_b200 import _lib
+    names = declared("include/cgx_meshgen.h")
+    L = ctypes.CDLL(_lib.path("libcgx_meshgen.so"))
+    assert names and all(hasattr(L, n) for n in names)
+
+
+def test_oracle_exports_every_declared_symbol(built):
+    names = declared("oracle/oracle.h")
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    assert names and all(hasattr(L, n) for n in names)
+
+
+def test_params_default_are_the_reference_defaults(built):
+    from nextgen_b200 import cgx
+    p = cgx.Params()
+    cgx.lib().cgx_params_default(ctypes.byref(p))
+    # IdealGasSolver.hpp:147-155, IdealGasSolverSgs.cpp:209-213, IdealGasSolver.cpp:202-203,904
+    assert p.gamma == 1.4 and p.mu_power_law == 0.75 and p.Pr_lam == 0.7
+    assert p.vreman_coeff == 0.07 and p.a_sgs_coeff == 0.05 and p.a_sgs_coeff2 == 0.0015
+    assert p.lambda_dil_coeff == 0.0 and p.Pr_t == 0.9
+    assert p.coeff_p == 0.5 and p.coeff_h == 0.1 and p.gr_nrm == 0.03
+    q = cgx.Params()
+    for f, _ in cgx.Params._fields_:
+        if f != "dt_data":
+            assert getattr(q, f) == getattr(p, f), f
+
+
+def test_libcgx_is_sm100a_only(built):
+    """The CUDA library carries sm_100a code and nothing else."""
+    import subprocess
+    from nextgen_b200 import _lib
+    out = subprocess.run(["cuobjdump", "--list-elf", _lib.path("libcgx.so")],
+                         stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True).stdout
+    arches = set(re.findall(r"sm_(\d+a?)", out))
+    assert arches == {"100a"}, out
+
+
+def test_product_never_imports_the_oracle():
+    pkg = os.path.join(ROOT, "nextgen_b200")
+    for dp, _, fs in os.walk(pkg):
+        for f in fs:
+            if f.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
+                txt = open(os.path.join(dp, f)).read()
+                assert "import oracle" not in txt and "from oracle" not in txt, f
+                assert "liboracle" not in txt and "libref" not in txt, f
