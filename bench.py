@@ -210,12 +210,13 @@ def run_cgx(args):
     st = gm.stats()
     e, f = st.e_per_cell, st.f_per_cell
     N = m.ncv
-    x_cv = np.array(m.x_cv[:N])
+    vol_cv = np.array(m.vol_cv)
     m.close()
 
     solvers = {}
     res = {}
-    for prec_name, prec in (("fp64", cgx.CGX_FP64),):
+    precs = [("fp64", cgx.CGX_FP64)] + ([("mixed", cgx.CGX_MIXED)] if not args.no_mixed else [])
+    for prec_name, prec in precs:
         s = cgx.Solver(gm, prm, prec)
         s.set_state_primitive(rho, u, p)
         s.initComplete()
@@ -230,11 +231,40 @@ def run_cgx(args):
         dist.barrier()
         launches = s.launch_count() - n0
         ms_max = dist.max_over_ranks(ms)
-        res[prec_name] = {"ms": ms_max, "launches": launches, "clocks": clk.summary()}
+        res[prec_name] = {"ms": ms_max, "launches": launches, "clocks": clk.summary(),
+                          "kernel_ms": s.kernel_times(reps=3), "tuning": s.tuning()}
         solvers[prec_name] = s
 
     s = solvers["fp64"]
-    ktimes = s.kernel_times(reps=3)
+    ktimes = res["fp64"]["kernel_ms"]
+    tuning = res["fp64"]["tuning"]
+    mixed = None
+    if "mixed" in solvers:
+        # both forms advanced W + K steps from the same initial state:
+        # errors of the mixed form against the FP64 path
+        r64, u64, _ = s.get_state()
+        r32, u32, _ = solvers["mixed"].get_state()
+        p64 = s.primitive()[0]
+        p32 = solvers["mixed"].primitive()[0]
+        vol = np.array(vol_cv)
+        ke64 = 0.5 * (r64 * (u64 * u64).sum(1) * vol).sum()
+        ke32 = 0.5 * (r32 * (u32 * u32).sum(1) * vol).sum()
+        ke0 = 0.5 * (rho * (u * u).sum(1) * vol).sum()
+        du = u32 - u64
+        pf = p64 - p64.mean()
+        ms_mixed = res["mixed"]["ms"]
+        mixed = {"value": world * N * args.steps / (ms_mixed * 1e-3), "unit": UNIT,
+                 "ms_per_step": ms_mixed / args.steps,
+                 "speedup_vs_fp64": res["fp64"]["ms"] / ms_mixed,
+                 "kernel_ms": res["mixed"]["kernel_ms"], "tuning": res["mixed"]["tuning"],
+                 "gpu_launches": res["mixed"]["launches"], "clocks": res["mixed"]["clocks"],
+                 "error_vs_fp64_after_steps": args.warmup + args.steps,
+                 "u_l2_rel": float(np.sqrt((du ** 2).mean() / (u64 ** 2).mean())),
+                 "u_linf_rel": float(np.abs(du).max() / np.abs(u64).max()),
+                 "p_l2_rel_fluct": float(np.sqrt(((p32 - p64) ** 2).mean() / max((pf ** 2).mean(), 1e-300))),
+                 "p_linf_rel_fluct": float(np.abs(p32 - p64).max() / max(np.abs(pf).max(), 1e-300)),
+                 "ke_rel": float(abs(ke32 - ke64) / ke64),
+                 "ke_decay_rel": float(abs(ke32 - ke64) / max(abs(ke0 - ke64), 1e-300))}
     step_bytes, rhs_bytes = bytes_model(e, f)
     peak, peak_kind = measured_peaks()
     ms_step = res["fp64"]["ms"] / args.steps
@@ -281,13 +311,15 @@ def run_cgx(args):
                                     "cgx_get_state (device -> pinned host); host wall clock"},
         "gpu_launches": res["fp64"]["launches"],
         "clocks": res["fp64"]["clocks"],
-        "roofline": {"bound": "hbm", "kernel": "k_rhs (calcRhsBase)", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_rhs_ext + k_rhs_comp (calcRhsBase)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_cell": rhs_bytes,
                      "launch_ms": ktimes["rhs"]},
         "step_roofline": {"bytes_per_cell_step": step_bytes, "achieved": value / world * step_bytes / 1e9,
                           "frac": value / world * step_bytes / 1e9 / peak, "unit": "GB/s"},
         "kernel_ms": ktimes,
+        "tuning": tuning,
+        "mixed": mixed,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds, n=args.cpu_n)
@@ -312,6 +344,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=48)
     ap.add_argument("--ref-n", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         sys.exit("steps >= 1, warmup >= 0")

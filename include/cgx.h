@@ -196,6 +196,10 @@ int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms);
  * ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is kept),
  * ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/CFL. */
 int cgx_kernel_times(cgx_solver* s, int reps, double ms[4]);
+/* Lanes per cell chosen by the autotuner that cgx_init_complete runs (timed
+ * candidates per kernel, cached per mesh-size bucket and precision):
+ * out = {face fluxes, compact closures, gradient, once-per-step kernel}. */
+int cgx_get_tuning(const cgx_solver* s, int out[4]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
 

@@ -136,7 +136,7 @@ EXPORTS = [
     "cgx_get_state", "cgx_init_complete", "cgx_update_primitive", "cgx_calc_sgs_props",
     "cgx_calc_rhs", "cgx_rk3_step", "cgx_calc_cfl", "cgx_advance_solution", "cgx_step",
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
-    "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times",
+    "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
 ]
 
 _LIB = None
@@ -177,6 +177,7 @@ def lib():
         "cgx_last_error": (ctypes.c_char_p, []),
         "cgx_step_timed": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
         "cgx_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
+        "cgx_get_tuning": (ctypes.c_int, [vp, c_int_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -330,6 +331,12 @@ class Solver:
         ms = np.zeros(4)
         _check(lib().cgx_kernel_times(self.h, int(reps), _dp(ms)))
         return dict(zip(("rhs", "rk_prim", "grad", "step_end"), ms.tolist()))
+
+    def tuning(self):
+        """Lanes per cell picked by the autotuner: ext, comp, grad, step_end."""
+        t = (ctypes.c_int * 4)()
+        _check(lib().cgx_get_tuning(self.h, t))
+        return dict(zip(("ext", "comp", "grad", "step_end"), list(t)))
 
     def set_state_ptr(self, rho_ptr, u_ptr, rhoE_ptr):
         """cgx_set_state from raw host pointers (e.g. pinned buffers)."""

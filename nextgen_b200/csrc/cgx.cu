@@ -32,6 +32,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -49,12 +51,40 @@ namespace {
 thread_local std::string g_err;
 
 constexpr int kBlock = 128;
+constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) + step_end
 
 // ===========================================================================
 // device helpers
 // ===========================================================================
 __device__ __forceinline__ double2 ldg2(const void* p) {
   return __ldg(reinterpret_cast<const double2*>(p));
+}
+
+// 1/x by Newton-Raphson refinement (two steps, r <- r + r(1 - x r)) of the
+// hardware reciprocal approximation (PTX rcp.approx.ftz.f64); within 1 ulp of
+// the correctly rounded quotient for the normal, O(1) arguments used here.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+
+// Sum / max over the G lanes of a group (xor butterfly: every lane ends with
+// the same, order-fixed result).  All 32 lanes of the warp must call it.
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int G>
+__device__ __forceinline__ double group_max(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
 }
 
 __device__ __forceinline__ void load_L(const LRec* base, int j, LRec& r) {
@@ -84,7 +114,7 @@ struct Flux {
 // order; returns the face averages the other two parts reuse.
 __device__ __forceinline__ void skew_flux(Flux& F, const double n[3], const LRec& a, const LRec& b,
                                           double uf[3], double& rho_f, double& h_f) {
-  rho_f = 2.0 / (a.sp_vol + b.sp_vol);
+  rho_f = 2.0 * rcp_nr(a.sp_vol + b.sp_vol);
   const double p_f = 0.5 * (b.p + a.p);
   double un = 0.0, uaub = 0.0;
 #pragma unroll
@@ -110,7 +140,8 @@ __device__ __forceinline__ void sym_flux_add(Flux& F, const double c[3], const L
   double du_c = 0.0, uf_c = 0.0;
   const double dp = b.p - a.p;
   double dH = b.h - a.h;
-  const double drho = (a.sp_vol - b.sp_vol) / (a.sp_vol * b.sp_vol);
+  // (v_a - v_b)/(v_a v_b) of the reference is rho_b - rho_a
+  const double drho = b.rho - a.rho;
   double G[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -131,11 +162,10 @@ __device__ __forceinline__ void sym_flux_add(Flux& F, const double c[3], const L
 
 // Compact closures (IdealGasSolverFlux.hpp:93-215), subtracted from F.
 __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], double area, double aod,
-                                                 const LRec& a, const LRec& b, const PRec& ax,
-                                                 const PRec& bx, const double uf[3], double h_f,
-                                                 const double ga[9], const double gb[9]) {
+                                                 double delta, const LRec& a, const LRec& b,
+                                                 const PRec& ax, const PRec& bx, const double uf[3],
+                                                 double h_f, const double ga[9], const double gb[9]) {
   const double half_aod = 0.5 * aod;
-  const double delta = area / aod;
   const double mu_area = 0.5 * (ax.mu_total + bx.mu_total) * area;
   const double mu_aod = (ax.mu_total + bx.mu_total) * half_aod;
   const double k_aod = (ax.loc_total + bx.loc_total) * half_aod;
@@ -150,14 +180,14 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
     unb += b.u[d] * un_[d];
   }
   const double dun = unb - una;
-  const double dun_3 = dun / 3.0;
-  const double dun2_6 = (unb * unb - una * una) / 6.0;
+  const double dun_3 = dun * (1.0 / 3.0);
+  const double dun2_6 = (unb * unb - una * una) * (1.0 / 6.0);
   const double dp = b.p - a.p;
   const double fgr_f = 0.5 * (bx.fgr + ax.fgr);
   const double rho_m = 0.5 * (b.rho + a.rho);
   const double un_m = 0.5 * (una + unb);
   const double c_m = 0.5 * (a.sos + b.sos);
-  const double mach_n = fabs(un_m) / c_m;
+  const double mach_n = fabs(un_m) * rcp_nr(c_m);
   const double drho = b.rho - a.rho;
   const double lf = fmin(fgr_f * mach_n, 0.5) * (c_m + fabs(un_m)) * area;
   const double lf_drho = lf * drho;
@@ -195,8 +225,8 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
     gnn_3 += gn[k] * un_[k];
     div_23 += ga[4 * k] + gb[4 * k];
   }
-  div_23 /= 3.0;
-  gnn_3 /= 3.0;
+  div_23 *= (1.0 / 3.0);
+  gnn_3 *= (1.0 / 3.0);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const double t = (gn[d] - un_[d] * (gnn_3 + div_23)) * mu_area;
@@ -209,64 +239,34 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 // kernels
 // ===========================================================================
 
-// calcRhsBase, cell-centric: rhs[i] = -sum over i's faces of F(i -> j).
-__global__ void __launch_bounds__(kBlock) k_rhs(MeshDev m, StateDev s, int stage) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m.N) return;
-  const long long base = m.slice_off[i >> 5] + (i & 31);
-  const int meta = __ldg(m.meta + i);
-  const int deg = meta & 0xffff, ncomp = meta >> 16;
+// calcRhsBase, cell-centric, in two passes over each cell's face list, a
+// group of G lanes per cell (lane l takes entries l, l+G, ...; the group's
+// partial sums are combined by a fixed butterfly):
+//   k_rhs_ext : rhs[i] = -sum over all of i's extended faces of the skew +
+//               symmetric flux F(i -> j)
+//   k_rhs_comp: rhs[i] -= sum over i's compact faces of the viscous/dissipation
+//               closure
+// Every face is evaluated by each of its two cells with the orientation
+// reversed (n -> -n, unit_n -> -unit_n, c kept), which gives the negated flux.
+template <int G>
+__global__ void __launch_bounds__(256, 3) k_rhs_ext(MeshDev m, StateDev s, int stage) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G;
+  const int lane = t & (G - 1);
+  const bool valid = i < m.N;
+  long long b = 0, e = 0;
   LRec Li;
-  load_L(s.L, i, Li);
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  if (ncomp > 0) {
-    PRec Pi;
-    load_P(s.P, i, Pi);
-    double gi[9];
-    load_G(s.G, i, gi);
-    for (int k = 0; k < ncomp; ++k) {
-      const long long e = base + 32LL * k;
-      const int j = __ldg(m.nbr + e);
-      const int f = __ldg(m.fid + e);
-      const int fi = f & kFidMask;
-      const double sg = (f < 0) ? -1.0 : 1.0;
-      const double2* ge = reinterpret_cast<const double2*>(m.ef + fi);
-      const double2 g0 = __ldg(ge), g1 = __ldg(ge + 1), g2 = __ldg(ge + 2);
-      const double n[3] = {sg * g0.x, sg * g0.y, sg * g1.x};
-      const double c[3] = {g1.y, g2.x, g2.y};
-      const double2* gc = reinterpret_cast<const double2*>(m.cf + fi);
-      const double2 h0 = __ldg(gc), h1 = __ldg(gc + 1), h2 = __ldg(gc + 2);
-      const double un[3] = {sg * h0.x, sg * h0.y, sg * h1.x};
-      const double area = h1.y, aod = h2.x;
-      LRec Lj;
-      load_L(s.L, j, Lj);
-      PRec Pj;
-      load_P(s.P, j, Pj);
-      double gj[9];
-      load_G(s.G, j, gj);
-      Flux F;
-      double uf[3], rho_f, h_f;
-      skew_flux(F, n, Li, Lj, uf, rho_f, h_f);
-      // the reference adds the compact closure to the skew flux first, then
-      // the symmetric part (IdealGasSolver.cpp:386-400)
-      Flux C;
-      C.rho = 0.0; C.ru[0] = C.ru[1] = C.ru[2] = 0.0; C.rE = 0.0;
-      sym_flux_add(C, c, Li, Lj, uf, rho_f, h_f);
-      compact_flux_add(F, un, area, aod, Li, Lj, Pi, Pj, uf, h_f, gi, gj);
-      acc[0] -= F.rho + C.rho;
-      acc[1] -= F.ru[0] + C.ru[0];
-      acc[2] -= F.ru[1] + C.ru[1];
-      acc[3] -= F.ru[2] + C.ru[2];
-      acc[4] -= F.rE + C.rE;
-    }
+  if (valid) {
+    b = m.off[i];
+    e = m.off[i + 1];
+    load_L(s.L, i, Li);
   }
-  for (int k = ncomp; k < deg; ++k) {
-    const long long e = base + 32LL * k;
-    const int j = __ldg(m.nbr + e);
-    const int f = __ldg(m.fid + e);
-    const int fi = f & kFidMask;
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long k = b + lane; k < e; k += G) {
+    const int j = __ldg(m.nbr + k);
+    const int f = __ldg(m.fid + k);
     const double sg = (f < 0) ? -1.0 : 1.0;
-    const double2* ge = reinterpret_cast<const double2*>(m.ef + fi);
+    const double2* ge = reinterpret_cast<const double2*>(m.ef + (f & kFidMask));
     const double2 g0 = __ldg(ge), g1 = __ldg(ge + 1), g2 = __ldg(ge + 2);
     const double n[3] = {sg * g0.x, sg * g0.y, sg * g1.x};
     const double c[3] = {g1.y, g2.x, g2.y};
@@ -284,15 +284,76 @@ __global__ void __launch_bounds__(kBlock) k_rhs(MeshDev m, StateDev s, int stage
     acc[3] -= F.ru[2] + C.ru[2];
     acc[4] -= F.rE + C.rE;
   }
-  double* r = s.rhs + size_t(stage) * 5 * m.N;
-  r[i] = acc[0];
-  r[size_t(m.N) + i] = acc[1];
-  r[2 * size_t(m.N) + i] = acc[2];
-  r[3 * size_t(m.N) + i] = acc[3];
-  r[4 * size_t(m.N) + i] = acc[4];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
+  if (valid) {
+    double* r = s.rhs + size_t(stage) * 5 * m.N;
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+      if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
+  }
 }
 
-// packed primitive state of one cell (updateExtendedState)
+template <int G>
+__global__ void __launch_bounds__(256, 2) k_rhs_comp(MeshDev m, StateDev s, int stage) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G;
+  const int lane = t & (G - 1);
+  const bool valid = i < m.N;
+  long long b = 0, e = 0;
+  LRec Li;
+  PRec Pi;
+  double gi[9];
+  if (valid) {
+    b = m.off[i];
+    e = b + __ldg(m.ncomp + i);
+    if (e > b + lane) {
+      load_L(s.L, i, Li);
+      load_P(s.P, i, Pi);
+      load_G(s.G, i, gi);
+    }
+  }
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long k = b + lane; k < e; k += G) {
+    const int j = __ldg(m.nbr + k);
+    const int f = __ldg(m.fid + k);
+    const double sg = (f < 0) ? -1.0 : 1.0;
+    const double2* gc = reinterpret_cast<const double2*>(m.cf + (f & kFidMask));
+    const double2 h0 = __ldg(gc), h1 = __ldg(gc + 1), h2 = __ldg(gc + 2);
+    const double un[3] = {sg * h0.x, sg * h0.y, sg * h1.x};
+    LRec Lj;
+    load_L(s.L, j, Lj);
+    PRec Pj;
+    load_P(s.P, j, Pj);
+    double gj[9];
+    load_G(s.G, j, gj);
+    // face averages of the skew flux (IdealGasSolverFlux.hpp:23-37)
+    double uf[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uf[d] = 0.5 * (Li.u[d] + Lj.u[d]);
+    const double uaub = Li.u[0] * Lj.u[0] + Li.u[1] * Lj.u[1] + Li.u[2] * Lj.u[2];
+    const double h_f = 0.5 * ((Lj.h + Li.h) + uaub);
+    Flux F;
+    F.rho = 0.0; F.ru[0] = F.ru[1] = F.ru[2] = 0.0; F.rE = 0.0;
+    compact_flux_add(F, un, h1.y, h2.x, h2.y, Li, Lj, Pi, Pj, uf, h_f, gi, gj);
+    acc[0] -= F.rho;
+    acc[1] -= F.ru[0];
+    acc[2] -= F.ru[1];
+    acc[3] -= F.ru[2];
+    acc[4] -= F.rE;
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
+  if (valid && e > b) {
+    double* r = s.rhs + size_t(stage) * 5 * m.N;
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+      if (c % G == lane) r[size_t(c) * m.N + i] += acc[c];
+  }
+}
+
+// packed primitive state of one cell (updateExtendedState); FP64 always,
+// rounded into the FP32 records for mixed-precision solvers
 __device__ __forceinline__ void write_prim(const Phys& ph, StateDev& s, int i, double rho, double u0,
                                            double u1, double u2, double rhoE, bool writeQ) {
   const double gm1 = ph.gamma - 1.0;
@@ -301,6 +362,15 @@ __device__ __forceinline__ void write_prim(const Phys& ph, StateDev& s, int i, d
   const double p = gm1 * (rhoE - 0.5 * rho * usq);
   const double T = p / (rho * ph.R);
   const double sos = sqrt(ph.gamma * ph.R * T);
+  if (s.LF) {
+    float4* L = reinterpret_cast<float4*>(s.LF + i);
+    L[0] = make_float4(float(u0), float(u1), float(u2), float(1.0 / rho));
+    L[1] = make_float4(float(p - ph.p_ref), float(Rgogm1 * T - ph.h_ref), float(rho), float(sos));
+    if (writeQ)
+      s.QF[i] = QRecF{float(log(p * (1.0 / ph.p_ref))), float(p - ph.p_ref), float(1.0 / rho),
+                      float(1.0 / (ph.R * T))};
+    return;
+  }
   double2* L = reinterpret_cast<double2*>(s.L + i);
   L[0] = make_double2(u0, u1);
   L[1] = make_double2(u2, 1.0 / rho);
@@ -348,21 +418,26 @@ __global__ void __launch_bounds__(kBlock) k_rk_prim(MeshDev m, StateDev s, Phys 
   write_prim(ph, s, i, rho, u0, u1, u2, rhoE, writeQ != 0);
 }
 
-// _calcCvGradRange over the compact CSR (gradient SELL).
-__global__ void __launch_bounds__(kBlock) k_grad(MeshDev m, StateDev s, const int* __restrict__ cnbr,
-                                                 const int* __restrict__ cdeg) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m.N) return;
-  const long long base = m.cslice_off[i >> 5] + (i & 31);
-  const int deg = __ldg(cdeg + i);
-  const double2* Li = reinterpret_cast<const double2*>(s.L + i);
-  const double2 a = __ldg(Li), b = __ldg(Li + 1);
-  const double ui[3] = {a.x, a.y, b.x};
+// _calcCvGradRange over the compact CSR, a group of G lanes per cell.
+template <int G>
+__global__ void __launch_bounds__(256) k_grad(MeshDev m, StateDev s) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G;
+  const int lane = t & (G - 1);
+  const bool valid = i < m.N;
+  long long b = 0, e = 0;
+  double ui[3] = {0.0, 0.0, 0.0};
+  if (valid) {
+    b = m.coff[i];
+    e = m.coff[i + 1];
+    const double2* Li = reinterpret_cast<const double2*>(s.L + i);
+    const double2 a = __ldg(Li), c = __ldg(Li + 1);
+    ui[0] = a.x; ui[1] = a.y; ui[2] = c.x;
+  }
   double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int k = 0; k < deg; ++k) {
-    const long long e = base + 32LL * k;
-    const int j = __ldg(cnbr + e);
-    const double cx = __ldg(m.gcx + e), cy = __ldg(m.gcy + e), cz = __ldg(m.gcz + e);
+  for (long long k = b + lane; k < e; k += G) {
+    const int j = __ldg(m.cnbr + k);
+    const double cx = __ldg(m.gcx + k), cy = __ldg(m.gcy + k), cz = __ldg(m.gcz + k);
     const double2* Lj = reinterpret_cast<const double2*>(s.L + j);
     const double2 ja = __ldg(Lj), jb = __ldg(Lj + 1);
     const double du[3] = {ja.x - ui[0], ja.y - ui[1], jb.x - ui[2]};
@@ -373,39 +448,131 @@ __global__ void __launch_bounds__(kBlock) k_grad(MeshDev m, StateDev s, const in
       g[3 * d + 2] += cz * du[d];
     }
   }
-  double2* G = reinterpret_cast<double2*>(s.G + i);
-  G[0] = make_double2(g[0], g[1]);
-  G[1] = make_double2(g[2], g[3]);
-  G[2] = make_double2(g[4], g[5]);
-  G[3] = make_double2(g[6], g[7]);
-  G[4] = make_double2(g[8], 0.0);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) g[c] = group_sum<G>(g[c]);
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      if (c % G == lane) s.G[i].g[c] = g[c];
+  }
+}
+
+// Last block of a once-per-step kernel: reduce the per-block CFL maxima and
+// NaN flags (fixed order) and update the control block: time/step advance
+// (mode bit 0) and the next dt from setDt's formula (mode bit 1).
+// Called by all 256 threads of that block.
+__device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode) {
+  constexpr int kThreads = 256;
+  __shared__ double fin_cfl[kThreads];
+  __shared__ int fin_nan[kThreads];
+  double mx = 0.0;
+  int anynan = 0;
+  for (int bb = threadIdx.x; bb < gridDim.x; bb += blockDim.x) {
+    mx = fmax(mx, ((volatile double*)s.red)[bb]);
+    anynan |= (((volatile double*)s.red)[gridDim.x + bb] != 0.0);
+  }
+  fin_cfl[threadIdx.x] = mx;
+  fin_nan[threadIdx.x] = anynan;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      fin_cfl[threadIdx.x] = fmax(fin_cfl[threadIdx.x], fin_cfl[threadIdx.x + w]);
+      fin_nan[threadIdx.x] |= fin_nan[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    Ctl* c = s.ctl;
+    const double cmax = fin_cfl[0];
+    c->cfl_max = cmax;
+    if (fin_nan[0]) c->nan = 1;
+    if (mode & 1) {
+      c->dt_last = c->dt;
+      c->time += c->dt;
+      c->step += 1;
+    }
+    if (mode & 2) {
+      double dt;
+      if (ph.dt_mode == CGX_DT_CONST)
+        dt = c->dt_data0;
+      else if (ph.dt_mode == CGX_DT_CFL)
+        dt = c->dt_data0 / cmax;
+      else
+        dt = fmin(ph.dt_max, c->dt_data0 / fmax(cmax, 1.0E-12));
+      c->dt = dt;
+    }
+    c->blocks_done = 0;
+  }
 }
 
 // Once per step: computeSgsVreman + calcSgsAndMaterialProperties + setFgrCvs
-// + calcCfl(NULL, 1.0) for the next step's dt + checkForNans.
+// + calcCfl(NULL, 1.0) for the next step's dt + checkForNans, a group of G
+// lanes per cell for the face loops.
 // mode bit 0: advance time/step by the dt just used; bit 1: set dt from CFL.
-__global__ void __launch_bounds__(kBlock) k_step_end(MeshDev m, StateDev s, Phys ph, int mode) {
-  __shared__ double sh_cfl[kBlock];
-  __shared__ int sh_nan[kBlock];
+template <int G>
+__global__ void __launch_bounds__(256) k_step_end(MeshDev m, StateDev s, Phys ph, int mode) {
+  constexpr int kThreads = 256;
+  constexpr int kCells = kThreads / G;
+  __shared__ double sh_cfl[kCells];
+  __shared__ int sh_nan[kCells];
   __shared__ bool am_last;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double cfl = 0.0;
-  int nan = 0;
-  if (i < m.N) {
-    LRec Li;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G;
+  const int lane = t & (G - 1);
+  const int cl = threadIdx.x / G;
+  const bool valid = i < m.N;
+  long long b = 0, e = 0, ec = 0;
+  LRec Li;
+  double2 qa = make_double2(0.0, 0.0), qb = make_double2(0.0, 0.0);
+  if (valid) {
+    b = m.off[i];
+    e = m.off[i + 1];
+    ec = b + __ldg(m.ncomp + i);
     load_L(s.L, i, Li);
+    const double2* Qi = reinterpret_cast<const double2*>(s.Q + i);
+    qa = __ldg(Qi);
+    qb = __ldg(Qi + 1);
+  }
+  // ---- Gibbs remainder over the extended faces, CFL over the compact ones
+  double vv2 = 0.0, cfl = 0.0;
+  for (long long k = b + lane; k < e; k += G) {
+    const int j = __ldg(m.nbr + k);
+    const double2* Qj = reinterpret_cast<const double2*>(s.Q + j);
+    const double2 ja = __ldg(Qj), jb = __ldg(Qj + 1);
+    const double dp = ja.y - qa.y;
+    const double v_avg = 0.5 * (qb.x + jb.x);
+    const double beta = 0.5 * (qb.y + jb.y);
+    const double gr = ja.x - qa.x - v_avg * dp * beta;
+    vv2 = fmax(vv2, fabs(gr));
+    if (k < ec) {
+      const int f = __ldg(m.fid + k);
+      const double sg = (f < 0) ? -1.0 : 1.0;
+      const double2* cr = reinterpret_cast<const double2*>(m.cf + (f & kFidMask));
+      const double2 h0 = __ldg(cr), h1 = __ldg(cr + 1);
+      const double un[3] = {sg * h0.x, sg * h0.y, sg * h1.x};
+      const double area = h1.y;
+      LRec Lj;
+      load_L(s.L, j, Lj);
+      const double undA = 0.5 * area * ((Li.u[0] * un[0] + Li.u[1] * un[1] + Li.u[2] * un[2]) +
+                                        (Lj.u[0] * un[0] + Lj.u[1] * un[1] + Lj.u[2] * un[2]));
+      cfl += fabs(undA) + area * (0.5 * (Li.sos + Lj.sos));
+    }
+  }
+  vv2 = group_max<G>(vv2);
+  cfl = group_sum<G>(cfl);
+  int nan = 0;
+  if (valid && lane == 0) {
     double g[9];
     load_G(s.G, i, g);
     // {dx, dx2_approx, dcmag_hat, sa_to_vol}
     const double2 cc01 = __ldg(reinterpret_cast<const double2*>(m.cc + i));
     const double2 cc23 = __ldg(reinterpret_cast<const double2*>(m.cc + i) + 1);
-    const double4 cc = make_double4(cc01.x, cc01.y, cc23.x, cc23.y);
     const double rho = Li.rho, sos = Li.sos;
     const double T = Li.p / (rho * ph.R);
     // ---- computeSgsVreman
     double mu_sgs = 0.0, a_sgs = 0.0, loc_sgs = 0.0;
     if (ph.sgs_model == CGX_SGS_VREMAN) {
-      const double dx = cc.x;
+      const double dx = cc01.x;
       const double dx2 = dx * dx;
       const double a11 = g[0], a12 = g[1], a13 = g[2];
       const double a21 = g[3], a22 = g[4], a23 = g[5];
@@ -427,10 +594,10 @@ __global__ void __launch_bounds__(kBlock) k_step_end(MeshDev m, StateDev s, Phys
       const double inv_sos2 = 1.0 / (sos * sos);
       a_sgs = ph.a_sgs_coeff * s_mag / dx2;
       const double dil = g[0] + g[4] + g[8];
-      const double t = fabs(dil) * dx / sos;
-      if (t > 0.01) {
+      const double tt = fabs(dil) * dx / sos;
+      if (tt > 0.01) {
         const double Masq = (Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2]) * inv_sos2;
-        a_sgs += ph.a_sgs_coeff2 * cc.w * fmin(Masq, 10.0) * sos;
+        a_sgs += ph.a_sgs_coeff2 * cc23.y * fmin(Masq, 10.0) * sos;
       }
       a_sgs *= inv_sos2;
       loc_sgs = ph.lambda_dil_coeff * rho * fabs(dil) * dx2;
@@ -441,43 +608,8 @@ __global__ void __launch_bounds__(kBlock) k_step_end(MeshDev m, StateDev s, Phys
     const double loc_lam = mu_lam * (1.0 / ph.Pr_lam);
     const double sos2 = ph.gamma * Li.p / rho;
     const double lambda = sqrt(Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2]) + sqrt(sos2);
-    const double symp = fmax(ph.coeff_p * cc.z * lambda / sos2 - cc.y * a_sgs, 0.0);
-    const double symh = ph.coeff_h * cc.z;
-    // ---- Gibbs sensor and CFL over the cell's faces
-    const long long base = m.slice_off[i >> 5] + (i & 31);
-    const int meta = __ldg(m.meta + i);
-    const int deg = meta & 0xffff, ncomp = meta >> 16;
-    const double2* Qi = reinterpret_cast<const double2*>(s.Q + i);
-    const double2 qa = __ldg(Qi), qb = __ldg(Qi + 1);
-    double vv2 = 0.0;
-    for (int k = 0; k < deg; ++k) {
-      const long long e = base + 32LL * k;
-      const int j = __ldg(m.nbr + e);
-      const double2* Qj = reinterpret_cast<const double2*>(s.Q + j);
-      const double2 ja = __ldg(Qj), jb = __ldg(Qj + 1);
-      const double dp = ja.y - qa.y;
-      const double v_avg = 0.5 * (qb.x + jb.x);
-      const double beta = 0.5 * (qb.y + jb.y);
-      const double gr = ja.x - qa.x - v_avg * dp * beta;
-      vv2 = fmax(vv2, fabs(gr));
-      if (k < ncomp) {
-        const int f = __ldg(m.fid + e);
-        const int fi = f & kFidMask;
-        const double sg = (f < 0) ? -1.0 : 1.0;
-        // CFRec: un[0..2], area [3], aod [4], n_fa [5..7]
-        const double* cfr = reinterpret_cast<const double*>(m.cf + fi);
-        const double area = __ldg(cfr + 3);
-        const double2 n12 = __ldg(reinterpret_cast<const double2*>(cfr + 6));
-        const double n0 = sg * __ldg(cfr + 5), n1 = sg * n12.x, n2 = sg * n12.y;
-        LRec Lj;
-        load_L(s.L, j, Lj);
-        const double undA = 0.5 * ((Li.u[0] * n0 + Li.u[1] * n1 + Li.u[2] * n2) +
-                                   (Lj.u[0] * n0 + Lj.u[1] * n1 + Lj.u[2] * n2));
-        const double sos_avg = 0.5 * (sos + Lj.sos);
-        cfl += fabs(undA) + area * sos_avg;
-      }
-    }
-    cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
+    const double symp = fmax(ph.coeff_p * cc23.x * lambda / sos2 - cc01.y * a_sgs, 0.0);
+    const double symh = ph.coeff_h * cc23.x;
     double fgr = 0.5 / (1.0 + exp(-2.0 * (vv2 - ph.gr_nrm) / 5.0e-03));
     if (ph.diss_mode == CGX_DISS_NONE) fgr = 0.0;
     if (ph.diss_mode == CGX_DISS_ALL) fgr = 0.5;
@@ -486,21 +618,23 @@ __global__ void __launch_bounds__(kBlock) k_step_end(MeshDev m, StateDev s, Phys
     P[1] = make_double2(a_sgs, fgr);
     P[2] = make_double2(symh, symp);
     nan = (rho != rho) || (Li.p != Li.p) || (T != T);
+    cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
   }
   // ---- block reductions, last block finalises the control block
-  sh_cfl[threadIdx.x] = cfl;
-  sh_nan[threadIdx.x] = nan;
-  __syncthreads();
-  for (int w = kBlock / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-      sh_cfl[threadIdx.x] = fmax(sh_cfl[threadIdx.x], sh_cfl[threadIdx.x + w]);
-      sh_nan[threadIdx.x] |= sh_nan[threadIdx.x + w];
-    }
-    __syncthreads();
+  if (lane == 0) {
+    sh_cfl[cl] = valid ? cfl : 0.0;
+    sh_nan[cl] = nan;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    s.red[blockIdx.x] = sh_cfl[0];
-    s.red[gridDim.x + blockIdx.x] = double(sh_nan[0]);
+    double mx = 0.0;
+    int an = 0;
+    for (int c = 0; c < kCells; ++c) {
+      mx = fmax(mx, sh_cfl[c]);
+      an |= sh_nan[c];
+    }
+    s.red[blockIdx.x] = mx;
+    s.red[gridDim.x + blockIdx.x] = double(an);
     __threadfence();
     const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
     am_last = (done == gridDim.x - 1);
@@ -508,45 +642,10 @@ __global__ void __launch_bounds__(kBlock) k_step_end(MeshDev m, StateDev s, Phys
   __syncthreads();
   if (!am_last) return;
   __threadfence();
-  double mx = 0.0;
-  int anynan = 0;
-  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-    mx = fmax(mx, ((volatile double*)s.red)[b]);
-    anynan |= (((volatile double*)s.red)[gridDim.x + b] != 0.0);
-  }
-  sh_cfl[threadIdx.x] = mx;
-  sh_nan[threadIdx.x] = anynan;
-  __syncthreads();
-  for (int w = kBlock / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-      sh_cfl[threadIdx.x] = fmax(sh_cfl[threadIdx.x], sh_cfl[threadIdx.x + w]);
-      sh_nan[threadIdx.x] |= sh_nan[threadIdx.x + w];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    Ctl* c = s.ctl;
-    const double cmax = sh_cfl[0];
-    c->cfl_max = cmax;
-    if (sh_nan[0]) c->nan = 1;
-    if (mode & 1) {
-      c->dt_last = c->dt;
-      c->time += c->dt;
-      c->step += 1;
-    }
-    if (mode & 2) {
-      double dt;
-      if (ph.dt_mode == CGX_DT_CONST)
-        dt = c->dt_data0;
-      else if (ph.dt_mode == CGX_DT_CFL)
-        dt = c->dt_data0 / cmax;
-      else
-        dt = fmin(ph.dt_max, c->dt_data0 / fmax(cmax, 1.0E-12));
-      c->dt = dt;
-    }
-    c->blocks_done = 0;
-  }
+  finalize_ctl(s, ph, mode);
 }
+
+#include "cgx_mixed.cuh"
 
 // report() totals: per-block partial sums in a fixed tree, then one block
 // sums the partials in block order (deterministic).
@@ -623,13 +722,31 @@ __global__ void k_state_out(int N, const int* __restrict__ perm, double* __restr
 // generic "k values per cell from the solver's buffers" -> reference order
 // what: 0 rhs(stage) [5], 1 p,T,sos [3], 2 dudx [9], 3 aux [6]
 __global__ void k_diag_out(int N, const int* __restrict__ perm, double* __restrict__ out, StateDev s,
-                           int what, int stage, double R) {
+                           int what, int stage, double R, double p_ref) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const int o = perm[i];
   if (what == 0) {
     const double* r = s.rhs + size_t(stage) * 5 * N;
     for (int c = 0; c < 5; ++c) out[5 * size_t(o) + c] = r[size_t(c) * N + i];
+  } else if (s.LF) {  // mixed-precision records
+    if (what == 1) {
+      const LRecF& L = s.LF[i];
+      const double p = p_ref + double(L.pp);
+      out[3 * size_t(o)] = p;
+      out[3 * size_t(o) + 1] = p / (double(L.rho) * R);
+      out[3 * size_t(o) + 2] = L.sos;
+    } else if (what == 2) {
+      for (int c = 0; c < 9; ++c) out[9 * size_t(o) + c] = s.GF[i].g[c];
+    } else {
+      const PRecF& P = s.PF[i];
+      out[6 * size_t(o) + 0] = P.mu_total;
+      out[6 * size_t(o) + 1] = P.loc_total;
+      out[6 * size_t(o) + 2] = P.a_sgs;
+      out[6 * size_t(o) + 3] = P.fgr;
+      out[6 * size_t(o) + 4] = P.symh;
+      out[6 * size_t(o) + 5] = P.symp;
+    }
   } else if (what == 1) {
     const LRec& L = s.L[i];
     out[3 * size_t(o)] = L.p;
@@ -648,28 +765,70 @@ __global__ void k_diag_out(int N, const int* __restrict__ perm, double* __restri
   }
 }
 
+// FP32 copies of the mesh geometry and gradient coefficients (mixed form)
+__global__ void k_geom32(int nef, int ncf, long long nc, const EFRec* __restrict__ ef,
+                         const CFRec* __restrict__ cf, const double* __restrict__ gx,
+                         const double* __restrict__ gy, const double* __restrict__ gz, EFRecF* ef32,
+                         CFRecF* cf32, float* gx32, float* gy32, float* gz32) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < nef) {
+    const EFRec& a = ef[t];
+    EFRecF r;
+    for (int k = 0; k < 3; ++k) {
+      r.n[k] = float(a.n[k]);
+      r.c[k] = float(a.c[k]);
+    }
+    r.pad[0] = r.pad[1] = 0.0f;
+    ef32[t] = r;
+  }
+  if (t < ncf) {
+    const CFRec& a = cf[t];
+    CFRecF r;
+    for (int k = 0; k < 3; ++k) r.un[k] = float(a.un[k]);
+    r.area = float(a.area);
+    r.aod = float(a.aod);
+    r.delta = float(a.delta);
+    r.pad[0] = r.pad[1] = 0.0f;
+    cf32[t] = r;
+  }
+  if (t < nc) {
+    gx32[t] = float(gx[t]);
+    gy32[t] = float(gy[t]);
+    gz32[t] = float(gz[t]);
+  }
+}
+
 // calcCfl(cfl, dt) per cell (diagnostic; the stepping path uses k_step_end)
 __global__ void k_cfl_cells(MeshDev m, StateDev s, const int* __restrict__ perm, double dt,
                             double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.N) return;
-  LRec Li;
-  load_L(s.L, i, Li);
-  const long long base = m.slice_off[i >> 5] + (i & 31);
-  const int ncomp = __ldg(m.meta + i) >> 16;
+  auto vel = [&](int c, double u[3], double& sos) {
+    if (s.LF) {
+      const LRecF& L = s.LF[c];
+      u[0] = L.u[0]; u[1] = L.u[1]; u[2] = L.u[2];
+      sos = L.sos;
+    } else {
+      const LRec& L = s.L[c];
+      u[0] = L.u[0]; u[1] = L.u[1]; u[2] = L.u[2];
+      sos = L.sos;
+    }
+  };
+  double ui[3], si;
+  vel(i, ui, si);
+  const long long b = m.off[i], ec = b + m.ncomp[i];
   double cfl = 0.0;
-  for (int k = 0; k < ncomp; ++k) {
-    const long long e = base + 32LL * k;
-    const int j = __ldg(m.nbr + e);
-    const int f = __ldg(m.fid + e);
+  for (long long k = b; k < ec; ++k) {
+    const int j = m.nbr[k];
+    const int f = m.fid[k];
     const double sg = (f < 0) ? -1.0 : 1.0;
     const CFRec& cr = m.cf[f & kFidMask];
-    const double n[3] = {sg * cr.nfa[0], sg * cr.nfa[1], sg * cr.nfa[2]};
-    LRec Lj;
-    load_L(s.L, j, Lj);
-    const double undA = 0.5 * ((Li.u[0] * n[0] + Li.u[1] * n[1] + Li.u[2] * n[2]) +
-                               (Lj.u[0] * n[0] + Lj.u[1] * n[1] + Lj.u[2] * n[2]));
-    cfl += fabs(undA) + cr.area * (0.5 * (Li.sos + Lj.sos));
+    const double un[3] = {sg * cr.un[0], sg * cr.un[1], sg * cr.un[2]};
+    double uj[3], sj;
+    vel(j, uj, sj);
+    const double undA = 0.5 * cr.area * ((ui[0] * un[0] + ui[1] * un[1] + ui[2] * un[2]) +
+                                         (uj[0] * un[0] + uj[1] * un[1] + uj[2] * un[2]));
+    cfl += fabs(undA) + cr.area * (0.5 * (si + sj));
   }
   out[perm[i]] = cfl * (0.5 * dt * m.inv_vol[i]);
 }
@@ -727,18 +886,23 @@ inline uint64_t spread3(uint64_t x) {  // 21 bits -> every third bit
 struct cgx_mesh {
   int device = 0;
   int N = 0, ncv_g2 = 0;
+  long long nef = 0, ncf = 0, nc_dir = 0;  // record counts (for the FP32 copies)
+  bool have32 = false;
   std::vector<int> perm;  // new -> old
   MeshDev md{};
   int* d_perm = nullptr;
-  int* d_cnbr = nullptr;
-  int* d_cdeg = nullptr;
   std::vector<void*> allocs;
   size_t bytes = 0;
   cgx_mesh_stats stats{};
 };
 
+struct Tune {
+  int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4;
+};
+
 struct cgx_solver {
   cgx_mesh* mesh = nullptr;
+  Tune tune;
   cgx_params prm{};
   cgx_precision prec = CGX_FP64;
   Phys ph{};
@@ -752,6 +916,7 @@ struct cgx_solver {
   bool have_store = false;
   std::vector<void*> allocs;
   int nblocks = 0;
+  int nblocks_end = 0;
   bool state_set = false;
   bool inited = false;
   cudaGraphExec_t graph = nullptr;
@@ -774,19 +939,213 @@ int enqueue_prim(cgx_solver* s, int nw, const double* w, double dt_arg, bool wri
   return launch_check(s, 1);
 }
 
-int enqueue_grad(cgx_solver* s) {
-  k_grad<<<s->nblocks, kBlock, 0, s->stream>>>(s->mesh->md, s->sd, s->mesh->d_cnbr, s->mesh->d_cdeg);
+// Lanes per cell of the group-per-cell kernels, chosen per mesh-size bucket
+// by autotune() (timed candidates, cached process-wide).
+inline int groups_grid(int N, int G) { return int((static_cast<long long>(N) * G + 255) / 256); }
+
+template <int G>
+void launch_grad_g(cgx_solver* s) {
+  k_grad<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd);
+}
+template <int G>
+void launch_ext_g(cgx_solver* s, int st) {
+  k_rhs_ext<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st);
+}
+template <int G>
+void launch_comp_g(cgx_solver* s, int st) {
+  k_rhs_comp<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st);
+}
+template <int G>
+void launch_end_g(cgx_solver* s, int mode) {
+  k_step_end<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, s->ph, mode);
+}
+
+int enqueue_grad_g(cgx_solver* s, int G) {
+  switch (G) {
+    case 1: launch_grad_g<1>(s); break;
+    case 2: launch_grad_g<2>(s); break;
+    case 4: launch_grad_g<4>(s); break;
+    case 8: launch_grad_g<8>(s); break;
+    default: launch_grad_g<16>(s); break;
+  }
   return launch_check(s, 1);
 }
+int enqueue_ext_g(cgx_solver* s, int G, int st) {
+  switch (G) {
+    case 4: launch_ext_g<4>(s, st); break;
+    case 8: launch_ext_g<8>(s, st); break;
+    case 32: launch_ext_g<32>(s, st); break;
+    default: launch_ext_g<16>(s, st); break;
+  }
+  return launch_check(s, 1);
+}
+int enqueue_comp_g(cgx_solver* s, int G, int st) {
+  switch (G) {
+    case 2: launch_comp_g<2>(s, st); break;
+    case 4: launch_comp_g<4>(s, st); break;
+    case 8: launch_comp_g<8>(s, st); break;
+    default: launch_comp_g<16>(s, st); break;
+  }
+  return launch_check(s, 1);
+}
+int enqueue_end_g(cgx_solver* s, int G, int mode) {
+  switch (G) {
+    case 1: launch_end_g<1>(s, mode); break;
+    case 4: launch_end_g<4>(s, mode); break;
+    case 8: launch_end_g<8>(s, mode); break;
+    default: launch_end_g<16>(s, mode); break;
+  }
+  return launch_check(s, 1);
+}
+
+// mixed-precision variants
+template <int G>
+void launch_grad_f(cgx_solver* s) {
+  k_grad_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd);
+}
+template <int G>
+void launch_ext_f(cgx_solver* s, int st) {
+  k_rhs_ext_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st, s->ph.h_ref);
+}
+template <int G>
+void launch_comp_f(cgx_solver* s, int st) {
+  k_rhs_comp_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st, s->ph.h_ref,
+                                                                      float(s->ph.p_ref));
+}
+template <int G>
+void launch_end_f(cgx_solver* s, int mode) {
+  k_step_end_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, s->ph, mode);
+}
+int enqueue_grad_fg(cgx_solver* s, int G) {
+  switch (G) {
+    case 1: launch_grad_f<1>(s); break;
+    case 2: launch_grad_f<2>(s); break;
+    case 4: launch_grad_f<4>(s); break;
+    case 8: launch_grad_f<8>(s); break;
+    default: launch_grad_f<16>(s); break;
+  }
+  return launch_check(s, 1);
+}
+int enqueue_ext_fg(cgx_solver* s, int G, int st) {
+  switch (G) {
+    case 4: launch_ext_f<4>(s, st); break;
+    case 8: launch_ext_f<8>(s, st); break;
+    case 32: launch_ext_f<32>(s, st); break;
+    default: launch_ext_f<16>(s, st); break;
+  }
+  return launch_check(s, 1);
+}
+int enqueue_comp_fg(cgx_solver* s, int G, int st) {
+  switch (G) {
+    case 2: launch_comp_f<2>(s, st); break;
+    case 4: launch_comp_f<4>(s, st); break;
+    case 8: launch_comp_f<8>(s, st); break;
+    default: launch_comp_f<16>(s, st); break;
+  }
+  return launch_check(s, 1);
+}
+int enqueue_end_fg(cgx_solver* s, int G, int mode) {
+  switch (G) {
+    case 1: launch_end_f<1>(s, mode); break;
+    case 4: launch_end_f<4>(s, mode); break;
+    case 8: launch_end_f<8>(s, mode); break;
+    default: launch_end_f<16>(s, mode); break;
+  }
+  return launch_check(s, 1);
+}
+
+inline bool mixed(const cgx_solver* s) { return s->prec == CGX_MIXED; }
+
+int grad_var(cgx_solver* s, int G) { return mixed(s) ? enqueue_grad_fg(s, G) : enqueue_grad_g(s, G); }
+int ext_var(cgx_solver* s, int G, int st) { return mixed(s) ? enqueue_ext_fg(s, G, st) : enqueue_ext_g(s, G, st); }
+int comp_var(cgx_solver* s, int G, int st) { return mixed(s) ? enqueue_comp_fg(s, G, st) : enqueue_comp_g(s, G, st); }
+int end_var(cgx_solver* s, int G, int mode) { return mixed(s) ? enqueue_end_fg(s, G, mode) : enqueue_end_g(s, G, mode); }
+
+int enqueue_grad(cgx_solver* s) { return grad_var(s, s->tune.g_grad); }
 
 int enqueue_rhs(cgx_solver* s, int stage0) {
-  k_rhs<<<s->nblocks, kBlock, 0, s->stream>>>(s->mesh->md, s->sd, stage0);
-  return launch_check(s, 1);
+  int rc = ext_var(s, s->tune.g_ext, stage0);
+  if (rc) return rc;
+  return comp_var(s, s->tune.g_comp, stage0);
 }
 
-int enqueue_step_end(cgx_solver* s, int mode) {
-  k_step_end<<<s->nblocks, kBlock, 0, s->stream>>>(s->mesh->md, s->sd, s->ph, mode);
-  return launch_check(s, 1);
+int enqueue_step_end(cgx_solver* s, int mode) { return end_var(s, s->tune.g_end, mode); }
+
+std::mutex g_tune_mu;
+std::map<int, Tune> g_tune_cache;
+
+int tune_bucket(const cgx_solver* s) {
+  int b = 0;
+  for (long long n = s->mesh->N; n > 1; n >>= 1) ++b;
+  return b * 4 + int(s->prec);
+}
+
+// Time each candidate lane count of each kernel on this solver's mesh and
+// keep the fastest; results are cached per mesh-size bucket (log2 of the
+// cell count) and precision.  All candidates compute the same values (only
+// the order of the per-cell sums changes), and none changes the state.
+int autotune(cgx_solver* s) {
+  const int bucket = tune_bucket(s);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(bucket);
+    if (it != g_tune_cache.end()) {
+      s->tune = it->second;
+      return CGX_OK;
+    }
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto time_it = [&](auto&& fn, float* ms) -> int {
+    int rc = fn();  // warm-up
+    if (rc) return rc;
+    CK(cudaEventRecord(e0, s->stream));
+    for (int r = 0; r < 3 && rc == CGX_OK; ++r) rc = fn();
+    CK(cudaEventRecord(e1, s->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return rc;
+  };
+  Tune best = s->tune;
+  float bt;
+  int rc = CGX_OK;
+  const int ext_c[] = {4, 8, 16, 32}, comp_c[] = {2, 4, 8, 16}, grad_c[] = {1, 2, 4, 8, 16},
+            end_c[] = {1, 4, 8, 16};
+  bt = 1e30f;
+  for (int G : ext_c) {
+    float ms;
+    if ((rc = time_it([&] { return ext_var(s, G, 0); }, &ms))) break;
+    if (ms < bt) { bt = ms; best.g_ext = G; }
+  }
+  bt = 1e30f;
+  for (int G : comp_c) {
+    if (rc) break;
+    float ms;
+    if ((rc = time_it([&] { return comp_var(s, G, 0); }, &ms))) break;
+    if (ms < bt) { bt = ms; best.g_comp = G; }
+  }
+  bt = 1e30f;
+  for (int G : grad_c) {
+    if (rc) break;
+    float ms;
+    if ((rc = time_it([&] { return grad_var(s, G); }, &ms))) break;
+    if (ms < bt) { bt = ms; best.g_grad = G; }
+  }
+  bt = 1e30f;
+  for (int G : end_c) {
+    if (rc) break;
+    float ms;
+    if ((rc = time_it([&] { return end_var(s, G, 0); }, &ms))) break;
+    if (ms < bt) { bt = ms; best.g_end = G; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  s->tune = best;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[bucket] = best;
+  return CGX_OK;
 }
 
 // SSP-RK3 weights in increment form (src/charles/RkWeights.hpp:108-110)
@@ -1019,23 +1378,22 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         r.c[k] = d->c_ef[3 * size_t(f) + k];
       }
       for (int k = 0; k < 3; ++k) r.c[k] *= 0.5;  // FlowSolver.hpp:2256-2259
-      r.pad0 = r.pad1 = 0.0;
       const int fa = cf_of_ef[f];
       if (fa >= 0) {
+        // FaCompact (FlowSolver.hpp:1871-1884): unit normal along the
+        // extended face, area, area_over_delta; delta = area/area_over_delta
+        // as calcInternalCompactFluxNewGrad forms it
         CFRec& c = cfr[fnew[f]];
         const double* n = d->n_fa + 3 * size_t(fa);
         const double area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
         const double inv_area = 1.0 / area;
-        const double sg = cf_rev[f] ? -1.0 : 1.0;
-        for (int k = 0; k < 3; ++k) {
-          c.un[k] = cf_rev[f] ? -n[k] * inv_area : n[k] * inv_area;
-          c.nfa[k] = sg * n[k];
-        }
+        for (int k = 0; k < 3; ++k) c.un[k] = cf_rev[f] ? -n[k] * inv_area : n[k] * inv_area;
         c.area = area;
         c.aod = d->area_over_delta_fa[fa];
+        c.delta = area / c.aod;
       }
     }
-    // ---- directed entries per cell (new numbering)
+    // ---- directed entries per cell (new numbering): CSR, compact faces first
     std::vector<int> deg(N, 0), ncomp(N, 0);
     for (int f = 0; f < nef; ++f) {
       const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
@@ -1050,10 +1408,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       }
     }
     std::vector<long long> cell_off(N + 1, 0);
-    for (int i = 0; i < N; ++i) {
-      if (deg[i] > 0xffff || ncomp[i] > 0x7fff) return bail(fail(CGX_E_ARG, "cell degree too large"));
-      cell_off[i + 1] = cell_off[i] + deg[i];
-    }
+    for (int i = 0; i < N; ++i) cell_off[i + 1] = cell_off[i] + deg[i];
     std::vector<int> e_nbr(cell_off[N]), e_fid(cell_off[N]);
     {
       std::vector<long long> fill(cell_off.begin(), cell_off.end() - 1);
@@ -1069,86 +1424,43 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         }
       }
     }
-#pragma omp parallel for schedule(dynamic, 4096)
-    for (int i = 0; i < N; ++i) {
-      const long long b = cell_off[i], e = cell_off[i + 1];
+#pragma omp parallel
+    {
       std::vector<std::pair<int, int>> tmp;
-      tmp.reserve(e - b);
-      for (long long k = b; k < e; ++k) tmp.push_back({e_fid[k], e_nbr[k]});
-      // compact faces (ids < ncf) first, each part by face id
-      std::sort(tmp.begin(), tmp.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
-        return (x.first & kFidMask) < (y.first & kFidMask);
-      });
-      for (long long k = b; k < e; ++k) {
-        e_fid[k] = tmp[k - b].first;
-        e_nbr[k] = tmp[k - b].second;
-      }
-    }
-    // ---- SELL-32
-    const int nsl = (N + 31) / 32;
-    std::vector<long long> soff(nsl + 1, 0);
-    std::vector<int> sw(nsl, 0);
-    for (int sl = 0; sl < nsl; ++sl) {
-      int w = 0;
-      for (int i = sl * 32; i < std::min(N, sl * 32 + 32); ++i) w = std::max(w, deg[i]);
-      sw[sl] = w;
-      soff[sl + 1] = soff[sl] + 32LL * w;
-    }
-    std::vector<int> s_nbr(soff[nsl]), s_fid(soff[nsl]);
-    std::vector<int> meta(N);
-#pragma omp parallel for schedule(static)
-    for (int sl = 0; sl < nsl; ++sl) {
-      for (int l = 0; l < 32; ++l) {
-        const int i = sl * 32 + l;
-        for (int k = 0; k < sw[sl]; ++k) {
-          const long long slot = soff[sl] + 32LL * k + l;
-          if (i < N && k < deg[i]) {
-            s_nbr[slot] = e_nbr[cell_off[i] + k];
-            s_fid[slot] = e_fid[cell_off[i] + k];
-          } else {
-            s_nbr[slot] = (i < N) ? i : 0;
-            s_fid[slot] = 0;
-          }
+#pragma omp for schedule(dynamic, 4096)
+      for (int i = 0; i < N; ++i) {
+        const long long b = cell_off[i], e = cell_off[i + 1];
+        tmp.clear();
+        for (long long k = b; k < e; ++k) tmp.push_back({e_fid[k], e_nbr[k]});
+        // compact faces (ids < ncf) first, each part by face id
+        std::sort(tmp.begin(), tmp.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+          return (x.first & kFidMask) < (y.first & kFidMask);
+        });
+        for (long long k = b; k < e; ++k) {
+          e_fid[k] = tmp[k - b].first;
+          e_nbr[k] = tmp[k - b].second;
         }
-        if (i < N) meta[i] = deg[i] | (ncomp[i] << 16);
       }
     }
-    std::vector<int>().swap(e_nbr);
-    std::vector<int>().swap(e_fid);
-    // ---- gradient SELL (cvocv without the diagonal)
-    std::vector<int> cdeg(N);
+    // ---- gradient CSR (cvocv without the diagonal, reference order)
+    std::vector<long long> coff(N + 1, 0);
     for (int i = 0; i < N; ++i) {
       const int o = perm[i];
-      cdeg[i] = d->cvocv_i[o + 1] - d->cvocv_i[o] - 1;
-      if (cdeg[i] < 0) return bail(fail(CGX_E_ARG, "cvocv without diagonal"));
+      const int cd = d->cvocv_i[o + 1] - d->cvocv_i[o] - 1;
+      if (cd < 0) return bail(fail(CGX_E_ARG, "cvocv without diagonal"));
+      coff[i + 1] = coff[i] + cd;
     }
-    std::vector<long long> csoff(nsl + 1, 0);
-    std::vector<int> csw(nsl, 0);
-    for (int sl = 0; sl < nsl; ++sl) {
-      int w = 0;
-      for (int i = sl * 32; i < std::min(N, sl * 32 + 32); ++i) w = std::max(w, cdeg[i]);
-      csw[sl] = w;
-      csoff[sl + 1] = csoff[sl] + 32LL * w;
-    }
-    std::vector<int> c_nbr(csoff[nsl]);
-    std::vector<double> gx(csoff[nsl]), gy(csoff[nsl]), gz(csoff[nsl]);
+    std::vector<int> c_nbr(coff[N]);
+    std::vector<double> gx(coff[N]), gy(coff[N]), gz(coff[N]);
 #pragma omp parallel for schedule(static)
-    for (int sl = 0; sl < nsl; ++sl) {
-      for (int l = 0; l < 32; ++l) {
-        const int i = sl * 32 + l;
-        for (int k = 0; k < csw[sl]; ++k) {
-          const long long slot = csoff[sl] + 32LL * k + l;
-          if (i < N && k < cdeg[i]) {
-            const int coc = d->cvocv_i[perm[i]] + 1 + k;
-            c_nbr[slot] = nw(d->cvocv_v[coc]);
-            gx[slot] = d->cvocv_grad_coeff[3 * size_t(coc)];
-            gy[slot] = d->cvocv_grad_coeff[3 * size_t(coc) + 1];
-            gz[slot] = d->cvocv_grad_coeff[3 * size_t(coc) + 2];
-          } else {
-            c_nbr[slot] = (i < N) ? i : 0;
-            gx[slot] = gy[slot] = gz[slot] = 0.0;
-          }
-        }
+    for (int i = 0; i < N; ++i) {
+      const int coc0 = d->cvocv_i[perm[i]] + 1;
+      for (long long k = coff[i]; k < coff[i + 1]; ++k) {
+        const int coc = coc0 + int(k - coff[i]);
+        c_nbr[k] = nw(d->cvocv_v[coc]);
+        gx[k] = d->cvocv_grad_coeff[3 * size_t(coc)];
+        gy[k] = d->cvocv_grad_coeff[3 * size_t(coc) + 1];
+        gz[k] = d->cvocv_grad_coeff[3 * size_t(coc) + 2];
       }
     }
     // ---- per-cell constants (pow on the host: the reference's libm values)
@@ -1165,22 +1477,21 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     // ---- upload
     size_t* acc = &M->bytes;
     int rc;
-    long long* d_soff;
-    int *d_sw, *d_meta, *d_nbr, *d_fid;
-    long long* d_csoff;
+    long long *d_off, *d_coff;
+    int *d_ncomp, *d_nbr, *d_fid, *d_cnbr;
     double *d_gx, *d_gy, *d_gz, *d_vol, *d_ivol;
     EFRec* d_ef;
     CFRec* d_cf;
     double4* d_cc;
-#define UP(ptr, vec)                      \
+#define UP(ptr, vec)                                   \
   if ((rc = dupload(&ptr, vec, acc))) return bail(rc); \
   M->allocs.push_back(ptr);
-    UP(d_soff, soff);
-    UP(d_sw, sw);
-    UP(d_meta, meta);
-    UP(d_nbr, s_nbr);
-    UP(d_fid, s_fid);
-    UP(d_csoff, csoff);
+    UP(d_off, cell_off);
+    UP(d_ncomp, ncomp);
+    UP(d_nbr, e_nbr);
+    UP(d_fid, e_fid);
+    UP(d_coff, coff);
+    UP(d_cnbr, c_nbr);
     UP(d_gx, gx);
     UP(d_gy, gy);
     UP(d_gz, gz);
@@ -1190,18 +1501,15 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     UP(d_ivol, inv_vol);
     UP(d_cc, cc);
     UP(M->d_perm, perm);
-    UP(M->d_cnbr, c_nbr);
-    UP(M->d_cdeg, cdeg);
 #undef UP
     MeshDev& md = M->md;
     md.N = N;
-    md.nslices = nsl;
-    md.slice_off = d_soff;
-    md.slice_w = d_sw;
-    md.cslice_off = d_csoff;
-    md.meta = d_meta;
+    md.off = d_off;
+    md.ncomp = d_ncomp;
     md.nbr = d_nbr;
     md.fid = d_fid;
+    md.coff = d_coff;
+    md.cnbr = d_cnbr;
     md.gcx = d_gx;
     md.gcy = d_gy;
     md.gcz = d_gz;
@@ -1210,6 +1518,12 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     md.vol = d_vol;
     md.inv_vol = d_ivol;
     md.cc = d_cc;
+    md.ef32 = nullptr;
+    md.cf32 = nullptr;
+    md.gcx32 = md.gcy32 = md.gcz32 = nullptr;
+    M->nef = nef;
+    M->ncf = ncf;
+    M->nc_dir = coff[N];
     long long n_ef_dir = cell_off[N], n_cf_dir = 0;
     for (int i = 0; i < N; ++i) n_cf_dir += ncomp[i];
     M->stats.ncv = N;
@@ -1246,7 +1560,6 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   if (!m || !p || !out) return fail(CGX_E_ARG, "cgx_solver_create: null argument");
   *out = nullptr;
   if (prec != CGX_FP64 && prec != CGX_MIXED) return fail(CGX_E_ARG, "unknown precision");
-  if (prec == CGX_MIXED) return fail(CGX_E_ARG, "mixed precision is not available in this build");
   if (!(p->gamma > 1.0) || !(p->p_ref > 0) || !(p->rho_ref > 0) || !(p->T_ref > 0) || !(p->Pr_lam > 0) ||
       !(p->Pr_t > 0) || p->dt_mode < 0 || p->dt_mode > 2 || p->sgs_model < 0 || p->sgs_model > 1)
     return fail(CGX_E_ARG, "cgx_solver_create: invalid parameters");
@@ -1275,8 +1588,10 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   ph.diss_mode = p->diss_mode;
   ph.dt_mode = p->dt_mode;
   ph.dt_max = p->dt_data[1];
+  ph.h_ref = ph.R * p->gamma / (p->gamma - 1.0) * p->T_ref;
   const size_t N = m->N;
   s->nblocks = int((N + kBlock - 1) / kBlock);
+  s->nblocks_end = int((static_cast<long long>(N) * 16 + 255) / 256);  // largest G candidate
   auto bail = [&](int rc) {
     for (void* q : s->allocs) cudaFree(q);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1297,20 +1612,69 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   AL(sd.u2, N);
   AL(sd.rhoE, N);
   AL(sd.rhs, 15 * N);
-  AL(sd.L, N);
-  AL(sd.P, N);
-  AL(sd.G, N);
-  AL(sd.Q, N);
+  if (prec == CGX_MIXED) {
+    sd.L = nullptr;
+    sd.P = nullptr;
+    sd.G = nullptr;
+    sd.Q = nullptr;
+    AL(sd.LF, N);
+    AL(sd.PF, N);
+    AL(sd.GF, N);
+    AL(sd.QF, N);
+    if (!m->have32) {
+      EFRecF* ef32;
+      CFRecF* cf32;
+      float *gx32, *gy32, *gz32;
+      size_t* mb = &m->bytes;
+      if ((rc = dalloc(&ef32, m->nef, mb))) return bail(rc);
+      m->allocs.push_back(ef32);
+      if ((rc = dalloc(&cf32, std::max<long long>(m->ncf, 1), mb))) return bail(rc);
+      m->allocs.push_back(cf32);
+      if ((rc = dalloc(&gx32, m->nc_dir, mb))) return bail(rc);
+      m->allocs.push_back(gx32);
+      if ((rc = dalloc(&gy32, m->nc_dir, mb))) return bail(rc);
+      m->allocs.push_back(gy32);
+      if ((rc = dalloc(&gz32, m->nc_dir, mb))) return bail(rc);
+      m->allocs.push_back(gz32);
+      const long long nmax = std::max(m->nef, std::max(m->ncf, m->nc_dir));
+      k_geom32<<<int((nmax + 255) / 256), 256, 0, s->stream>>>(int(m->nef), int(m->ncf), m->nc_dir, m->md.ef,
+                                                               m->md.cf, m->md.gcx, m->md.gcy, m->md.gcz,
+                                                               ef32, cf32, gx32, gy32, gz32);
+      if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s->stream) != cudaSuccess)
+        return bail(fail(CGX_E_CUDA, "FP32 geometry conversion failed"));
+      m->md.ef32 = ef32;
+      m->md.cf32 = cf32;
+      m->md.gcx32 = gx32;
+      m->md.gcy32 = gy32;
+      m->md.gcz32 = gz32;
+      m->stats.device_bytes = m->bytes;
+      m->have32 = true;
+    }
+  } else {
+    sd.LF = nullptr;
+    sd.PF = nullptr;
+    sd.GF = nullptr;
+    sd.QF = nullptr;
+    AL(sd.L, N);
+    AL(sd.P, N);
+    AL(sd.G, N);
+    AL(sd.Q, N);
+  }
   AL(sd.ctl, 1);
-  AL(sd.red, 2 * size_t(s->nblocks));
+  AL(sd.red, 2 * size_t(std::max(s->nblocks, s->nblocks_end)));
   AL(s->d_stage, 9 * N);
   AL(s->d_part, 5 * size_t(s->nblocks) + 5);
   AL(s->d_store[0], 5 * N);
   AL(s->d_store[1], 5 * N);
 #undef AL
-  if (cudaMemsetAsync(sd.rhs, 0, 15 * N * sizeof(double), s->stream) != cudaSuccess ||
-      cudaMemsetAsync(sd.P, 0, N * sizeof(PRec), s->stream) != cudaSuccess ||
-      cudaMemsetAsync(sd.G, 0, N * sizeof(GRec), s->stream) != cudaSuccess)
+  const bool zero_ok =
+      cudaMemsetAsync(sd.rhs, 0, 15 * N * sizeof(double), s->stream) == cudaSuccess &&
+      (prec == CGX_MIXED
+           ? (cudaMemsetAsync(sd.PF, 0, N * sizeof(PRecF), s->stream) == cudaSuccess &&
+              cudaMemsetAsync(sd.GF, 0, N * sizeof(GRecF), s->stream) == cudaSuccess)
+           : (cudaMemsetAsync(sd.P, 0, N * sizeof(PRec), s->stream) == cudaSuccess &&
+              cudaMemsetAsync(sd.G, 0, N * sizeof(GRec), s->stream) == cudaSuccess));
+  if (!zero_ok)
     return bail(fail(CGX_E_CUDA, "cudaMemset failed"));
   Ctl c{};
   c.dt_data0 = p->dt_data[0];
@@ -1406,6 +1770,8 @@ extern "C" int cgx_init_complete(cgx_solver* s) {
   int rc = cgx_update_primitive(s);
   if (rc) return rc;
   if ((rc = cgx_calc_sgs_props(s))) return rc;
+  if ((rc = autotune(s))) return rc;
+  if ((rc = cgx_calc_sgs_props(s))) return rc;
   s->inited = true;
   s->have_store = false;
   return store_state(s);
@@ -1421,7 +1787,7 @@ extern "C" int cgx_calc_rhs(cgx_solver* s, double* rhs_out, double time, int rk_
   if (rc) return rc;
   if (rhs_out) {
     const int N = s->mesh->N;
-    k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, 0, rk_stage - 1, s->ph.R);
+    k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, 0, rk_stage - 1, s->ph.R, s->ph.p_ref);
     if ((rc = launch_check(s, 1))) return rc;
     CK(cudaMemcpyAsync(rhs_out, s->d_stage, 5 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   }
@@ -1490,7 +1856,7 @@ extern "C" int cgx_step(cgx_solver* s, int nsteps) {
     const int batch = std::min(ci, nsteps - done);
     for (int k = 0; k < batch; ++k) {
       CK(cudaGraphLaunch(s->graph, s->stream));
-      s->launches += 10;
+      s->launches += kLaunchesPerStep;
     }
     done += batch;
     bool nan = false;
@@ -1535,7 +1901,7 @@ extern "C" int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms) {
   CK(cudaEventRecord(e0, s->stream));
   for (int k = 0; k < nsteps; ++k) {
     CK(cudaGraphLaunch(s->graph, s->stream));
-    s->launches += 10;
+    s->launches += kLaunchesPerStep;
   }
   CK(cudaEventRecord(e1, s->stream));
   CK(cudaEventSynchronize(e1));
@@ -1607,7 +1973,7 @@ extern "C" int cgx_totals(cgx_solver* s, double out[5]) {
 static int diag(cgx_solver* s, int what, int k, double* out) {
   CK(cudaSetDevice(s->mesh->device));
   const int N = s->mesh->N;
-  k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, what, 0, s->ph.R);
+  k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, what, 0, s->ph.R, s->ph.p_ref);
   int rc = launch_check(s, 1);
   if (rc) return rc;
   CK(cudaMemcpyAsync(out, s->d_stage, size_t(k) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -1643,6 +2009,15 @@ extern "C" int cgx_synchronize(cgx_solver* s) {
   if (!s) return fail(CGX_E_ARG, "null solver");
   CK(cudaSetDevice(s->mesh->device));
   CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
+extern "C" int cgx_get_tuning(const cgx_solver* s, int out[4]) {
+  if (!s || !out) return fail(CGX_E_ARG, "null argument");
+  out[0] = s->tune.g_ext;
+  out[1] = s->tune.g_comp;
+  out[2] = s->tune.g_grad;
+  out[3] = s->tune.g_end;
   return CGX_OK;
 }
 
