@@ -203,6 +203,41 @@ int cgx_get_tuning(const cgx_solver* s, int out[4]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
 
+/*
+ * Batched and served form (no single reference counterpart: the reference
+ * runs one case per process, FlowSolver::run, FlowSolver.hpp:2445-2678).
+ * A batch holds many resident cases of uneven size on one device and
+ * advances them together: each step is one replay of a CUDA graph whose
+ * kernels walk a packed work list of cell blocks across all active cases.
+ * Cases join and leave between steps (continuous batching); their state
+ * stays on the device.  Every case keeps its own parameters, dt (its own
+ * CFL reduction), time, step count and NaN recovery.
+ */
+typedef struct cgx_batch cgx_batch;
+
+/* max_cases resident at once; hbm_budget_bytes bounds the device memory the
+ * batch's cases may hold (their meshes counted once each). */
+int cgx_batch_create(int device, cgx_precision prec, int max_cases, size_t hbm_budget_bytes,
+                     cgx_batch** out);
+int cgx_batch_destroy(cgx_batch* b);
+/* Admit a case on a device mesh (shared with other cases, not owned): state
+ * from rho, u, p as cgx_set_state_primitive, then initComplete.  The case
+ * advances with the batch until it has taken nsteps steps.  Returns
+ * CGX_E_OOM, allocating nothing, when the case would exceed the budget. */
+int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
+                  const double* u, const double* pres, int nsteps, int* case_id);
+/* Advance every active case by up to nsteps steps (a case stops at its own
+ * step count); *n_done = cases that have finished and not been removed. */
+int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done);
+/* Ids of finished cases not yet removed (up to max). */
+int cgx_batch_done(cgx_batch* b, int* ids, int max, int* n);
+int cgx_batch_get_state(cgx_batch* b, int case_id, double* rho, double* u, double* rhoE);
+int cgx_batch_get_time(cgx_batch* b, int case_id, double* time, double* dt, int* step);
+int cgx_batch_remove(cgx_batch* b, int case_id);
+/* Device bytes held by resident cases (meshes once each) and the budget. */
+int cgx_batch_bytes(const cgx_batch* b, size_t* used, size_t* budget);
+long long cgx_batch_launch_count(const cgx_batch* b);
+
 const char* cgx_last_error(void);
 
 #ifdef __cplusplus

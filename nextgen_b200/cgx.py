@@ -178,6 +178,18 @@ def lib():
         "cgx_step_timed": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
         "cgx_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_get_tuning": (ctypes.c_int, [vp, c_int_p]),
+        "cgx_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                             ctypes.POINTER(vp)]),
+        "cgx_batch_destroy": (ctypes.c_int, [vp]),
+        "cgx_batch_add": (ctypes.c_int, [vp, vp, ctypes.POINTER(Params), c_dbl_p, c_dbl_p, c_dbl_p,
+                                          ctypes.c_int, c_int_p]),
+        "cgx_batch_step": (ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
+        "cgx_batch_done": (ctypes.c_int, [vp, c_int_p, ctypes.c_int, c_int_p]),
+        "cgx_batch_get_state": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]),
+        "cgx_batch_get_time": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_int_p]),
+        "cgx_batch_remove": (ctypes.c_int, [vp, ctypes.c_int]),
+        "cgx_batch_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+        "cgx_batch_launch_count": (ctypes.c_longlong, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -356,6 +368,82 @@ class Solver:
     def close(self):
         if self.h:
             lib().cgx_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Resident cases advanced together (cgx_batch_*): continuous batching.
+
+    add() admits a case (returns its id, or None when the HBM budget is
+    full), step() advances every active case, done() lists finished cases,
+    get_state()/remove() retire them."""
+
+    def __init__(self, device=0, precision=CGX_FP64, max_cases=256, hbm_budget=64 << 30):
+        h = ctypes.c_void_p()
+        _check(lib().cgx_batch_create(int(device), int(precision), int(max_cases), int(hbm_budget),
+                                      ctypes.byref(h)))
+        self.h = h
+        self.precision = precision
+        self.ncv = {}
+        self._meshes = {}
+
+    def add(self, mesh, params, rho, u, p, nsteps):
+        rho, u, p = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, p))
+        cid = ctypes.c_int()
+        rc = lib().cgx_batch_add(self.h, mesh.h, ctypes.byref(params), _dp(rho), _dp(u), _dp(p),
+                                 int(nsteps), ctypes.byref(cid))
+        if rc == -2:
+            return None
+        _check(rc)
+        self.ncv[cid.value] = mesh.ncv
+        self._meshes[cid.value] = mesh
+        return cid.value
+
+    def step(self, nsteps):
+        n = ctypes.c_int()
+        _check(lib().cgx_batch_step(self.h, int(nsteps), ctypes.byref(n)))
+        return n.value
+
+    def done(self):
+        n = ctypes.c_int()
+        _check(lib().cgx_batch_done(self.h, None, 0, ctypes.byref(n)))
+        ids = (ctypes.c_int * max(n.value, 1))()
+        _check(lib().cgx_batch_done(self.h, ids, n.value, ctypes.byref(n)))
+        return list(ids)[: n.value]
+
+    def get_state(self, cid):
+        n = self.ncv[cid]
+        rho, u, rhoE = _out(n), _out(n, 3), _out(n)
+        _check(lib().cgx_batch_get_state(self.h, int(cid), _dp(rho), _dp(u), _dp(rhoE)))
+        return rho, u, rhoE
+
+    def time(self, cid):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().cgx_batch_get_time(self.h, int(cid), ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))
+        return t.value, dt.value, st.value
+
+    def remove(self, cid):
+        _check(lib().cgx_batch_remove(self.h, int(cid)))
+        self.ncv.pop(cid, None)
+        self._meshes.pop(cid, None)
+
+    def bytes(self):
+        u, b = ctypes.c_size_t(), ctypes.c_size_t()
+        _check(lib().cgx_batch_bytes(self.h, ctypes.byref(u), ctypes.byref(b)))
+        return u.value, b.value
+
+    def launch_count(self):
+        return int(lib().cgx_batch_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().cgx_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -56,9 +56,6 @@ constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) 
 // ===========================================================================
 // device helpers
 // ===========================================================================
-__device__ __forceinline__ double2 ldg2(const void* p) {
-  return __ldg(reinterpret_cast<const double2*>(p));
-}
 
 // 1/x by Newton-Raphson refinement (two steps, r <- r + r(1 - x r)) of the
 // hardware reciprocal approximation (PTX rcp.approx.ftz.f64); within 1 ulp of
@@ -239,6 +236,30 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 // kernels
 // ===========================================================================
 
+
+// Every step kernel walks a work list of items (kItemCells cells of one case
+// each) with a grid-stride loop, 256 threads per CTA.  A kernel that puts G
+// lanes on a cell covers an item in G rounds of 256/G cells.  Inside the loop
+// `m`, `s` are the item's case mesh and state, `i` the cell, `lane` the
+// lane in the cell's group and `valid` whether the cell exists (items of a
+// case's last cells are partial).
+#define CASE_ARGS \
+  const CaseDev* __restrict__ cases, const Item* __restrict__ items, const int* __restrict__ nitems
+#define ITEM_LOOP_BEGIN(G)                                             \
+  const int n_items_ = *nitems;                                        \
+  for (int w_ = blockIdx.x; w_ < n_items_; w_ += gridDim.x) {          \
+    const Item it_ = items[w_];                                        \
+    const MeshDev m = cases[it_.c].m;                                  \
+    const StateDev s = cases[it_.c].s;                                 \
+    for (int sub_ = 0; sub_ < (G); ++sub_) {                           \
+      const int loc_ = sub_ * (256 / (G)) + int(threadIdx.x) / (G);    \
+      const int i = it_.cell0 + loc_;                                  \
+      const int lane = int(threadIdx.x) & ((G) - 1);                   \
+      const bool valid = loc_ < it_.ncell;
+#define ITEM_LOOP_END \
+  }                   \
+  }
+
 // calcRhsBase, cell-centric, in two passes over each cell's face list, a
 // group of G lanes per cell (lane l takes entries l, l+G, ...; the group's
 // partial sums are combined by a fixed butterfly):
@@ -249,11 +270,8 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 // Every face is evaluated by each of its two cells with the orientation
 // reversed (n -> -n, unit_n -> -unit_n, c kept), which gives the negated flux.
 template <int G>
-__global__ void __launch_bounds__(256, 3) k_rhs_ext(MeshDev m, StateDev s, int stage) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
-  const bool valid = i < m.N;
+__global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
+  ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
   LRec Li;
   if (valid) {
@@ -292,14 +310,12 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(MeshDev m, StateDev s, int s
     for (int c = 0; c < 5; ++c)
       if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
   }
+  ITEM_LOOP_END
 }
 
 template <int G>
-__global__ void __launch_bounds__(256, 2) k_rhs_comp(MeshDev m, StateDev s, int stage) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
-  const bool valid = i < m.N;
+__global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
+  ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
   LRec Li;
   PRec Pi;
@@ -350,6 +366,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp(MeshDev m, StateDev s, int 
     for (int c = 0; c < 5; ++c)
       if (c % G == lane) r[size_t(c) * m.N + i] += acc[c];
   }
+  ITEM_LOOP_END
 }
 
 // packed primitive state of one cell (updateExtendedState); FP64 always,
@@ -383,48 +400,50 @@ __device__ __forceinline__ void write_prim(const Phys& ph, StateDev& s, int i, d
   }
 }
 
-// rk3Step (when nw > 0) fused with the packed-state update of the new state.
-// dt_arg < 0 takes dt from the device control block.
-__global__ void __launch_bounds__(kBlock) k_rk_prim(MeshDev m, StateDev s, Phys ph, int nw, double w0,
-                                                    double w1, double w2, double dt_arg, int writeQ) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m.N) return;
-  double rho = s.rho[i], u0 = s.u0[i], u1 = s.u1[i], u2 = s.u2[i], rhoE = s.rhoE[i];
-  if (nw > 0) {
-    const double dt = (dt_arg < 0.0) ? s.ctl->dt : dt_arg;
-    const double tmp = dt * __ldg(m.inv_vol + i);
-    const size_t N = m.N;
-    double a[5];
+// rk3Step (when nw > 0) fused with the packed-state update of the new state,
+// one thread per cell.  dt_arg < 0 takes each case's dt from its control block.
+__global__ void __launch_bounds__(256) k_rk_prim(CASE_ARGS, int nw, double w0, double w1, double w2,
+                                                 double dt_arg, int writeQ) {
+  ITEM_LOOP_BEGIN(1)
+  (void)lane;
+  if (valid) {
+    const Phys& ph = cases[it_.c].ph;
+    double rho = s.rho[i], u0 = s.u0[i], u1 = s.u1[i], u2 = s.u2[i], rhoE = s.rhoE[i];
+    if (nw > 0) {
+      const double dt = (dt_arg < 0.0) ? s.ctl->dt : dt_arg;
+      const double tmp = dt * __ldg(m.inv_vol + i);
+      const size_t N = m.N;
+      double a[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      double v = w0 * s.rhs[c * N + i];
-      if (nw > 1) v += w1 * s.rhs[(5 + c) * N + i];
-      if (nw > 2) v += w2 * s.rhs[(10 + c) * N + i];
-      a[c] = tmp * v;
+      for (int c = 0; c < 5; ++c) {
+        double v = w0 * s.rhs[c * N + i];
+        if (nw > 1) v += w1 * s.rhs[(5 + c) * N + i];
+        if (nw > 2) v += w2 * s.rhs[(10 + c) * N + i];
+        a[c] = tmp * v;
+      }
+      const double rho_old = rho;
+      rho += a[0];
+      const double inv_rho = 1.0 / rho;
+      u0 = (rho_old * u0 + a[1]) * inv_rho;
+      u1 = (rho_old * u1 + a[2]) * inv_rho;
+      u2 = (rho_old * u2 + a[3]) * inv_rho;
+      rhoE += a[4];
+      s.rho[i] = rho;
+      s.u0[i] = u0;
+      s.u1[i] = u1;
+      s.u2[i] = u2;
+      s.rhoE[i] = rhoE;
     }
-    const double rho_old = rho;
-    rho += a[0];
-    const double inv_rho = 1.0 / rho;
-    u0 = (rho_old * u0 + a[1]) * inv_rho;
-    u1 = (rho_old * u1 + a[2]) * inv_rho;
-    u2 = (rho_old * u2 + a[3]) * inv_rho;
-    rhoE += a[4];
-    s.rho[i] = rho;
-    s.u0[i] = u0;
-    s.u1[i] = u1;
-    s.u2[i] = u2;
-    s.rhoE[i] = rhoE;
+    StateDev sw = s;
+    write_prim(ph, sw, i, rho, u0, u1, u2, rhoE, writeQ != 0);
   }
-  write_prim(ph, s, i, rho, u0, u1, u2, rhoE, writeQ != 0);
+  ITEM_LOOP_END
 }
 
 // _calcCvGradRange over the compact CSR, a group of G lanes per cell.
 template <int G>
-__global__ void __launch_bounds__(256) k_grad(MeshDev m, StateDev s) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
-  const bool valid = i < m.N;
+__global__ void __launch_bounds__(256) k_grad(CASE_ARGS) {
+  ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
   double ui[3] = {0.0, 0.0, 0.0};
   if (valid) {
@@ -455,21 +474,22 @@ __global__ void __launch_bounds__(256) k_grad(MeshDev m, StateDev s) {
     for (int c = 0; c < 9; ++c)
       if (c % G == lane) s.G[i].g[c] = g[c];
   }
+  ITEM_LOOP_END
 }
 
 // Last block of a once-per-step kernel: reduce the per-block CFL maxima and
 // NaN flags (fixed order) and update the control block: time/step advance
 // (mode bit 0) and the next dt from setDt's formula (mode bit 1).
 // Called by all 256 threads of that block.
-__device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode) {
+__device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, int nparts) {
   constexpr int kThreads = 256;
   __shared__ double fin_cfl[kThreads];
   __shared__ int fin_nan[kThreads];
   double mx = 0.0;
   int anynan = 0;
-  for (int bb = threadIdx.x; bb < gridDim.x; bb += blockDim.x) {
+  for (int bb = threadIdx.x; bb < nparts; bb += blockDim.x) {
     mx = fmax(mx, ((volatile double*)s.red)[bb]);
-    anynan |= (((volatile double*)s.red)[gridDim.x + bb] != 0.0);
+    anynan |= (((volatile double*)s.red)[nparts + bb] != 0.0);
   }
   fin_cfl[threadIdx.x] = mx;
   fin_nan[threadIdx.x] = anynan;
@@ -510,17 +530,20 @@ __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode) {
 // lanes per cell for the face loops.
 // mode bit 0: advance time/step by the dt just used; bit 1: set dt from CFL.
 template <int G>
-__global__ void __launch_bounds__(256) k_step_end(MeshDev m, StateDev s, Phys ph, int mode) {
-  constexpr int kThreads = 256;
-  constexpr int kCells = kThreads / G;
+__global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
+  constexpr int kCells = 256 / G;
   __shared__ double sh_cfl[kCells];
   __shared__ int sh_nan[kCells];
   __shared__ bool am_last;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
   const int cl = threadIdx.x / G;
-  const bool valid = i < m.N;
+  double t_cfl = 0.0;  // per-thread running max / flag over the item's rounds
+  int t_nan = 0;
+  ITEM_LOOP_BEGIN(G)
+  const Phys& ph = cases[it_.c].ph;
+  if (sub_ == 0) {
+    t_cfl = 0.0;
+    t_nan = 0;
+  }
   long long b = 0, e = 0, ec = 0;
   LRec Li;
   double2 qa = make_double2(0.0, 0.0), qb = make_double2(0.0, 0.0);
@@ -620,29 +643,39 @@ __global__ void __launch_bounds__(256) k_step_end(MeshDev m, StateDev s, Phys ph
     nan = (rho != rho) || (Li.p != Li.p) || (T != T);
     cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
   }
-  // ---- block reductions, last block finalises the control block
-  if (lane == 0) {
-    sh_cfl[cl] = valid ? cfl : 0.0;
-    sh_nan[cl] = nan;
+  if (lane == 0 && valid) {
+    t_cfl = fmax(t_cfl, cfl);
+    t_nan |= nan;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mx = 0.0;
-    int an = 0;
-    for (int c = 0; c < kCells; ++c) {
-      mx = fmax(mx, sh_cfl[c]);
-      an |= sh_nan[c];
+  if (sub_ == G - 1) {
+    // ---- item reduction; the last item of a case finalises its control block
+    if (lane == 0) {
+      sh_cfl[cl] = t_cfl;
+      sh_nan[cl] = t_nan;
     }
-    s.red[blockIdx.x] = mx;
-    s.red[gridDim.x + blockIdx.x] = double(an);
-    __threadfence();
-    const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
-    am_last = (done == gridDim.x - 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mx = 0.0;
+      int an = 0;
+      for (int c = 0; c < kCells; ++c) {
+        mx = fmax(mx, sh_cfl[c]);
+        an |= sh_nan[c];
+      }
+      const int np = cases[it_.c].nitems;
+      s.red[it_.idx] = mx;
+      s.red[np + it_.idx] = double(an);
+      __threadfence();
+      const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
+      am_last = (done == unsigned(np) - 1u);
+    }
+    __syncthreads();
+    if (am_last) {
+      __threadfence();
+      finalize_ctl(s, ph, mode, cases[it_.c].nitems);
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  finalize_ctl(s, ph, mode);
+  ITEM_LOOP_END
 }
 
 #include "cgx_mixed.cuh"
@@ -900,15 +933,35 @@ struct Tune {
   int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4;
 };
 
+// What a launch needs: the case table and work list on the device, the grid,
+// the stream, the lane counts and the precision.  A single solver runs one
+// case; a batch runs all of its resident cases through the same kernels.
+struct Runner {
+  const CaseDev* cases = nullptr;
+  const Item* items = nullptr;
+  const int* nitems = nullptr;  // device: number of items in the list
+  int grid = 0;                 // CTAs per launch (items are walked grid-stride)
+  cudaStream_t stream = nullptr;
+  Tune tune;
+  cgx_precision prec = CGX_FP64;
+  std::atomic<long long>* launches = nullptr;
+};
+
 struct cgx_solver {
   cgx_mesh* mesh = nullptr;
-  Tune tune;
   cgx_params prm{};
   cgx_precision prec = CGX_FP64;
   Phys ph{};
   cudaStream_t stream = nullptr;
   StateDev sd{};
-  double* d_stage = nullptr;  // [5N] staging in reference order
+  CaseDev* d_case = nullptr;  // this solver's one-entry case table
+  CaseDev hcase{};            // host copy (batches place it in their table)
+  size_t bytes = 0;           // device bytes held by the solver
+  Item* d_items = nullptr;
+  int* d_nitems = nullptr;
+  int nitems = 0;
+  Runner run;
+  double* d_stage = nullptr;  // [9N] staging in reference order
   double* d_part = nullptr;   // totals partials
   double* d_store[2] = {nullptr, nullptr};
   int store_step[2] = {0, 0};
@@ -916,7 +969,6 @@ struct cgx_solver {
   bool have_store = false;
   std::vector<void*> allocs;
   int nblocks = 0;
-  int nblocks_end = 0;
   bool state_set = false;
   bool inited = false;
   cudaGraphExec_t graph = nullptr;
@@ -925,172 +977,139 @@ struct cgx_solver {
 
 namespace {
 
-int launch_check(cgx_solver* s, int nk) {
-  s->launches += nk;
+int launch_check(const Runner& R, int nk) {
+  if (R.launches) *R.launches += nk;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(CGX_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return CGX_OK;
 }
 
-int enqueue_prim(cgx_solver* s, int nw, const double* w, double dt_arg, bool writeQ) {
-  const int nb = s->nblocks;
-  k_rk_prim<<<nb, kBlock, 0, s->stream>>>(s->mesh->md, s->sd, s->ph, nw, w ? w[0] : 0.0,
-                                          w ? w[1] : 0.0, w ? w[2] : 0.0, dt_arg, writeQ ? 1 : 0);
-  return launch_check(s, 1);
+#define RARGS R.cases, R.items, R.nitems
+
+int enqueue_prim(const Runner& R, int nw, const double* w, double dt_arg, bool writeQ) {
+  k_rk_prim<<<R.grid, 256, 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0, w ? w[2] : 0.0, dt_arg,
+                                          writeQ ? 1 : 0);
+  return launch_check(R, 1);
 }
 
 // Lanes per cell of the group-per-cell kernels, chosen per mesh-size bucket
 // by autotune() (timed candidates, cached process-wide).
-inline int groups_grid(int N, int G) { return int((static_cast<long long>(N) * G + 255) / 256); }
-
-template <int G>
-void launch_grad_g(cgx_solver* s) {
-  k_grad<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd);
+template <int G, bool MIX>
+void launch_grad(const Runner& R) {
+  if (MIX)
+    k_grad_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS);
+  else
+    k_grad<G><<<R.grid, 256, 0, R.stream>>>(RARGS);
 }
-template <int G>
-void launch_ext_g(cgx_solver* s, int st) {
-  k_rhs_ext<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st);
+template <int G, bool MIX>
+void launch_ext(const Runner& R, int st) {
+  if (MIX)
+    k_rhs_ext_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
+  else
+    k_rhs_ext<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
 }
-template <int G>
-void launch_comp_g(cgx_solver* s, int st) {
-  k_rhs_comp<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st);
+template <int G, bool MIX>
+void launch_comp(const Runner& R, int st) {
+  if (MIX)
+    k_rhs_comp_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
+  else
+    k_rhs_comp<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
 }
-template <int G>
-void launch_end_g(cgx_solver* s, int mode) {
-  k_step_end<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, s->ph, mode);
-}
-
-int enqueue_grad_g(cgx_solver* s, int G) {
-  switch (G) {
-    case 1: launch_grad_g<1>(s); break;
-    case 2: launch_grad_g<2>(s); break;
-    case 4: launch_grad_g<4>(s); break;
-    case 8: launch_grad_g<8>(s); break;
-    default: launch_grad_g<16>(s); break;
-  }
-  return launch_check(s, 1);
-}
-int enqueue_ext_g(cgx_solver* s, int G, int st) {
-  switch (G) {
-    case 4: launch_ext_g<4>(s, st); break;
-    case 8: launch_ext_g<8>(s, st); break;
-    case 32: launch_ext_g<32>(s, st); break;
-    default: launch_ext_g<16>(s, st); break;
-  }
-  return launch_check(s, 1);
-}
-int enqueue_comp_g(cgx_solver* s, int G, int st) {
-  switch (G) {
-    case 2: launch_comp_g<2>(s, st); break;
-    case 4: launch_comp_g<4>(s, st); break;
-    case 8: launch_comp_g<8>(s, st); break;
-    default: launch_comp_g<16>(s, st); break;
-  }
-  return launch_check(s, 1);
-}
-int enqueue_end_g(cgx_solver* s, int G, int mode) {
-  switch (G) {
-    case 1: launch_end_g<1>(s, mode); break;
-    case 4: launch_end_g<4>(s, mode); break;
-    case 8: launch_end_g<8>(s, mode); break;
-    default: launch_end_g<16>(s, mode); break;
-  }
-  return launch_check(s, 1);
+template <int G, bool MIX>
+void launch_end(const Runner& R, int mode) {
+  if (MIX)
+    k_step_end_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS, mode);
+  else
+    k_step_end<G><<<R.grid, 256, 0, R.stream>>>(RARGS, mode);
 }
 
-// mixed-precision variants
-template <int G>
-void launch_grad_f(cgx_solver* s) {
-  k_grad_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd);
-}
-template <int G>
-void launch_ext_f(cgx_solver* s, int st) {
-  k_rhs_ext_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st, s->ph.h_ref);
-}
-template <int G>
-void launch_comp_f(cgx_solver* s, int st) {
-  k_rhs_comp_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, st, s->ph.h_ref,
-                                                                      float(s->ph.p_ref));
-}
-template <int G>
-void launch_end_f(cgx_solver* s, int mode) {
-  k_step_end_f<G><<<groups_grid(s->mesh->N, G), 256, 0, s->stream>>>(s->mesh->md, s->sd, s->ph, mode);
-}
-int enqueue_grad_fg(cgx_solver* s, int G) {
+template <bool MIX>
+void grad_g(const Runner& R, int G) {
   switch (G) {
-    case 1: launch_grad_f<1>(s); break;
-    case 2: launch_grad_f<2>(s); break;
-    case 4: launch_grad_f<4>(s); break;
-    case 8: launch_grad_f<8>(s); break;
-    default: launch_grad_f<16>(s); break;
+    case 1: launch_grad<1, MIX>(R); break;
+    case 2: launch_grad<2, MIX>(R); break;
+    case 4: launch_grad<4, MIX>(R); break;
+    case 8: launch_grad<8, MIX>(R); break;
+    default: launch_grad<16, MIX>(R); break;
   }
-  return launch_check(s, 1);
 }
-int enqueue_ext_fg(cgx_solver* s, int G, int st) {
+template <bool MIX>
+void ext_g(const Runner& R, int G, int st) {
   switch (G) {
-    case 4: launch_ext_f<4>(s, st); break;
-    case 8: launch_ext_f<8>(s, st); break;
-    case 32: launch_ext_f<32>(s, st); break;
-    default: launch_ext_f<16>(s, st); break;
+    case 4: launch_ext<4, MIX>(R, st); break;
+    case 8: launch_ext<8, MIX>(R, st); break;
+    case 32: launch_ext<32, MIX>(R, st); break;
+    default: launch_ext<16, MIX>(R, st); break;
   }
-  return launch_check(s, 1);
 }
-int enqueue_comp_fg(cgx_solver* s, int G, int st) {
+template <bool MIX>
+void comp_g(const Runner& R, int G, int st) {
   switch (G) {
-    case 2: launch_comp_f<2>(s, st); break;
-    case 4: launch_comp_f<4>(s, st); break;
-    case 8: launch_comp_f<8>(s, st); break;
-    default: launch_comp_f<16>(s, st); break;
+    case 2: launch_comp<2, MIX>(R, st); break;
+    case 4: launch_comp<4, MIX>(R, st); break;
+    case 8: launch_comp<8, MIX>(R, st); break;
+    default: launch_comp<16, MIX>(R, st); break;
   }
-  return launch_check(s, 1);
 }
-int enqueue_end_fg(cgx_solver* s, int G, int mode) {
+template <bool MIX>
+void end_g(const Runner& R, int G, int mode) {
   switch (G) {
-    case 1: launch_end_f<1>(s, mode); break;
-    case 4: launch_end_f<4>(s, mode); break;
-    case 8: launch_end_f<8>(s, mode); break;
-    default: launch_end_f<16>(s, mode); break;
+    case 1: launch_end<1, MIX>(R, mode); break;
+    case 4: launch_end<4, MIX>(R, mode); break;
+    case 8: launch_end<8, MIX>(R, mode); break;
+    default: launch_end<16, MIX>(R, mode); break;
   }
-  return launch_check(s, 1);
 }
 
-inline bool mixed(const cgx_solver* s) { return s->prec == CGX_MIXED; }
+inline bool is_mixed(const Runner& R) { return R.prec == CGX_MIXED; }
 
-int grad_var(cgx_solver* s, int G) { return mixed(s) ? enqueue_grad_fg(s, G) : enqueue_grad_g(s, G); }
-int ext_var(cgx_solver* s, int G, int st) { return mixed(s) ? enqueue_ext_fg(s, G, st) : enqueue_ext_g(s, G, st); }
-int comp_var(cgx_solver* s, int G, int st) { return mixed(s) ? enqueue_comp_fg(s, G, st) : enqueue_comp_g(s, G, st); }
-int end_var(cgx_solver* s, int G, int mode) { return mixed(s) ? enqueue_end_fg(s, G, mode) : enqueue_end_g(s, G, mode); }
+int grad_var(const Runner& R, int G) {
+  is_mixed(R) ? grad_g<true>(R, G) : grad_g<false>(R, G);
+  return launch_check(R, 1);
+}
+int ext_var(const Runner& R, int G, int st) {
+  is_mixed(R) ? ext_g<true>(R, G, st) : ext_g<false>(R, G, st);
+  return launch_check(R, 1);
+}
+int comp_var(const Runner& R, int G, int st) {
+  is_mixed(R) ? comp_g<true>(R, G, st) : comp_g<false>(R, G, st);
+  return launch_check(R, 1);
+}
+int end_var(const Runner& R, int G, int mode) {
+  is_mixed(R) ? end_g<true>(R, G, mode) : end_g<false>(R, G, mode);
+  return launch_check(R, 1);
+}
 
-int enqueue_grad(cgx_solver* s) { return grad_var(s, s->tune.g_grad); }
+int enqueue_grad(const Runner& R) { return grad_var(R, R.tune.g_grad); }
 
-int enqueue_rhs(cgx_solver* s, int stage0) {
-  int rc = ext_var(s, s->tune.g_ext, stage0);
+int enqueue_rhs(const Runner& R, int stage0) {
+  int rc = ext_var(R, R.tune.g_ext, stage0);
   if (rc) return rc;
-  return comp_var(s, s->tune.g_comp, stage0);
+  return comp_var(R, R.tune.g_comp, stage0);
 }
 
-int enqueue_step_end(cgx_solver* s, int mode) { return end_var(s, s->tune.g_end, mode); }
+int enqueue_step_end(const Runner& R, int mode) { return end_var(R, R.tune.g_end, mode); }
 
 std::mutex g_tune_mu;
 std::map<int, Tune> g_tune_cache;
 
-int tune_bucket(const cgx_solver* s) {
+int tune_bucket(long long ncells, cgx_precision prec) {
   int b = 0;
-  for (long long n = s->mesh->N; n > 1; n >>= 1) ++b;
-  return b * 4 + int(s->prec);
+  for (long long n = ncells; n > 1; n >>= 1) ++b;
+  return b * 4 + int(prec);
 }
 
-// Time each candidate lane count of each kernel on this solver's mesh and
-// keep the fastest; results are cached per mesh-size bucket (log2 of the
-// cell count) and precision.  All candidates compute the same values (only
-// the order of the per-cell sums changes), and none changes the state.
-int autotune(cgx_solver* s) {
-  const int bucket = tune_bucket(s);
+// Time each candidate lane count of each kernel on the runner's cases and
+// keep the fastest; results are cached per size bucket (log2 of the cell
+// count) and precision.  All candidates compute the same values (only the
+// order of the per-cell sums changes), and none changes the state.
+int autotune(Runner& R, long long ncells) {
+  const int bucket = tune_bucket(ncells, R.prec);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(bucket);
     if (it != g_tune_cache.end()) {
-      s->tune = it->second;
+      R.tune = it->second;
       return CGX_OK;
     }
   }
@@ -1100,14 +1119,14 @@ int autotune(cgx_solver* s) {
   auto time_it = [&](auto&& fn, float* ms) -> int {
     int rc = fn();  // warm-up
     if (rc) return rc;
-    CK(cudaEventRecord(e0, s->stream));
+    CK(cudaEventRecord(e0, R.stream));
     for (int r = 0; r < 3 && rc == CGX_OK; ++r) rc = fn();
-    CK(cudaEventRecord(e1, s->stream));
+    CK(cudaEventRecord(e1, R.stream));
     CK(cudaEventSynchronize(e1));
     CK(cudaEventElapsedTime(ms, e0, e1));
     return rc;
   };
-  Tune best = s->tune;
+  Tune best = R.tune;
   float bt;
   int rc = CGX_OK;
   const int ext_c[] = {4, 8, 16, 32}, comp_c[] = {2, 4, 8, 16}, grad_c[] = {1, 2, 4, 8, 16},
@@ -1115,34 +1134,34 @@ int autotune(cgx_solver* s) {
   bt = 1e30f;
   for (int G : ext_c) {
     float ms;
-    if ((rc = time_it([&] { return ext_var(s, G, 0); }, &ms))) break;
+    if ((rc = time_it([&] { return ext_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_ext = G; }
   }
   bt = 1e30f;
   for (int G : comp_c) {
     if (rc) break;
     float ms;
-    if ((rc = time_it([&] { return comp_var(s, G, 0); }, &ms))) break;
+    if ((rc = time_it([&] { return comp_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_comp = G; }
   }
   bt = 1e30f;
   for (int G : grad_c) {
     if (rc) break;
     float ms;
-    if ((rc = time_it([&] { return grad_var(s, G); }, &ms))) break;
+    if ((rc = time_it([&] { return grad_var(R, G); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_grad = G; }
   }
   bt = 1e30f;
   for (int G : end_c) {
     if (rc) break;
     float ms;
-    if ((rc = time_it([&] { return end_var(s, G, 0); }, &ms))) break;
+    if ((rc = time_it([&] { return end_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_end = G; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  s->tune = best;
+  R.tune = best;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[bucket] = best;
   return CGX_OK;
@@ -1152,14 +1171,14 @@ int autotune(cgx_solver* s) {
 const double kRkW[3][3] = {{1.0, 0.0, 0.0}, {-0.75, 0.25, 0.0}, {-1.0 / 12.0, -1.0 / 12.0, 8.0 / 12.0}};
 
 // one full step: 3 x (rhs, rk+prim, grad) + step_end(advance time, next dt)
-int enqueue_step(cgx_solver* s) {
+int enqueue_step(const Runner& R) {
   int rc;
   for (int st = 0; st < 3; ++st) {
-    if ((rc = enqueue_rhs(s, st))) return rc;
-    if ((rc = enqueue_prim(s, st + 1, kRkW[st], -1.0, st == 2))) return rc;
-    if ((rc = enqueue_grad(s))) return rc;
+    if ((rc = enqueue_rhs(R, st))) return rc;
+    if ((rc = enqueue_prim(R, st + 1, kRkW[st], -1.0, st == 2))) return rc;
+    if ((rc = enqueue_grad(R))) return rc;
   }
-  return enqueue_step_end(s, 3);
+  return enqueue_step_end(R, 3);
 }
 
 int read_ctl(cgx_solver* s, Ctl* c) {
@@ -1214,9 +1233,9 @@ int restore_state(cgx_solver* s) {
   s->prm.dt_data[0] *= 0.8;
   c.dt_data0 = s->prm.dt_data[0];
   CK(cudaMemcpyAsync(s->sd.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s->stream));
-  if ((rc = enqueue_prim(s, 0, nullptr, 0.0, true))) return rc;
-  if ((rc = enqueue_grad(s))) return rc;
-  if ((rc = enqueue_step_end(s, 2))) return rc;
+  if ((rc = enqueue_prim(s->run, 0, nullptr, 0.0, true))) return rc;
+  if ((rc = enqueue_grad(s->run))) return rc;
+  if ((rc = enqueue_step_end(s->run, 2))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
@@ -1591,7 +1610,7 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   ph.h_ref = ph.R * p->gamma / (p->gamma - 1.0) * p->T_ref;
   const size_t N = m->N;
   s->nblocks = int((N + kBlock - 1) / kBlock);
-  s->nblocks_end = int((static_cast<long long>(N) * 16 + 255) / 256);  // largest G candidate
+  s->nitems = int((N + kItemCells - 1) / kItemCells);
   auto bail = [&](int rc) {
     for (void* q : s->allocs) cudaFree(q);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1661,7 +1680,10 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     AL(sd.Q, N);
   }
   AL(sd.ctl, 1);
-  AL(sd.red, 2 * size_t(std::max(s->nblocks, s->nblocks_end)));
+  AL(sd.red, 2 * size_t(s->nitems));
+  AL(s->d_case, 1);
+  AL(s->d_items, s->nitems);
+  AL(s->d_nitems, 1);
   AL(s->d_stage, 9 * N);
   AL(s->d_part, 5 * size_t(s->nblocks) + 5);
   AL(s->d_store[0], 5 * N);
@@ -1676,6 +1698,31 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
               cudaMemsetAsync(sd.G, 0, N * sizeof(GRec), s->stream) == cudaSuccess));
   if (!zero_ok)
     return bail(fail(CGX_E_CUDA, "cudaMemset failed"));
+  {  // work list (one item per kItemCells cells) and the one-entry case table
+    std::vector<Item> items(s->nitems);
+    for (int k = 0; k < s->nitems; ++k)
+      items[k] = Item{0, k * kItemCells, int(std::min<size_t>(kItemCells, N - size_t(k) * kItemCells)), k};
+    CaseDev cd{};
+    cd.m = m->md;
+    cd.s = sd;
+    cd.ph = ph;
+    cd.nitems = s->nitems;
+    s->hcase = cd;
+    if (cudaMemcpyAsync(s->d_items, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice,
+                        s->stream) != cudaSuccess ||
+        cudaMemcpyAsync(s->d_case, &cd, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaMemcpyAsync(s->d_nitems, &s->nitems, sizeof(int), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+      return bail(fail(CGX_E_CUDA, "work list upload failed"));
+    Runner& R = s->run;
+    R.cases = s->d_case;
+    R.items = s->d_items;
+    R.nitems = s->d_nitems;
+    R.grid = s->nitems;
+    R.stream = s->stream;
+    R.prec = prec;
+    R.launches = &s->launches;
+  }
+  s->bytes = bytes;
   Ctl c{};
   c.dt_data0 = p->dt_data[0];
   c.dt = (p->dt_mode == CGX_DT_CONST) ? p->dt_data[0] : 0.0;
@@ -1712,7 +1759,7 @@ extern "C" int cgx_set_state(cgx_solver* s, const double* rho, const double* u, 
   if (rc) return rc;
   const int N = s->mesh->N;
   k_state_in<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd);
-  if ((rc = launch_check(s, 1))) return rc;
+  if ((rc = launch_check(s->run, 1))) return rc;
   s->state_set = true;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -1725,7 +1772,7 @@ extern "C" int cgx_set_state_primitive(cgx_solver* s, const double* rho, const d
   if (rc) return rc;
   const int N = s->mesh->N;
   k_state_in_prim<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, s->prm.gamma);
-  if ((rc = launch_check(s, 1))) return rc;
+  if ((rc = launch_check(s->run, 1))) return rc;
   s->state_set = true;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -1736,7 +1783,7 @@ extern "C" int cgx_get_state(cgx_solver* s, double* rho, double* u, double* rhoE
   CK(cudaSetDevice(s->mesh->device));
   const int N = s->mesh->N;
   k_state_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd);
-  int rc = launch_check(s, 1);
+  int rc = launch_check(s->run, 1);
   if (rc) return rc;
   if (rho) CK(cudaMemcpyAsync(rho, s->d_stage, N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   if (u) CK(cudaMemcpyAsync(u, s->d_stage + N, 3 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -1750,8 +1797,8 @@ extern "C" int cgx_update_primitive(cgx_solver* s) {
   if (!s->state_set) return fail(CGX_E_STATE, "state not set");
   CK(cudaSetDevice(s->mesh->device));
   int rc;
-  if ((rc = enqueue_prim(s, 0, nullptr, 0.0, true))) return rc;
-  if ((rc = enqueue_grad(s))) return rc;
+  if ((rc = enqueue_prim(s->run, 0, nullptr, 0.0, true))) return rc;
+  if ((rc = enqueue_grad(s->run))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
@@ -1760,7 +1807,7 @@ extern "C" int cgx_calc_sgs_props(cgx_solver* s) {
   if (!s) return fail(CGX_E_ARG, "null solver");
   if (!s->state_set) return fail(CGX_E_STATE, "state not set");
   CK(cudaSetDevice(s->mesh->device));
-  int rc = enqueue_step_end(s, 2);
+  int rc = enqueue_step_end(s->run, 2);
   if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -1770,7 +1817,10 @@ extern "C" int cgx_init_complete(cgx_solver* s) {
   int rc = cgx_update_primitive(s);
   if (rc) return rc;
   if ((rc = cgx_calc_sgs_props(s))) return rc;
-  if ((rc = autotune(s))) return rc;
+  if ((rc = autotune(s->run, s->mesh->N))) return rc;
+  // recompute with the tuned lane counts so that the initial packed state,
+  // gradient and properties do not depend on whether tuning ran or was cached
+  if ((rc = cgx_update_primitive(s))) return rc;
   if ((rc = cgx_calc_sgs_props(s))) return rc;
   s->inited = true;
   s->have_store = false;
@@ -1783,12 +1833,12 @@ extern "C" int cgx_calc_rhs(cgx_solver* s, double* rhs_out, double time, int rk_
   if (rk_stage < 1 || rk_stage > 3) return fail(CGX_E_ARG, "rk_stage must be 1..3");
   if (!s->inited) return fail(CGX_E_STATE, "cgx_init_complete not called");
   CK(cudaSetDevice(s->mesh->device));
-  int rc = enqueue_rhs(s, rk_stage - 1);
+  int rc = enqueue_rhs(s->run, rk_stage - 1);
   if (rc) return rc;
   if (rhs_out) {
     const int N = s->mesh->N;
     k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, 0, rk_stage - 1, s->ph.R, s->ph.p_ref);
-    if ((rc = launch_check(s, 1))) return rc;
+    if ((rc = launch_check(s->run, 1))) return rc;
     CK(cudaMemcpyAsync(rhs_out, s->d_stage, 5 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   }
   CK(cudaStreamSynchronize(s->stream));
@@ -1802,7 +1852,7 @@ extern "C" int cgx_rk3_step(cgx_solver* s, const double w[3], double dt, int rk_
   for (int k = rk_stage; k < 3; ++k)
     if (w[k] != 0.0) return fail(CGX_E_ARG, "rk weight of a later stage must be zero");
   CK(cudaSetDevice(s->mesh->device));
-  int rc = enqueue_prim(s, rk_stage, w, dt, true);
+  int rc = enqueue_prim(s->run, rk_stage, w, dt, true);
   if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -1814,7 +1864,7 @@ extern "C" int cgx_calc_cfl(cgx_solver* s, double dt, double* cfl_max, double* c
   CK(cudaSetDevice(s->mesh->device));
   const int N = s->mesh->N;
   k_cfl_cells<<<(N + kBlock - 1) / kBlock, kBlock, 0, s->stream>>>(s->mesh->md, s->sd, s->mesh->d_perm, dt, s->d_stage);
-  int rc = launch_check(s, 1);
+  int rc = launch_check(s->run, 1);
   if (rc) return rc;
   std::vector<double> h(N);
   CK(cudaMemcpyAsync(h.data(), s->d_stage, N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -1830,7 +1880,7 @@ extern "C" int cgx_advance_solution(cgx_solver* s) {
   if (!s) return fail(CGX_E_ARG, "null solver");
   if (!s->inited) return fail(CGX_E_STATE, "cgx_init_complete not called");
   CK(cudaSetDevice(s->mesh->device));
-  int rc = enqueue_step(s);
+  int rc = enqueue_step(s->run);
   if (rc) return rc;
   bool nan = false;
   if ((rc = check_nan(s, &nan))) return rc;
@@ -1877,7 +1927,7 @@ static int ensure_graph(cgx_solver* s) {
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   const long long before = s->launches.load();
-  int rc = enqueue_step(s);
+  int rc = enqueue_step(s->run);
   cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
   s->launches = before;  // capturing launches nothing
   if (rc) return rc;
@@ -1929,10 +1979,10 @@ extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[4]) {
   for (int which = 0; which < 4 && rc == CGX_OK; ++which) {
     CK(cudaEventRecord(e0, s->stream));
     for (int r = 0; r < reps && rc == CGX_OK; ++r) {
-      if (which == 0) rc = enqueue_rhs(s, 0);
-      else if (which == 1) rc = enqueue_prim(s, 3, kRkW[2], 0.0, true);
-      else if (which == 2) rc = enqueue_grad(s);
-      else rc = enqueue_step_end(s, 0);
+      if (which == 0) rc = enqueue_rhs(s->run, 0);
+      else if (which == 1) rc = enqueue_prim(s->run, 3, kRkW[2], 0.0, true);
+      else if (which == 2) rc = enqueue_grad(s->run);
+      else rc = enqueue_step_end(s->run, 0);
     }
     CK(cudaEventRecord(e1, s->stream));
     CK(cudaEventSynchronize(e1));
@@ -1963,7 +2013,7 @@ extern "C" int cgx_totals(cgx_solver* s, double out[5]) {
   const int nb = s->nblocks;
   k_totals_partial<<<nb, kBlock, 0, s->stream>>>(s->mesh->md, s->sd, s->d_part);
   k_totals_final<<<1, 32, 0, s->stream>>>(s->d_part, nb, s->d_part + 5 * size_t(nb));
-  int rc = launch_check(s, 2);
+  int rc = launch_check(s->run, 2);
   if (rc) return rc;
   CK(cudaMemcpyAsync(out, s->d_part + 5 * size_t(nb), 5 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -1974,7 +2024,7 @@ static int diag(cgx_solver* s, int what, int k, double* out) {
   CK(cudaSetDevice(s->mesh->device));
   const int N = s->mesh->N;
   k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, what, 0, s->ph.R, s->ph.p_ref);
-  int rc = launch_check(s, 1);
+  int rc = launch_check(s->run, 1);
   if (rc) return rc;
   CK(cudaMemcpyAsync(out, s->d_stage, size_t(k) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -2014,11 +2064,368 @@ extern "C" int cgx_synchronize(cgx_solver* s) {
 
 extern "C" int cgx_get_tuning(const cgx_solver* s, int out[4]) {
   if (!s || !out) return fail(CGX_E_ARG, "null argument");
-  out[0] = s->tune.g_ext;
-  out[1] = s->tune.g_comp;
-  out[2] = s->tune.g_grad;
-  out[3] = s->tune.g_end;
+  out[0] = s->run.tune.g_ext;
+  out[1] = s->run.tune.g_comp;
+  out[2] = s->run.tune.g_grad;
+  out[3] = s->run.tune.g_end;
   return CGX_OK;
 }
 
 extern "C" long long cgx_launch_count(const cgx_solver* s) { return s ? s->launches.load() : 0; }
+
+// ===========================================================================
+// batched / served form
+// ===========================================================================
+namespace {
+
+// device bytes a solver of N cells allocates (cgx_solver_create)
+size_t solver_bytes(long long N, cgx_precision prec) {
+  const long long nitems = (N + kItemCells - 1) / kItemCells;
+  const long long nblocks = (N + kBlock - 1) / kBlock;
+  size_t rec = (prec == CGX_MIXED) ? sizeof(LRecF) + sizeof(PRecF) + sizeof(GRecF) + sizeof(QRecF)
+                                   : sizeof(LRec) + sizeof(PRec) + sizeof(GRec) + sizeof(QRec);
+  return size_t(N) * (5 + 15 + 9 + 10) * sizeof(double) + size_t(N) * rec + sizeof(Ctl) +
+         size_t(2 * nitems) * sizeof(double) + sizeof(CaseDev) + size_t(nitems) * sizeof(Item) +
+         sizeof(int) + size_t(5 * nblocks + 5) * sizeof(double) + 4096;
+}
+
+size_t mesh32_bytes(const cgx_mesh* m) {
+  return size_t(m->nef) * sizeof(EFRecF) + size_t(std::max<long long>(m->ncf, 1)) * sizeof(CFRecF) +
+         size_t(m->nc_dir) * 3 * sizeof(float);
+}
+
+}  // namespace
+
+struct BatchCase {
+  int id = -1;
+  cgx_solver* s = nullptr;
+  cgx_mesh* mesh = nullptr;
+  int target = 0;
+  int steps = 0;  // steps taken (host count, equal to the case's device step count)
+  bool finished = false;
+  size_t bytes = 0;
+};
+
+struct cgx_batch {
+  int device = 0;
+  cgx_precision prec = CGX_FP64;
+  int max_cases = 0;
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<BatchCase> slots;  // slot index = position in the case table
+  std::map<int, int> slot_of;    // case id -> slot
+  int next_id = 0;
+  std::map<cgx_mesh*, int> mesh_refs;
+  CaseDev* d_cases = nullptr;
+  Item* d_items = nullptr;
+  int item_cap = 0;
+  int* d_nitems = nullptr;
+  Item* h_items = nullptr;  // pinned staging for the work list
+  int* h_nitems = nullptr;
+  cudaEvent_t staged = nullptr;
+  bool dirty = true;
+  int nitems = 0;
+  long long active_cells = 0;
+  int tuned_bucket = -1;
+  Runner run;
+  cudaGraphExec_t graph = nullptr;
+  std::atomic<long long> launches{0};
+  int grid = 0;
+};
+
+namespace {
+
+void batch_free_graph(cgx_batch* b) {
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+}
+
+// Rebuild the packed work list of the active cases and stage it to the
+// device (stream-ordered: the next replay sees it).
+int batch_rebuild(cgx_batch* b) {
+  std::vector<Item> items;
+  long long cells = 0;
+  for (size_t k = 0; k < b->slots.size(); ++k) {
+    const BatchCase& c = b->slots[k];
+    if (!c.s || c.finished) continue;
+    const int N = c.s->mesh->N;
+    cells += N;
+    for (int it = 0; it < c.s->nitems; ++it)
+      items.push_back(Item{int(k), it * kItemCells, std::min(kItemCells, N - it * kItemCells), it});
+  }
+  if (int(items.size()) > b->item_cap) {
+    int cap = std::max(1024, b->item_cap);
+    while (cap < int(items.size())) cap *= 2;
+    CK(cudaStreamSynchronize(b->stream));
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->h_items) cudaFreeHost(b->h_items);
+    b->d_items = nullptr;
+    b->h_items = nullptr;
+    CK(cudaMalloc(&b->d_items, size_t(cap) * sizeof(Item)));
+    CK(cudaMallocHost(&b->h_items, size_t(cap) * sizeof(Item)));
+    b->item_cap = cap;
+    batch_free_graph(b);  // the graph holds the old work-list pointer
+  }
+  CK(cudaEventSynchronize(b->staged));  // previous staging copy done
+  std::copy(items.begin(), items.end(), b->h_items);
+  *b->h_nitems = int(items.size());
+  if (!items.empty())
+    CK(cudaMemcpyAsync(b->d_items, b->h_items, items.size() * sizeof(Item), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_nitems, b->h_nitems, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaEventRecord(b->staged, b->stream));
+  b->nitems = int(items.size());
+  b->active_cells = cells;
+  b->run.items = b->d_items;
+  b->dirty = false;
+  return CGX_OK;
+}
+
+int batch_check_nan(cgx_batch* b) {
+  CK(cudaStreamSynchronize(b->stream));
+  for (BatchCase& c : b->slots) {
+    if (!c.s || c.finished) continue;
+    Ctl h;
+    CK(cudaMemcpy(&h, c.s->sd.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+    if (h.nan) {
+      // checkForNans -> restoreData for this case only; it repeats the lost steps
+      int rc = restore_state(c.s);
+      if (rc) return rc;
+      CK(cudaMemcpy(&h, c.s->sd.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+      c.steps = h.step;
+    }
+  }
+  return CGX_OK;
+}
+
+}  // namespace
+
+extern "C" int cgx_batch_create(int device, cgx_precision prec, int max_cases, size_t hbm_budget_bytes,
+                                cgx_batch** out) {
+  if (!out || max_cases < 1 || (prec != CGX_FP64 && prec != CGX_MIXED))
+    return fail(CGX_E_ARG, "cgx_batch_create: invalid argument");
+  *out = nullptr;
+  CK(cudaSetDevice(device));
+  cgx_batch* b = new cgx_batch();
+  b->device = device;
+  b->prec = prec;
+  b->max_cases = max_cases;
+  b->budget = hbm_budget_bytes;
+  b->slots.resize(max_cases);
+  auto bail = [&](int rc) {
+    if (b->d_cases) cudaFree(b->d_cases);
+    if (b->d_nitems) cudaFree(b->d_nitems);
+    if (b->h_nitems) cudaFreeHost(b->h_nitems);
+    if (b->staged) cudaEventDestroy(b->staged);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->d_cases, size_t(max_cases) * sizeof(CaseDev)) != cudaSuccess ||
+      cudaMalloc(&b->d_nitems, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&b->h_nitems, sizeof(int)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(b->staged, b->stream) != cudaSuccess)
+    return bail(fail(CGX_E_CUDA, "cgx_batch_create: CUDA allocation failed"));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  b->grid = nsm * 8;  // persistent grid: CTAs walk the work list grid-stride
+  Runner& R = b->run;
+  R.cases = b->d_cases;
+  R.items = nullptr;
+  R.nitems = b->d_nitems;
+  R.grid = b->grid;
+  R.stream = b->stream;
+  R.prec = prec;
+  R.launches = &b->launches;
+  *out = b;
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_destroy(cgx_batch* b) {
+  if (!b) return CGX_OK;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  batch_free_graph(b);
+  for (BatchCase& c : b->slots)
+    if (c.s) cgx_solver_destroy(c.s);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->h_items) cudaFreeHost(b->h_items);
+  cudaFree(b->d_cases);
+  cudaFree(b->d_nitems);
+  cudaFreeHost(b->h_nitems);
+  cudaEventDestroy(b->staged);
+  cudaStreamDestroy(b->stream);
+  delete b;
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
+                             const double* u, const double* pres, int nsteps, int* case_id) {
+  if (!b || !mesh || !p || !rho || !u || !pres || nsteps < 0)
+    return fail(CGX_E_ARG, "cgx_batch_add: invalid argument");
+  if (mesh->device != b->device) return fail(CGX_E_ARG, "cgx_batch_add: mesh on another device");
+  int slot = -1;
+  for (int k = 0; k < b->max_cases; ++k)
+    if (!b->slots[k].s) {
+      slot = k;
+      break;
+    }
+  if (slot < 0) return fail(CGX_E_OOM, "cgx_batch_add: all case slots in use");
+  size_t need = solver_bytes(mesh->N, b->prec);
+  if (!b->mesh_refs.count(mesh)) need += mesh->bytes;
+  if (b->prec == CGX_MIXED && !mesh->have32) need += mesh32_bytes(mesh);
+  if (b->used + need > b->budget) return fail(CGX_E_OOM, "cgx_batch_add: HBM budget exceeded");
+  CK(cudaSetDevice(b->device));
+  const size_t mesh_before = mesh->bytes;
+  cgx_solver* s = nullptr;
+  int rc = cgx_solver_create(mesh, p, b->prec, &s);
+  if (rc) return rc;
+  if ((rc = cgx_set_state_primitive(s, rho, u, pres)) || (rc = cgx_init_complete(s))) {
+    cgx_solver_destroy(s);
+    return rc;
+  }
+  BatchCase& c = b->slots[slot];
+  c.id = b->next_id++;
+  c.s = s;
+  c.mesh = mesh;
+  c.target = nsteps;
+  c.finished = (nsteps == 0);
+  c.bytes = s->bytes;
+  b->used += s->bytes + (mesh->bytes - mesh_before);
+  if (b->mesh_refs[mesh]++ == 0) b->used += mesh_before;
+  b->slot_of[c.id] = slot;
+  // the case's descriptor into the table (mesh records as of now)
+  s->hcase.m = mesh->md;
+  CK(cudaMemcpyAsync(b->d_cases + slot, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  b->dirty = true;
+  if (case_id) *case_id = c.id;
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
+  if (!b || nsteps < 0) return fail(CGX_E_ARG, "cgx_batch_step: invalid argument");
+  CK(cudaSetDevice(b->device));
+  int rc;
+  int left = nsteps;
+  while (left > 0) {
+    if (b->dirty && (rc = batch_rebuild(b))) return rc;
+    if (b->nitems == 0) break;
+    // lane counts for this batch size (cached per bucket); re-derive the
+    // gradients with the chosen counts afterwards
+    const int bucket = tune_bucket(b->active_cells, b->prec);
+    if (bucket != b->tuned_bucket) {
+      if ((rc = autotune(b->run, b->active_cells))) return rc;
+      if ((rc = enqueue_grad(b->run))) return rc;
+      b->tuned_bucket = bucket;
+      batch_free_graph(b);
+    }
+    if (!b->graph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      const long long before = b->launches.load();
+      rc = enqueue_step(b->run);
+      cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+      b->launches = before;
+      if (rc) return rc;
+      if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+      ec = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec));
+    }
+    // steps until the next case finishes (or the request is served)
+    int run = left;
+    for (const BatchCase& c : b->slots)
+      if (c.s && !c.finished) run = std::min(run, c.target - c.steps);
+    run = std::max(run, 1);
+    for (int k = 0; k < run; ++k) {
+      CK(cudaGraphLaunch(b->graph, b->stream));
+      b->launches += kLaunchesPerStep;
+    }
+    left -= run;
+    for (BatchCase& c : b->slots) {
+      if (!c.s || c.finished) continue;
+      c.steps += run;
+      if (c.steps >= c.target) {
+        c.finished = true;
+        b->dirty = true;
+      }
+    }
+    if (b->dirty && (rc = batch_check_nan(b))) return rc;
+  }
+  if ((rc = batch_check_nan(b))) return rc;
+  if (n_done) {
+    int n = 0;
+    for (const BatchCase& c : b->slots)
+      if (c.s && c.finished) ++n;
+    *n_done = n;
+  }
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_done(cgx_batch* b, int* ids, int max, int* n) {
+  if (!b || !n) return fail(CGX_E_ARG, "cgx_batch_done: null argument");
+  int k = 0;
+  for (const BatchCase& c : b->slots)
+    if (c.s && c.finished) {
+      if (ids && k < max) ids[k] = c.id;
+      ++k;
+    }
+  *n = k;
+  return CGX_OK;
+}
+
+static BatchCase* batch_case(cgx_batch* b, int id) {
+  auto it = b->slot_of.find(id);
+  if (it == b->slot_of.end()) return nullptr;
+  return &b->slots[it->second];
+}
+
+extern "C" int cgx_batch_get_state(cgx_batch* b, int case_id, double* rho, double* u, double* rhoE) {
+  if (!b) return fail(CGX_E_ARG, "null batch");
+  BatchCase* c = batch_case(b, case_id);
+  if (!c) return fail(CGX_E_ARG, "unknown case id");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  return cgx_get_state(c->s, rho, u, rhoE);
+}
+
+extern "C" int cgx_batch_get_time(cgx_batch* b, int case_id, double* time, double* dt, int* step) {
+  if (!b) return fail(CGX_E_ARG, "null batch");
+  BatchCase* c = batch_case(b, case_id);
+  if (!c) return fail(CGX_E_ARG, "unknown case id");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  return cgx_get_time(c->s, time, dt, step);
+}
+
+extern "C" int cgx_batch_remove(cgx_batch* b, int case_id) {
+  if (!b) return fail(CGX_E_ARG, "null batch");
+  auto it = b->slot_of.find(case_id);
+  if (it == b->slot_of.end()) return fail(CGX_E_ARG, "unknown case id");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  BatchCase& c = b->slots[it->second];
+  b->used -= c.bytes;
+  if (--b->mesh_refs[c.mesh] == 0) {
+    b->used -= c.mesh->bytes;
+    b->mesh_refs.erase(c.mesh);
+  }
+  cgx_solver_destroy(c.s);
+  c = BatchCase();
+  b->slot_of.erase(it);
+  b->dirty = true;
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_bytes(const cgx_batch* b, size_t* used, size_t* budget) {
+  if (!b) return fail(CGX_E_ARG, "null batch");
+  if (used) *used = b->used;
+  if (budget) *budget = b->budget;
+  return CGX_OK;
+}
+
+extern "C" long long cgx_batch_launch_count(const cgx_batch* b) { return b ? b->launches.load() : 0; }

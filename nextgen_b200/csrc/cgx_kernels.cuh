@@ -175,6 +175,25 @@ struct StateDev {
   double* red;  // per-block partials: [nblocks] cfl max, [nblocks] nan
 };
 
+// One resident case: its mesh, its state and its parameters.  The step
+// kernels take a table of these and a work list of items.
+struct CaseDev {
+  MeshDev m;
+  StateDev s;
+  Phys ph;
+  int nitems;  // work items of this case (partials of the per-step reduction)
+  int pad;
+};
+
+// A work item: up to kItemCells consecutive cells of one case.
+constexpr int kItemCells = 256;
+struct Item {
+  int c;      // case slot in the table
+  int cell0;  // first cell
+  int ncell;  // cells in this item (<= kItemCells)
+  int idx;    // item index within its case
+};
+
 }  // namespace cgx
 
 #endif

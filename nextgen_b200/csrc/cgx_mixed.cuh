@@ -168,11 +168,8 @@ __device__ __forceinline__ void compact_flux_add_f(FluxF& F, const float un_[3],
 }
 
 template <int G>
-__global__ void __launch_bounds__(256, 4) k_rhs_ext_f(MeshDev m, StateDev s, int stage, double h_ref) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
-  const bool valid = i < m.N;
+__global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
+  ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
   LRecF Li;
   if (valid) {
@@ -205,22 +202,19 @@ __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(MeshDev m, StateDev s, int
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  acc[4] += h_ref * acc[0];
+  acc[4] += cases[it_.c].ph.h_ref * acc[0];
   if (valid) {
     double* r = s.rhs + size_t(stage) * 5 * m.N;
 #pragma unroll
     for (int c = 0; c < 5; ++c)
       if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
   }
+  ITEM_LOOP_END
 }
 
 template <int G>
-__global__ void __launch_bounds__(256, 2) k_rhs_comp_f(MeshDev m, StateDev s, int stage, double h_ref,
-                                                       float p_ref) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
-  const bool valid = i < m.N;
+__global__ void __launch_bounds__(256, 2) k_rhs_comp_f(CASE_ARGS, int stage) {
+  ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
   LRecF Li;
   PRecF Pi;
@@ -255,7 +249,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp_f(MeshDev m, StateDev s, in
     const float h_f = 0.5f * ((Lj.hh + Li.hh) + uaub);
     FluxF F;
     F.rho = 0.0f; F.ru[0] = F.ru[1] = F.ru[2] = 0.0f; F.rE = 0.0f;
-    compact_flux_add_f(F, un, h0.w, h1.x, h1.y, Li, Lj, Pi, Pj, uf, h_f, gi, gj, p_ref);
+    compact_flux_add_f(F, un, h0.w, h1.x, h1.y, Li, Lj, Pi, Pj, uf, h_f, gi, gj,
+                       float(cases[it_.c].ph.p_ref));
     acc[0] -= double(F.rho);
     acc[1] -= double(F.ru[0]);
     acc[2] -= double(F.ru[1]);
@@ -264,21 +259,19 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp_f(MeshDev m, StateDev s, in
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  acc[4] += h_ref * acc[0];
+  acc[4] += cases[it_.c].ph.h_ref * acc[0];
   if (valid && e > b) {
     double* r = s.rhs + size_t(stage) * 5 * m.N;
 #pragma unroll
     for (int c = 0; c < 5; ++c)
       if (c % G == lane) r[size_t(c) * m.N + i] += acc[c];
   }
+  ITEM_LOOP_END
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) k_grad_f(MeshDev m, StateDev s) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
-  const bool valid = i < m.N;
+__global__ void __launch_bounds__(256) k_grad_f(CASE_ARGS) {
+  ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
   float ui[3] = {0.0f, 0.0f, 0.0f};
   if (valid) {
@@ -310,22 +303,26 @@ __global__ void __launch_bounds__(256) k_grad_f(MeshDev m, StateDev s) {
     for (int c = 0; c < 9; ++c)
       if (c % G == lane) s.GF[i].g[c] = g[c];
   }
+  ITEM_LOOP_END
 }
 
 // once per step, mixed form: FP32 SGS/properties/sensor, FP64 CFL sums and
 // reductions (same structure as k_step_end)
 template <int G>
-__global__ void __launch_bounds__(256) k_step_end_f(MeshDev m, StateDev s, Phys ph, int mode) {
-  constexpr int kThreads = 256;
-  constexpr int kCells = kThreads / G;
+__global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
+  constexpr int kCells = 256 / G;
   __shared__ double sh_cfl[kCells];
   __shared__ int sh_nan[kCells];
   __shared__ bool am_last;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / G;
-  const int lane = t & (G - 1);
   const int cl = threadIdx.x / G;
-  const bool valid = i < m.N;
+  double t_cfl = 0.0;
+  int t_nan = 0;
+  ITEM_LOOP_BEGIN(G)
+  const Phys& ph = cases[it_.c].ph;
+  if (sub_ == 0) {
+    t_cfl = 0.0;
+    t_nan = 0;
+  }
   long long b = 0, e = 0, ec = 0;
   LRecF Li;
   float4 qi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -420,28 +417,38 @@ __global__ void __launch_bounds__(256) k_step_end_f(MeshDev m, StateDev s, Phys 
     nan = (rho != rho) || (p != p) || (T != T);
     cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
   }
-  if (lane == 0) {
-    sh_cfl[cl] = valid ? cfl : 0.0;
-    sh_nan[cl] = nan;
+  if (lane == 0 && valid) {
+    t_cfl = fmax(t_cfl, cfl);
+    t_nan |= nan;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mx = 0.0;
-    int an = 0;
-    for (int c = 0; c < kCells; ++c) {
-      mx = fmax(mx, sh_cfl[c]);
-      an |= sh_nan[c];
+  if (sub_ == G - 1) {
+    if (lane == 0) {
+      sh_cfl[cl] = t_cfl;
+      sh_nan[cl] = t_nan;
     }
-    s.red[blockIdx.x] = mx;
-    s.red[gridDim.x + blockIdx.x] = double(an);
-    __threadfence();
-    const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
-    am_last = (done == gridDim.x - 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mx = 0.0;
+      int an = 0;
+      for (int c = 0; c < kCells; ++c) {
+        mx = fmax(mx, sh_cfl[c]);
+        an |= sh_nan[c];
+      }
+      const int np = cases[it_.c].nitems;
+      s.red[it_.idx] = mx;
+      s.red[np + it_.idx] = double(an);
+      __threadfence();
+      const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
+      am_last = (done == unsigned(np) - 1u);
+    }
+    __syncthreads();
+    if (am_last) {
+      __threadfence();
+      finalize_ctl(s, ph, mode, cases[it_.c].nitems);
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  finalize_ctl(s, ph, mode);
+  ITEM_LOOP_END
 }
 
 #endif
