@@ -147,6 +147,57 @@ def cpu_baseline(seconds=12.0, n=48, lib_kind="reference"):
                       "%d OpenMP ranks over contiguous cell ranges" % (steps, what, n, m.ncv, cores)}
 
 
+def served_stream(nreq=16, seed=4242, budget_gb=60):
+    """The served configuration: requests arrive as a seeded Poisson process;
+    each is a jittered-lattice periodic Voronoi box with edge uniform in
+    [16, 96] (rounded to a multiple of 8 so that requests share device
+    meshes), Taylor-Green or random-solenoidal (k0 = 4) initial state, Mach
+    uniform in [0.1, 0.5], steps uniform in [200, 2000], FP64 or mixed.  The
+    rate is set to twice the GPU's estimated throughput so the device stays
+    saturated.  Also runs the same cases one at a time on the plain FP64
+    path."""
+    from nextgen_b200 import cases, cgx, serve
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    rng = np.random.default_rng(seed)
+    edges = [int(8 * round(e / 8)) for e in rng.uniform(16, 96, size=nreq)]
+    meshes = {}
+    t0 = time.perf_counter()
+    for n in sorted(set(edges)):
+        hm = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED + n)
+        meshes[n] = (hm, cgx.Mesh(hm))
+    t_mesh = time.perf_counter() - t0
+    reqs = []
+    for k, n in enumerate(edges):
+        hm, gm = meshes[n]
+        Ma = float(rng.uniform(0.1, 0.5))
+        if rng.random() < 0.5:
+            prm = cases.tgv_params(Ma=Ma, Re=float(rng.uniform(400, 3200)))
+            rho, u, p = cases.tgv_state(hm.x_cv[: hm.ncv], prm)
+            kind = "tgv"
+        else:
+            prm = cases.hit_params(Mt=Ma)
+            rho, u, p = cases.hit_state(n, prm, Mt=Ma, k0=4.0, seed=4321 + k)
+            kind = "solenoidal"
+        prm.check_interval = 20
+        prec = cgx.CGX_FP64 if rng.random() < 0.5 else cgx.CGX_MIXED
+        reqs.append(serve.Request(k, gm, prm, rho, u, p, int(rng.integers(200, 2001)), prec))
+        reqs[-1].kind = kind
+    total_cs = sum(r.cell_steps for r in reqs)
+    rate = 2.0 * 1.5e8 / (total_cs / nreq)  # requests/s: twice the estimated service rate
+    for r, a in zip(reqs, serve.poisson_arrivals(nreq, rate, seed=seed + 1)):
+        r.arrival = float(a)
+    out = serve.serve(reqs, hbm_budget=int(budget_gb * (1 << 30)), chunk=16, keep_state=False)
+    seq, _ = serve.run_sequential(reqs, precision=cgx.CGX_FP64)
+    out.update({"sequential_plain_fp64_cell_steps_per_s": seq["cell_steps_per_s"],
+                "sequential_plain_fp64_seconds": seq["seconds"],
+                "speedup_vs_sequential_plain_fp64": out["cell_steps_per_s"] / seq["cell_steps_per_s"],
+                "poisson_rate_per_s": rate, "mesh_build_s": round(t_mesh, 2),
+                "mix": {"fp64": sum(r.precision == cgx.CGX_FP64 for r in reqs),
+                        "mixed": sum(r.precision == cgx.CGX_MIXED for r in reqs),
+                        "edges": edges, "steps_total": int(sum(r.nsteps for r in reqs))}})
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -321,13 +372,16 @@ def run_cgx(args):
         "tuning": tuning,
         "mixed": mixed,
     }
+    for k in list(solvers):
+        solvers[k].close()
+    solvers = {}
+    gm.close()
+    if rank == 0 and world == 1 and not args.no_served:
+        out["served"] = served_stream(nreq=args.served_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds, n=args.cpu_n)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    for k in list(solvers):
-        solvers[k].close()
-    gm.close()
     dist.finalize()
     return 0
 
@@ -345,6 +399,8 @@ def main():
     ap.add_argument("--ref-n", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         sys.exit("steps >= 1, warmup >= 0")

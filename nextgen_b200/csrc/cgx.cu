@@ -51,6 +51,7 @@ namespace {
 thread_local std::string g_err;
 
 constexpr int kBlock = 128;
+constexpr int kMaxRounds = 16;  // largest lanes-per-cell of the once-per-step kernel
 constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) + step_end
 
 // ===========================================================================
@@ -239,23 +240,36 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 
 // Every step kernel walks a work list of items (kItemCells cells of one case
 // each) with a grid-stride loop, 256 threads per CTA.  A kernel that puts G
-// lanes on a cell covers an item in G rounds of 256/G cells.  Inside the loop
+// lanes on a cell splits an item into G rounds of 256/G cells; one round is
+// the unit a CTA takes from the list.  Inside the loop
 // `m`, `s` are the item's case mesh and state, `i` the cell, `lane` the
 // lane in the cell's group and `valid` whether the cell exists (items of a
 // case's last cells are partial).
-#define CASE_ARGS \
-  const CaseDev* __restrict__ cases, const Item* __restrict__ items, const int* __restrict__ nitems
-#define ITEM_LOOP_BEGIN(G)                                             \
-  const int n_items_ = *nitems;                                        \
-  for (int w_ = blockIdx.x; w_ < n_items_; w_ += gridDim.x) {          \
-    const Item it_ = items[w_];                                        \
-    const MeshDev m = cases[it_.c].m;                                  \
-    const StateDev s = cases[it_.c].s;                                 \
-    for (int sub_ = 0; sub_ < (G); ++sub_) {                           \
-      const int loc_ = sub_ * (256 / (G)) + int(threadIdx.x) / (G);    \
-      const int i = it_.cell0 + loc_;                                  \
-      const int lane = int(threadIdx.x) & ((G) - 1);                   \
+#define CASE_ARGS                                                              \
+  const CaseDev* __restrict__ cases, const Item* __restrict__ items,           \
+      const int* __restrict__ nitems, const CaseDev dcase
+// DIRECT (a template parameter of every step kernel): one case passed by value
+// in `dcase`, items computed from the cell count (no table or list loads).
+#define ITEM_LOOP_BEGIN(G)                                                     \
+  const int n_work_ = (DIRECT ? dcase.nitems : *nitems) * (G);                 \
+  for (int v_ = blockIdx.x; v_ < n_work_; v_ += gridDim.x) {                   \
+    Item it_;                                                                  \
+    if (DIRECT) {                                                              \
+      const int w_ = v_ / (G);                                                 \
+      it_ = Item{0, w_ * kItemCells, min(kItemCells, dcase.m.N - w_ * kItemCells), w_}; \
+    } else {                                                                   \
+      it_ = items[v_ / (G)];                                                   \
+    }                                                                          \
+    const int sub_ = v_ % (G);                                                 \
+    const MeshDev& m = DIRECT ? dcase.m : cases[it_.c].m;                      \
+    const StateDev& s = DIRECT ? dcase.s : cases[it_.c].s;                     \
+    {                                                                          \
+      const int loc_ = sub_ * (256 / (G)) + int(threadIdx.x) / (G);            \
+      const int i = it_.cell0 + loc_;                                          \
+      const int lane = int(threadIdx.x) & ((G) - 1);                           \
       const bool valid = loc_ < it_.ncell;
+#define CASE_PH (DIRECT ? dcase.ph : cases[it_.c].ph)
+#define CASE_NITEMS (DIRECT ? dcase.nitems : cases[it_.c].nitems)
 #define ITEM_LOOP_END \
   }                   \
   }
@@ -269,7 +283,7 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 //               closure
 // Every face is evaluated by each of its two cells with the orientation
 // reversed (n -> -n, unit_n -> -unit_n, c kept), which gives the negated flux.
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
   ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
@@ -313,7 +327,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
   ITEM_LOOP_END
 }
 
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
   ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
@@ -402,12 +416,13 @@ __device__ __forceinline__ void write_prim(const Phys& ph, StateDev& s, int i, d
 
 // rk3Step (when nw > 0) fused with the packed-state update of the new state,
 // one thread per cell.  dt_arg < 0 takes each case's dt from its control block.
+template <bool DIRECT>
 __global__ void __launch_bounds__(256) k_rk_prim(CASE_ARGS, int nw, double w0, double w1, double w2,
                                                  double dt_arg, int writeQ) {
   ITEM_LOOP_BEGIN(1)
   (void)lane;
   if (valid) {
-    const Phys& ph = cases[it_.c].ph;
+    const Phys& ph = CASE_PH;
     double rho = s.rho[i], u0 = s.u0[i], u1 = s.u1[i], u2 = s.u2[i], rhoE = s.rhoE[i];
     if (nw > 0) {
       const double dt = (dt_arg < 0.0) ? s.ctl->dt : dt_arg;
@@ -441,7 +456,7 @@ __global__ void __launch_bounds__(256) k_rk_prim(CASE_ARGS, int nw, double w0, d
 }
 
 // _calcCvGradRange over the compact CSR, a group of G lanes per cell.
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_grad(CASE_ARGS) {
   ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
@@ -529,21 +544,15 @@ __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, i
 // + calcCfl(NULL, 1.0) for the next step's dt + checkForNans, a group of G
 // lanes per cell for the face loops.
 // mode bit 0: advance time/step by the dt just used; bit 1: set dt from CFL.
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   constexpr int kCells = 256 / G;
   __shared__ double sh_cfl[kCells];
   __shared__ int sh_nan[kCells];
   __shared__ bool am_last;
   const int cl = threadIdx.x / G;
-  double t_cfl = 0.0;  // per-thread running max / flag over the item's rounds
-  int t_nan = 0;
   ITEM_LOOP_BEGIN(G)
-  const Phys& ph = cases[it_.c].ph;
-  if (sub_ == 0) {
-    t_cfl = 0.0;
-    t_nan = 0;
-  }
+  const Phys& ph = CASE_PH;
   long long b = 0, e = 0, ec = 0;
   LRec Li;
   double2 qa = make_double2(0.0, 0.0), qb = make_double2(0.0, 0.0);
@@ -643,38 +652,33 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
     nan = (rho != rho) || (Li.p != Li.p) || (T != T);
     cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
   }
-  if (lane == 0 && valid) {
-    t_cfl = fmax(t_cfl, cfl);
-    t_nan |= nan;
+  // ---- round reduction; the last round of a case finalises its control block
+  if (lane == 0) {
+    sh_cfl[cl] = valid ? cfl : 0.0;
+    sh_nan[cl] = valid ? nan : 0;
   }
-  if (sub_ == G - 1) {
-    // ---- item reduction; the last item of a case finalises its control block
-    if (lane == 0) {
-      sh_cfl[cl] = t_cfl;
-      sh_nan[cl] = t_nan;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mx = 0.0;
+    int an = 0;
+    for (int c = 0; c < kCells; ++c) {
+      mx = fmax(mx, sh_cfl[c]);
+      an |= sh_nan[c];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double mx = 0.0;
-      int an = 0;
-      for (int c = 0; c < kCells; ++c) {
-        mx = fmax(mx, sh_cfl[c]);
-        an |= sh_nan[c];
-      }
-      const int np = cases[it_.c].nitems;
-      s.red[it_.idx] = mx;
-      s.red[np + it_.idx] = double(an);
-      __threadfence();
-      const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
-      am_last = (done == unsigned(np) - 1u);
-    }
-    __syncthreads();
-    if (am_last) {
-      __threadfence();
-      finalize_ctl(s, ph, mode, cases[it_.c].nitems);
-    }
-    __syncthreads();
+    const int np = CASE_NITEMS * G;
+    const int part = it_.idx * G + sub_;
+    s.red[part] = mx;
+    s.red[np + part] = double(an);
+    __threadfence();
+    const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
+    am_last = (done == unsigned(np) - 1u);
   }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    finalize_ctl(s, ph, mode, CASE_NITEMS * G);
+  }
+  __syncthreads();
   ITEM_LOOP_END
 }
 
@@ -940,7 +944,10 @@ struct Runner {
   const CaseDev* cases = nullptr;
   const Item* items = nullptr;
   const int* nitems = nullptr;  // device: number of items in the list
-  int grid = 0;                 // CTAs per launch (items are walked grid-stride)
+  int grid = 0;                 // CTAs per launch when the item count lives on the device
+  int nitems_host = -1;         // item count when fixed (single case): exact grids
+  bool direct = false;          // single case passed by value (no table/list loads)
+  CaseDev dcase{};
   cudaStream_t stream = nullptr;
   Tune tune;
   cgx_precision prec = CGX_FP64;
@@ -984,43 +991,68 @@ int launch_check(const Runner& R, int nk) {
   return CGX_OK;
 }
 
-#define RARGS R.cases, R.items, R.nitems
+#define RARGS R.cases, R.items, R.nitems, R.dcase
+
+// CTAs for a kernel with G rounds per item
+inline int grid_for(const Runner& R, int G) {
+  return R.nitems_host >= 0 ? std::max(1, R.nitems_host * G) : R.grid;
+}
 
 int enqueue_prim(const Runner& R, int nw, const double* w, double dt_arg, bool writeQ) {
-  k_rk_prim<<<R.grid, 256, 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0, w ? w[2] : 0.0, dt_arg,
+  if (R.direct)
+    k_rk_prim<true><<<grid_for(R, 1), 256, 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0,
+                                                          w ? w[2] : 0.0, dt_arg, writeQ ? 1 : 0);
+  else
+    k_rk_prim<false><<<grid_for(R, 1), 256, 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0, w ? w[2] : 0.0, dt_arg,
                                           writeQ ? 1 : 0);
   return launch_check(R, 1);
 }
 
 // Lanes per cell of the group-per-cell kernels, chosen per mesh-size bucket
 // by autotune() (timed candidates, cached process-wide).
+template <int G, bool MIX, bool DIRECT>
+void launch_grad_d(const Runner& R) {
+  if (MIX)
+    k_grad_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS);
+  else
+    k_grad<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS);
+}
+template <int G, bool MIX, bool DIRECT>
+void launch_ext_d(const Runner& R, int st) {
+  if (MIX)
+    k_rhs_ext_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+  else
+    k_rhs_ext<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+}
+template <int G, bool MIX, bool DIRECT>
+void launch_comp_d(const Runner& R, int st) {
+  if (MIX)
+    k_rhs_comp_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+  else
+    k_rhs_comp<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+}
+template <int G, bool MIX, bool DIRECT>
+void launch_end_d(const Runner& R, int mode) {
+  if (MIX)
+    k_step_end_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, mode);
+  else
+    k_step_end<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, mode);
+}
 template <int G, bool MIX>
 void launch_grad(const Runner& R) {
-  if (MIX)
-    k_grad_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS);
-  else
-    k_grad<G><<<R.grid, 256, 0, R.stream>>>(RARGS);
+  R.direct ? launch_grad_d<G, MIX, true>(R) : launch_grad_d<G, MIX, false>(R);
 }
 template <int G, bool MIX>
 void launch_ext(const Runner& R, int st) {
-  if (MIX)
-    k_rhs_ext_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
-  else
-    k_rhs_ext<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
+  R.direct ? launch_ext_d<G, MIX, true>(R, st) : launch_ext_d<G, MIX, false>(R, st);
 }
 template <int G, bool MIX>
 void launch_comp(const Runner& R, int st) {
-  if (MIX)
-    k_rhs_comp_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
-  else
-    k_rhs_comp<G><<<R.grid, 256, 0, R.stream>>>(RARGS, st);
+  R.direct ? launch_comp_d<G, MIX, true>(R, st) : launch_comp_d<G, MIX, false>(R, st);
 }
 template <int G, bool MIX>
 void launch_end(const Runner& R, int mode) {
-  if (MIX)
-    k_step_end_f<G><<<R.grid, 256, 0, R.stream>>>(RARGS, mode);
-  else
-    k_step_end<G><<<R.grid, 256, 0, R.stream>>>(RARGS, mode);
+  R.direct ? launch_end_d<G, MIX, true>(R, mode) : launch_end_d<G, MIX, false>(R, mode);
 }
 
 template <bool MIX>
@@ -1680,7 +1712,7 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     AL(sd.Q, N);
   }
   AL(sd.ctl, 1);
-  AL(sd.red, 2 * size_t(s->nitems));
+  AL(sd.red, 2 * size_t(s->nitems) * kMaxRounds);
   AL(s->d_case, 1);
   AL(s->d_items, s->nitems);
   AL(s->d_nitems, 1);
@@ -1717,7 +1749,10 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     R.cases = s->d_case;
     R.items = s->d_items;
     R.nitems = s->d_nitems;
-    R.grid = s->nitems;
+    R.grid = s->nitems * kMaxRounds;
+    R.nitems_host = s->nitems;
+    R.direct = true;
+    R.dcase = cd;
     R.stream = s->stream;
     R.prec = prec;
     R.launches = &s->launches;
@@ -2085,7 +2120,7 @@ size_t solver_bytes(long long N, cgx_precision prec) {
   size_t rec = (prec == CGX_MIXED) ? sizeof(LRecF) + sizeof(PRecF) + sizeof(GRecF) + sizeof(QRecF)
                                    : sizeof(LRec) + sizeof(PRec) + sizeof(GRec) + sizeof(QRec);
   return size_t(N) * (5 + 15 + 9 + 10) * sizeof(double) + size_t(N) * rec + sizeof(Ctl) +
-         size_t(2 * nitems) * sizeof(double) + sizeof(CaseDev) + size_t(nitems) * sizeof(Item) +
+         size_t(2 * nitems) * kMaxRounds * sizeof(double) + sizeof(CaseDev) + size_t(nitems) * sizeof(Item) +
          sizeof(int) + size_t(5 * nblocks + 5) * sizeof(double) + 4096;
 }
 
@@ -2318,10 +2353,15 @@ extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
     // gradients with the chosen counts afterwards
     const int bucket = tune_bucket(b->active_cells, b->prec);
     if (bucket != b->tuned_bucket) {
+      const Tune old = b->run.tune;
       if ((rc = autotune(b->run, b->active_cells))) return rc;
-      if ((rc = enqueue_grad(b->run))) return rc;
+      const Tune& t = b->run.tune;
+      if (b->tuned_bucket < 0 || t.g_ext != old.g_ext || t.g_comp != old.g_comp || t.g_grad != old.g_grad ||
+          t.g_end != old.g_end) {
+        if ((rc = enqueue_grad(b->run))) return rc;  // dudx summed in the new grouping
+        batch_free_graph(b);
+      }
       b->tuned_bucket = bucket;
-      batch_free_graph(b);
     }
     if (!b->graph) {
       cudaGraph_t g;
@@ -2429,3 +2469,4 @@ extern "C" int cgx_batch_bytes(const cgx_batch* b, size_t* used, size_t* budget)
 }
 
 extern "C" long long cgx_batch_launch_count(const cgx_batch* b) { return b ? b->launches.load() : 0; }
+

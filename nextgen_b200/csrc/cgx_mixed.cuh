@@ -167,7 +167,7 @@ __device__ __forceinline__ void compact_flux_add_f(FluxF& F, const float un_[3],
   }
 }
 
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
   ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  acc[4] += cases[it_.c].ph.h_ref * acc[0];
+  acc[4] += CASE_PH.h_ref * acc[0];
   if (valid) {
     double* r = s.rhs + size_t(stage) * 5 * m.N;
 #pragma unroll
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
   ITEM_LOOP_END
 }
 
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 2) k_rhs_comp_f(CASE_ARGS, int stage) {
   ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp_f(CASE_ARGS, int stage) {
     FluxF F;
     F.rho = 0.0f; F.ru[0] = F.ru[1] = F.ru[2] = 0.0f; F.rE = 0.0f;
     compact_flux_add_f(F, un, h0.w, h1.x, h1.y, Li, Lj, Pi, Pj, uf, h_f, gi, gj,
-                       float(cases[it_.c].ph.p_ref));
+                       float(CASE_PH.p_ref));
     acc[0] -= double(F.rho);
     acc[1] -= double(F.ru[0]);
     acc[2] -= double(F.ru[1]);
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp_f(CASE_ARGS, int stage) {
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  acc[4] += cases[it_.c].ph.h_ref * acc[0];
+  acc[4] += CASE_PH.h_ref * acc[0];
   if (valid && e > b) {
     double* r = s.rhs + size_t(stage) * 5 * m.N;
 #pragma unroll
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp_f(CASE_ARGS, int stage) {
   ITEM_LOOP_END
 }
 
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_grad_f(CASE_ARGS) {
   ITEM_LOOP_BEGIN(G)
   long long b = 0, e = 0;
@@ -308,21 +308,15 @@ __global__ void __launch_bounds__(256) k_grad_f(CASE_ARGS) {
 
 // once per step, mixed form: FP32 SGS/properties/sensor, FP64 CFL sums and
 // reductions (same structure as k_step_end)
-template <int G>
+template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   constexpr int kCells = 256 / G;
   __shared__ double sh_cfl[kCells];
   __shared__ int sh_nan[kCells];
   __shared__ bool am_last;
   const int cl = threadIdx.x / G;
-  double t_cfl = 0.0;
-  int t_nan = 0;
   ITEM_LOOP_BEGIN(G)
-  const Phys& ph = cases[it_.c].ph;
-  if (sub_ == 0) {
-    t_cfl = 0.0;
-    t_nan = 0;
-  }
+  const Phys& ph = CASE_PH;
   long long b = 0, e = 0, ec = 0;
   LRecF Li;
   float4 qi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -417,37 +411,32 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
     nan = (rho != rho) || (p != p) || (T != T);
     cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
   }
-  if (lane == 0 && valid) {
-    t_cfl = fmax(t_cfl, cfl);
-    t_nan |= nan;
+  if (lane == 0) {
+    sh_cfl[cl] = valid ? cfl : 0.0;
+    sh_nan[cl] = valid ? nan : 0;
   }
-  if (sub_ == G - 1) {
-    if (lane == 0) {
-      sh_cfl[cl] = t_cfl;
-      sh_nan[cl] = t_nan;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mx = 0.0;
+    int an = 0;
+    for (int c = 0; c < kCells; ++c) {
+      mx = fmax(mx, sh_cfl[c]);
+      an |= sh_nan[c];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double mx = 0.0;
-      int an = 0;
-      for (int c = 0; c < kCells; ++c) {
-        mx = fmax(mx, sh_cfl[c]);
-        an |= sh_nan[c];
-      }
-      const int np = cases[it_.c].nitems;
-      s.red[it_.idx] = mx;
-      s.red[np + it_.idx] = double(an);
-      __threadfence();
-      const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
-      am_last = (done == unsigned(np) - 1u);
-    }
-    __syncthreads();
-    if (am_last) {
-      __threadfence();
-      finalize_ctl(s, ph, mode, cases[it_.c].nitems);
-    }
-    __syncthreads();
+    const int np = CASE_NITEMS * G;
+    const int part = it_.idx * G + sub_;
+    s.red[part] = mx;
+    s.red[np + part] = double(an);
+    __threadfence();
+    const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
+    am_last = (done == unsigned(np) - 1u);
   }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    finalize_ctl(s, ph, mode, CASE_NITEMS * G);
+  }
+  __syncthreads();
   ITEM_LOOP_END
 }
 

@@ -51,10 +51,13 @@ def test_batch_matches_alone(three, prec, tol):
     b = cgx.Batch(0, prec, max_cases=8, hbm_budget=8 << 30)
     ids = [b.add(gm, prm, rho, u, p, n) for (m, gm, prm, rho, u, p), n in zip(three, steps)]
     assert None not in ids
+    b.step(1)  # first step tunes the lane counts for this batch size
     n0 = b.launch_count()
     b.step(100)
     assert sorted(b.done()) == sorted(ids)
-    assert b.launch_count() - n0 == 8 * 13  # one graph replay per step of the longest case
+    # one graph replay (13 kernels) per step of the longest case, plus at most
+    # a re-tuning when the batch shrinks into another size bucket
+    assert 7 * 13 <= b.launch_count() - n0 < 7 * 13 + 30
     for cid, (m, gm, prm, rho, u, p), n in zip(ids, three, steps):
         got = b.get_state(cid)
         ref, (t_ref, dt_ref, st_ref) = alone(gm, prm, rho, u, p, n, prec)
