@@ -238,6 +238,26 @@ int cgx_batch_remove(cgx_batch* b, int case_id);
 int cgx_batch_bytes(const cgx_batch* b, size_t* used, size_t* budget);
 long long cgx_batch_launch_count(const cgx_batch* b);
 
+/*
+ * report() totals that allocate nothing (no counterpart in the reference).
+ * For host solvers that cannot call cudaMalloc -- for instance because their
+ * device memory comes from another allocator or is fixed at start-up -- this
+ * computes {sum rho V, sum rho u V (3), sum rhoE V} over caller-owned device
+ * arrays rho[n], u[n][3] (the reference's interleaved layout), rhoE[n],
+ * vol[n] into the caller's device array out5[5], on `stream` (a
+ * cudaStream_t; NULL for the legacy default stream), without allocating.
+ * The reduction's scratch is a file-scope device array of 8192 x 5 doubles
+ * (320 KiB, held by every GPU that loads this library until the process
+ * exits); n is limited to 16,777,216 cells (8192 blocks of 2048) and larger
+ * n is rejected with CGX_E_ARG.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race, so serialise them.  Returns without waiting for
+ * the GPU.
+ */
+int cgx_totals_noalloc(long long n, const double* rho, const double* u, const double* rhoE,
+                       const double* vol, double* out5, void* stream);
+
 const char* cgx_last_error(void);
 
 #ifdef __cplusplus

@@ -2470,3 +2470,96 @@ extern "C" int cgx_batch_bytes(const cgx_batch* b, size_t* used, size_t* budget)
 
 extern "C" long long cgx_batch_launch_count(const cgx_batch* b) { return b ? b->launches.load() : 0; }
 
+// ===========================================================================
+// report() totals without allocation
+// ===========================================================================
+// For host solvers that cannot call cudaMalloc (their device memory comes
+// from another allocator, or is fixed at start-up): the conservation totals
+// over caller-owned device arrays, with the reduction's scratch in a
+// file-scope device array instead of an allocation.  The array lives in every
+// GPU that loads this library until the process exits.
+namespace {
+
+constexpr int kNoAllocThreads = 256;
+constexpr int kNoAllocCellsPerThread = 8;
+constexpr int kNoAllocMaxBlocks = 8192;  // scratch: 8192 x 5 doubles = 320 KiB
+constexpr long long kNoAllocMaxCells =
+    (long long)kNoAllocMaxBlocks * kNoAllocThreads * kNoAllocCellsPerThread;  // 16,777,216
+
+// Partial sums of one block each.  Every call writes the slots it then reads,
+// so nothing has to start at zero; it keeps the last call's partials.
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks * 5];
+
+__global__ void __launch_bounds__(kNoAllocThreads) k_totals_noalloc_partial(
+    long long n, const double* __restrict__ rho, const double* __restrict__ u,
+    const double* __restrict__ rhoE, const double* __restrict__ vol, double* __restrict__ part) {
+  __shared__ double sh[5][kNoAllocThreads];
+  double v[5] = {0, 0, 0, 0, 0};
+  const long long base = (long long)blockIdx.x * kNoAllocThreads * kNoAllocCellsPerThread + threadIdx.x;
+  for (int k = 0; k < kNoAllocCellsPerThread; ++k) {
+    const long long i = base + (long long)k * kNoAllocThreads;
+    if (i < n) {
+      const double V = vol[i], r = rho[i];
+      v[0] += r * V;
+      v[1] += r * u[3 * i] * V;
+      v[2] += r * u[3 * i + 1] * V;
+      v[3] += r * u[3 * i + 2] * V;
+      v[4] += rhoE[i] * V;
+    }
+  }
+  for (int c = 0; c < 5; ++c) sh[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int w = kNoAllocThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 5; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) part[5 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// the partials summed in block order (deterministic)
+__global__ void k_totals_noalloc_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  if (threadIdx.x < 5) {
+    double acc = 0.0;
+    for (int b = 0; b < nb; ++b) acc += part[5 * b + threadIdx.x];
+    out[threadIdx.x] = acc;
+  }
+}
+
+// device address of the scratch array, looked up once per device
+std::mutex g_noalloc_mu;
+std::map<int, double*> g_noalloc_ptr;
+
+}  // namespace
+
+extern "C" int cgx_totals_noalloc(long long n, const double* rho, const double* u, const double* rhoE,
+                                  const double* vol, double* out5, void* stream) {
+  if (n < 0 || (n > 0 && (!rho || !u || !rhoE || !vol)) || !out5)
+    return fail(CGX_E_ARG, "cgx_totals_noalloc: null argument or negative size");
+  if (n > kNoAllocMaxCells)
+    return fail(CGX_E_ARG, "cgx_totals_noalloc: " + std::to_string(n) + " cells exceed the maximum of " +
+                               std::to_string(kNoAllocMaxCells) + " (8192 blocks of 2048 cells)");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  double* part = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    auto it = g_noalloc_ptr.find(dev);
+    if (it == g_noalloc_ptr.end()) {
+      // in host code the array's name is a host stand-in: the kernels get
+      // its device address, taken with this device current
+      CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&part), g_noalloc_partials));
+      g_noalloc_ptr[dev] = part;
+    } else {
+      part = it->second;
+    }
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long per_block = (long long)kNoAllocThreads * kNoAllocCellsPerThread;
+  const int nb = int(std::max<long long>(1, (n + per_block - 1) / per_block));
+  k_totals_noalloc_partial<<<nb, kNoAllocThreads, 0, st>>>(n, rho, u, rhoE, vol, part);
+  k_totals_noalloc_final<<<1, 32, 0, st>>>(part, nb, out5);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CGX_E_CUDA, std::string("cgx_totals_noalloc: ") + cudaGetErrorString(e));
+  return CGX_OK;
+}
