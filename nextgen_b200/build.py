@@ -60,7 +60,7 @@ def build_meshgen(force=False):
 
 def build_cgx(force=False, verbose=False):
     out = os.path.join(LIB, "libcgx.so")
-    srcs = [os.path.join(CSRC, f) for f in ("cgx.cu", "cgx_kernels.cuh")] + [os.path.join(INC, "cgx.h")]
+    srcs = [os.path.join(CSRC, f) for f in ("cgx.cu", "cgx_kernels.cuh", "cgx_mixed.cuh")] + [os.path.join(INC, "cgx.h")]
     if force or _stale(out, srcs):
         os.makedirs(LIB, exist_ok=True)
         cmd = [_nvcc(), "-O3", "-std=c++17"] + NVCC_ARCH + [

@@ -1,7 +1,8 @@
 // cgx.cu -- B200 (sm_100a) kernels and the C ABI of include/cgx.h.
 //
-// One RK3 step on the device is ten kernels, replayed from a CUDA graph:
-//   3 x { k_rhs (face fluxes, cell-centric over the extended-face SELL),
+// One RK3 step on the device is thirteen kernels, replayed from a CUDA graph:
+//   3 x { k_rhs_ext + k_rhs_comp (face fluxes, cell-centric over each cell's
+//         extended / compact entries),
 //         k_rk_prim (rk3Step fused with the primitive/packed-state update),
 //         k_grad (compact-CSR velocity gradient) }
 //   k_step_end (Vreman SGS, material properties, Gibbs sensor, calcCfl ->
@@ -36,6 +37,7 @@
 #include <mutex>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -51,7 +53,12 @@ namespace {
 thread_local std::string g_err;
 
 constexpr int kBlock = 128;
-constexpr int kMaxRounds = 16;  // largest lanes-per-cell of the once-per-step kernel
+constexpr int kMaxRounds = 16;  // most rounds per item of a once-per-step kernel
+// largest neighbour unions an item may have (shared-memory budget of the
+// staged face kernels: 64 B per extended-face neighbour record, 192 B per
+// compact-face one)
+constexpr int kMaxUnionExt = 3000;
+constexpr int kMaxUnionComp = 1100;
 constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) + step_end
 
 // ===========================================================================
@@ -85,88 +92,258 @@ __device__ __forceinline__ double group_max(double v) {
   return v;
 }
 
+// 256-bit read-only global loads (sm_100): a 32 B-aligned record piece per
+// lane in one instruction, one sector per lane.
+__device__ __forceinline__ double4 ld4(const void* p) {
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ void st4(void* p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+
 __device__ __forceinline__ void load_L(const LRec* base, int j, LRec& r) {
-  const double2* p = reinterpret_cast<const double2*>(base + j);
-  const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+  const double* p = reinterpret_cast<const double*>(base + j);
+  const double4 a = ld4(p), b = ld4(p + 4);
+  r.u[0] = a.x; r.u[1] = a.y; r.u[2] = a.z; r.sp_vol = a.w;
+  r.p = b.x; r.h = b.y; r.rho = b.z; r.sos = b.w;
+}
+
+// properties and dudx of one cell (the whole 128 B record)
+__device__ __forceinline__ void load_V(const VRec* base, int j, VRec& r) {
+  const double* p = reinterpret_cast<const double*>(base + j);
+  const double4 a = ld4(p), b = ld4(p + 4), c = ld4(p + 8), d = ld4(p + 12);
+  r.mu_total = a.x; r.loc_total = a.y; r.a_sgs = a.z; r.fgr = a.w;
+  r.symh = b.x; r.symp = b.y; r.g[0] = b.z; r.g[1] = b.w;
+  r.g[2] = c.x; r.g[3] = c.y; r.g[4] = c.z; r.g[5] = c.w;
+  r.g[6] = d.x; r.g[7] = d.y; r.g[8] = d.z;
+}
+
+// dudx of one cell
+__device__ __forceinline__ void load_Vg(const VRec* base, int j, double g[9]) {
+  const double* p = reinterpret_cast<const double*>(base + j);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p + 6));
+  const double4 c = ld4(p + 8), d = ld4(p + 12);
+  g[0] = b.x; g[1] = b.y;
+  g[2] = c.x; g[3] = c.y; g[4] = c.z; g[5] = c.w;
+  g[6] = d.x; g[7] = d.y; g[8] = d.z;
+}
+
+// ---- shared-memory staging of neighbour records -------------------------
+// Record arrays in shared memory hold records of R 16-byte chunks (R = 2, 4
+// or 8).  Chunk c of record j sits at 16-byte slot (j mod P)*R + (c xor
+// ((j/P) mod R)) of 128-byte row j/P, P = 8/R records per row: the same chunk
+// of records j..j+7 lands in eight different 16-byte bank groups, so the G
+// lanes of a cell reading different neighbours rarely conflict.
+template <int R>
+__device__ __forceinline__ int swz(int j, int c) {
+  constexpr int P = 8 / R;
+  return (j / P) * 8 + (j % P) * R + (c ^ ((j / P) % R));
+}
+// 16-byte chunks a record array of n records occupies (whole rows)
+template <int R>
+__host__ __device__ constexpr int swz_chunks(int n) {
+  return ((n * R + 7) / 8) * 8;
+}
+
+__device__ __forceinline__ void cp_async16(int4* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Asynchronous prefetch of a byte range into L2 by the bulk-copy engine
+// (start rounded down, end rounded up to 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void* p, long long bytes) {
+  if (bytes <= 0) return;
+  const unsigned long long a = reinterpret_cast<unsigned long long>(p) & ~15ULL;
+  const unsigned long long e = (reinterpret_cast<unsigned long long>(p) + bytes + 15ULL) & ~15ULL;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(unsigned(e - a)) : "memory");
+}
+
+// L2 prefetch of the per-entry streams (six planes of TB-byte values and a
+// 16-bit index) of entries [k0, k1); threads 0..6 of the CTA issue one each.
+template <class TB>
+__device__ __forceinline__ void prefetch_entries(const TB* planes, long long stride,
+                                                 const unsigned short* idx, long long k0, long long k1) {
+  const int t = threadIdx.x;
+  if (t < 6)
+    prefetch_l2(planes + t * stride + k0, (k1 - k0) * static_cast<long long>(sizeof(TB)));
+  else if (t == 6)
+    prefetch_l2(idx + k0, (k1 - k0) * 2);
+}
+
+// The entries a staged kernel reads in round `sub` of item `it` (cells
+// it.cell0 + [sub*cpr, (sub+1)*cpr)): extended (COMP false) or compact.
+template <bool COMP, class TB>
+__device__ __forceinline__ void prefetch_round(const MeshDev& m, const TB* planes, const Item& it, int sub,
+                                               int cpr) {
+  const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
+  if (a >= b || threadIdx.x >= 7) return;
+  const long long* o = COMP ? m.qoff : m.off;
+  prefetch_entries(planes, COMP ? m.Q : m.E, COMP ? m.clidx : m.lidx, __ldg(o + it.cell0 + a),
+                   __ldg(o + it.cell0 + b));
+}
+
+// The streams the once-per-step kernel reads in round `sub` of item `it`:
+// the extended entries' local indices, the compact entries' local indices,
+// unit normals and areas.
+__device__ __forceinline__ void prefetch_end(const MeshDev& m, const Item& it, int sub, int cpr) {
+  const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
+  const int t = threadIdx.x;
+  if (a >= b || t >= 6) return;
+  if (t == 0) {
+    const long long k0 = __ldg(m.off + it.cell0 + a), k1 = __ldg(m.off + it.cell0 + b);
+    prefetch_l2(m.lidx + k0, (k1 - k0) * 2);
+    return;
+  }
+  const long long q0 = __ldg(m.qoff + it.cell0 + a), q1 = __ldg(m.qoff + it.cell0 + b);
+  if (t == 5)
+    prefetch_l2(m.clidx + q0, (q1 - q0) * 2);
+  else
+    prefetch_l2(m.qg + (t - 1) * m.Q + q0, (q1 - q0) * 8);
+}
+
+// the gradient kernel's streams: local indices and three coefficient planes
+// (TB-byte values) of the round's gradient entries
+template <class TB>
+__device__ __forceinline__ void prefetch_grad(const MeshDev& m, const TB* gx, const TB* gy, const TB* gz,
+                                              const Item& it, int sub, int cpr) {
+  const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
+  const int t = threadIdx.x;
+  if (a >= b || t >= 4) return;
+  const long long k0 = __ldg(m.coff + it.cell0 + a), k1 = __ldg(m.coff + it.cell0 + b);
+  if (t == 0) {
+    prefetch_l2(m.cglidx + k0, (k1 - k0) * 2);
+    return;
+  }
+  const TB* p = (t == 1) ? gx : (t == 2) ? gy : gz;
+  prefetch_l2(p + k0, (k1 - k0) * static_cast<long long>(sizeof(TB)));
+}
+
+// Copy the records (R chunks each) of an item's cells, then of its halo
+// cells, into a swizzled shared array.  Asynchronous: complete with
+// stage_wait().
+// RS: the global record's size in chunks (the first R are copied).
+template <int R, int RS = R>
+__device__ __forceinline__ void stage_records(int4* sm, const void* base, const Item& it,
+                                              const int* __restrict__ halo, int nh) {
+  const int4* b = reinterpret_cast<const int4*>(base);
+  const int nu = it.ncell + nh;
+  for (int x = threadIdx.x; x < nu * R; x += blockDim.x) {
+    const int u = x / R, c = x % R;
+    const int cell = (u < it.ncell) ? it.cell0 + u : __ldg(halo + (u - it.ncell));
+    cp_async16(sm + swz<R>(u, c), b + size_t(cell) * RS + c);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void stage_wait() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+}
+
+__device__ __forceinline__ void smem_L(const int4* sm, int j, LRec& r) {
+  const double2* p = reinterpret_cast<const double2*>(sm);
+  const double2 a = p[swz<4>(j, 0)], b = p[swz<4>(j, 1)], c = p[swz<4>(j, 2)], d = p[swz<4>(j, 3)];
   r.u[0] = a.x; r.u[1] = a.y; r.u[2] = b.x; r.sp_vol = b.y;
   r.p = c.x; r.h = c.y; r.rho = d.x; r.sos = d.y;
 }
 
-__device__ __forceinline__ void load_P(const PRec* base, int j, PRec& r) {
-  const double2* p = reinterpret_cast<const double2*>(base + j);
-  const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
-  r.mu_total = a.x; r.loc_total = a.y; r.a_sgs = b.x; r.fgr = b.y; r.symh = c.x; r.symp = c.y;
+__device__ __forceinline__ void smem_V(const int4* sm, int j, VRec& r) {
+  const double2* p = reinterpret_cast<const double2*>(sm);
+  double2 x = p[swz<8>(j, 0)];
+  r.mu_total = x.x; r.loc_total = x.y;
+  x = p[swz<8>(j, 1)];
+  r.a_sgs = x.x; r.fgr = x.y;
+  x = p[swz<8>(j, 2)];
+  r.symh = x.x; r.symp = x.y;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    x = p[swz<8>(j, 3 + c)];
+    r.g[2 * c] = x.x;
+    r.g[2 * c + 1] = x.y;
+  }
+  r.g[8] = p[swz<8>(j, 7)].x;
 }
 
-__device__ __forceinline__ void load_G(const GRec* base, int j, double g[9]) {
-  const double2* p = reinterpret_cast<const double2*>(base + j);
-  const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4);
-  g[0] = a.x; g[1] = a.y; g[2] = b.x; g[3] = b.y; g[4] = c.x; g[5] = c.y; g[6] = d.x; g[7] = d.y; g[8] = e.x;
+// field-wise sum of two cells' viscous records in shared memory
+__device__ __forceinline__ void smem_V_sum(const int4* sm, int a, int b, VRec& r) {
+  const double2* p = reinterpret_cast<const double2*>(sm);
+  double2 x = p[swz<8>(a, 0)], y = p[swz<8>(b, 0)];
+  r.mu_total = x.x + y.x; r.loc_total = x.y + y.y;
+  x = p[swz<8>(a, 1)]; y = p[swz<8>(b, 1)];
+  r.a_sgs = x.x + y.x; r.fgr = x.y + y.y;
+  x = p[swz<8>(a, 2)]; y = p[swz<8>(b, 2)];
+  r.symh = x.x + y.x; r.symp = x.y + y.y;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    x = p[swz<8>(a, 3 + c)];
+    y = p[swz<8>(b, 3 + c)];
+    r.g[2 * c] = x.x + y.x;
+    r.g[2 * c + 1] = x.y + y.y;
+  }
+  r.g[8] = p[swz<8>(a, 7)].x + p[swz<8>(b, 7)].x;
+}
+
+__device__ __forceinline__ double4 smem_Q(const int4* sm, int j) {
+  const double2* p = reinterpret_cast<const double2*>(sm);
+  const double2 a = p[swz<2>(j, 0)], b = p[swz<2>(j, 1)];
+  return make_double4(a.x, a.y, b.x, b.y);
 }
 
 struct Flux {
   double rho, ru[3], rE;
 };
 
-// Skew-symmetric central flux (IdealGasSolverFlux.hpp:9-39), same operation
-// order; returns the face averages the other two parts reuse.
-__device__ __forceinline__ void skew_flux(Flux& F, const double n[3], const LRec& a, const LRec& b,
-                                          double uf[3], double& rho_f, double& h_f) {
-  rho_f = 2.0 * rcp_nr(a.sp_vol + b.sp_vol);
-  const double p_f = 0.5 * (b.p + a.p);
-  double un = 0.0, uaub = 0.0;
+// Skew-symmetric flux plus its symmetric "c" part (IdealGasSolverFlux.hpp:
+// 9-39 and 41-90) of the face a -> b, as one 5-vector.  The reference's two
+// functions produce the same terms; here they are grouped around the total
+// mass flux M = mdot + dmdot:
+//   F.rho = M
+//   F.ru  = p_f n + dp c + M uf + mdot_c du
+//   F.rE  = M h_f + mdot_c (dh + uf.du)
+// (mdot = rho_f uf.n, dmdot = uf.c drho + rho_f du.c, mdot_c = rho_f uf.c).
+// Every term changes sign exactly under (a <-> b, n -> -n, c kept), so the
+// two cells of a face see exactly opposite fluxes.
+__device__ __forceinline__ void ext_flux(double F[5], const double n[3], const double c[3], const LRec& a,
+                                         const LRec& b) {
+  const double rho_f = 2.0 * rcp_nr(a.sp_vol + b.sp_vol);
+  double uf[3], du[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double um = 0.5 * (a.u[d] + b.u[d]);
-    un += um * n[d];
-    uaub += a.u[d] * b.u[d];
-    uf[d] = um;
-    F.ru[d] = p_f * n[d];
+    uf[d] = 0.5 * (a.u[d] + b.u[d]);
+    du[d] = b.u[d] - a.u[d];
   }
+  const double un = uf[0] * n[0] + uf[1] * n[1] + uf[2] * n[2];
+  const double uc = uf[0] * c[0] + uf[1] * c[1] + uf[2] * c[2];
+  const double duc = du[0] * c[0] + du[1] * c[1] + du[2] * c[2];
+  const double uaub = a.u[0] * b.u[0] + a.u[1] * b.u[1] + a.u[2] * b.u[2];
+  const double ufdu = uf[0] * du[0] + uf[1] * du[1] + uf[2] * du[2];
   const double mdot = un * rho_f;
-  F.rho = mdot;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) F.ru[d] += mdot * uf[d];
-  h_f = 0.5 * ((b.h + a.h) + uaub);
-  F.rE = mdot * h_f;
-}
-
-// Symmetric "c" part (IdealGasSolverFlux.hpp:41-90), added into F.
-__device__ __forceinline__ void sym_flux_add(Flux& F, const double c[3], const LRec& a, const LRec& b,
-                                             const double uf[3], double rho_f, double h_f) {
-  double du[3];
-  double du_c = 0.0, uf_c = 0.0;
+  const double dmdot = uc * (b.rho - a.rho) + rho_f * duc;
+  const double mdot_c = uc * rho_f;
+  const double M = mdot + dmdot;
+  const double p_f = 0.5 * (a.p + b.p);
   const double dp = b.p - a.p;
-  double dH = b.h - a.h;
-  // (v_a - v_b)/(v_a v_b) of the reference is rho_b - rho_a
-  const double drho = b.rho - a.rho;
-  double G[3];
+  const double h_f = 0.5 * ((a.h + b.h) + uaub);
+  const double dH = (b.h - a.h) + ufdu;
+  F[0] = M;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const double dd = b.u[d] - a.u[d];
-    du[d] = dd;
-    du_c += dd * c[d];
-    uf_c += uf[d] * c[d];
-    dH += uf[d] * dd;
-    G[d] = dp * c[d];
-  }
-  const double dmdot = uf_c * drho + rho_f * du_c;
-  const double mdot_c = uf_c * rho_f;
-  F.rho += dmdot;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) F.ru[d] += G[d] + (mdot_c * du[d] + uf[d] * dmdot);
-  F.rE += h_f * dmdot + mdot_c * dH;
+  for (int d = 0; d < 3; ++d) F[1 + d] = p_f * n[d] + dp * c[d] + M * uf[d] + mdot_c * du[d];
+  F[4] = M * h_f + mdot_c * dH;
 }
 
 // Compact closures (IdealGasSolverFlux.hpp:93-215), subtracted from F.
+// The closures use the two cells' properties and gradients only through
+// their sums: vs holds V_a + V_b field by field (same IEEE sums as the
+// reference's a + b forms, addition being commutative).
 __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], double area, double aod,
-                                                 double delta, const LRec& a, const LRec& b,
-                                                 const PRec& ax, const PRec& bx, const double uf[3],
-                                                 double h_f, const double ga[9], const double gb[9]) {
+                                                 double delta, const LRec& a, const LRec& b, const VRec& vs,
+                                                 const double uf[3], double h_f) {
   const double half_aod = 0.5 * aod;
-  const double mu_area = 0.5 * (ax.mu_total + bx.mu_total) * area;
-  const double mu_aod = (ax.mu_total + bx.mu_total) * half_aod;
-  const double k_aod = (ax.loc_total + bx.loc_total) * half_aod;
+  const double mu_area = 0.5 * vs.mu_total * area;
+  const double mu_aod = vs.mu_total * half_aod;
+  const double k_aod = vs.loc_total * half_aod;
   const double hua = 0.5 * (a.u[0] * a.u[0] + a.u[1] * a.u[1] + a.u[2] * a.u[2]);
   const double hub = 0.5 * (b.u[0] * b.u[0] + b.u[1] * b.u[1] + b.u[2] * b.u[2]);
   const double d_half_usq = hub - hua;
@@ -181,7 +358,7 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
   const double dun_3 = dun * (1.0 / 3.0);
   const double dun2_6 = (unb * unb - una * una) * (1.0 / 6.0);
   const double dp = b.p - a.p;
-  const double fgr_f = 0.5 * (bx.fgr + ax.fgr);
+  const double fgr_f = 0.5 * vs.fgr;
   const double rho_m = 0.5 * (b.rho + a.rho);
   const double un_m = 0.5 * (una + unb);
   const double c_m = 0.5 * (a.sos + b.sos);
@@ -190,8 +367,8 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
   const double lf = fmin(fgr_f * mach_n, 0.5) * (c_m + fabs(un_m)) * area;
   const double lf_drho = lf * drho;
   const double lf_rho = lf * rho_m;
-  double ap = 0.5 * (ax.a_sgs + bx.a_sgs) * delta * area;
-  ap += (ax.symp + bx.symp) * half_aod;
+  double ap = 0.5 * vs.a_sgs * delta * area;
+  ap += vs.symp * half_aod;
   const double ap_dp = ap * dp;
 
   F.rho -= lf_drho + ap_dp;
@@ -203,7 +380,7 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
     F.ru[d] -= uf[d] * ap_dp;
   }
   F.rE -= mu_aod * (d_half_usq + dun2_6);
-  double hs = (ax.symh + bx.symh) * rho_m * fabs(un_m) * half_aod;
+  double hs = vs.symh * rho_m * fabs(un_m) * half_aod;
   hs = fmax(hs - k_aod, 0.0);
   F.rE -= (k_aod + hs) * dh;
   F.rE -= ap_dp * h_f;
@@ -218,10 +395,9 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
   double gnn_3 = 0.0, div_23 = 0.0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    gn[k] = 0.5 * ((ga[k] + gb[k]) * un_[0] + (ga[3 + k] + gb[3 + k]) * un_[1] +
-                   (ga[6 + k] + gb[6 + k]) * un_[2]);
+    gn[k] = 0.5 * (vs.g[k] * un_[0] + vs.g[3 + k] * un_[1] + vs.g[6 + k] * un_[2]);
     gnn_3 += gn[k] * un_[k];
-    div_23 += ga[4 * k] + gb[4 * k];
+    div_23 += vs.g[4 * k];
   }
   div_23 *= (1.0 / 3.0);
   gnn_3 *= (1.0 / 3.0);
@@ -238,33 +414,36 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 // ===========================================================================
 
 
-// Every step kernel walks a work list of items (kItemCells cells of one case
-// each) with a grid-stride loop, 256 threads per CTA.  A kernel that puts G
-// lanes on a cell splits an item into G rounds of 256/G cells; one round is
-// the unit a CTA takes from the list.  Inside the loop
-// `m`, `s` are the item's case mesh and state, `i` the cell, `lane` the
-// lane in the cell's group and `valid` whether the cell exists (items of a
-// case's last cells are partial).
+// Every step kernel walks a work list of items (at most kItemCells cells of
+// one case each) with a grid-stride loop.  A kernel that puts G lanes on a
+// cell runs kThreads(G) = min(256, G*kItemCells) threads per CTA and splits
+// an item into kRounds(G) rounds of kThreads/G cells; one round is the unit a
+// CTA takes from the list.  Inside the loop `m`, `s` are the item's case mesh
+// and state, `i` the cell, `lane` the lane in the cell's group and `valid`
+// whether the cell exists (items are often shorter than a round).
+template <int G>
+__host__ __device__ constexpr int kThreads() {
+  return G * kItemCells >= 256 ? 256 : G * kItemCells;
+}
+template <int G>
+__host__ __device__ constexpr int kRounds() {
+  return (G * kItemCells + kThreads<G>() - 1) / kThreads<G>();
+}
 #define CASE_ARGS                                                              \
   const CaseDev* __restrict__ cases, const Item* __restrict__ items,           \
       const int* __restrict__ nitems, const CaseDev dcase
 // DIRECT (a template parameter of every step kernel): one case passed by value
-// in `dcase`, items computed from the cell count (no table or list loads).
+// in `dcase`, items read from its mesh's own item table.
 #define ITEM_LOOP_BEGIN(G)                                                     \
-  const int n_work_ = (DIRECT ? dcase.nitems : *nitems) * (G);                 \
+  constexpr int kR_ = kRounds<G>();                                            \
+  const int n_work_ = (DIRECT ? dcase.nitems : *nitems) * kR_;                 \
   for (int v_ = blockIdx.x; v_ < n_work_; v_ += gridDim.x) {                   \
-    Item it_;                                                                  \
-    if (DIRECT) {                                                              \
-      const int w_ = v_ / (G);                                                 \
-      it_ = Item{0, w_ * kItemCells, min(kItemCells, dcase.m.N - w_ * kItemCells), w_}; \
-    } else {                                                                   \
-      it_ = items[v_ / (G)];                                                   \
-    }                                                                          \
-    const int sub_ = v_ % (G);                                                 \
+    const Item it_ = DIRECT ? dcase.m.items[v_ / kR_] : items[v_ / kR_];       \
+    const int sub_ = v_ % kR_;                                                 \
     const MeshDev& m = DIRECT ? dcase.m : cases[it_.c].m;                      \
     const StateDev& s = DIRECT ? dcase.s : cases[it_.c].s;                     \
     {                                                                          \
-      const int loc_ = sub_ * (256 / (G)) + int(threadIdx.x) / (G);            \
+      const int loc_ = sub_ * (kThreads<G>() / (G)) + int(threadIdx.x) / (G);  \
       const int i = it_.cell0 + loc_;                                          \
       const int lane = int(threadIdx.x) & ((G) - 1);                           \
       const bool valid = loc_ < it_.ncell;
@@ -272,6 +451,39 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 #define CASE_NITEMS (DIRECT ? dcase.nitems : cases[it_.c].nitems)
 #define ITEM_LOOP_END \
   }                   \
+  }
+
+// The face-flux kernels take a whole item per CTA (256 threads): they stage
+// the item's neighbour records in shared memory, then run its rounds.  The
+// entry streams of the round ahead (the next item's first round during the
+// last one) are prefetched into L2 by the bulk-copy engine meanwhile;
+// PREFETCH(item, mesh, round) names the kernel's stream.
+#define STAGED_LOOP_BEGIN(PREFETCH)                                            \
+  const int n_items_ = DIRECT ? dcase.nitems : *nitems;                        \
+  if (blockIdx.x < n_items_) {                                                 \
+    const Item f_ = DIRECT ? dcase.m.items[blockIdx.x] : items[blockIdx.x];    \
+    PREFETCH(f_, (DIRECT ? dcase.m : cases[f_.c].m), 0);                       \
+  }                                                                            \
+  for (int v_ = blockIdx.x; v_ < n_items_; v_ += gridDim.x) {                  \
+    const Item it_ = DIRECT ? dcase.m.items[v_] : items[v_];                   \
+    const MeshDev& m = DIRECT ? dcase.m : cases[it_.c].m;                      \
+    const StateDev& s = DIRECT ? dcase.s : cases[it_.c].s;
+#define STAGED_ROUNDS_BEGIN(G, PREFETCH)                                       \
+    for (int sub_ = 0; sub_ < (kItemCells * (G) + 255) / 256; ++sub_) {        \
+      if ((sub_ + 1) * (256 / (G)) < it_.ncell) {                              \
+        PREFETCH(it_, m, sub_ + 1);                                            \
+      } else if ((sub_ == 0 || sub_ * (256 / (G)) < it_.ncell) &&              \
+                 v_ + int(gridDim.x) < n_items_) {                             \
+        const Item n_ = DIRECT ? dcase.m.items[v_ + gridDim.x] : items[v_ + gridDim.x]; \
+        PREFETCH(n_, (DIRECT ? dcase.m : cases[n_.c].m), 0);                   \
+      }                                                                        \
+      const int loc_ = sub_ * (256 / (G)) + int(threadIdx.x) / (G);            \
+      const int i = it_.cell0 + loc_;                                          \
+      const int lane = int(threadIdx.x) & ((G) - 1);                           \
+      const bool valid = loc_ < it_.ncell;
+#define STAGED_ROUNDS_END }
+#define STAGED_LOOP_END \
+    __syncthreads();    \
   }
 
 // calcRhsBase, cell-centric, in two passes over each cell's face list, a
@@ -285,36 +497,32 @@ __device__ __forceinline__ void compact_flux_add(Flux& F, const double un_[3], d
 // reversed (n -> -n, unit_n -> -unit_n, c kept), which gives the negated flux.
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
-  ITEM_LOOP_BEGIN(G)
+  extern __shared__ int4 smem[];
+#define PF_EXT(it, mm, r) prefetch_round<false>(mm, mm.en, it, r, 256 / G)
+  STAGED_LOOP_BEGIN(PF_EXT)
+  stage_records<4>(smem, s.L, it_, m.hcell + it_.hoff, it_.nh);
+  stage_wait();
+  const long long E = m.E;
+  STAGED_ROUNDS_BEGIN(G, PF_EXT)
   long long b = 0, e = 0;
   LRec Li;
   if (valid) {
     b = m.off[i];
     e = m.off[i + 1];
-    load_L(s.L, i, Li);
+    smem_L(smem, loc_, Li);
   }
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (long long k = b + lane; k < e; k += G) {
-    const int j = __ldg(m.nbr + k);
-    const int f = __ldg(m.fid + k);
-    const double sg = (f < 0) ? -1.0 : 1.0;
-    const double2* ge = reinterpret_cast<const double2*>(m.ef + (f & kFidMask));
-    const double2 g0 = __ldg(ge), g1 = __ldg(ge + 1), g2 = __ldg(ge + 2);
-    const double n[3] = {sg * g0.x, sg * g0.y, sg * g1.x};
-    const double c[3] = {g1.y, g2.x, g2.y};
+    const int jl = __ldg(m.lidx + k);
+    const double* g = m.en + k;
+    const double n[3] = {__ldg(g), __ldg(g + E), __ldg(g + 2 * E)};
+    const double c[3] = {__ldg(g + 3 * E), __ldg(g + 4 * E), __ldg(g + 5 * E)};
     LRec Lj;
-    load_L(s.L, j, Lj);
-    Flux F;
-    double uf[3], rho_f, h_f;
-    skew_flux(F, n, Li, Lj, uf, rho_f, h_f);
-    Flux C;
-    C.rho = 0.0; C.ru[0] = C.ru[1] = C.ru[2] = 0.0; C.rE = 0.0;
-    sym_flux_add(C, c, Li, Lj, uf, rho_f, h_f);
-    acc[0] -= F.rho + C.rho;
-    acc[1] -= F.ru[0] + C.ru[0];
-    acc[2] -= F.ru[1] + C.ru[1];
-    acc[3] -= F.ru[2] + C.ru[2];
-    acc[4] -= F.rE + C.rE;
+    smem_L(smem, jl, Lj);
+    double F[5];
+    ext_flux(F, n, c, Li, Lj);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc[q] -= F[q];
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
@@ -324,39 +532,40 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
     for (int c = 0; c < 5; ++c)
       if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
   }
-  ITEM_LOOP_END
+  STAGED_ROUNDS_END
+  STAGED_LOOP_END
+#undef PF_EXT
 }
 
 template <int G, bool DIRECT>
-__global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
-  ITEM_LOOP_BEGIN(G)
-  long long b = 0, e = 0;
+__global__ void __launch_bounds__(256, 3) k_rhs_comp(CASE_ARGS, int stage) {
+  extern __shared__ int4 smem[];
+#define PF_COMP(it, mm, r) prefetch_round<true>(mm, mm.qg, it, r, 256 / G)
+  STAGED_LOOP_BEGIN(PF_COMP)
+  const int nu = it_.ncell + it_.nch;
+  int4* sV = smem + swz_chunks<4>(nu);
+  stage_records<4>(smem, s.L, it_, m.chcell + it_.choff, it_.nch);
+  stage_records<8>(sV, s.V, it_, m.chcell + it_.choff, it_.nch);
+  stage_wait();
+  const long long Q = m.Q;
+  STAGED_ROUNDS_BEGIN(G, PF_COMP)
+  long long q0 = 0, q1 = 0;
   LRec Li;
-  PRec Pi;
-  double gi[9];
   if (valid) {
-    b = m.off[i];
-    e = b + __ldg(m.ncomp + i);
-    if (e > b + lane) {
-      load_L(s.L, i, Li);
-      load_P(s.P, i, Pi);
-      load_G(s.G, i, gi);
-    }
+    q0 = m.qoff[i];
+    q1 = m.qoff[i + 1];
+    smem_L(smem, loc_, Li);
   }
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (long long k = b + lane; k < e; k += G) {
-    const int j = __ldg(m.nbr + k);
-    const int f = __ldg(m.fid + k);
-    const double sg = (f < 0) ? -1.0 : 1.0;
-    const double2* gc = reinterpret_cast<const double2*>(m.cf + (f & kFidMask));
-    const double2 h0 = __ldg(gc), h1 = __ldg(gc + 1), h2 = __ldg(gc + 2);
-    const double un[3] = {sg * h0.x, sg * h0.y, sg * h1.x};
+  for (long long q = q0 + lane; q < q1; q += G) {
+    const int jl = __ldg(m.clidx + q);
+    const double* h = m.qg + q;
+    const double un[3] = {__ldg(h), __ldg(h + Q), __ldg(h + 2 * Q)};
+    const double area = __ldg(h + 3 * Q), aod = __ldg(h + 4 * Q), delta = __ldg(h + 5 * Q);
     LRec Lj;
-    load_L(s.L, j, Lj);
-    PRec Pj;
-    load_P(s.P, j, Pj);
-    double gj[9];
-    load_G(s.G, j, gj);
+    smem_L(smem, jl, Lj);
+    VRec Vs;
+    smem_V_sum(sV, loc_, jl, Vs);
     // face averages of the skew flux (IdealGasSolverFlux.hpp:23-37)
     double uf[3];
 #pragma unroll
@@ -365,7 +574,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
     const double h_f = 0.5 * ((Lj.h + Li.h) + uaub);
     Flux F;
     F.rho = 0.0; F.ru[0] = F.ru[1] = F.ru[2] = 0.0; F.rE = 0.0;
-    compact_flux_add(F, un, h1.y, h2.x, h2.y, Li, Lj, Pi, Pj, uf, h_f, gi, gj);
+    compact_flux_add(F, un, area, aod, delta, Li, Lj, Vs, uf, h_f);
     acc[0] -= F.rho;
     acc[1] -= F.ru[0];
     acc[2] -= F.ru[1];
@@ -374,13 +583,15 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  if (valid && e > b) {
+  if (valid && q1 > q0) {
     double* r = s.rhs + size_t(stage) * 5 * m.N;
 #pragma unroll
     for (int c = 0; c < 5; ++c)
       if (c % G == lane) r[size_t(c) * m.N + i] += acc[c];
   }
-  ITEM_LOOP_END
+  STAGED_ROUNDS_END
+  STAGED_LOOP_END
+#undef PF_COMP
 }
 
 // packed primitive state of one cell (updateExtendedState); FP64 always,
@@ -402,16 +613,10 @@ __device__ __forceinline__ void write_prim(const Phys& ph, StateDev& s, int i, d
                       float(1.0 / (ph.R * T))};
     return;
   }
-  double2* L = reinterpret_cast<double2*>(s.L + i);
-  L[0] = make_double2(u0, u1);
-  L[1] = make_double2(u2, 1.0 / rho);
-  L[2] = make_double2(p, Rgogm1 * T);
-  L[3] = make_double2(rho, sos);
-  if (writeQ) {
-    double2* Q = reinterpret_cast<double2*>(s.Q + i);
-    Q[0] = make_double2(log(p * (1.0 / ph.p_ref)), p);
-    Q[1] = make_double2(1.0 / rho, 1.0 / (ph.R * T));
-  }
+  double* L = reinterpret_cast<double*>(s.L + i);
+  st4(L, u0, u1, u2, 1.0 / rho);
+  st4(L + 4, p, Rgogm1 * T, rho, sos);
+  if (writeQ) st4(s.Q + i, log(p * (1.0 / ph.p_ref)), p, 1.0 / rho, 1.0 / (ph.R * T));
 }
 
 // rk3Step (when nw > 0) fused with the packed-state update of the new state,
@@ -455,25 +660,32 @@ __global__ void __launch_bounds__(256) k_rk_prim(CASE_ARGS, int nw, double w0, d
   ITEM_LOOP_END
 }
 
-// _calcCvGradRange over the compact CSR, a group of G lanes per cell.
+// _calcCvGradRange over the compact CSR (the reference's cvocv order), one
+// item per CTA, a group of G lanes per cell; the velocities of the item's
+// compact-face union are staged in shared memory (the first 32 bytes of each
+// LRec) and read through the per-entry local index cglidx.
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_grad(CASE_ARGS) {
-  ITEM_LOOP_BEGIN(G)
+  extern __shared__ int4 smem[];
+#define PF_GRAD(it, mm, r) prefetch_grad(mm, mm.gcx, mm.gcy, mm.gcz, it, r, 256 / G)
+  STAGED_LOOP_BEGIN(PF_GRAD)
+  stage_records<2, 4>(smem, s.L, it_, m.chcell + it_.choff, it_.nch);
+  stage_wait();
+  const double2* su = reinterpret_cast<const double2*>(smem);
+  STAGED_ROUNDS_BEGIN(G, PF_GRAD)
   long long b = 0, e = 0;
   double ui[3] = {0.0, 0.0, 0.0};
   if (valid) {
     b = m.coff[i];
     e = m.coff[i + 1];
-    const double2* Li = reinterpret_cast<const double2*>(s.L + i);
-    const double2 a = __ldg(Li), c = __ldg(Li + 1);
+    const double2 a = su[swz<2>(loc_, 0)], c = su[swz<2>(loc_, 1)];
     ui[0] = a.x; ui[1] = a.y; ui[2] = c.x;
   }
   double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (long long k = b + lane; k < e; k += G) {
-    const int j = __ldg(m.cnbr + k);
+    const int jl = __ldg(m.cglidx + k);
     const double cx = __ldg(m.gcx + k), cy = __ldg(m.gcy + k), cz = __ldg(m.gcz + k);
-    const double2* Lj = reinterpret_cast<const double2*>(s.L + j);
-    const double2 ja = __ldg(Lj), jb = __ldg(Lj + 1);
+    const double2 ja = su[swz<2>(jl, 0)], jb = su[swz<2>(jl, 1)];
     const double du[3] = {ja.x - ui[0], ja.y - ui[1], jb.x - ui[2]};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -487,9 +699,11 @@ __global__ void __launch_bounds__(256) k_grad(CASE_ARGS) {
   if (valid) {
 #pragma unroll
     for (int c = 0; c < 9; ++c)
-      if (c % G == lane) s.G[i].g[c] = g[c];
+      if (c % G == lane) s.V[i].g[c] = g[c];
   }
-  ITEM_LOOP_END
+  STAGED_ROUNDS_END
+  STAGED_LOOP_END
+#undef PF_GRAD
 }
 
 // Last block of a once-per-step kernel: reduce the per-block CFL maxima and
@@ -497,9 +711,8 @@ __global__ void __launch_bounds__(256) k_grad(CASE_ARGS) {
 // (mode bit 0) and the next dt from setDt's formula (mode bit 1).
 // Called by all 256 threads of that block.
 __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, int nparts) {
-  constexpr int kThreads = 256;
-  __shared__ double fin_cfl[kThreads];
-  __shared__ int fin_nan[kThreads];
+  __shared__ double fin_cfl[256];
+  __shared__ int fin_nan[256];
   double mx = 0.0;
   int anynan = 0;
   for (int bb = threadIdx.x; bb < nparts; bb += blockDim.x) {
@@ -509,7 +722,7 @@ __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, i
   fin_cfl[threadIdx.x] = mx;
   fin_nan[threadIdx.x] = anynan;
   __syncthreads();
-  for (int w = kThreads / 2; w > 0; w >>= 1) {
+  for (int w = int(blockDim.x) / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
       fin_cfl[threadIdx.x] = fmax(fin_cfl[threadIdx.x], fin_cfl[threadIdx.x + w]);
       fin_nan[threadIdx.x] |= fin_nan[threadIdx.x + w];
@@ -540,135 +753,148 @@ __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, i
   }
 }
 
-// Once per step: computeSgsVreman + calcSgsAndMaterialProperties + setFgrCvs
-// + calcCfl(NULL, 1.0) for the next step's dt + checkForNans, a group of G
-// lanes per cell for the face loops.
+// computeSgsVreman + calcSgsAndMaterialProperties + setFgrCvs for cell i
+// (its packed state Li, its Gibbs maximum vv2); writes the cell's lagged
+// properties and returns whether rho, p or T is NaN.
+__device__ __forceinline__ int cell_props(const Phys& ph, const MeshDev& m, const StateDev& s, int i,
+                                          const LRec& Li, double vv2) {
+  double g[9];
+  load_Vg(s.V, i, g);
+  // {dx, dx2_approx, dcmag_hat, sa_to_vol}
+  const double2 cc01 = __ldg(reinterpret_cast<const double2*>(m.cc + i));
+  const double2 cc23 = __ldg(reinterpret_cast<const double2*>(m.cc + i) + 1);
+  const double rho = Li.rho, sos = Li.sos;
+  const double T = Li.p / (rho * ph.R);
+  // ---- computeSgsVreman
+  double mu_sgs = 0.0, a_sgs = 0.0, loc_sgs = 0.0;
+  if (ph.sgs_model == CGX_SGS_VREMAN) {
+    const double dx = cc01.x;
+    const double dx2 = dx * dx;
+    const double a11 = g[0], a12 = g[1], a13 = g[2];
+    const double a21 = g[3], a22 = g[4], a23 = g[5];
+    const double a31 = g[6], a32 = g[7], a33 = g[8];
+    const double a11s = a11 * a11, a22s = a22 * a22, a33s = a33 * a33;
+    const double a12s = a12 * a12, a13s = a13 * a13, a23s = a23 * a23;
+    const double a21s = a21 * a21, a31s = a31 * a31, a32s = a32 * a32;
+    const double b11 = dx2 * (a11s + a21s + a31s);
+    const double b22 = dx2 * (a12s + a22s + a32s);
+    const double b33 = dx2 * (a13s + a23s + a33s);
+    const double b12 = dx2 * (a11 * a12 + a21 * a22 + a31 * a32);
+    const double b13 = dx2 * (a11 * a13 + a21 * a23 + a31 * a33);
+    const double b23 = dx2 * (a12 * a13 + a22 * a23 + a32 * a33);
+    double B = (b11 * b22 - b12 * b12) + (b11 * b33 - b13 * b13) + (b22 * b33 - b23 * b23);
+    B = (B + fabs(B)) * 0.5;
+    const double alal = ((a11s + a22s) + (a33s + a12s)) + ((a13s + a23s) + (a21s + a31s)) + a32s;
+    const double s_mag = sqrt(B / (alal + 1.0E-20));
+    mu_sgs = rho * ph.vreman_coeff * s_mag;
+    const double inv_sos2 = 1.0 / (sos * sos);
+    a_sgs = ph.a_sgs_coeff * s_mag / dx2;
+    const double dil = g[0] + g[4] + g[8];
+    const double tt = fabs(dil) * dx / sos;
+    if (tt > 0.01) {
+      const double Masq = (Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2]) * inv_sos2;
+      a_sgs += ph.a_sgs_coeff2 * cc23.y * fmin(Masq, 10.0) * sos;
+    }
+    a_sgs *= inv_sos2;
+    loc_sgs = ph.lambda_dil_coeff * rho * fabs(dil) * dx2;
+    loc_sgs += mu_sgs * (1.0 / ph.Pr_t);
+  }
+  // ---- material properties (fast_pow_posx = 1 + expm1(p log x))
+  const double mu_lam = ph.mu_ref * (1.0 + expm1(ph.mu_power_law * log(T * (1.0 / ph.T_ref))));
+  const double loc_lam = mu_lam * (1.0 / ph.Pr_lam);
+  const double sos2 = ph.gamma * Li.p / rho;
+  const double lambda = sqrt(Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2]) + sqrt(sos2);
+  const double symp = fmax(ph.coeff_p * cc23.x * lambda / sos2 - cc01.y * a_sgs, 0.0);
+  const double symh = ph.coeff_h * cc23.x;
+  double fgr = 0.5 / (1.0 + exp(-2.0 * (vv2 - ph.gr_nrm) / 5.0e-03));
+  if (ph.diss_mode == CGX_DISS_NONE) fgr = 0.0;
+  if (ph.diss_mode == CGX_DISS_ALL) fgr = 0.5;
+  double* P = reinterpret_cast<double*>(s.V + i);
+  st4(P, mu_lam + mu_sgs, loc_lam + loc_sgs, a_sgs, fgr);
+  reinterpret_cast<double2*>(P)[2] = make_double2(symh, symp);
+  return (rho != rho) || (Li.p != Li.p) || (T != T);
+}
+
+// Once per step: cell_props + calcCfl(NULL, 1.0) for the next step's dt +
+// checkForNans, one item per CTA, a group of G lanes per cell for the face
+// loops.  The Gibbs remainder reads the item's extended-face union of QRec
+// and the CFL sum its compact-face union of LRec, both staged in shared
+// memory.  Each item leaves one partial (CFL maximum, NaN flag); the last
+// item of a case reduces them in item order and updates the control block.
 // mode bit 0: advance time/step by the dt just used; bit 1: set dt from CFL.
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
-  constexpr int kCells = 256 / G;
-  __shared__ double sh_cfl[kCells];
-  __shared__ int sh_nan[kCells];
+  extern __shared__ int4 smem[];
+  __shared__ double sh_cfl[256];
+  __shared__ int sh_nan[256];
   __shared__ bool am_last;
-  const int cl = threadIdx.x / G;
-  ITEM_LOOP_BEGIN(G)
+#define PF_END(it, mm, r) prefetch_end(mm, it, r, 256 / G)
+  STAGED_LOOP_BEGIN(PF_END)
   const Phys& ph = CASE_PH;
-  long long b = 0, e = 0, ec = 0;
+  const int nu = it_.ncell + it_.nh;
+  int4* sL = smem + swz_chunks<2>(nu);
+  stage_records<2>(smem, s.Q, it_, m.hcell + it_.hoff, it_.nh);
+  stage_records<4>(sL, s.L, it_, m.chcell + it_.choff, it_.nch);
+  stage_wait();
+  const long long Q = m.Q;
+  double cmax = 0.0;
+  int anynan = 0;
+  STAGED_ROUNDS_BEGIN(G, PF_END)
+  long long b = 0, e = 0, q0 = 0, q1 = 0;
   LRec Li;
-  double2 qa = make_double2(0.0, 0.0), qb = make_double2(0.0, 0.0);
+  double4 qi = make_double4(0.0, 0.0, 0.0, 0.0);
   if (valid) {
     b = m.off[i];
     e = m.off[i + 1];
-    ec = b + __ldg(m.ncomp + i);
-    load_L(s.L, i, Li);
-    const double2* Qi = reinterpret_cast<const double2*>(s.Q + i);
-    qa = __ldg(Qi);
-    qb = __ldg(Qi + 1);
+    q0 = m.qoff[i];
+    q1 = m.qoff[i + 1];
+    smem_L(sL, loc_, Li);
+    qi = smem_Q(smem, loc_);
   }
-  // ---- Gibbs remainder over the extended faces, CFL over the compact ones
+  // ---- Gibbs remainder over the extended faces (a maximum: any order)
   double vv2 = 0.0, cfl = 0.0;
   for (long long k = b + lane; k < e; k += G) {
-    const int j = __ldg(m.nbr + k);
-    const double2* Qj = reinterpret_cast<const double2*>(s.Q + j);
-    const double2 ja = __ldg(Qj), jb = __ldg(Qj + 1);
-    const double dp = ja.y - qa.y;
-    const double v_avg = 0.5 * (qb.x + jb.x);
-    const double beta = 0.5 * (qb.y + jb.y);
-    const double gr = ja.x - qa.x - v_avg * dp * beta;
+    const double4 qj = smem_Q(smem, __ldg(m.lidx + k));
+    const double dp = qj.y - qi.y;
+    const double v_avg = 0.5 * (qi.z + qj.z);
+    const double beta = 0.5 * (qi.w + qj.w);
+    const double gr = qj.x - qi.x - v_avg * dp * beta;
     vv2 = fmax(vv2, fabs(gr));
-    if (k < ec) {
-      const int f = __ldg(m.fid + k);
-      const double sg = (f < 0) ? -1.0 : 1.0;
-      const double2* cr = reinterpret_cast<const double2*>(m.cf + (f & kFidMask));
-      const double2 h0 = __ldg(cr), h1 = __ldg(cr + 1);
-      const double un[3] = {sg * h0.x, sg * h0.y, sg * h1.x};
-      const double area = h1.y;
-      LRec Lj;
-      load_L(s.L, j, Lj);
-      const double undA = 0.5 * area * ((Li.u[0] * un[0] + Li.u[1] * un[1] + Li.u[2] * un[2]) +
-                                        (Lj.u[0] * un[0] + Lj.u[1] * un[1] + Lj.u[2] * un[2]));
-      cfl += fabs(undA) + area * (0.5 * (Li.sos + Lj.sos));
-    }
+  }
+  // ---- CFL over the compact faces
+  for (long long q = q0 + lane; q < q1; q += G) {
+    const int jl = __ldg(m.clidx + q);
+    const double* h = m.qg + q;
+    const double un[3] = {__ldg(h), __ldg(h + Q), __ldg(h + 2 * Q)};
+    const double area = __ldg(h + 3 * Q);
+    LRec Lj;
+    smem_L(sL, jl, Lj);
+    const double undA = 0.5 * area * ((Li.u[0] * un[0] + Li.u[1] * un[1] + Li.u[2] * un[2]) +
+                                      (Lj.u[0] * un[0] + Lj.u[1] * un[1] + Lj.u[2] * un[2]));
+    cfl += fabs(undA) + area * (0.5 * (Li.sos + Lj.sos));
   }
   vv2 = group_max<G>(vv2);
   cfl = group_sum<G>(cfl);
-  int nan = 0;
   if (valid && lane == 0) {
-    double g[9];
-    load_G(s.G, i, g);
-    // {dx, dx2_approx, dcmag_hat, sa_to_vol}
-    const double2 cc01 = __ldg(reinterpret_cast<const double2*>(m.cc + i));
-    const double2 cc23 = __ldg(reinterpret_cast<const double2*>(m.cc + i) + 1);
-    const double rho = Li.rho, sos = Li.sos;
-    const double T = Li.p / (rho * ph.R);
-    // ---- computeSgsVreman
-    double mu_sgs = 0.0, a_sgs = 0.0, loc_sgs = 0.0;
-    if (ph.sgs_model == CGX_SGS_VREMAN) {
-      const double dx = cc01.x;
-      const double dx2 = dx * dx;
-      const double a11 = g[0], a12 = g[1], a13 = g[2];
-      const double a21 = g[3], a22 = g[4], a23 = g[5];
-      const double a31 = g[6], a32 = g[7], a33 = g[8];
-      const double a11s = a11 * a11, a22s = a22 * a22, a33s = a33 * a33;
-      const double a12s = a12 * a12, a13s = a13 * a13, a23s = a23 * a23;
-      const double a21s = a21 * a21, a31s = a31 * a31, a32s = a32 * a32;
-      const double b11 = dx2 * (a11s + a21s + a31s);
-      const double b22 = dx2 * (a12s + a22s + a32s);
-      const double b33 = dx2 * (a13s + a23s + a33s);
-      const double b12 = dx2 * (a11 * a12 + a21 * a22 + a31 * a32);
-      const double b13 = dx2 * (a11 * a13 + a21 * a23 + a31 * a33);
-      const double b23 = dx2 * (a12 * a13 + a22 * a23 + a32 * a33);
-      double B = (b11 * b22 - b12 * b12) + (b11 * b33 - b13 * b13) + (b22 * b33 - b23 * b23);
-      B = (B + fabs(B)) * 0.5;
-      const double alal = ((a11s + a22s) + (a33s + a12s)) + ((a13s + a23s) + (a21s + a31s)) + a32s;
-      const double s_mag = sqrt(B / (alal + 1.0E-20));
-      mu_sgs = rho * ph.vreman_coeff * s_mag;
-      const double inv_sos2 = 1.0 / (sos * sos);
-      a_sgs = ph.a_sgs_coeff * s_mag / dx2;
-      const double dil = g[0] + g[4] + g[8];
-      const double tt = fabs(dil) * dx / sos;
-      if (tt > 0.01) {
-        const double Masq = (Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2]) * inv_sos2;
-        a_sgs += ph.a_sgs_coeff2 * cc23.y * fmin(Masq, 10.0) * sos;
-      }
-      a_sgs *= inv_sos2;
-      loc_sgs = ph.lambda_dil_coeff * rho * fabs(dil) * dx2;
-      loc_sgs += mu_sgs * (1.0 / ph.Pr_t);
-    }
-    // ---- material properties (fast_pow_posx = 1 + expm1(p log x))
-    const double mu_lam = ph.mu_ref * (1.0 + expm1(ph.mu_power_law * log(T * (1.0 / ph.T_ref))));
-    const double loc_lam = mu_lam * (1.0 / ph.Pr_lam);
-    const double sos2 = ph.gamma * Li.p / rho;
-    const double lambda = sqrt(Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2]) + sqrt(sos2);
-    const double symp = fmax(ph.coeff_p * cc23.x * lambda / sos2 - cc01.y * a_sgs, 0.0);
-    const double symh = ph.coeff_h * cc23.x;
-    double fgr = 0.5 / (1.0 + exp(-2.0 * (vv2 - ph.gr_nrm) / 5.0e-03));
-    if (ph.diss_mode == CGX_DISS_NONE) fgr = 0.0;
-    if (ph.diss_mode == CGX_DISS_ALL) fgr = 0.5;
-    double2* P = reinterpret_cast<double2*>(s.P + i);
-    P[0] = make_double2(mu_lam + mu_sgs, loc_lam + loc_sgs);
-    P[1] = make_double2(a_sgs, fgr);
-    P[2] = make_double2(symh, symp);
-    nan = (rho != rho) || (Li.p != Li.p) || (T != T);
-    cfl *= 0.5 * 1.0 * __ldg(m.inv_vol + i);
+    anynan |= cell_props(ph, m, s, i, Li, vv2);
+    cmax = fmax(cmax, cfl * (0.5 * 1.0 * __ldg(m.inv_vol + i)));
   }
-  // ---- round reduction; the last round of a case finalises its control block
-  if (lane == 0) {
-    sh_cfl[cl] = valid ? cfl : 0.0;
-    sh_nan[cl] = valid ? nan : 0;
-  }
+  STAGED_ROUNDS_END
+  // ---- the item's partial; the last item of the case finalises
+  sh_cfl[threadIdx.x] = cmax;
+  sh_nan[threadIdx.x] = anynan;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double mx = 0.0;
-    int an = 0;
-    for (int c = 0; c < kCells; ++c) {
-      mx = fmax(mx, sh_cfl[c]);
-      an |= sh_nan[c];
+  for (int w = 128; w > 0; w >>= 1) {
+    if (int(threadIdx.x) < w) {
+      sh_cfl[threadIdx.x] = fmax(sh_cfl[threadIdx.x], sh_cfl[threadIdx.x + w]);
+      sh_nan[threadIdx.x] |= sh_nan[threadIdx.x + w];
     }
-    const int np = CASE_NITEMS * G;
-    const int part = it_.idx * G + sub_;
-    s.red[part] = mx;
-    s.red[np + part] = double(an);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int np = CASE_NITEMS;
+    s.red[it_.idx] = sh_cfl[0];
+    s.red[np + it_.idx] = double(sh_nan[0]);
     __threadfence();
     const unsigned int done = atomicAdd(&s.ctl->blocks_done, 1u);
     am_last = (done == unsigned(np) - 1u);
@@ -676,10 +902,10 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   __syncthreads();
   if (am_last) {
     __threadfence();
-    finalize_ctl(s, ph, mode, CASE_NITEMS * G);
+    finalize_ctl(s, ph, mode, CASE_NITEMS);
   }
-  __syncthreads();
-  ITEM_LOOP_END
+  STAGED_LOOP_END
+#undef PF_END
 }
 
 #include "cgx_mixed.cuh"
@@ -774,9 +1000,9 @@ __global__ void k_diag_out(int N, const int* __restrict__ perm, double* __restri
       out[3 * size_t(o) + 1] = p / (double(L.rho) * R);
       out[3 * size_t(o) + 2] = L.sos;
     } else if (what == 2) {
-      for (int c = 0; c < 9; ++c) out[9 * size_t(o) + c] = s.GF[i].g[c];
+      for (int c = 0; c < 9; ++c) out[9 * size_t(o) + c] = s.VF[i].g[c];
     } else {
-      const PRecF& P = s.PF[i];
+      const VRecF& P = s.VF[i];
       out[6 * size_t(o) + 0] = P.mu_total;
       out[6 * size_t(o) + 1] = P.loc_total;
       out[6 * size_t(o) + 2] = P.a_sgs;
@@ -790,9 +1016,9 @@ __global__ void k_diag_out(int N, const int* __restrict__ perm, double* __restri
     out[3 * size_t(o) + 1] = L.p / (L.rho * R);
     out[3 * size_t(o) + 2] = L.sos;
   } else if (what == 2) {
-    for (int c = 0; c < 9; ++c) out[9 * size_t(o) + c] = s.G[i].g[c];
+    for (int c = 0; c < 9; ++c) out[9 * size_t(o) + c] = s.V[i].g[c];
   } else {
-    const PRec& P = s.P[i];
+    const VRec& P = s.V[i];
     out[6 * size_t(o) + 0] = P.mu_total;
     out[6 * size_t(o) + 1] = P.loc_total;
     out[6 * size_t(o) + 2] = P.a_sgs;
@@ -802,32 +1028,43 @@ __global__ void k_diag_out(int N, const int* __restrict__ perm, double* __restri
   }
 }
 
-// FP32 copies of the mesh geometry and gradient coefficients (mixed form)
-__global__ void k_geom32(int nef, int ncf, long long nc, const EFRec* __restrict__ ef,
-                         const CFRec* __restrict__ cf, const double* __restrict__ gx,
-                         const double* __restrict__ gy, const double* __restrict__ gz, EFRecF* ef32,
-                         CFRecF* cf32, float* gx32, float* gy32, float* gz32) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t < nef) {
-    const EFRec& a = ef[t];
-    EFRecF r;
-    for (int k = 0; k < 3; ++k) {
-      r.n[k] = float(a.n[k]);
-      r.c[k] = float(a.c[k]);
+// Per-entry geometry planes from the per-face records: entry k of the
+// extended CSR reads face fid[k] (bit 31: the cell is the face's second cell,
+// normal negated); compact entry q = qoff[i] + t mirrors extended entry
+// off[i] + t (eofq[q]).  One thread per entry.
+__global__ void k_expand_entries(long long E, long long Q, const int* __restrict__ fid,
+                                 const EFRec* __restrict__ ef, const CFRec* __restrict__ cf,
+                                 const long long* __restrict__ eofq, double* __restrict__ en,
+                                 double* __restrict__ qg) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k < E) {
+    const int f = fid[k];
+    const EFRec r = ef[f & kFidMask];
+    const double sg = (f < 0) ? -1.0 : 1.0;
+    for (int d = 0; d < 3; ++d) {
+      en[d * E + k] = sg * r.n[d];
+      en[(3 + d) * E + k] = r.c[d];
     }
-    r.pad[0] = r.pad[1] = 0.0f;
-    ef32[t] = r;
   }
-  if (t < ncf) {
-    const CFRec& a = cf[t];
-    CFRecF r;
-    for (int k = 0; k < 3; ++k) r.un[k] = float(a.un[k]);
-    r.area = float(a.area);
-    r.aod = float(a.aod);
-    r.delta = float(a.delta);
-    r.pad[0] = r.pad[1] = 0.0f;
-    cf32[t] = r;
+  if (k < Q) {
+    const int f = fid[eofq[k]];
+    const CFRec r = cf[f & kFidMask];
+    const double sg = (f < 0) ? -1.0 : 1.0;
+    for (int d = 0; d < 3; ++d) qg[d * Q + k] = sg * r.un[d];
+    qg[3 * Q + k] = r.area;
+    qg[4 * Q + k] = r.aod;
+    qg[5 * Q + k] = r.delta;
   }
+}
+
+// FP32 copies of the entry geometry and gradient coefficients (mixed form)
+__global__ void k_geom32(long long ne, long long nq, long long nc, const double* __restrict__ en,
+                         const double* __restrict__ qg, const double* __restrict__ gx,
+                         const double* __restrict__ gy, const double* __restrict__ gz, float* en32,
+                         float* qg32, float* gx32, float* gy32, float* gz32) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < ne) en32[t] = float(en[t]);
+  if (t < nq) qg32[t] = float(qg[t]);
   if (t < nc) {
     gx32[t] = float(gx[t]);
     gy32[t] = float(gy[t]);
@@ -853,19 +1090,17 @@ __global__ void k_cfl_cells(MeshDev m, StateDev s, const int* __restrict__ perm,
   };
   double ui[3], si;
   vel(i, ui, si);
-  const long long b = m.off[i], ec = b + m.ncomp[i];
+  const long long b = m.off[i], q0 = m.qoff[i], q1 = m.qoff[i + 1];
   double cfl = 0.0;
-  for (long long k = b; k < ec; ++k) {
-    const int j = m.nbr[k];
-    const int f = m.fid[k];
-    const double sg = (f < 0) ? -1.0 : 1.0;
-    const CFRec& cr = m.cf[f & kFidMask];
-    const double un[3] = {sg * cr.un[0], sg * cr.un[1], sg * cr.un[2]};
+  for (long long q = q0; q < q1; ++q) {
+    const int j = m.nbr[b + (q - q0)];
+    const double un[3] = {m.qg[q], m.qg[m.Q + q], m.qg[2 * m.Q + q]};
+    const double area = m.qg[3 * m.Q + q];
     double uj[3], sj;
     vel(j, uj, sj);
-    const double undA = 0.5 * cr.area * ((ui[0] * un[0] + ui[1] * un[1] + ui[2] * un[2]) +
-                                         (uj[0] * un[0] + uj[1] * un[1] + uj[2] * un[2]));
-    cfl += fabs(undA) + cr.area * (0.5 * (si + sj));
+    const double undA = 0.5 * area * ((ui[0] * un[0] + ui[1] * un[1] + ui[2] * un[2]) +
+                                      (uj[0] * un[0] + uj[1] * un[1] + uj[2] * un[2]));
+    cfl += fabs(undA) + area * (0.5 * (si + sj));
   }
   out[perm[i]] = cfl * (0.5 * dt * m.inv_vol[i]);
 }
@@ -891,12 +1126,15 @@ template <class T>
 int dalloc(T** p, size_t n, size_t* acc) {
   *p = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  // 32 bytes of slack past the end: L2 prefetches of a stream's tail are
+  // rounded up to 16 bytes
+  const size_t bytes = ((n * sizeof(T) + 15) & ~size_t(15)) + 32;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
   if (e != cudaSuccess) {
     g_err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? CGX_E_OOM : CGX_E_CUDA;
   }
-  if (acc) *acc += n * sizeof(T);
+  if (acc) *acc += bytes;
   return CGX_OK;
 }
 
@@ -923,11 +1161,14 @@ inline uint64_t spread3(uint64_t x) {  // 21 bits -> every third bit
 struct cgx_mesh {
   int device = 0;
   int N = 0, ncv_g2 = 0;
-  long long nef = 0, ncf = 0, nc_dir = 0;  // record counts (for the FP32 copies)
+  long long nc_dir = 0;  // gradient entries (for the FP32 copies)
   bool have32 = false;
   std::vector<int> perm;  // new -> old
   MeshDev md{};
   int* d_perm = nullptr;
+  std::vector<Item> items;  // work items (host copy of md.items)
+  int max_union = 0;        // largest extended-face union of an item (records)
+  int max_cunion = 0;       // largest compact-face union of an item
   std::vector<void*> allocs;
   size_t bytes = 0;
   cgx_mesh_stats stats{};
@@ -951,6 +1192,8 @@ struct Runner {
   cudaStream_t stream = nullptr;
   Tune tune;
   cgx_precision prec = CGX_FP64;
+  int max_union = 0;            // staging sizes: largest unions over the cases
+  int max_cunion = 0;
   std::atomic<long long>* launches = nullptr;
 };
 
@@ -993,18 +1236,42 @@ int launch_check(const Runner& R, int nk) {
 
 #define RARGS R.cases, R.items, R.nitems, R.dcase
 
-// CTAs for a kernel with G rounds per item
+// rounds per item and CTAs for a kernel with G lanes per cell
+inline int rounds_host(int G) {
+  const int t = std::min(256, G * kItemCells);
+  return (G * kItemCells + t - 1) / t;
+}
 inline int grid_for(const Runner& R, int G) {
-  return R.nitems_host >= 0 ? std::max(1, R.nitems_host * G) : R.grid;
+  return R.nitems_host >= 0 ? std::max(1, R.nitems_host * rounds_host(G)) : R.grid;
+}
+// the face-flux kernels take one item per CTA
+inline int grid_staged(const Runner& R) { return R.nitems_host >= 0 ? std::max(1, R.nitems_host) : R.grid; }
+
+// dynamic shared memory of the staged face-flux kernels
+inline size_t smem_ext(const Runner& R) {
+  return size_t(R.prec == CGX_MIXED ? swz_chunks<2>(R.max_union) : swz_chunks<4>(R.max_union)) * 16;
+}
+inline size_t smem_grad(const Runner& R) {
+  return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_cunion) : swz_chunks<2>(R.max_cunion)) * 16;
+}
+inline size_t smem_end(const Runner& R) {
+  return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_union) + swz_chunks<2>(R.max_cunion)
+                                    : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) *
+         16;
+}
+inline size_t smem_comp(const Runner& R) {
+  return size_t(R.prec == CGX_MIXED ? swz_chunks<2>(R.max_cunion) + swz_chunks<4>(R.max_cunion)
+                                    : swz_chunks<4>(R.max_cunion) + swz_chunks<8>(R.max_cunion)) *
+         16;
 }
 
 int enqueue_prim(const Runner& R, int nw, const double* w, double dt_arg, bool writeQ) {
   if (R.direct)
-    k_rk_prim<true><<<grid_for(R, 1), 256, 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0,
-                                                          w ? w[2] : 0.0, dt_arg, writeQ ? 1 : 0);
+    k_rk_prim<true><<<grid_for(R, 1), kThreads<1>(), 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0,
+                                                                     w ? w[2] : 0.0, dt_arg, writeQ ? 1 : 0);
   else
-    k_rk_prim<false><<<grid_for(R, 1), 256, 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0, w ? w[2] : 0.0, dt_arg,
-                                          writeQ ? 1 : 0);
+    k_rk_prim<false><<<grid_for(R, 1), kThreads<1>(), 0, R.stream>>>(RARGS, nw, w ? w[0] : 0.0, w ? w[1] : 0.0,
+                                                                      w ? w[2] : 0.0, dt_arg, writeQ ? 1 : 0);
   return launch_check(R, 1);
 }
 
@@ -1013,30 +1280,107 @@ int enqueue_prim(const Runner& R, int nw, const double* w, double dt_arg, bool w
 template <int G, bool MIX, bool DIRECT>
 void launch_grad_d(const Runner& R) {
   if (MIX)
-    k_grad_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS);
+    k_grad_f<G, DIRECT><<<grid_staged(R), 256, smem_grad(R), R.stream>>>(RARGS);
   else
-    k_grad<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS);
+    k_grad<G, DIRECT><<<grid_staged(R), 256, smem_grad(R), R.stream>>>(RARGS);
 }
 template <int G, bool MIX, bool DIRECT>
 void launch_ext_d(const Runner& R, int st) {
   if (MIX)
-    k_rhs_ext_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+    k_rhs_ext_f<G, DIRECT><<<grid_staged(R), 256, smem_ext(R), R.stream>>>(RARGS, st);
   else
-    k_rhs_ext<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+    k_rhs_ext<G, DIRECT><<<grid_staged(R), 256, smem_ext(R), R.stream>>>(RARGS, st);
 }
 template <int G, bool MIX, bool DIRECT>
 void launch_comp_d(const Runner& R, int st) {
   if (MIX)
-    k_rhs_comp_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+    k_rhs_comp_f<G, DIRECT><<<grid_staged(R), 256, smem_comp(R), R.stream>>>(RARGS, st);
   else
-    k_rhs_comp<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, st);
+    k_rhs_comp<G, DIRECT><<<grid_staged(R), 256, smem_comp(R), R.stream>>>(RARGS, st);
 }
 template <int G, bool MIX, bool DIRECT>
 void launch_end_d(const Runner& R, int mode) {
   if (MIX)
-    k_step_end_f<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, mode);
+    k_step_end_f<G, DIRECT><<<grid_staged(R), 256, smem_end(R), R.stream>>>(RARGS, mode);
   else
-    k_step_end<G, DIRECT><<<grid_for(R, G), 256, 0, R.stream>>>(RARGS, mode);
+    k_step_end<G, DIRECT><<<grid_staged(R), 256, smem_end(R), R.stream>>>(RARGS, mode);
+}
+
+// The staged kernels may use more than the default 48 KB of dynamic shared
+// memory; raise their limit on the current device (once per device) to the
+// opt-in maximum less their static shared memory.
+int g_smem_optin = 0;
+template <class K>
+void allow_dyn_smem(K kernel) {
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       g_smem_optin - int(fa.sharedSizeBytes));
+}
+template <int G, bool DIRECT>
+void allow_smem_ext() {
+  allow_dyn_smem(k_rhs_ext<G, DIRECT>);
+  allow_dyn_smem(k_rhs_ext_f<G, DIRECT>);
+}
+template <int G, bool DIRECT>
+void allow_smem_end() {
+  allow_dyn_smem(k_step_end<G, DIRECT>);
+  allow_dyn_smem(k_step_end_f<G, DIRECT>);
+}
+template <int G, bool DIRECT>
+void allow_smem_grad() {
+  allow_dyn_smem(k_grad<G, DIRECT>);
+  allow_dyn_smem(k_grad_f<G, DIRECT>);
+}
+template <int G, bool DIRECT>
+void allow_smem_comp() {
+  allow_dyn_smem(k_rhs_comp<G, DIRECT>);
+  allow_dyn_smem(k_rhs_comp_f<G, DIRECT>);
+}
+std::mutex g_smem_mu;
+unsigned long long g_smem_done = 0;
+int prepare_kernels(int device) {
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  if (device < 0 || device >= 64 || ((g_smem_done >> device) & 1ULL)) return CGX_OK;
+  CK(cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  allow_smem_ext<4, true>();
+  allow_smem_ext<4, false>();
+  allow_smem_ext<8, true>();
+  allow_smem_ext<8, false>();
+  allow_smem_ext<16, true>();
+  allow_smem_ext<16, false>();
+  allow_smem_ext<32, true>();
+  allow_smem_ext<32, false>();
+  allow_smem_comp<2, true>();
+  allow_smem_comp<2, false>();
+  allow_smem_comp<4, true>();
+  allow_smem_comp<4, false>();
+  allow_smem_comp<8, true>();
+  allow_smem_comp<8, false>();
+  allow_smem_comp<16, true>();
+  allow_smem_comp<16, false>();
+  allow_smem_grad<1, true>();
+  allow_smem_grad<1, false>();
+  allow_smem_grad<2, true>();
+  allow_smem_grad<2, false>();
+  allow_smem_grad<4, true>();
+  allow_smem_grad<4, false>();
+  allow_smem_grad<8, true>();
+  allow_smem_grad<8, false>();
+  allow_smem_grad<16, true>();
+  allow_smem_grad<16, false>();
+  allow_smem_end<1, true>();
+  allow_smem_end<1, false>();
+  allow_smem_end<4, true>();
+  allow_smem_end<4, false>();
+  allow_smem_end<8, true>();
+  allow_smem_end<8, false>();
+  allow_smem_end<16, true>();
+  allow_smem_end<16, false>();
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CGX_E_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  g_smem_done |= 1ULL << device;
+  return CGX_OK;
 }
 template <int G, bool MIX>
 void launch_grad(const Runner& R) {
@@ -1135,8 +1479,27 @@ int tune_bucket(long long ncells, cgx_precision prec) {
 // keep the fastest; results are cached per size bucket (log2 of the cell
 // count) and precision.  All candidates compute the same values (only the
 // order of the per-cell sums changes), and none changes the state.
+// CGX_TUNE="ext,comp,grad,end" (lanes per cell) skips the timing and fixes
+// the lane counts, e.g. to profile one variant.
+bool fixed_tune(Tune* t) {
+  const char* e = std::getenv("CGX_TUNE");
+  if (!e) return false;
+  int a, b, c, d;
+  if (std::sscanf(e, "%d,%d,%d,%d", &a, &b, &c, &d) != 4) return false;
+  auto ok = [](int g, std::initializer_list<int> allowed) {
+    for (int x : allowed)
+      if (g == x) return true;
+    return false;
+  };
+  if (!ok(a, {4, 8, 16, 32}) || !ok(b, {2, 4, 8, 16}) || !ok(c, {1, 2, 4, 8, 16}) || !ok(d, {1, 4, 8, 16}))
+    return false;
+  *t = Tune{a, b, c, d};
+  return true;
+}
+
 int autotune(Runner& R, long long ncells) {
   const int bucket = tune_bucket(ncells, R.prec);
+  if (fixed_tune(&R.tune)) return CGX_OK;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(bucket);
@@ -1525,58 +1888,193 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       cc[i] = make_double4(std::pow(v, 1.0 / 3.0), std::pow(v, 2.0 / 3.0), d->dcmag_hat_cv[o],
                            d->sa_to_vol_ratio[o]);
     }
-    // ---- upload
+    // ---- work items (runs of consecutive cells) and their halos; an item
+    // whose neighbour unions exceed the shared-memory budget is split
+    std::vector<Item> items;
+    std::vector<int> hcell, chcell;
+    std::vector<unsigned short> lidx(std::max(cell_off[N], 1LL)), clidx;
+    std::vector<long long> qoff(N + 1, 0);
+    for (int i = 0; i < N; ++i) qoff[i + 1] = qoff[i] + ncomp[i];
+    clidx.resize(std::max(qoff[N], 1LL));
+    std::vector<unsigned short> cglidx(std::max(coff[N], 1LL));
+    int max_u = 0, max_cu = 0;
+    {
+      std::vector<int> mark(N, -1), slot(N, 0), cmark(N, -1), cslot(N, 0);
+      std::vector<int> halo, chalo;
+      // halo of [c0, c0+nc): cells outside it reached by its entries
+      auto unions = [&](int c0, int nc, int tag) {
+        halo.clear();
+        chalo.clear();
+        for (int i = c0; i < c0 + nc; ++i)
+          for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
+            const int j = e_nbr[k];
+            if (j >= c0 && j < c0 + nc) continue;
+            if (mark[j] != tag) {
+              mark[j] = tag;
+              halo.push_back(j);
+            }
+            if (k < cell_off[i] + ncomp[i] && cmark[j] != tag) {
+              cmark[j] = tag;
+              chalo.push_back(j);
+            }
+          }
+        // the gradient stencil (cvocv) reads the compact union too
+        for (int i = c0; i < c0 + nc; ++i)
+          for (long long k = coff[i]; k < coff[i + 1]; ++k) {
+            const int j = c_nbr[k];
+            if (j >= c0 && j < c0 + nc) continue;
+            if (cmark[j] != tag) {
+              cmark[j] = tag;
+              chalo.push_back(j);
+            }
+          }
+        std::sort(halo.begin(), halo.end());
+        std::sort(chalo.begin(), chalo.end());
+      };
+      int tag = 0;
+      std::vector<std::pair<int, int>> todo;
+      for (int c0 = N - (N - 1) % kItemCells - 1; c0 >= 0; c0 -= kItemCells)
+        todo.push_back({c0, std::min(kItemCells, N - c0)});
+      while (!todo.empty()) {
+        const auto [c0, nc] = todo.back();
+        todo.pop_back();
+        unions(c0, nc, ++tag);
+        const int nu = nc + int(halo.size()), ncu = nc + int(chalo.size());
+        if ((nu > kMaxUnionExt || ncu > kMaxUnionComp) && nc > 1) {
+          const int h1 = nc / 2;  // split, first half processed first
+          todo.push_back({c0 + h1, nc - h1});
+          todo.push_back({c0, h1});
+          continue;
+        }
+        if (nu > kMaxUnionExt || ncu > kMaxUnionComp)
+          return bail(fail(CGX_E_ARG, "a cell has more neighbours than the face kernels can stage"));
+        Item it{0, c0, nc, int(items.size()), int(hcell.size()), int(halo.size()), int(chcell.size()),
+                int(chalo.size())};
+        for (size_t t = 0; t < halo.size(); ++t) slot[halo[t]] = nc + int(t);
+        for (size_t t = 0; t < chalo.size(); ++t) cslot[chalo[t]] = nc + int(t);
+        for (int i = c0; i < c0 + nc; ++i)
+          for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
+            const int j = e_nbr[k];
+            const bool in = j >= c0 && j < c0 + nc;
+            lidx[k] = (unsigned short)(in ? j - c0 : slot[j]);
+            const long long t = k - cell_off[i];
+            if (t < ncomp[i]) clidx[qoff[i] + t] = (unsigned short)(in ? j - c0 : cslot[j]);
+          }
+        for (int i = c0; i < c0 + nc; ++i)
+          for (long long k = coff[i]; k < coff[i + 1]; ++k) {
+            const int j = c_nbr[k];
+            cglidx[k] = (unsigned short)((j >= c0 && j < c0 + nc) ? j - c0 : cslot[j]);
+          }
+        hcell.insert(hcell.end(), halo.begin(), halo.end());
+        chcell.insert(chcell.end(), chalo.begin(), chalo.end());
+        if (hcell.size() > size_t(0x7ffffff0) || chcell.size() > size_t(0x7ffffff0))
+          return bail(fail(CGX_E_ARG, "mesh too large"));
+        items.push_back(it);
+        max_u = std::max(max_u, nu);
+        max_cu = std::max(max_cu, ncu);
+      }
+    }
+    if (hcell.empty()) hcell.push_back(0);
+    if (chcell.empty()) chcell.push_back(0);
+    // ---- upload; the per-face records are expanded on the device into the
+    // per-entry planes and then released
     size_t* acc = &M->bytes;
     int rc;
-    long long *d_off, *d_coff;
-    int *d_ncomp, *d_nbr, *d_fid, *d_cnbr;
-    double *d_gx, *d_gy, *d_gz, *d_vol, *d_ivol;
-    EFRec* d_ef;
-    CFRec* d_cf;
+    const long long E = cell_off[N];
+    const long long Qn = qoff[N];
+    long long *d_off, *d_qoff, *d_coff;
+    int *d_nbr, *d_cnbr, *d_hcell, *d_chcell;
+    unsigned short *d_lidx, *d_clidx, *d_cglidx;
+    double *d_gx, *d_gy, *d_gz, *d_vol, *d_ivol, *d_en, *d_qg;
     double4* d_cc;
+    Item* d_items;
 #define UP(ptr, vec)                                   \
   if ((rc = dupload(&ptr, vec, acc))) return bail(rc); \
   M->allocs.push_back(ptr);
+    UP(d_items, items);
+    UP(d_hcell, hcell);
+    UP(d_chcell, chcell);
     UP(d_off, cell_off);
-    UP(d_ncomp, ncomp);
+    UP(d_qoff, qoff);
     UP(d_nbr, e_nbr);
-    UP(d_fid, e_fid);
+    UP(d_lidx, lidx);
+    UP(d_clidx, clidx);
+    UP(d_cglidx, cglidx);
     UP(d_coff, coff);
     UP(d_cnbr, c_nbr);
     UP(d_gx, gx);
     UP(d_gy, gy);
     UP(d_gz, gz);
-    UP(d_ef, efr);
-    UP(d_cf, cfr);
     UP(d_vol, vol);
     UP(d_ivol, inv_vol);
     UP(d_cc, cc);
     UP(M->d_perm, perm);
 #undef UP
+    if ((rc = dalloc(&d_en, 6 * size_t(std::max(E, 1LL)), acc))) return bail(rc);
+    M->allocs.push_back(d_en);
+    if ((rc = dalloc(&d_qg, 6 * size_t(std::max(Qn, 1LL)), acc))) return bail(rc);
+    M->allocs.push_back(d_qg);
+    {
+      std::vector<long long> eofq(std::max(Qn, 1LL), 0);
+      for (int i = 0; i < N; ++i)
+        for (int t = 0; t < ncomp[i]; ++t) eofq[qoff[i] + t] = cell_off[i] + t;
+      int* t_fid = nullptr;
+      EFRec* t_ef = nullptr;
+      CFRec* t_cf = nullptr;
+      long long* t_eofq = nullptr;
+      auto free_tmp = [&] {
+        cudaFree(t_fid);
+        cudaFree(t_ef);
+        cudaFree(t_cf);
+        cudaFree(t_eofq);
+      };
+      if ((rc = dupload(&t_fid, e_fid, nullptr)) || (rc = dupload(&t_ef, efr, nullptr)) ||
+          (rc = dupload(&t_cf, cfr, nullptr)) || (rc = dupload(&t_eofq, eofq, nullptr))) {
+        free_tmp();
+        return bail(rc);
+      }
+      const long long nmax = std::max(E, Qn);
+      if (nmax > 0)
+        k_expand_entries<<<int((nmax + 255) / 256), 256>>>(E, Qn, t_fid, t_ef, t_cf, t_eofq, d_en, d_qg);
+      const cudaError_t ke = cudaGetLastError();
+      const cudaError_t se = cudaDeviceSynchronize();
+      free_tmp();
+      if (ke != cudaSuccess || se != cudaSuccess)
+        return bail(fail(CGX_E_CUDA, std::string("entry expansion: ") +
+                                         cudaGetErrorString(ke != cudaSuccess ? ke : se)));
+    }
     MeshDev& md = M->md;
     md.N = N;
+    md.nitems = int(items.size());
+    md.E = E;
+    md.Q = Qn;
+    md.items = d_items;
+    md.hcell = d_hcell;
+    md.chcell = d_chcell;
     md.off = d_off;
-    md.ncomp = d_ncomp;
+    md.qoff = d_qoff;
     md.nbr = d_nbr;
-    md.fid = d_fid;
+    md.lidx = d_lidx;
+    md.clidx = d_clidx;
+    md.cglidx = d_cglidx;
+    md.en = d_en;
+    md.qg = d_qg;
     md.coff = d_coff;
     md.cnbr = d_cnbr;
     md.gcx = d_gx;
     md.gcy = d_gy;
     md.gcz = d_gz;
-    md.ef = d_ef;
-    md.cf = d_cf;
     md.vol = d_vol;
     md.inv_vol = d_ivol;
     md.cc = d_cc;
-    md.ef32 = nullptr;
-    md.cf32 = nullptr;
+    md.en32 = nullptr;
+    md.qg32 = nullptr;
     md.gcx32 = md.gcy32 = md.gcz32 = nullptr;
-    M->nef = nef;
-    M->ncf = ncf;
+    M->items = items;
+    M->max_union = max_u;
+    M->max_cunion = max_cu;
     M->nc_dir = coff[N];
-    long long n_ef_dir = cell_off[N], n_cf_dir = 0;
-    for (int i = 0; i < N; ++i) n_cf_dir += ncomp[i];
+    long long n_ef_dir = cell_off[N], n_cf_dir = qoff[N];
     M->stats.ncv = N;
     M->stats.n_ef_dir = n_ef_dir;
     M->stats.n_cf_dir = n_cf_dir;
@@ -1615,6 +2113,7 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
       !(p->Pr_t > 0) || p->dt_mode < 0 || p->dt_mode > 2 || p->sgs_model < 0 || p->sgs_model > 1)
     return fail(CGX_E_ARG, "cgx_solver_create: invalid parameters");
   CK(cudaSetDevice(m->device));
+  if (int rc0 = prepare_kernels(m->device)) return rc0;
   cgx_solver* s = new cgx_solver();
   s->mesh = m;
   s->prm = *p;
@@ -1642,7 +2141,7 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   ph.h_ref = ph.R * p->gamma / (p->gamma - 1.0) * p->T_ref;
   const size_t N = m->N;
   s->nblocks = int((N + kBlock - 1) / kBlock);
-  s->nitems = int((N + kItemCells - 1) / kItemCells);
+  s->nitems = m->md.nitems;
   auto bail = [&](int rc) {
     for (void* q : s->allocs) cudaFree(q);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1665,36 +2164,33 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   AL(sd.rhs, 15 * N);
   if (prec == CGX_MIXED) {
     sd.L = nullptr;
-    sd.P = nullptr;
-    sd.G = nullptr;
+    sd.V = nullptr;
     sd.Q = nullptr;
     AL(sd.LF, N);
-    AL(sd.PF, N);
-    AL(sd.GF, N);
+    AL(sd.VF, N);
     AL(sd.QF, N);
     if (!m->have32) {
-      EFRecF* ef32;
-      CFRecF* cf32;
-      float *gx32, *gy32, *gz32;
+      float *en32, *qg32, *gx32, *gy32, *gz32;
       size_t* mb = &m->bytes;
-      if ((rc = dalloc(&ef32, m->nef, mb))) return bail(rc);
-      m->allocs.push_back(ef32);
-      if ((rc = dalloc(&cf32, std::max<long long>(m->ncf, 1), mb))) return bail(rc);
-      m->allocs.push_back(cf32);
+      const MeshDev& md = m->md;
+      if ((rc = dalloc(&en32, 6 * size_t(std::max(md.E, 1LL)), mb))) return bail(rc);
+      m->allocs.push_back(en32);
+      if ((rc = dalloc(&qg32, 6 * size_t(std::max(md.Q, 1LL)), mb))) return bail(rc);
+      m->allocs.push_back(qg32);
       if ((rc = dalloc(&gx32, m->nc_dir, mb))) return bail(rc);
       m->allocs.push_back(gx32);
       if ((rc = dalloc(&gy32, m->nc_dir, mb))) return bail(rc);
       m->allocs.push_back(gy32);
       if ((rc = dalloc(&gz32, m->nc_dir, mb))) return bail(rc);
       m->allocs.push_back(gz32);
-      const long long nmax = std::max(m->nef, std::max(m->ncf, m->nc_dir));
-      k_geom32<<<int((nmax + 255) / 256), 256, 0, s->stream>>>(int(m->nef), int(m->ncf), m->nc_dir, m->md.ef,
-                                                               m->md.cf, m->md.gcx, m->md.gcy, m->md.gcz,
-                                                               ef32, cf32, gx32, gy32, gz32);
+      const long long nmax = std::max(6 * md.E, std::max(6 * md.Q, m->nc_dir));
+      k_geom32<<<int((nmax + 255) / 256), 256, 0, s->stream>>>(6 * md.E, 6 * md.Q, m->nc_dir, md.en, md.qg,
+                                                               md.gcx, md.gcy, md.gcz, en32, qg32, gx32,
+                                                               gy32, gz32);
       if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s->stream) != cudaSuccess)
         return bail(fail(CGX_E_CUDA, "FP32 geometry conversion failed"));
-      m->md.ef32 = ef32;
-      m->md.cf32 = cf32;
+      m->md.en32 = en32;
+      m->md.qg32 = qg32;
       m->md.gcx32 = gx32;
       m->md.gcy32 = gy32;
       m->md.gcz32 = gz32;
@@ -1703,12 +2199,10 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     }
   } else {
     sd.LF = nullptr;
-    sd.PF = nullptr;
-    sd.GF = nullptr;
+    sd.VF = nullptr;
     sd.QF = nullptr;
     AL(sd.L, N);
-    AL(sd.P, N);
-    AL(sd.G, N);
+    AL(sd.V, N);
     AL(sd.Q, N);
   }
   AL(sd.ctl, 1);
@@ -1723,17 +2217,12 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
 #undef AL
   const bool zero_ok =
       cudaMemsetAsync(sd.rhs, 0, 15 * N * sizeof(double), s->stream) == cudaSuccess &&
-      (prec == CGX_MIXED
-           ? (cudaMemsetAsync(sd.PF, 0, N * sizeof(PRecF), s->stream) == cudaSuccess &&
-              cudaMemsetAsync(sd.GF, 0, N * sizeof(GRecF), s->stream) == cudaSuccess)
-           : (cudaMemsetAsync(sd.P, 0, N * sizeof(PRec), s->stream) == cudaSuccess &&
-              cudaMemsetAsync(sd.G, 0, N * sizeof(GRec), s->stream) == cudaSuccess));
+      (prec == CGX_MIXED ? cudaMemsetAsync(sd.VF, 0, N * sizeof(VRecF), s->stream) == cudaSuccess
+                         : cudaMemsetAsync(sd.V, 0, N * sizeof(VRec), s->stream) == cudaSuccess);
   if (!zero_ok)
     return bail(fail(CGX_E_CUDA, "cudaMemset failed"));
-  {  // work list (one item per kItemCells cells) and the one-entry case table
-    std::vector<Item> items(s->nitems);
-    for (int k = 0; k < s->nitems; ++k)
-      items[k] = Item{0, k * kItemCells, int(std::min<size_t>(kItemCells, N - size_t(k) * kItemCells)), k};
+  {  // work list (the mesh's items) and the one-entry case table
+    const std::vector<Item>& items = m->items;
     CaseDev cd{};
     cd.m = m->md;
     cd.s = sd;
@@ -1755,6 +2244,8 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     R.dcase = cd;
     R.stream = s->stream;
     R.prec = prec;
+    R.max_union = m->max_union;
+    R.max_cunion = m->max_cunion;
     R.launches = &s->launches;
   }
   s->bytes = bytes;
@@ -2114,18 +2605,17 @@ extern "C" long long cgx_launch_count(const cgx_solver* s) { return s ? s->launc
 namespace {
 
 // device bytes a solver of N cells allocates (cgx_solver_create)
-size_t solver_bytes(long long N, cgx_precision prec) {
-  const long long nitems = (N + kItemCells - 1) / kItemCells;
+size_t solver_bytes(long long N, long long nitems, cgx_precision prec) {
   const long long nblocks = (N + kBlock - 1) / kBlock;
-  size_t rec = (prec == CGX_MIXED) ? sizeof(LRecF) + sizeof(PRecF) + sizeof(GRecF) + sizeof(QRecF)
-                                   : sizeof(LRec) + sizeof(PRec) + sizeof(GRec) + sizeof(QRec);
+  size_t rec = (prec == CGX_MIXED) ? sizeof(LRecF) + sizeof(VRecF) + sizeof(QRecF)
+                                   : sizeof(LRec) + sizeof(VRec) + sizeof(QRec);
   return size_t(N) * (5 + 15 + 9 + 10) * sizeof(double) + size_t(N) * rec + sizeof(Ctl) +
          size_t(2 * nitems) * kMaxRounds * sizeof(double) + sizeof(CaseDev) + size_t(nitems) * sizeof(Item) +
          sizeof(int) + size_t(5 * nblocks + 5) * sizeof(double) + 4096;
 }
 
 size_t mesh32_bytes(const cgx_mesh* m) {
-  return size_t(m->nef) * sizeof(EFRecF) + size_t(std::max<long long>(m->ncf, 1)) * sizeof(CFRecF) +
+  return 6 * size_t(std::max(m->md.E, 1LL)) * sizeof(float) + 6 * size_t(std::max(m->md.Q, 1LL)) * sizeof(float) +
          size_t(m->nc_dir) * 3 * sizeof(float);
 }
 
@@ -2182,13 +2672,18 @@ void batch_free_graph(cgx_batch* b) {
 int batch_rebuild(cgx_batch* b) {
   std::vector<Item> items;
   long long cells = 0;
+  int mu = 0, mcu = 0;
   for (size_t k = 0; k < b->slots.size(); ++k) {
     const BatchCase& c = b->slots[k];
     if (!c.s || c.finished) continue;
-    const int N = c.s->mesh->N;
-    cells += N;
-    for (int it = 0; it < c.s->nitems; ++it)
-      items.push_back(Item{int(k), it * kItemCells, std::min(kItemCells, N - it * kItemCells), it});
+    cells += c.s->mesh->N;
+    mu = std::max(mu, c.s->mesh->max_union);
+    mcu = std::max(mcu, c.s->mesh->max_cunion);
+    for (const Item& mi : c.s->mesh->items) {
+      Item it = mi;
+      it.c = int(k);
+      items.push_back(it);
+    }
   }
   if (int(items.size()) > b->item_cap) {
     int cap = std::max(1024, b->item_cap);
@@ -2213,6 +2708,11 @@ int batch_rebuild(cgx_batch* b) {
   b->nitems = int(items.size());
   b->active_cells = cells;
   b->run.items = b->d_items;
+  if (mu != b->run.max_union || mcu != b->run.max_cunion) {
+    b->run.max_union = mu;  // shared-memory sizes of the staged kernels
+    b->run.max_cunion = mcu;
+    batch_free_graph(b);
+  }
   b->dirty = false;
   return CGX_OK;
 }
@@ -2242,6 +2742,7 @@ extern "C" int cgx_batch_create(int device, cgx_precision prec, int max_cases, s
     return fail(CGX_E_ARG, "cgx_batch_create: invalid argument");
   *out = nullptr;
   CK(cudaSetDevice(device));
+  if (int rc0 = prepare_kernels(device)) return rc0;
   cgx_batch* b = new cgx_batch();
   b->device = device;
   b->prec = prec;
@@ -2309,7 +2810,7 @@ extern "C" int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, 
       break;
     }
   if (slot < 0) return fail(CGX_E_OOM, "cgx_batch_add: all case slots in use");
-  size_t need = solver_bytes(mesh->N, b->prec);
+  size_t need = solver_bytes(mesh->N, mesh->md.nitems, b->prec);
   if (!b->mesh_refs.count(mesh)) need += mesh->bytes;
   if (b->prec == CGX_MIXED && !mesh->have32) need += mesh32_bytes(mesh);
   if (b->used + need > b->budget) return fail(CGX_E_OOM, "cgx_batch_add: HBM budget exceeded");

@@ -5,16 +5,29 @@
 //   state    rho[N], u0[N], u1[N], u2[N], rhoE[N]          (SoA, FP64)
 //   rhs      rhs[stage][5][N]                              (SoA, FP64)
 //   LRec[N]  {u0,u1,u2, 1/rho, p, h, rho, sos}  64 B       neighbour gathers
-//   PRec[N]  {mu_total, loc_total, a_sgs, fgr, symh, symp, -, -}  64 B (per step)
-//   GRec[N]  dudx[3][3] + pad                   80 B
+//   VRec[N]  {mu_total, loc_total, a_sgs, fgr, symh, symp, dudx[9], -}
+//            128 B: lagged properties (per step) and the velocity gradient
+//            (per stage), one 128 B line per neighbour gather
 //   QRec[N]  {log(p/p_ref), p, 1/rho, 1/(R T)}  32 B (Gibbs sensor)
-//   extended faces: one 48 B record {n[3], c[3] (halved)} per face;
-//   compact faces (ids [0, n_cf) of the same numbering) one 48 B record
-//   {unit_n[3], area, area_over_delta, area/area_over_delta}.
-//   Per-cell face lists (CSR over cells): entries {nbr cell, face id |
-//   0x80000000 when the cell is the face's second cell}; a cell's compact
-//   faces come first.  The lists are walked by a group of G lanes per cell.
-//   Gradient coefficients per directed compact entry in a second CSR.
+//   Work items: runs of at most kItemCells consecutive cells.  For each item
+//   the mesh lists its halo, the cells outside the item that its cells'
+//   extended faces reach (hcell) and, separately, those their compact faces
+//   reach (chcell), ascending.  The face-flux kernels copy the packed records
+//   of an item's cells and halo into shared memory once, then every face reads
+//   its neighbour there through a 16-bit local index (the item's own cells
+//   first, then the halo in list order).
+//   Extended-face entries: a CSR over cells (off[N+1]) of directed entries,
+//   one per (cell, face) pair, a cell's compact faces first.  Per entry: the
+//   local index lidx[k], the global neighbour nbr[k] and six FP64 planes
+//   en[d*E + k] {normal along the entry (n[3], negated for the face's second
+//   cell), the halved c vector (c[3])}, streamed contiguously by the cell's G
+//   lanes.
+//   Compact-face entries: the first ncomp(i) = qoff[i+1]-qoff[i] extended
+//   entries of each cell; their local indices in the compact union clidx[q]
+//   and six FP64 planes qg[d*Q + q] {unit normal along the entry (3), area,
+//   area_over_delta, area/area_over_delta} at q = qoff[i] + t.
+//   Gradient coefficients per directed compact entry in a second CSR (coff,
+//   the reference's cvocv order).
 #ifndef CGX_KERNELS_CUH
 #define CGX_KERNELS_CUH
 
@@ -25,7 +38,7 @@ namespace cgx {
 constexpr int kRevBit = 0x80000000;
 constexpr int kFidMask = 0x7fffffff;
 
-struct alignas(16) LRec {
+struct alignas(32) LRec {
   double u[3];
   double sp_vol;
   double p;
@@ -34,28 +47,27 @@ struct alignas(16) LRec {
   double sos;
 };
 
-struct alignas(16) PRec {
+// per-cell viscous record: lagged properties then dudx[i][j] at g[3*i+j]
+struct alignas(128) VRec {
   double mu_total;
   double loc_total;
   double a_sgs;
   double fgr;
   double symh;
   double symp;
-  double pad0, pad1;
-};
-
-struct alignas(16) GRec {
-  double g[9];  // dudx[i][j] at 3*i+j
+  double g[9];
   double pad;
 };
 
-struct alignas(16) QRec {
+struct alignas(32) QRec {
   double logp;
   double p;
   double iv;  // 1/rho
   double ib;  // 1/(R T)
 };
 
+// geometry of one face as built on the host (expanded into the per-entry
+// planes on the device)
 struct alignas(16) EFRec {
   double n[3];
   double c[3];  // already halved
@@ -71,7 +83,7 @@ struct alignas(16) CFRec {
 // Mixed-precision records (FP32).  Pressure and enthalpy are stored as
 // perturbations about p_ref and h_ref = R gamma/(gamma-1) T_ref so that their
 // differences keep FP32's relative precision at low Mach.
-struct alignas(16) LRecF {
+struct alignas(32) LRecF {
   float u[3];
   float sp_vol;
   float pp;  // p - p_ref
@@ -80,31 +92,14 @@ struct alignas(16) LRecF {
   float sos;
 };
 
-struct alignas(16) PRecF {
-  float mu_total, loc_total, a_sgs, fgr, symh, symp, pad0, pad1;
-};
-
-struct alignas(16) GRecF {
+struct alignas(64) VRecF {
+  float mu_total, loc_total, a_sgs, fgr, symh, symp;
   float g[9];
-  float pad[3];
+  float pad;
 };
 
 struct alignas(16) QRecF {
   float logp, pp, iv, ib;
-};
-
-struct alignas(16) EFRecF {
-  float n[3];
-  float c[3];
-  float pad[2];
-};
-
-struct alignas(16) CFRecF {
-  float un[3];
-  float area;
-  float aod;
-  float delta;
-  float pad[2];
 };
 
 struct Phys {
@@ -131,25 +126,47 @@ struct Ctl {
   int pad;
 };
 
+// A work item: up to kItemCells consecutive cells of one case and where its
+// halo lists start.
+constexpr int kItemCells = 128;
+struct alignas(32) Item {
+  int c;      // case slot in the table (0 in a mesh's own table)
+  int cell0;  // first cell
+  int ncell;  // cells in this item (<= kItemCells)
+  int idx;    // item index within its case
+  int hoff;   // extended-face halo: hcell[hoff, hoff + nh)
+  int nh;
+  int choff;  // compact-face halo: chcell[choff, choff + nch)
+  int nch;
+};
+
 struct MeshDev {
   int N;                        // owned cells
-  const long long* off;         // [N+1] extended-face CSR
-  const int* ncomp;             // [N] compact faces at the head of each list
-  const int* nbr;               // [E_dir]
-  const int* fid;               // [E_dir]
+  int nitems;                   // work items (mesh order)
+  long long E;                  // directed extended entries
+  long long Q;                  // directed compact entries
+  const Item* items;            // [nitems]
+  const int* hcell;             // extended-face halos
+  const int* chcell;            // compact-face halos
+  const long long* off;         // [N+1] extended-entry CSR
+  const long long* qoff;        // [N+1] compact-entry CSR
+  const int* nbr;               // [E] neighbour (new numbering, ghosts -> owner)
+  const unsigned short* lidx;   // [E] neighbour in the item's extended union
+  const unsigned short* clidx;  // [Q] neighbour in the item's compact union
+  const double* en;             // [6][E] n (along the entry), c/2
+  const double* qg;             // [6][Q] unit normal, area, aod, delta
   const long long* coff;        // [N+1] gradient CSR (cvocv without the diagonal)
   const int* cnbr;              // [C_dir]
+  const unsigned short* cglidx; // [C_dir] neighbour in the item's compact union
   const double* gcx;            // [C_dir]
   const double* gcy;
   const double* gcz;
-  const EFRec* ef;
-  const CFRec* cf;
   const double* vol;
   const double* inv_vol;
   const double4* cc;            // {pow(vol,1/3), pow(vol,2/3), dcmag_hat, sa_to_vol}
   // FP32 copies for the mixed-precision form (null until a mixed solver exists)
-  const EFRecF* ef32;
-  const CFRecF* cf32;
+  const float* en32;            // [6][E]
+  const float* qg32;            // [6][Q]
   const float* gcx32;
   const float* gcy32;
   const float* gcz32;
@@ -163,13 +180,11 @@ struct StateDev {
   double* rhoE;
   double* rhs;  // [3][5][N]
   LRec* L;
-  PRec* P;
-  GRec* G;
+  VRec* V;
   QRec* Q;
   // mixed-precision records (null for FP64 solvers)
   LRecF* LF;
-  PRecF* PF;
-  GRecF* GF;
+  VRecF* VF;
   QRecF* QF;
   Ctl* ctl;
   double* red;  // per-block partials: [nblocks] cfl max, [nblocks] nan
@@ -183,15 +198,6 @@ struct CaseDev {
   Phys ph;
   int nitems;  // work items of this case (partials of the per-step reduction)
   int pad;
-};
-
-// A work item: up to kItemCells consecutive cells of one case.
-constexpr int kItemCells = 256;
-struct Item {
-  int c;      // case slot in the table
-  int cell0;  // first cell
-  int ncell;  // cells in this item (<= kItemCells)
-  int idx;    // item index within its case
 };
 
 }  // namespace cgx
