@@ -44,10 +44,13 @@ def bytes_model(e, f):
                                     CFL 40 + 32f, totals 40)
       calcRhs    56e + 40f + 200   (extended faces 56e, compact geometry 40f,
                                     lagged properties 48, packed state 40,
-                                    dudx 72, rhs write 40)"""
+                                    dudx 72, rhs write 40)
+    calcRhs is two kernels: k_rhs_ext (extended faces 56e, packed state 40,
+    rhs write 40) and k_rhs_comp (compact geometry 40f, lagged properties 48,
+    dudx 72)."""
     step = 3 * (504 + 56 * e + 96 * f) + (320 + 8 * e + 32 * f)
     rhs = 56 * e + 40 * f + 200
-    return step, rhs
+    return step, rhs, {"k_rhs_ext": 56 * e + 80, "k_rhs_comp": 40 * f + 120}
 
 
 def measured_peaks():
@@ -316,7 +319,7 @@ def run_cgx(args):
                  "p_linf_rel_fluct": float(np.abs(p32 - p64).max() / max(np.abs(pf).max(), 1e-300)),
                  "ke_rel": float(abs(ke32 - ke64) / ke64),
                  "ke_decay_rel": float(abs(ke32 - ke64) / max(abs(ke0 - ke64), 1e-300))}
-    step_bytes, rhs_bytes = bytes_model(e, f)
+    step_bytes, rhs_bytes, split_bytes = bytes_model(e, f)
     peak, peak_kind = measured_peaks()
     ms_step = res["fp64"]["ms"] / args.steps
     value = world * N * args.steps / (res["fp64"]["ms"] * 1e-3)
@@ -338,13 +341,24 @@ def run_cgx(args):
     el = dist.max_over_ranks(el)
     e2e = world * N * ke / el
 
-    traffic = None
+    # DRAM traffic per cell of each face kernel from a committed ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum per launch / cells),
+    # scaled to this mesh's cell count
+    traffic, per_kernel_dram = None, {}
     tp = os.path.join(ROOT, "profiles", "rhs_dram_bytes_per_cell.json")
     if os.path.exists(tp):
         try:
-            traffic = float(json.load(open(tp))["dram_bytes_per_cell"]) * N
+            tj = json.load(open(tp))
+            traffic = float(tj["dram_bytes_per_cell"]) * N
+            per_kernel_dram = {k: float(tj[k]) for k in ("k_rhs_ext", "k_rhs_comp") if k in tj}
         except Exception:
             traffic = None
+    kernels = {}
+    for kname, key in (("k_rhs_ext", "ext"), ("k_rhs_comp", "comp")):
+        if key in ktimes and ktimes[key] > 0:
+            kernels[kname] = {"launch_ms": ktimes[key], "algorithmic_bytes_per_cell": split_bytes[kname],
+                              "achieved_gbs": split_bytes[kname] * N / (ktimes[key] * 1e-3) / 1e9,
+                              "dram_bytes_per_cell": per_kernel_dram.get(kname)}
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -365,7 +379,7 @@ def run_cgx(args):
         "roofline": {"bound": "hbm", "kernel": "k_rhs_ext + k_rhs_comp (calcRhsBase)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_cell": rhs_bytes,
-                     "launch_ms": ktimes["rhs"]},
+                     "launch_ms": ktimes["rhs"], "kernels": kernels},
         "step_roofline": {"bytes_per_cell_step": step_bytes, "achieved": value / world * step_bytes / 1e9,
                           "frac": value / world * step_bytes / 1e9 / peak, "unit": "GB/s"},
         "kernel_ms": ktimes,

@@ -151,6 +151,20 @@ int cgx_set_state_primitive(cgx_solver* s, const double* rho, const double* u,
                             const double* p);
 int cgx_get_state(cgx_solver* s, double* rho, double* u, double* rhoE);
 
+/* Passive transport scalars (FP64 solvers): nsc (0..8) scalars per cell in
+ * the reference's order sc[icv*nsc + isc] (transport_scalar_vec,
+ * IdealGasSolver.hpp).  Once set, calcRhs also forms rhs_sc as
+ * calcRhsScalars does (IdealGasSolver.cpp:537-693: convective flux
+ * 0.5 (sc0 + sc1) mf on every extended face with mf its mass flux, minus the
+ * unity-Lewis diffusion on compact faces) and every rk3Step advances them as
+ * advanceScalars does (IdealGasSolver.cpp:874-892).  nsc = 0 removes them.
+ * Like the reference's storeData, NaN recovery does not restore scalars. */
+int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc);
+int cgx_get_scalars(cgx_solver* s, double* sc);
+/* rhs_sc of stage rk_stage (1..3) as the last calcRhs/step left it,
+ * [ncv][nsc] in reference order (unscaled face sums). */
+int cgx_get_rhs_sc(cgx_solver* s, int rk_stage, double* rhs_sc);
+
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */
 int cgx_init_complete(cgx_solver* s);
@@ -192,10 +206,12 @@ int cgx_synchronize(cgx_solver* s);
  * their device time from CUDA events on the solver's stream. */
 int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms);
 /* Average device time of one launch of each step kernel, measured with CUDA
- * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs),
- * ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is kept),
- * ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/CFL. */
-int cgx_kernel_times(cgx_solver* s, int reps, double ms[4]);
+ * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs, both
+ * kernels), ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is
+ * kept), ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/CFL,
+ * ms[4] the extended-face flux kernel alone, ms[5] the compact-closure kernel
+ * alone.  Overwrites the stage-0 rhs. */
+int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]);
 /* Lanes per cell chosen by the autotuner that cgx_init_complete runs (timed
  * candidates per kernel, cached per mesh-size bucket and precision):
  * out = {face fluxes, compact closures, gradient, once-per-step kernel}. */

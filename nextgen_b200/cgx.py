@@ -137,6 +137,7 @@ EXPORTS = [
     "cgx_calc_rhs", "cgx_rk3_step", "cgx_calc_cfl", "cgx_advance_solution", "cgx_step",
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
+    "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc",
 ]
 
 _LIB = None
@@ -178,6 +179,9 @@ def lib():
         "cgx_step_timed": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
         "cgx_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_get_tuning": (ctypes.c_int, [vp, c_int_p]),
+        "cgx_set_scalars": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
+        "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
+        "cgx_get_rhs_sc": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
                                              ctypes.POINTER(vp)]),
         "cgx_batch_destroy": (ctypes.c_int, [vp]),
@@ -265,6 +269,26 @@ class Solver:
         _check(lib().cgx_get_state(self.h, _dp(rho), _dp(u), _dp(rhoE)))
         return rho, u, rhoE
 
+    # -- passive transport scalars (transport_scalar_vec) ---------------------
+    def set_scalars(self, sc):
+        """Transport scalars sc[ncv][nsc] (nsc <= 8, FP64 solvers); from now
+        on calcRhs forms rhs_sc (calcRhsScalars) and the steps advance them
+        (advanceScalars).  An empty second axis removes them."""
+        sc = np.ascontiguousarray(sc, dtype=np.float64).reshape(self.ncv, -1)
+        _check(lib().cgx_set_scalars(self.h, int(sc.shape[1]), _dp(sc) if sc.size else None))
+        self.nsc = sc.shape[1]
+
+    def get_scalars(self):
+        sc = _out(self.ncv, getattr(self, "nsc", 0))
+        _check(lib().cgx_get_scalars(self.h, _dp(sc)))
+        return sc
+
+    def rhs_sc(self, rk_stage=1):
+        """rhs_sc[ncv][nsc] of a stage (unscaled face sums)."""
+        out = _out(self.ncv, getattr(self, "nsc", 0))
+        _check(lib().cgx_get_rhs_sc(self.h, int(rk_stage), _dp(out)))
+        return out
+
     # -- reference calls ----------------------------------------------------
     def initComplete(self):
         _check(lib().cgx_init_complete(self.h))
@@ -339,10 +363,11 @@ class Solver:
         return float(ms.value)
 
     def kernel_times(self, reps=5):
-        """Average ms per launch of {rhs, rk+prim, grad, step_end}."""
-        ms = np.zeros(4)
+        """Average ms per launch of {rhs (both face kernels), rk+prim, grad,
+        step_end, ext (extended-face kernel), comp (compact closures)}."""
+        ms = np.zeros(6)
         _check(lib().cgx_kernel_times(self.h, int(reps), _dp(ms)))
-        return dict(zip(("rhs", "rk_prim", "grad", "step_end"), ms.tolist()))
+        return dict(zip(("rhs", "rk_prim", "grad", "step_end", "ext", "comp"), ms.tolist()))
 
     def tuning(self):
         """Lanes per cell picked by the autotuner: ext, comp, grad, step_end."""

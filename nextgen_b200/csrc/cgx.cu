@@ -521,6 +521,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
     smem_L(smem, jl, Lj);
     double F[5];
     ext_flux(F, n, c, Li, Lj);
+    if (s.mf) s.mf[k] = F[0];  // mf[ief] of calcRhsBase, for calcRhsScalars
 #pragma unroll
     for (int q = 0; q < 5; ++q) acc[q] -= F[q];
   }
@@ -537,8 +538,11 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
 #undef PF_EXT
 }
 
+// Two CTAs per SM: the closure needs about 126 registers per thread, and at
+// three CTAs per SM (80 registers) it spills ~200 B per thread to local
+// memory, which measured 1.5x slower on the jittered 128^3 mesh.
 template <int G, bool DIRECT>
-__global__ void __launch_bounds__(256, 3) k_rhs_comp(CASE_ARGS, int stage) {
+__global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
   extern __shared__ int4 smem[];
 #define PF_COMP(it, mm, r) prefetch_round<true>(mm, mm.qg, it, r, 256 / G)
   STAGED_LOOP_BEGIN(PF_COMP)
@@ -575,6 +579,9 @@ __global__ void __launch_bounds__(256, 3) k_rhs_comp(CASE_ARGS, int stage) {
     Flux F;
     F.rho = 0.0; F.ru[0] = F.ru[1] = F.ru[2] = 0.0; F.rE = 0.0;
     compact_flux_add(F, un, area, aod, delta, Li, Lj, Vs, uf, h_f);
+    // the closure's part of the face's mass flux (compact entries are the
+    // first entries of the cell's extended list)
+    if (s.mf) s.mf[m.off[i] + (q - q0)] += F.rho;
     acc[0] -= F.rho;
     acc[1] -= F.ru[0];
     acc[2] -= F.ru[1];
@@ -592,6 +599,67 @@ __global__ void __launch_bounds__(256, 3) k_rhs_comp(CASE_ARGS, int stage) {
   STAGED_ROUNDS_END
   STAGED_LOOP_END
 #undef PF_COMP
+}
+
+// calcRhsScalars (IdealGasSolver.cpp:537-693), cell-centric over each
+// cell's extended entries after both face kernels have left the entries'
+// mass fluxes in mf: rhs_sc[i] = -sum over the entries of
+// 0.5 (sc_i + sc_j) mf_ij, minus, on compact entries, the diffusive
+// -d_coeff (sc_j - sc_i) with d_coeff = 0.5 (loc_total_i + loc_total_j)
+// area_over_delta (unity Lewis number; loc_total = loc_lam + loc_sgs).
+// A group of G lanes per cell, lane l takes entries l, l+G, ...; partial
+// sums are combined by the fixed butterfly (deterministic).  The neighbour's
+// scalars and properties are gathered from global memory (scalar transport
+// runs on single-case solvers only).
+template <int G>
+__global__ void __launch_bounds__(256) k_rhs_sc(const CaseDev c, int stage) {
+  const MeshDev& m = c.m;
+  const StateDev& s = c.s;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G, lane = t & (G - 1);
+  const bool valid = i < m.N;
+  const int nsc = s.nsc;
+  const size_t N = size_t(m.N);
+  double acc[kMaxScalars], si[kMaxScalars];
+#pragma unroll
+  for (int a = 0; a < kMaxScalars; ++a) {
+    acc[a] = 0.0;
+    si[a] = (valid && a < nsc) ? s.sc[a * N + i] : 0.0;
+  }
+  long long b = 0, e = 0;
+  int ncomp = 0;
+  double loc_i = 0.0;
+  if (valid) {
+    b = m.off[i];
+    e = m.off[i + 1];
+    ncomp = int(m.qoff[i + 1] - m.qoff[i]);
+    loc_i = s.V[i].loc_total;
+  }
+  const long long q0 = valid ? m.qoff[i] : 0;
+  for (long long k = b + lane; k < e; k += G) {
+    const int j = __ldg(m.nbr + k);
+    const double mfk = s.mf[k];
+    const int tk = int(k - b);
+    double dc = 0.0;
+    if (tk < ncomp) dc = 0.5 * (loc_i + s.V[j].loc_total) * __ldg(m.qg + 4 * m.Q + q0 + tk);
+#pragma unroll
+    for (int a = 0; a < kMaxScalars; ++a) {
+      if (a < nsc) {
+        const double sj = s.sc[a * N + j];
+        double flux = 0.5 * (si[a] + sj) * mfk;
+        flux -= dc * (sj - si[a]);
+        acc[a] -= flux;
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < kMaxScalars; ++a) acc[a] = group_sum<G>(acc[a]);
+  if (valid && lane == 0) {
+    double* r = s.rhs_sc + size_t(stage) * nsc * N;
+#pragma unroll
+    for (int a = 0; a < kMaxScalars; ++a)
+      if (a < nsc) r[a * N + i] = acc[a];
+  }
 }
 
 // packed primitive state of one cell (updateExtendedState); FP64 always,
@@ -653,6 +721,15 @@ __global__ void __launch_bounds__(256) k_rk_prim(CASE_ARGS, int nw, double w0, d
       s.u1[i] = u1;
       s.u2[i] = u2;
       s.rhoE[i] = rhoE;
+      // advanceScalars (IdealGasSolver.cpp:874-892) with this cell's rho_old
+      const int nsc = s.nsc;
+      for (int isc = 0; isc < nsc; ++isc) {
+        double v = w0 * s.rhs_sc[size_t(isc) * N + i];
+        if (nw > 1) v += w1 * s.rhs_sc[size_t(nsc + isc) * N + i];
+        if (nw > 2) v += w2 * s.rhs_sc[size_t(2 * nsc + isc) * N + i];
+        double* ph_ = s.sc + size_t(isc) * N + i;
+        *ph_ = (rho_old * *ph_ + tmp * v) * inv_rho;
+      }
     }
     StateDev sw = s;
     write_prim(ph, sw, i, rho, u0, u1, u2, rhoE, writeQ != 0);
@@ -969,6 +1046,25 @@ __global__ void k_state_in_prim(int N, const int* __restrict__ perm, const doubl
   s.u1[i] = u1;
   s.u2[i] = u2;
   s.rhoE[i] = p / (gamma - 1.0) + 0.5 * rho * (u0 * u0 + u1 * u1 + u2 * u2);
+}
+
+// transport scalars between the caller's order sc[icv*nsc + isc] and the
+// device's [isc][N] in cell order (dir 0: in, 1: out); also rhs_sc of one
+// stage out (dir 2)
+__global__ void k_scalars_io(int N, int nsc, const int* __restrict__ perm, double* __restrict__ host_order,
+                             StateDev s, int dir, int stage) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int o = perm[i];
+  for (int a = 0; a < nsc; ++a) {
+    double* h = host_order + size_t(o) * nsc + a;
+    if (dir == 0)
+      s.sc[size_t(a) * N + i] = *h;
+    else if (dir == 1)
+      *h = s.sc[size_t(a) * N + i];
+    else
+      *h = s.rhs_sc[(size_t(stage) * nsc + a) * N + i];
+  }
 }
 
 __global__ void k_state_out(int N, const int* __restrict__ perm, double* __restrict__ st, StateDev s) {
@@ -1461,7 +1557,19 @@ int enqueue_grad(const Runner& R) { return grad_var(R, R.tune.g_grad); }
 int enqueue_rhs(const Runner& R, int stage0) {
   int rc = ext_var(R, R.tune.g_ext, stage0);
   if (rc) return rc;
-  return comp_var(R, R.tune.g_comp, stage0);
+  if ((rc = comp_var(R, R.tune.g_comp, stage0))) return rc;
+  if (R.direct && R.dcase.s.nsc > 0) {  // calcRhsScalars, once mf is complete
+    constexpr int G = 4;
+    const long long thr = (long long)R.dcase.m.N * G;
+    k_rhs_sc<G><<<int((thr + 255) / 256), 256, 0, R.stream>>>(R.dcase, stage0);
+    return launch_check(R, 1);
+  }
+  return CGX_OK;
+}
+
+// kernel launches of one RK3 step (three more with transport scalars)
+inline int launches_per_step(const Runner& R) {
+  return kLaunchesPerStep + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0);
 }
 
 int enqueue_step_end(const Runner& R, int mode) { return end_var(R, R.tune.g_end, mode); }
@@ -2318,6 +2426,88 @@ extern "C" int cgx_get_state(cgx_solver* s, double* rho, double* u, double* rhoE
   return CGX_OK;
 }
 
+// The scalar arrays (sc, three stages of rhs_sc, per-entry mf) are allocated
+// at the first call with nsc > 0 and kept; a later call with another nsc
+// reallocates them.  Every copy of the case descriptor (host, device table,
+// the runner's by-value copy) is refreshed and the step graph re-captured.
+extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_scalars: null solver");
+  if (nsc < 0 || nsc > kMaxScalars) return fail(CGX_E_ARG, "cgx_set_scalars: nsc out of range 0..8");
+  if (nsc > 0 && !sc) return fail(CGX_E_ARG, "cgx_set_scalars: null scalars");
+  if (nsc > 0 && s->prec != CGX_FP64) return fail(CGX_E_ARG, "cgx_set_scalars: FP64 solvers only");
+  CK(cudaSetDevice(s->mesh->device));
+  CK(cudaStreamSynchronize(s->stream));
+  const size_t N = size_t(s->mesh->N);
+  StateDev& sd = s->sd;
+  if (nsc != sd.nsc) {
+    for (double* q : {sd.sc, sd.rhs_sc, sd.mf}) {
+      if (!q) continue;
+      cudaFree(q);
+      s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), static_cast<void*>(q)), s->allocs.end());
+    }
+    sd.sc = sd.rhs_sc = sd.mf = nullptr;
+    sd.nsc = 0;
+    if (nsc > 0) {
+      const size_t E = size_t(std::max(s->mesh->md.E, 1LL));
+      int rc;
+      if ((rc = dalloc(&sd.sc, size_t(nsc) * N, &s->bytes))) return rc;
+      s->allocs.push_back(sd.sc);
+      if ((rc = dalloc(&sd.rhs_sc, 3 * size_t(nsc) * N, &s->bytes))) return rc;
+      s->allocs.push_back(sd.rhs_sc);
+      if ((rc = dalloc(&sd.mf, E, &s->bytes))) return rc;
+      s->allocs.push_back(sd.mf);
+      CK(cudaMemsetAsync(sd.rhs_sc, 0, 3 * size_t(nsc) * N * sizeof(double), s->stream));
+      sd.nsc = nsc;
+    }
+    s->hcase.s = sd;
+    s->run.dcase.s = sd;
+    CK(cudaMemcpyAsync(s->d_case, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream));
+    if (s->graph) {
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+  }
+  if (nsc > 0) {
+    if (size_t(nsc) * N > 9 * N) return fail(CGX_E_ARG, "cgx_set_scalars: staging too small");
+    CK(cudaMemcpyAsync(s->d_stage, sc, size_t(nsc) * N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    k_scalars_io<<<int((N + 255) / 256), 256, 0, s->stream>>>(int(N), nsc, s->mesh->d_perm, s->d_stage, sd, 0, 0);
+    int rc = launch_check(s->run, 1);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
+extern "C" int cgx_get_scalars(cgx_solver* s, double* sc) {
+  if (!s || !sc) return fail(CGX_E_ARG, "cgx_get_scalars: null argument");
+  const int nsc = s->sd.nsc;
+  if (nsc == 0) return fail(CGX_E_STATE, "cgx_get_scalars: the solver has no transport scalars");
+  CK(cudaSetDevice(s->mesh->device));
+  const int N = s->mesh->N;
+  k_scalars_io<<<(N + 255) / 256, 256, 0, s->stream>>>(N, nsc, s->mesh->d_perm, s->d_stage, s->sd, 1, 0);
+  int rc = launch_check(s->run, 1);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(sc, s->d_stage, size_t(nsc) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
+extern "C" int cgx_get_rhs_sc(cgx_solver* s, int rk_stage, double* rhs_sc) {
+  if (!s || !rhs_sc) return fail(CGX_E_ARG, "cgx_get_rhs_sc: null argument");
+  if (rk_stage < 1 || rk_stage > 3) return fail(CGX_E_ARG, "rk_stage must be 1..3");
+  const int nsc = s->sd.nsc;
+  if (nsc == 0) return fail(CGX_E_STATE, "cgx_get_rhs_sc: the solver has no transport scalars");
+  CK(cudaSetDevice(s->mesh->device));
+  const int N = s->mesh->N;
+  k_scalars_io<<<(N + 255) / 256, 256, 0, s->stream>>>(N, nsc, s->mesh->d_perm, s->d_stage, s->sd, 2,
+                                                       rk_stage - 1);
+  int rc = launch_check(s->run, 1);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(rhs_sc, s->d_stage, size_t(nsc) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
 extern "C" int cgx_update_primitive(cgx_solver* s) {
   if (!s) return fail(CGX_E_ARG, "null solver");
   if (!s->state_set) return fail(CGX_E_STATE, "state not set");
@@ -2432,7 +2622,7 @@ extern "C" int cgx_step(cgx_solver* s, int nsteps) {
     const int batch = std::min(ci, nsteps - done);
     for (int k = 0; k < batch; ++k) {
       CK(cudaGraphLaunch(s->graph, s->stream));
-      s->launches += kLaunchesPerStep;
+      s->launches += launches_per_step(s->run);
     }
     done += batch;
     bool nan = false;
@@ -2477,7 +2667,7 @@ extern "C" int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms) {
   CK(cudaEventRecord(e0, s->stream));
   for (int k = 0; k < nsteps; ++k) {
     CK(cudaGraphLaunch(s->graph, s->stream));
-    s->launches += kLaunchesPerStep;
+    s->launches += launches_per_step(s->run);
   }
   CK(cudaEventRecord(e1, s->stream));
   CK(cudaEventSynchronize(e1));
@@ -2493,7 +2683,7 @@ extern "C" int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms) {
   return CGX_OK;
 }
 
-extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[4]) {
+extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]) {
   if (!s || !ms) return fail(CGX_E_ARG, "null argument");
   if (!s->inited) return fail(CGX_E_STATE, "cgx_init_complete not called");
   if (reps < 1) return fail(CGX_E_ARG, "reps < 1");
@@ -2502,13 +2692,15 @@ extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[4]) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   int rc = CGX_OK;
-  for (int which = 0; which < 4 && rc == CGX_OK; ++which) {
+  for (int which = 0; which < 6 && rc == CGX_OK; ++which) {
     CK(cudaEventRecord(e0, s->stream));
     for (int r = 0; r < reps && rc == CGX_OK; ++r) {
       if (which == 0) rc = enqueue_rhs(s->run, 0);
       else if (which == 1) rc = enqueue_prim(s->run, 3, kRkW[2], 0.0, true);
       else if (which == 2) rc = enqueue_grad(s->run);
-      else rc = enqueue_step_end(s->run, 0);
+      else if (which == 3) rc = enqueue_step_end(s->run, 0);
+      else if (which == 4) rc = ext_var(s->run, s->run.tune.g_ext, 0);
+      else rc = comp_var(s->run, s->run.tune.g_comp, 0);
     }
     CK(cudaEventRecord(e1, s->stream));
     CK(cudaEventSynchronize(e1));

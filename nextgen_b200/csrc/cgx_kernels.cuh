@@ -36,6 +36,7 @@
 namespace cgx {
 
 constexpr int kRevBit = 0x80000000;
+constexpr int kMaxScalars = 8;  // transport scalars per cell
 constexpr int kFidMask = 0x7fffffff;
 
 struct alignas(32) LRec {
@@ -188,6 +189,11 @@ struct StateDev {
   QRecF* QF;
   Ctl* ctl;
   double* red;  // per-block partials: [nblocks] cfl max, [nblocks] nan
+  // transport scalars (calcRhsScalars / advanceScalars), FP64 solvers only
+  int nsc;         // scalars per cell (0: none; the pointers below are null)
+  double* sc;      // [nsc][N]
+  double* rhs_sc;  // [3][nsc][N]
+  double* mf;      // [E] mass flux of each extended entry, entry direction
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

@@ -39,6 +39,16 @@ void orc_calc_sgs_props(orc_solver* o);
  * |face flux| per component, the conditioning scale of the face sum. */
 void orc_calc_rhs(orc_solver* o, int rk_stage, double* rhs_out, double* scale_out);
 void orc_rk3_step(orc_solver* o, const double w[3], double dt, int rk_stage);
+/* Transport scalars (calcRhsScalars / advanceScalars): nsc per cell,
+ * sc[icv*nsc + isc] over the ncv owned cells (ghosts are copies).  Once set,
+ * orc_calc_rhs and the steps also form and apply rhs_sc.  0, or -1 on a bad
+ * argument. */
+int orc_set_scalars(orc_solver* o, int nsc, const double* sc);
+void orc_get_scalars(const orc_solver* o, double* sc);
+/* rhs_sc[ncv][nsc] of stage rk_stage as the last orc_calc_rhs / step left it;
+ * scale_out (optional) = sum of |face flux| per cell and scalar (filled by an
+ * orc_calc_rhs called with a scale_out). */
+void orc_get_rhs_sc(const orc_solver* o, int rk_stage, double* rhs_sc, double* scale_out);
 double orc_calc_cfl(const orc_solver* o, double dt, double* cfl);
 /* setDt per dt_mode; returns dt */
 double orc_set_dt(orc_solver* o);

@@ -43,6 +43,9 @@ def _load(path):
         "orc_calc_sgs_props": (None, [vp]),
         "orc_calc_rhs": (None, [vp, ctypes.c_int, c_dbl_p, c_dbl_p]),
         "orc_rk3_step": (None, [vp, c_dbl_p, ctypes.c_double, ctypes.c_int]),
+        "orc_set_scalars": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
+        "orc_get_scalars": (None, [vp, c_dbl_p]),
+        "orc_get_rhs_sc": (None, [vp, ctypes.c_int, c_dbl_p, c_dbl_p]),
         "orc_calc_cfl": (ctypes.c_double, [vp, ctypes.c_double, c_dbl_p]),
         "orc_set_dt": (ctypes.c_double, [vp]),
         "orc_advance_solution": (ctypes.c_int, [vp]),
@@ -110,6 +113,27 @@ class Oracle:
         scale = np.empty((self.ncv, 5)) if want_scale else None
         self.L.orc_calc_rhs(self.h, int(rk_stage), _dp(rhs), _dp(scale))
         return (rhs, scale) if want_scale else rhs
+
+    def set_scalars(self, sc):
+        """Transport scalars sc[ncv][nsc] (calcRhsScalars / advanceScalars)."""
+        sc = np.ascontiguousarray(sc, dtype=np.float64).reshape(self.ncv, -1)
+        self.nsc = sc.shape[1]
+        if self.L.orc_set_scalars(self.h, int(self.nsc), _dp(sc)) != 0:
+            raise ValueError("orc_set_scalars failed")
+
+    def get_scalars(self):
+        sc = np.empty((self.ncv, getattr(self, "nsc", 0)))
+        if sc.size:
+            self.L.orc_get_scalars(self.h, _dp(sc))
+        return sc
+
+    def rhs_sc(self, rk_stage=1, want_scale=True):
+        """rhs_sc[ncv][nsc] (and its conditioning scale) of the last calc_rhs."""
+        nsc = getattr(self, "nsc", 0)
+        r = np.empty((self.ncv, nsc))
+        sc = np.empty((self.ncv, nsc)) if want_scale else None
+        self.L.orc_get_rhs_sc(self.h, int(rk_stage), _dp(r), _dp(sc))
+        return (r, sc) if want_scale else r
 
     def rk3_step(self, w, dt, stage):
         w = np.ascontiguousarray(w, dtype=np.float64)
