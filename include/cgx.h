@@ -151,13 +151,15 @@ int cgx_set_state_primitive(cgx_solver* s, const double* rho, const double* u,
                             const double* p);
 int cgx_get_state(cgx_solver* s, double* rho, double* u, double* rhoE);
 
-/* Passive transport scalars (FP64 solvers): nsc (0..8) scalars per cell in
+/* Passive transport scalars: nsc (0..8) scalars per cell in
  * the reference's order sc[icv*nsc + isc] (transport_scalar_vec,
  * IdealGasSolver.hpp).  Once set, calcRhs also forms rhs_sc as
  * calcRhsScalars does (IdealGasSolver.cpp:537-693: convective flux
  * 0.5 (sc0 + sc1) mf on every extended face with mf its mass flux, minus the
  * unity-Lewis diffusion on compact faces) and every rk3Step advances them as
  * advanceScalars does (IdealGasSolver.cpp:874-892).  nsc = 0 removes them.
+ * Scalars, their face sums and their update are FP64 in both precisions; a
+ * mixed-precision solver supplies mass fluxes from its FP32 flux arithmetic.
  * Like the reference's storeData, NaN recovery does not restore scalars. */
 int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc);
 int cgx_get_scalars(cgx_solver* s, double* sc);

@@ -271,7 +271,7 @@ class Solver:
 
     # -- passive transport scalars (transport_scalar_vec) ---------------------
     def set_scalars(self, sc):
-        """Transport scalars sc[ncv][nsc] (nsc <= 8, FP64 solvers); from now
+        """Transport scalars sc[ncv][nsc] (nsc <= 8, both precisions); from now
         on calcRhs forms rhs_sc (calcRhsScalars) and the steps advance them
         (advanceScalars).  An empty second axis removes them."""
         sc = np.ascontiguousarray(sc, dtype=np.float64).reshape(self.ncv, -1)

@@ -610,8 +610,10 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
 // A group of G lanes per cell, lane l takes entries l, l+G, ...; partial
 // sums are combined by the fixed butterfly (deterministic).  The neighbour's
 // scalars and properties are gathered from global memory (scalar transport
-// runs on single-case solvers only).
-template <int G>
+// runs on single-case solvers only).  MIX: the mixed-precision form, whose
+// mass fluxes come from the FP32 flux arithmetic and whose properties and
+// compact geometry are the FP32 records; scalars, fluxes and sums stay FP64.
+template <int G, bool MIX>
 __global__ void __launch_bounds__(256) k_rhs_sc(const CaseDev c, int stage) {
   const MeshDev& m = c.m;
   const StateDev& s = c.s;
@@ -633,7 +635,7 @@ __global__ void __launch_bounds__(256) k_rhs_sc(const CaseDev c, int stage) {
     b = m.off[i];
     e = m.off[i + 1];
     ncomp = int(m.qoff[i + 1] - m.qoff[i]);
-    loc_i = s.V[i].loc_total;
+    loc_i = MIX ? double(s.VF[i].loc_total) : s.V[i].loc_total;
   }
   const long long q0 = valid ? m.qoff[i] : 0;
   for (long long k = b + lane; k < e; k += G) {
@@ -641,7 +643,12 @@ __global__ void __launch_bounds__(256) k_rhs_sc(const CaseDev c, int stage) {
     const double mfk = s.mf[k];
     const int tk = int(k - b);
     double dc = 0.0;
-    if (tk < ncomp) dc = 0.5 * (loc_i + s.V[j].loc_total) * __ldg(m.qg + 4 * m.Q + q0 + tk);
+    if (tk < ncomp) {
+      if (MIX)
+        dc = 0.5 * (loc_i + double(s.VF[j].loc_total)) * double(__ldg(m.qg32 + 4 * m.Q + q0 + tk));
+      else
+        dc = 0.5 * (loc_i + s.V[j].loc_total) * __ldg(m.qg + 4 * m.Q + q0 + tk);
+    }
 #pragma unroll
     for (int a = 0; a < kMaxScalars; ++a) {
       if (a < nsc) {
@@ -928,15 +935,24 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
     smem_L(sL, loc_, Li);
     qi = smem_Q(smem, loc_);
   }
-  // ---- Gibbs remainder over the extended faces (a maximum: any order)
+  // ---- Gibbs remainder over the extended faces (a maximum: any order).
+  // Four entries per lane and pass: their local indices are loaded together,
+  // so the shared-memory reads of one pass wait on one round of L2 latency.
   double vv2 = 0.0, cfl = 0.0;
-  for (long long k = b + lane; k < e; k += G) {
-    const double4 qj = smem_Q(smem, __ldg(m.lidx + k));
-    const double dp = qj.y - qi.y;
-    const double v_avg = 0.5 * (qi.z + qj.z);
-    const double beta = 0.5 * (qi.w + qj.w);
-    const double gr = qj.x - qi.x - v_avg * dp * beta;
-    vv2 = fmax(vv2, fabs(gr));
+  for (long long k = b + lane; k < e; k += 4 * G) {
+    int jl[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) jl[u] = (k + u * G < e) ? int(__ldg(m.lidx + k + u * G)) : -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (jl[u] < 0) continue;
+      const double4 qj = smem_Q(smem, jl[u]);
+      const double dp = qj.y - qi.y;
+      const double v_avg = 0.5 * (qi.z + qj.z);
+      const double beta = 0.5 * (qi.w + qj.w);
+      const double gr = qj.x - qi.x - v_avg * dp * beta;
+      vv2 = fmax(vv2, fabs(gr));
+    }
   }
   // ---- CFL over the compact faces
   for (long long q = q0 + lane; q < q1; q += G) {
@@ -1561,7 +1577,10 @@ int enqueue_rhs(const Runner& R, int stage0) {
   if (R.direct && R.dcase.s.nsc > 0) {  // calcRhsScalars, once mf is complete
     constexpr int G = 4;
     const long long thr = (long long)R.dcase.m.N * G;
-    k_rhs_sc<G><<<int((thr + 255) / 256), 256, 0, R.stream>>>(R.dcase, stage0);
+    if (R.prec == CGX_MIXED)
+      k_rhs_sc<G, true><<<int((thr + 255) / 256), 256, 0, R.stream>>>(R.dcase, stage0);
+    else
+      k_rhs_sc<G, false><<<int((thr + 255) / 256), 256, 0, R.stream>>>(R.dcase, stage0);
     return launch_check(R, 1);
   }
   return CGX_OK;
@@ -2434,7 +2453,6 @@ extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
   if (!s) return fail(CGX_E_ARG, "cgx_set_scalars: null solver");
   if (nsc < 0 || nsc > kMaxScalars) return fail(CGX_E_ARG, "cgx_set_scalars: nsc out of range 0..8");
   if (nsc > 0 && !sc) return fail(CGX_E_ARG, "cgx_set_scalars: null scalars");
-  if (nsc > 0 && s->prec != CGX_FP64) return fail(CGX_E_ARG, "cgx_set_scalars: FP64 solvers only");
   CK(cudaSetDevice(s->mesh->device));
   CK(cudaStreamSynchronize(s->stream));
   const size_t N = size_t(s->mesh->N);

@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
     smem_LF(smem, jl, Lj);
     float F[5];
     ext_flux_f(F, n, c, Li, Lj);
+    if (s.mf) s.mf[k] = double(F[0]);  // mass flux for calcRhsScalars
 #pragma unroll
     for (int q = 0; q < 5; ++q) acc[q] -= double(F[q]);
   }
@@ -283,6 +284,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_comp_f(CASE_ARGS, int stage) {
     FluxF F;
     F.rho = 0.0f; F.ru[0] = F.ru[1] = F.ru[2] = 0.0f; F.rE = 0.0f;
     compact_flux_add_f(F, un, area, aod, delta, Li, Lj, Vs, uf, h_f, p_ref);
+    if (s.mf) s.mf[m.off[i] + (q - q0)] += double(F.rho);  // the closure's mass flux
     acc[0] -= double(F.rho);
     acc[1] -= double(F.ru[0]);
     acc[2] -= double(F.ru[1]);
@@ -445,13 +447,20 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   }
   float vv2 = 0.0f;
   double cfl = 0.0;
-  for (long long k = b + lane; k < e; k += G) {
-    const float4 qj = reinterpret_cast<const float4*>(smem)[__ldg(m.lidx + k)];
-    const float dp = qj.y - qi.y;
-    const float v_avg = 0.5f * (qi.z + qj.z);
-    const float beta = 0.5f * (qi.w + qj.w);
-    const float gr = qj.x - qi.x - v_avg * dp * beta;
-    vv2 = fmaxf(vv2, fabsf(gr));
+  for (long long k = b + lane; k < e; k += 4 * G) {  // four entries per pass (see k_step_end)
+    int jl[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) jl[u] = (k + u * G < e) ? int(__ldg(m.lidx + k + u * G)) : -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (jl[u] < 0) continue;
+      const float4 qj = reinterpret_cast<const float4*>(smem)[jl[u]];
+      const float dp = qj.y - qi.y;
+      const float v_avg = 0.5f * (qi.z + qj.z);
+      const float beta = 0.5f * (qi.w + qj.w);
+      const float gr = qj.x - qi.x - v_avg * dp * beta;
+      vv2 = fmaxf(vv2, fabsf(gr));
+    }
   }
   for (long long q = q0 + lane; q < q1; q += G) {
     const int jl = __ldg(m.clidx + q);
