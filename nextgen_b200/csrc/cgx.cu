@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <cmath>
@@ -794,14 +795,15 @@ __global__ void __launch_bounds__(256) k_grad(CASE_ARGS) {
 // NaN flags (fixed order) and update the control block: time/step advance
 // (mode bit 0) and the next dt from setDt's formula (mode bit 1).
 // Called by all 256 threads of that block.
-__device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, int nparts) {
+__device__ __noinline__ void finalize_ctl(Ctl* ctl, const double* red, int dt_mode, double dt_max, int mode,
+                                          int nparts) {
   __shared__ double fin_cfl[256];
   __shared__ int fin_nan[256];
   double mx = 0.0;
   int anynan = 0;
   for (int bb = threadIdx.x; bb < nparts; bb += blockDim.x) {
-    mx = fmax(mx, ((volatile double*)s.red)[bb]);
-    anynan |= (((volatile double*)s.red)[nparts + bb] != 0.0);
+    mx = fmax(mx, ((volatile const double*)red)[bb]);
+    anynan |= (((volatile const double*)red)[nparts + bb] != 0.0);
   }
   fin_cfl[threadIdx.x] = mx;
   fin_nan[threadIdx.x] = anynan;
@@ -814,7 +816,7 @@ __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, i
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    Ctl* c = s.ctl;
+    Ctl* c = ctl;
     const double cmax = fin_cfl[0];
     c->cfl_max = cmax;
     if (fin_nan[0]) c->nan = 1;
@@ -825,12 +827,12 @@ __device__ __noinline__ void finalize_ctl(StateDev s, const Phys ph, int mode, i
     }
     if (mode & 2) {
       double dt;
-      if (ph.dt_mode == CGX_DT_CONST)
+      if (dt_mode == CGX_DT_CONST)
         dt = c->dt_data0;
-      else if (ph.dt_mode == CGX_DT_CFL)
+      else if (dt_mode == CGX_DT_CFL)
         dt = c->dt_data0 / cmax;
       else
-        dt = fmin(ph.dt_max, c->dt_data0 / fmax(cmax, 1.0E-12));
+        dt = fmin(dt_max, c->dt_data0 / fmax(cmax, 1.0E-12));
       c->dt = dt;
     }
     c->blocks_done = 0;
@@ -935,24 +937,15 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
     smem_L(sL, loc_, Li);
     qi = smem_Q(smem, loc_);
   }
-  // ---- Gibbs remainder over the extended faces (a maximum: any order).
-  // Four entries per lane and pass: their local indices are loaded together,
-  // so the shared-memory reads of one pass wait on one round of L2 latency.
+  // ---- Gibbs remainder over the extended faces (a maximum: any order)
   double vv2 = 0.0, cfl = 0.0;
-  for (long long k = b + lane; k < e; k += 4 * G) {
-    int jl[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) jl[u] = (k + u * G < e) ? int(__ldg(m.lidx + k + u * G)) : -1;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (jl[u] < 0) continue;
-      const double4 qj = smem_Q(smem, jl[u]);
-      const double dp = qj.y - qi.y;
-      const double v_avg = 0.5 * (qi.z + qj.z);
-      const double beta = 0.5 * (qi.w + qj.w);
-      const double gr = qj.x - qi.x - v_avg * dp * beta;
-      vv2 = fmax(vv2, fabs(gr));
-    }
+  for (long long k = b + lane; k < e; k += G) {
+    const double4 qj = smem_Q(smem, __ldg(m.lidx + k));
+    const double dp = qj.y - qi.y;
+    const double v_avg = 0.5 * (qi.z + qj.z);
+    const double beta = 0.5 * (qi.w + qj.w);
+    const double gr = qj.x - qi.x - v_avg * dp * beta;
+    vv2 = fmax(vv2, fabs(gr));
   }
   // ---- CFL over the compact faces
   for (long long q = q0 + lane; q < q1; q += G) {
@@ -995,7 +988,7 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   __syncthreads();
   if (am_last) {
     __threadfence();
-    finalize_ctl(s, ph, mode, CASE_NITEMS);
+    finalize_ctl(s.ctl, s.red, ph.dt_mode, ph.dt_max, mode, CASE_NITEMS);
   }
   STAGED_LOOP_END
 #undef PF_END
@@ -1228,6 +1221,18 @@ __global__ void k_cfl_cells(MeshDev m, StateDev s, const int* __restrict__ perm,
       return CGX_E_CUDA;                                                           \
     }                                                                              \
   } while (0)
+
+// Set-up phase timings of cgx_mesh_create on stderr when CGX_MESH_VERBOSE is set.
+struct MeshPhaseTimer {
+  bool on = std::getenv("CGX_MESH_VERBOSE") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char* what) {
+    if (!on) return;
+    const auto n = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "cgx_mesh_create %-24s %8.3f s\n", what, std::chrono::duration<double>(n - t).count());
+    t = n;
+  }
+};
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -1822,6 +1827,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     return rc;
   };
   try {
+    MeshPhaseTimer PT;
     // ---- owners of ghosts
     for (int g = 0; g < ncv_g2 - N; ++g)
       if (d->icv_owner_g[g] < 0 || d->icv_owner_g[g] >= N) return bail(fail(CGX_E_ARG, "ghost owner out of range"));
@@ -1853,6 +1859,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
     auto nw = [&](int idx) { return iperm[owner(idx)]; };
 
+    PT.mark("renumbering");
     // ---- match compact faces to extended faces (FlowSolver.hpp:1833-1900)
     std::vector<int> ef_i(N + 1, 0);
     for (int f = 0; f < nef; ++f) {
@@ -1889,6 +1896,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       cf_of_ef[f] = fa;
       cf_rev[f] = rev;
     }
+    PT.mark("compact/extended match");
     // ---- face numbering: compact faces first, each group ordered by the
     // first cell (new numbering) that reads the face
     // (counting sort on the bucket 2*first + (extended only))
@@ -1934,6 +1942,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         c.delta = area / c.aod;
       }
     }
+    PT.mark("face numbering");
     // ---- directed entries per cell (new numbering): CSR, compact faces first
     std::vector<int> deg(N, 0), ncomp(N, 0);
     for (int f = 0; f < nef; ++f) {
@@ -1983,6 +1992,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         }
       }
     }
+    PT.mark("entry CSR");
     // ---- gradient CSR (cvocv without the diagonal, reference order)
     std::vector<long long> coff(N + 1, 0);
     for (int i = 0; i < N; ++i) {
@@ -2004,6 +2014,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         gz[k] = d->cvocv_grad_coeff[3 * size_t(coc) + 2];
       }
     }
+    PT.mark("gradient CSR");
     // ---- per-cell constants (pow on the host: the reference's libm values)
     std::vector<double> vol(N), inv_vol(N);
     std::vector<double4> cc(N);
@@ -2015,6 +2026,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       cc[i] = make_double4(std::pow(v, 1.0 / 3.0), std::pow(v, 2.0 / 3.0), d->dcmag_hat_cv[o],
                            d->sa_to_vol_ratio[o]);
     }
+    PT.mark("cell constants");
     // ---- work items (runs of consecutive cells) and their halos; an item
     // whose neighbour unions exceed the shared-memory budget is split
     std::vector<Item> items;
@@ -2103,6 +2115,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     }
     if (hcell.empty()) hcell.push_back(0);
     if (chcell.empty()) chcell.push_back(0);
+    PT.mark("items and halos");
     // ---- upload; the per-face records are expanded on the device into the
     // per-entry planes and then released
     size_t* acc = &M->bytes;
@@ -2170,6 +2183,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         return bail(fail(CGX_E_CUDA, std::string("entry expansion: ") +
                                          cudaGetErrorString(ke != cudaSuccess ? ke : se)));
     }
+    PT.mark("upload and expansion");
     MeshDev& md = M->md;
     md.N = N;
     md.nitems = int(items.size());

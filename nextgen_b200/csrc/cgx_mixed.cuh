@@ -447,20 +447,13 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   }
   float vv2 = 0.0f;
   double cfl = 0.0;
-  for (long long k = b + lane; k < e; k += 4 * G) {  // four entries per pass (see k_step_end)
-    int jl[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) jl[u] = (k + u * G < e) ? int(__ldg(m.lidx + k + u * G)) : -1;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (jl[u] < 0) continue;
-      const float4 qj = reinterpret_cast<const float4*>(smem)[jl[u]];
-      const float dp = qj.y - qi.y;
-      const float v_avg = 0.5f * (qi.z + qj.z);
-      const float beta = 0.5f * (qi.w + qj.w);
-      const float gr = qj.x - qi.x - v_avg * dp * beta;
-      vv2 = fmaxf(vv2, fabsf(gr));
-    }
+  for (long long k = b + lane; k < e; k += G) {
+    const float4 qj = reinterpret_cast<const float4*>(smem)[__ldg(m.lidx + k)];
+    const float dp = qj.y - qi.y;
+    const float v_avg = 0.5f * (qi.z + qj.z);
+    const float beta = 0.5f * (qi.w + qj.w);
+    const float gr = qj.x - qi.x - v_avg * dp * beta;
+    vv2 = fmaxf(vv2, fabsf(gr));
   }
   for (long long q = q0 + lane; q < q1; q += G) {
     const int jl = __ldg(m.clidx + q);
@@ -502,7 +495,7 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   __syncthreads();
   if (am_last) {
     __threadfence();
-    finalize_ctl(s, ph, mode, CASE_NITEMS);
+    finalize_ctl(s.ctl, s.red, ph.dt_mode, ph.dt_max, mode, CASE_NITEMS);
   }
   STAGED_LOOP_END
 #undef PF_ENDF
