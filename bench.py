@@ -7,8 +7,9 @@ one replica per GPU.
 Prints one JSON line (rank 0).  value = whole-job cell-steps/s from CUDA
 events on the solver's stream around K graph-replayed steps (max over ranks);
 e2e = the same metric through the C ABI with host buffers (pinned host state
-copied in and read back every step); roofline = the face-flux kernel's
-algorithmic bytes per launch over its measured launch time against the
+copied in and read back every step); roofline = the face-flux kernel pair's
+algorithmic bytes per launch over its launch time, timed by CUDA events
+recorded around the two kernels inside the timed steps, against the
 measured HBM copy bandwidth; cpu_baseline = the CPU oracle on the host cores
 on a bounded sample.  `--impl reference` times the reference's CPU path (the
 oracle built on the reference's own flux header when available) instead.
@@ -280,13 +281,18 @@ def run_cgx(args):
         s.synchronize()
         n0 = s.launch_count()
         with ClockSampler(device) as clk:
-            ms = s.step_timed(args.steps)
+            # the face kernels are timed inside these steps (events in the step graph)
+            ms, face = s.step_profiled(args.steps)
         s.synchronize()
         dist.barrier()
         launches = s.launch_count() - n0
         ms_max = dist.max_over_ranks(ms)
+        # the other kernels' launch times from back-to-back launches after the
+        # timed region; the face kernels' from inside it
+        kt = s.kernel_times(reps=3)
+        kt.update(face)
         res[prec_name] = {"ms": ms_max, "launches": launches, "clocks": clk.summary(),
-                          "kernel_ms": s.kernel_times(reps=3), "tuning": s.tuning()}
+                          "kernel_ms": kt, "tuning": s.tuning()}
         solvers[prec_name] = s
 
     s = solvers["fp64"]
@@ -323,7 +329,7 @@ def run_cgx(args):
     peak, peak_kind = measured_peaks()
     ms_step = res["fp64"]["ms"] / args.steps
     value = world * N * args.steps / (res["fp64"]["ms"] * 1e-3)
-    achieved = rhs_bytes * N / (ktimes["rhs"] * 1e-3) / 1e9
+    achieved = rhs_bytes * N / (dist.max_over_ranks(ktimes["rhs"]) * 1e-3) / 1e9
 
     # e2e: the C-ABI calls a host solver makes each step, with host buffers
     r_h = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -400,6 +406,117 @@ def run_cgx(args):
     return 0
 
 
+def _errors(m, vol, ref, got, init):
+    """Velocity, pressure (fluctuation) and kinetic-energy errors of `got`
+    against `ref`: (rho, u, p) triples on the same mesh."""
+    r64, u64, p64 = ref
+    r32, u32, p32 = got
+    rho0, u0 = init
+    ke = lambda r, u: 0.5 * (r * (u * u).sum(1) * vol).sum()
+    ke64, ke32, ke0 = ke(r64, u64), ke(r32, u32), ke(rho0, u0)
+    du = u32 - u64
+    pf = p64 - p64.mean()
+    return {"u_l2_rel": float(np.sqrt((du ** 2).mean() / (u64 ** 2).mean())),
+            "u_linf_rel": float(np.abs(du).max() / np.abs(u64).max()),
+            "p_l2_rel_fluct": float(np.sqrt(((p32 - p64) ** 2).mean() / max((pf ** 2).mean(), 1e-300))),
+            "p_linf_rel_fluct": float(np.abs(p32 - p64).max() / max(np.abs(pf).max(), 1e-300)),
+            "ke_rel": float(abs(ke32 - ke64) / ke64),
+            "ke_decay_fp64": float((ke0 - ke64) / ke0),
+            "ke_decay_rel_err": float(abs(ke32 - ke64) / max(abs(ke0 - ke64), 1e-300))}
+
+
+def run_accuracy(args):
+    """The mixed-precision form against the FP64 path on the jittered n^3 mesh
+    (200^3 = 8M cells by default): the Ma 0.1 Taylor-Green state and the
+    Mt 0.3 random-solenoidal state, each advanced `--accuracy-steps` RK3 steps
+    (500 by default) at CFL 0.8 by both precisions from the same initial state.
+    Prints one JSON line with the L2/L-inf errors of velocity and pressure and
+    the kinetic-energy (decay) error of the mixed form."""
+    from nextgen_b200 import cases, cgx
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    n, K = args.n, args.accuracy_steps
+    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED, nthreads=os.cpu_count() or 1)
+    gm = cgx.Mesh(m)
+    vol = np.array(m.vol_cv)
+    out = {"metric": "mixed-precision error vs FP64 after %d RK3 steps" % K, "cells": m.ncv,
+           "config": {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3, CFL 0.8, Vreman" % n},
+           "data": "synthetic", "cases": {}}
+    for kind in ("tgv", "solenoidal"):
+        if kind == "tgv":
+            prm = cases.tgv_params()
+            rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
+        else:
+            prm = cases.hit_params(Mt=0.3)
+            rho, u, p = cases.hit_state(n, prm, Mt=0.3, k0=4.0, seed=4321)
+        prm.check_interval = 50
+        res, ms = {}, {}
+        for name, prec in (("fp64", cgx.CGX_FP64), ("mixed", cgx.CGX_MIXED)):
+            s = cgx.Solver(gm, prm, prec)
+            s.set_state_primitive(rho, u, p)
+            s.initComplete()
+            ms[name] = s.step_timed(K)
+            r1, u1, _ = s.get_state()
+            res[name] = (r1, u1, s.primitive()[0])
+            s.close()
+        e = _errors(m, vol, res["fp64"], res["mixed"], (rho, u))
+        e.update({"fp64_ms_per_step": ms["fp64"] / K, "mixed_ms_per_step": ms["mixed"] / K,
+                  "speedup": ms["fp64"] / ms["mixed"]})
+        out["cases"][kind] = e
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_batch64(args, seed=64):
+    """64 independent Taylor-Green cases of uneven size in one batch: edges
+    log-uniform in [8, 64] (512 to 262,144 cells, +/-0.25h jitter), Mach
+    uniform in [0.1, 0.5], Re uniform in [400, 3200], advanced together for
+    `--batch-steps` steps (300 by default) in FP64 and in mixed precision; the
+    same cases one at a time on the plain FP64 path for comparison.  Prints one
+    JSON line with the cell-steps/s of each."""
+    from nextgen_b200 import cases, cgx
+    rng = np.random.default_rng(seed)
+    edges = [int(round(np.exp(x))) for x in rng.uniform(np.log(8), np.log(64), size=64)]
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    meshes = {}
+    for e in sorted(set(edges)):
+        hm = PeriodicBoxMesh(e, jitter=JITTER, seed=SEED + e)
+        meshes[e] = (hm, cgx.Mesh(hm))
+    cs = []
+    for k, e in enumerate(edges):
+        hm, gm = meshes[e]
+        prm = cases.tgv_params(Ma=float(rng.uniform(0.1, 0.5)), Re=float(rng.uniform(400, 3200)))
+        prm.check_interval = 50
+        cs.append((gm, prm) + tuple(cases.tgv_state(hm.x_cv[: hm.ncv], prm)))
+    K = args.batch_steps
+    total = float(sum(gm.ncv for gm, *_ in cs)) * K
+    out = {"metric": "batched uneven instances: cell-steps/s", "unit": UNIT, "cases": len(cs),
+           "cells": int(sum(gm.ncv for gm, *_ in cs)), "steps": K, "edges": edges, "data": "synthetic"}
+    for name, prec in (("fp64", cgx.CGX_FP64), ("mixed", cgx.CGX_MIXED)):
+        b = cgx.Batch(0, prec, max_cases=len(cs), hbm_budget=60 << 30)
+        for gm, prm, rho, u, p in cs:
+            assert b.add(gm, prm, rho, u, p, K + 2) is not None
+        b.step(2)  # warm-up (also runs the batch autotuner)
+        t0 = time.perf_counter()
+        b.step(K)
+        el = time.perf_counter() - t0
+        out["batch_" + name] = {"cell_steps_per_s": total / el, "seconds": el}
+        b.close()
+    t0 = time.perf_counter()
+    for gm, prm, rho, u, p in cs:
+        s = cgx.Solver(gm, prm)
+        s.set_state_primitive(rho, u, p)
+        s.initComplete()
+        s.step(K)
+        s.synchronize()
+        s.close()
+    el = time.perf_counter() - t0
+    out["sequential_plain_fp64"] = {"cell_steps_per_s": total / el, "seconds": el}
+    out["speedup_batch_fp64_vs_sequential"] = out["batch_fp64"]["cell_steps_per_s"] / (total / el)
+    out["speedup_batch_mixed_vs_sequential"] = out["batch_mixed"]["cell_steps_per_s"] / (total / el)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -415,11 +532,21 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=16)
+    ap.add_argument("--accuracy", action="store_true",
+                    help="instead of the throughput bench: mixed vs FP64 errors (TGV and solenoidal)")
+    ap.add_argument("--accuracy-steps", type=int, default=500)
+    ap.add_argument("--batch64", action="store_true",
+                    help="instead of the throughput bench: 64 uneven cases in one batch vs one at a time")
+    ap.add_argument("--batch-steps", type=int, default=300)
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         sys.exit("steps >= 1, warmup >= 0")
     if args.impl == "reference":
         return run_reference(args)
+    if args.accuracy:
+        return run_accuracy(args)
+    if args.batch64:
+        return run_batch64(args)
     return run_cgx(args)
 
 

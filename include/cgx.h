@@ -207,6 +207,13 @@ int cgx_synchronize(cgx_solver* s);
  * step, FlowSolver.hpp:2596-2605): run nsteps as cgx_step does and return
  * their device time from CUDA events on the solver's stream. */
 int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms);
+/* As cgx_step_timed, with the two face-flux kernels of calcRhs timed inside
+ * the steps by CUDA events recorded in the step graph around them:
+ * face_ms = {average launch time of the pair (extended faces + compact
+ * closures), of the extended-face kernel, of the compact-closure kernel}
+ * over the 3 x nsteps stages.  The host waits for each step before the next
+ * one (the marks are reused), which device_ms includes. */
+int cgx_step_profiled(cgx_solver* s, int nsteps, float* device_ms, double face_ms[3]);
 /* Average device time of one launch of each step kernel, measured with CUDA
  * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs, both
  * kernels), ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is

@@ -137,7 +137,7 @@ EXPORTS = [
     "cgx_calc_rhs", "cgx_rk3_step", "cgx_calc_cfl", "cgx_advance_solution", "cgx_step",
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
-    "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc",
+    "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled",
 ]
 
 _LIB = None
@@ -178,6 +178,7 @@ def lib():
         "cgx_last_error": (ctypes.c_char_p, []),
         "cgx_step_timed": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
         "cgx_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
+        "cgx_step_profiled": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), c_dbl_p]),
         "cgx_get_tuning": (ctypes.c_int, [vp, c_int_p]),
         "cgx_set_scalars": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
@@ -361,6 +362,14 @@ class Solver:
         ms = ctypes.c_float()
         _check(lib().cgx_step_timed(self.h, int(nsteps), ctypes.byref(ms)))
         return float(ms.value)
+
+    def step_profiled(self, nsteps):
+        """Run nsteps; return (device ms of the steps, {rhs, ext, comp}: the
+        face kernels' average launch time in ms, timed inside the steps)."""
+        ms = ctypes.c_float()
+        f = np.zeros(3)
+        _check(lib().cgx_step_profiled(self.h, int(nsteps), ctypes.byref(ms), _dp(f)))
+        return float(ms.value), dict(zip(("rhs", "ext", "comp"), f.tolist()))
 
     def kernel_times(self, reps=5):
         """Average ms per launch of {rhs (both face kernels), rk+prim, grad,

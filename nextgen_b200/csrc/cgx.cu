@@ -1339,6 +1339,8 @@ struct cgx_solver {
   bool state_set = false;
   bool inited = false;
   cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t pgraph = nullptr;  // the step with face-kernel timing events (cgx_step_profiled)
+  cudaEvent_t pev[9] = {};
   std::atomic<long long> launches{0};
 };
 
@@ -1575,11 +1577,9 @@ int end_var(const Runner& R, int G, int mode) {
 
 int enqueue_grad(const Runner& R) { return grad_var(R, R.tune.g_grad); }
 
-int enqueue_rhs(const Runner& R, int stage0) {
-  int rc = ext_var(R, R.tune.g_ext, stage0);
-  if (rc) return rc;
-  if ((rc = comp_var(R, R.tune.g_comp, stage0))) return rc;
-  if (R.direct && R.dcase.s.nsc > 0) {  // calcRhsScalars, once mf is complete
+// calcRhsScalars, once both face kernels have completed mf
+int enqueue_rhs_sc(const Runner& R, int stage0) {
+  {
     constexpr int G = 4;
     const long long thr = (long long)R.dcase.m.N * G;
     if (R.prec == CGX_MIXED)
@@ -1588,6 +1588,13 @@ int enqueue_rhs(const Runner& R, int stage0) {
       k_rhs_sc<G, false><<<int((thr + 255) / 256), 256, 0, R.stream>>>(R.dcase, stage0);
     return launch_check(R, 1);
   }
+}
+
+int enqueue_rhs(const Runner& R, int stage0) {
+  int rc = ext_var(R, R.tune.g_ext, stage0);
+  if (rc) return rc;
+  if ((rc = comp_var(R, R.tune.g_comp, stage0))) return rc;
+  if (R.direct && R.dcase.s.nsc > 0) return enqueue_rhs_sc(R, stage0);
   return CGX_OK;
 }
 
@@ -1698,10 +1705,25 @@ int autotune(Runner& R, long long ncells) {
 const double kRkW[3][3] = {{1.0, 0.0, 0.0}, {-0.75, 0.25, 0.0}, {-1.0 / 12.0, -1.0 / 12.0, 8.0 / 12.0}};
 
 // one full step: 3 x (rhs, rk+prim, grad) + step_end(advance time, next dt)
-int enqueue_step(const Runner& R) {
+// One RK3 step as enqueue_step enqueues it; with `marks`, events are recorded
+// on the stream before each stage's extended-face kernel (marks[3*st]),
+// between it and the compact-closure kernel (marks[3*st+1]) and after the
+// closures (marks[3*st+2]), so that the face kernels can be timed inside the
+// step.
+int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
   int rc;
   for (int st = 0; st < 3; ++st) {
-    if ((rc = enqueue_rhs(R, st))) return rc;
+    if (marks) {
+      // external records: captured into a graph they become event-record nodes
+      CK(cudaEventRecordWithFlags(marks[3 * st], R.stream, cudaEventRecordExternal));
+      if ((rc = ext_var(R, R.tune.g_ext, st))) return rc;
+      CK(cudaEventRecordWithFlags(marks[3 * st + 1], R.stream, cudaEventRecordExternal));
+      if ((rc = comp_var(R, R.tune.g_comp, st))) return rc;
+      CK(cudaEventRecordWithFlags(marks[3 * st + 2], R.stream, cudaEventRecordExternal));
+      if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, st))) return rc;
+    } else if ((rc = enqueue_rhs(R, st))) {
+      return rc;
+    }
     if ((rc = enqueue_prim(R, st + 1, kRkW[st], -1.0, st == 2))) return rc;
     if ((rc = enqueue_grad(R))) return rc;
   }
@@ -1944,17 +1966,28 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     }
     PT.mark("face numbering");
     // ---- directed entries per cell (new numbering): CSR, compact faces first
+    // (filled in parallel in any order: each cell's entries are sorted by
+    // face id below, so the result is deterministic)
     std::vector<int> deg(N, 0), ncomp(N, 0);
+#pragma omp parallel for schedule(static)
     for (int f = 0; f < nef; ++f) {
       const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
       const bool comp = cf_of_ef[f] >= 0;
       const int na = iperm[a];
+#pragma omp atomic
       ++deg[na];
-      if (comp) ++ncomp[na];
+      if (comp) {
+#pragma omp atomic
+        ++ncomp[na];
+      }
       if (b < N) {
         const int nb = iperm[b];
+#pragma omp atomic
         ++deg[nb];
-        if (comp) ++ncomp[nb];
+        if (comp) {
+#pragma omp atomic
+          ++ncomp[nb];
+        }
       }
     }
     std::vector<long long> cell_off(N + 1, 0);
@@ -1962,15 +1995,22 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     std::vector<int> e_nbr(cell_off[N]), e_fid(cell_off[N]);
     {
       std::vector<long long> fill(cell_off.begin(), cell_off.end() - 1);
+#pragma omp parallel for schedule(static)
       for (int f = 0; f < nef; ++f) {
         const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
         const int na = iperm[a];
         const int nb = nw(b);
-        e_nbr[fill[na]] = nb;
-        e_fid[fill[na]++] = fnew[f];
+        long long ka;
+#pragma omp atomic capture
+        ka = fill[na]++;
+        e_nbr[ka] = nb;
+        e_fid[ka] = fnew[f];
         if (b < N) {
-          e_nbr[fill[nb]] = na;
-          e_fid[fill[nb]++] = fnew[f] | kRevBit;
+          long long kb;
+#pragma omp atomic capture
+          kb = fill[nb]++;
+          e_nbr[kb] = na;
+          e_fid[kb] = fnew[f] | kRevBit;
         }
       }
     }
@@ -2038,80 +2078,95 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     std::vector<unsigned short> cglidx(std::max(coff[N], 1LL));
     int max_u = 0, max_cu = 0;
     {
-      std::vector<int> mark(N, -1), slot(N, 0), cmark(N, -1), cslot(N, 0);
-      std::vector<int> halo, chalo;
-      // halo of [c0, c0+nc): cells outside it reached by its entries
-      auto unions = [&](int c0, int nc, int tag) {
-        halo.clear();
-        chalo.clear();
-        for (int i = c0; i < c0 + nc; ++i)
-          for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
-            const int j = e_nbr[k];
-            if (j >= c0 && j < c0 + nc) continue;
-            if (mark[j] != tag) {
-              mark[j] = tag;
-              halo.push_back(j);
-            }
-            if (k < cell_off[i] + ncomp[i] && cmark[j] != tag) {
-              cmark[j] = tag;
-              chalo.push_back(j);
-            }
-          }
-        // the gradient stencil (cvocv) reads the compact union too
-        for (int i = c0; i < c0 + nc; ++i)
-          for (long long k = coff[i]; k < coff[i + 1]; ++k) {
-            const int j = c_nbr[k];
-            if (j >= c0 && j < c0 + nc) continue;
-            if (cmark[j] != tag) {
-              cmark[j] = tag;
-              chalo.push_back(j);
-            }
-          }
-        std::sort(halo.begin(), halo.end());
-        std::sort(chalo.begin(), chalo.end());
+      // Base items of kItemCells cells are independent: each is built in
+      // parallel (and split in halves, first half first, while its unions
+      // exceed the staging budget), then the items are concatenated in cell
+      // order.  The result does not depend on the thread count.
+      struct SubItem {
+        int c0, nc;
+        std::vector<int> halo, chalo;  // ascending
       };
-      int tag = 0;
-      std::vector<std::pair<int, int>> todo;
-      for (int c0 = N - (N - 1) % kItemCells - 1; c0 >= 0; c0 -= kItemCells)
-        todo.push_back({c0, std::min(kItemCells, N - c0)});
-      while (!todo.empty()) {
-        const auto [c0, nc] = todo.back();
-        todo.pop_back();
-        unions(c0, nc, ++tag);
-        const int nu = nc + int(halo.size()), ncu = nc + int(chalo.size());
-        if ((nu > kMaxUnionExt || ncu > kMaxUnionComp) && nc > 1) {
-          const int h1 = nc / 2;  // split, first half processed first
-          todo.push_back({c0 + h1, nc - h1});
-          todo.push_back({c0, h1});
-          continue;
+      const int nbase = (N + kItemCells - 1) / kItemCells;
+      std::vector<std::vector<SubItem>> sub(nbase);
+      int too_big = 0;
+#pragma omp parallel
+      {
+        // halo of [c0, c0+nc): cells outside it reached by its entries; the
+        // gradient stencil (cvocv) reads the compact union too
+        auto unions = [&](int c0, int nc, std::vector<int>& halo, std::vector<int>& chalo) {
+          halo.clear();
+          chalo.clear();
+          for (int i = c0; i < c0 + nc; ++i) {
+            for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
+              const int j = e_nbr[k];
+              if (j >= c0 && j < c0 + nc) continue;
+              halo.push_back(j);
+              if (k < cell_off[i] + ncomp[i]) chalo.push_back(j);
+            }
+            for (long long k = coff[i]; k < coff[i + 1]; ++k) {
+              const int j = c_nbr[k];
+              if (j < c0 || j >= c0 + nc) chalo.push_back(j);
+            }
+          }
+          std::sort(halo.begin(), halo.end());
+          halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
+          std::sort(chalo.begin(), chalo.end());
+          chalo.erase(std::unique(chalo.begin(), chalo.end()), chalo.end());
+        };
+        auto local = [](const std::vector<int>& h, int nc, int j) {
+          return (unsigned short)(nc + int(std::lower_bound(h.begin(), h.end(), j) - h.begin()));
+        };
+#pragma omp for schedule(dynamic, 16) reduction(| : too_big)
+        for (int bi = 0; bi < nbase; ++bi) {
+          std::vector<std::pair<int, int>> todo{{bi * kItemCells, std::min(kItemCells, N - bi * kItemCells)}};
+          while (!todo.empty()) {
+            const auto [c0, nc] = todo.back();
+            todo.pop_back();
+            SubItem si{c0, nc, {}, {}};
+            unions(c0, nc, si.halo, si.chalo);
+            const int nu = nc + int(si.halo.size()), ncu = nc + int(si.chalo.size());
+            if ((nu > kMaxUnionExt || ncu > kMaxUnionComp) && nc > 1) {
+              const int h1 = nc / 2;  // split, first half processed first
+              todo.push_back({c0 + h1, nc - h1});
+              todo.push_back({c0, h1});
+              continue;
+            }
+            if (nu > kMaxUnionExt || ncu > kMaxUnionComp) {
+              too_big = 1;
+              break;
+            }
+            for (int i = c0; i < c0 + nc; ++i) {
+              for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
+                const int j = e_nbr[k];
+                const bool in = j >= c0 && j < c0 + nc;
+                lidx[k] = in ? (unsigned short)(j - c0) : local(si.halo, nc, j);
+                const long long t = k - cell_off[i];
+                if (t < ncomp[i]) clidx[qoff[i] + t] = in ? (unsigned short)(j - c0) : local(si.chalo, nc, j);
+              }
+              for (long long k = coff[i]; k < coff[i + 1]; ++k) {
+                const int j = c_nbr[k];
+                cglidx[k] = (j >= c0 && j < c0 + nc) ? (unsigned short)(j - c0) : local(si.chalo, nc, j);
+              }
+            }
+            sub[bi].push_back(std::move(si));
+          }
         }
-        if (nu > kMaxUnionExt || ncu > kMaxUnionComp)
-          return bail(fail(CGX_E_ARG, "a cell has more neighbours than the face kernels can stage"));
-        Item it{0, c0, nc, int(items.size()), int(hcell.size()), int(halo.size()), int(chcell.size()),
-                int(chalo.size())};
-        for (size_t t = 0; t < halo.size(); ++t) slot[halo[t]] = nc + int(t);
-        for (size_t t = 0; t < chalo.size(); ++t) cslot[chalo[t]] = nc + int(t);
-        for (int i = c0; i < c0 + nc; ++i)
-          for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
-            const int j = e_nbr[k];
-            const bool in = j >= c0 && j < c0 + nc;
-            lidx[k] = (unsigned short)(in ? j - c0 : slot[j]);
-            const long long t = k - cell_off[i];
-            if (t < ncomp[i]) clidx[qoff[i] + t] = (unsigned short)(in ? j - c0 : cslot[j]);
-          }
-        for (int i = c0; i < c0 + nc; ++i)
-          for (long long k = coff[i]; k < coff[i + 1]; ++k) {
-            const int j = c_nbr[k];
-            cglidx[k] = (unsigned short)((j >= c0 && j < c0 + nc) ? j - c0 : cslot[j]);
-          }
-        hcell.insert(hcell.end(), halo.begin(), halo.end());
-        chcell.insert(chcell.end(), chalo.begin(), chalo.end());
-        if (hcell.size() > size_t(0x7ffffff0) || chcell.size() > size_t(0x7ffffff0))
-          return bail(fail(CGX_E_ARG, "mesh too large"));
-        items.push_back(it);
-        max_u = std::max(max_u, nu);
-        max_cu = std::max(max_cu, ncu);
       }
+      if (too_big) return bail(fail(CGX_E_ARG, "a cell has more neighbours than the face kernels can stage"));
+      for (int bi = 0; bi < nbase; ++bi)
+        for (SubItem& si : sub[bi]) {
+          const int nh = int(si.halo.size()), nch = int(si.chalo.size());
+          Item it{0, si.c0, si.nc, int(items.size()), int(hcell.size()), nh, int(chcell.size()), nch};
+          hcell.insert(hcell.end(), si.halo.begin(), si.halo.end());
+          chcell.insert(chcell.end(), si.chalo.begin(), si.chalo.end());
+          if (hcell.size() > size_t(0x7ffffff0) || chcell.size() > size_t(0x7ffffff0))
+            return bail(fail(CGX_E_ARG, "mesh too large"));
+          items.push_back(it);
+          max_u = std::max(max_u, si.nc + nh);
+          max_cu = std::max(max_cu, si.nc + nch);
+          std::vector<int>().swap(si.halo);
+          std::vector<int>().swap(si.chalo);
+        }
     }
     if (hcell.empty()) hcell.push_back(0);
     if (chcell.empty()) chcell.push_back(0);
@@ -2404,6 +2459,9 @@ extern "C" int cgx_solver_destroy(cgx_solver* s) {
   if (!s) return CGX_OK;
   cudaSetDevice(s->mesh->device);
   if (s->graph) cudaGraphExecDestroy(s->graph);
+  if (s->pgraph) cudaGraphExecDestroy(s->pgraph);
+  for (cudaEvent_t e : s->pev)
+    if (e) cudaEventDestroy(e);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void* q : s->allocs) cudaFree(q);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -2494,6 +2552,10 @@ extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
     s->hcase.s = sd;
     s->run.dcase.s = sd;
     CK(cudaMemcpyAsync(s->d_case, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream));
+    if (s->pgraph) {
+      cudaGraphExecDestroy(s->pgraph);
+      s->pgraph = nullptr;
+    }
     if (s->graph) {
       cudaGraphExecDestroy(s->graph);
       s->graph = nullptr;
@@ -2706,6 +2768,67 @@ extern "C" int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms) {
   CK(cudaEventElapsedTime(device_ms, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  bool nan = false;
+  if ((rc = check_nan(s, &nan))) return rc;
+  if (nan) {
+    if ((rc = restore_state(s))) return rc;
+    return fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8");
+  }
+  return CGX_OK;
+}
+
+// The step graph with the timing events; re-captured with the step graph.
+static int ensure_pgraph(cgx_solver* s) {
+  if (s->pgraph) return CGX_OK;
+  for (cudaEvent_t& e : s->pev)
+    if (!e) CK(cudaEventCreate(&e));
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  const long long before = s->launches.load();
+  int rc = enqueue_step(s->run, s->pev);
+  cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
+  s->launches = before;
+  if (rc) return rc;
+  if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+  ec = cudaGraphInstantiate(&s->pgraph, g, 0);
+  cudaGraphDestroy(g);
+  if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec));
+  return CGX_OK;
+}
+
+extern "C" int cgx_step_profiled(cgx_solver* s, int nsteps, float* device_ms, double face_ms[3]) {
+  if (!s || !device_ms || !face_ms) return fail(CGX_E_ARG, "null argument");
+  if (!s->inited) return fail(CGX_E_STATE, "cgx_init_complete not called");
+  if (nsteps < 1) return fail(CGX_E_ARG, "nsteps < 1");
+  CK(cudaSetDevice(s->mesh->device));
+  int rc = ensure_pgraph(s);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double ext = 0.0, comp = 0.0;
+  CK(cudaEventRecord(e0, s->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    CK(cudaGraphLaunch(s->pgraph, s->stream));
+    s->launches += launches_per_step(s->run);
+    CK(cudaEventSynchronize(s->pev[8]));  // this step's marks, before the next replay reuses them
+    for (int st = 0; st < 3; ++st) {
+      float a = 0.f, b = 0.f;
+      CK(cudaEventElapsedTime(&a, s->pev[3 * st], s->pev[3 * st + 1]));
+      CK(cudaEventElapsedTime(&b, s->pev[3 * st + 1], s->pev[3 * st + 2]));
+      ext += a;
+      comp += b;
+    }
+  }
+  CK(cudaEventRecord(e1, s->stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(device_ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const double n = 3.0 * nsteps;
+  face_ms[0] = (ext + comp) / n;
+  face_ms[1] = ext / n;
+  face_ms[2] = comp / n;
   bool nan = false;
   if ((rc = check_nan(s, &nan))) return rc;
   if (nan) {
