@@ -466,6 +466,52 @@ def run_accuracy(args):
     return 0
 
 
+def run_validate(args):
+    """The FP64 GPU path against the CPU oracle over many steps: the Mt 0.3
+    random-solenoidal state on the jittered n^3 mesh (128^3, about 2.1M cells,
+    by default) advanced `--validate-steps` RK3 steps (200 by default) at CFL
+    0.8 by both from the same initial state; the oracle runs on all host
+    cores.  Prints one JSON line with the relative differences of the state
+    and of the conserved totals, and the step counts and times reached."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    from nextgen_b200 import cases, cgx
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    n, K = args.validate_n, args.validate_steps
+    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED, nthreads=os.cpu_count() or 1)
+    prm = cases.hit_params(Mt=0.3)
+    prm.check_interval = 50
+    rho, u, p = cases.hit_state(n, prm, Mt=0.3, k0=4.0, seed=4321)
+    s = cgx.Solver(cgx.Mesh(m), prm)
+    s.set_state_primitive(rho, u, p)
+    s.initComplete()
+    o = Oracle(m, prm, nparts=os.cpu_count() or 1)
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    t0 = time.perf_counter()
+    assert s.step(K) == 0
+    t_gpu = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    assert o.step(K) == 0
+    t_cpu = time.perf_counter() - t0
+    g, r = s.get_state(), o.get_state()
+    rel = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())
+    tg, tr = s.totals(), o.totals()
+    vol = np.array(m.vol_cv)
+    scale = np.array([(r[0] * vol).sum()] + [np.abs(r[0] * r[1][:, k] * vol).sum() for k in range(3)] +
+                     [(r[2] * vol).sum()])
+    out = {"metric": "FP64 GPU vs CPU oracle after %d RK3 steps" % K, "cells": m.ncv,
+           "config": {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3, random solenoidal "
+                                  "Mt 0.3, CFL 0.8, Vreman" % n},
+           "rho_linf_rel": rel(g[0], r[0]), "u_linf_rel": rel(g[1], r[1]), "rhoE_linf_rel": rel(g[2], r[2]),
+           "totals_rel": float((np.abs(tg - tr) / scale).max()),
+           "time_gpu_vs_oracle_rel": abs(s.time()[0] - o.time()[0]) / o.time()[0],
+           "steps": [s.time()[2], o.time()[2]], "gpu_s": t_gpu, "oracle_s": t_cpu,
+           "oracle_threads": os.cpu_count() or 1, "data": "synthetic"}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_batch64(args, seed=64):
     """64 independent Taylor-Green cases of uneven size in one batch: edges
     log-uniform in [8, 64] (512 to 262,144 cells, +/-0.25h jitter), Mach
@@ -538,6 +584,10 @@ def main():
     ap.add_argument("--batch64", action="store_true",
                     help="instead of the throughput bench: 64 uneven cases in one batch vs one at a time")
     ap.add_argument("--batch-steps", type=int, default=300)
+    ap.add_argument("--validate", action="store_true",
+                    help="instead of the throughput bench: FP64 GPU vs CPU oracle over many steps")
+    ap.add_argument("--validate-n", type=int, default=128)
+    ap.add_argument("--validate-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         sys.exit("steps >= 1, warmup >= 0")
@@ -547,6 +597,8 @@ def main():
         return run_accuracy(args)
     if args.batch64:
         return run_batch64(args)
+    if args.validate:
+        return run_validate(args)
     return run_cgx(args)
 
 

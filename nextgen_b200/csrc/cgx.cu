@@ -104,22 +104,6 @@ __device__ __forceinline__ void st4(void* p, double a, double b, double c, doubl
   asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
 }
 
-__device__ __forceinline__ void load_L(const LRec* base, int j, LRec& r) {
-  const double* p = reinterpret_cast<const double*>(base + j);
-  const double4 a = ld4(p), b = ld4(p + 4);
-  r.u[0] = a.x; r.u[1] = a.y; r.u[2] = a.z; r.sp_vol = a.w;
-  r.p = b.x; r.h = b.y; r.rho = b.z; r.sos = b.w;
-}
-
-// properties and dudx of one cell (the whole 128 B record)
-__device__ __forceinline__ void load_V(const VRec* base, int j, VRec& r) {
-  const double* p = reinterpret_cast<const double*>(base + j);
-  const double4 a = ld4(p), b = ld4(p + 4), c = ld4(p + 8), d = ld4(p + 12);
-  r.mu_total = a.x; r.loc_total = a.y; r.a_sgs = a.z; r.fgr = a.w;
-  r.symh = b.x; r.symp = b.y; r.g[0] = b.z; r.g[1] = b.w;
-  r.g[2] = c.x; r.g[3] = c.y; r.g[4] = c.z; r.g[5] = c.w;
-  r.g[6] = d.x; r.g[7] = d.y; r.g[8] = d.z;
-}
 
 // dudx of one cell
 __device__ __forceinline__ void load_Vg(const VRec* base, int j, double g[9]) {
@@ -250,22 +234,6 @@ __device__ __forceinline__ void smem_L(const int4* sm, int j, LRec& r) {
   r.p = c.x; r.h = c.y; r.rho = d.x; r.sos = d.y;
 }
 
-__device__ __forceinline__ void smem_V(const int4* sm, int j, VRec& r) {
-  const double2* p = reinterpret_cast<const double2*>(sm);
-  double2 x = p[swz<8>(j, 0)];
-  r.mu_total = x.x; r.loc_total = x.y;
-  x = p[swz<8>(j, 1)];
-  r.a_sgs = x.x; r.fgr = x.y;
-  x = p[swz<8>(j, 2)];
-  r.symh = x.x; r.symp = x.y;
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    x = p[swz<8>(j, 3 + c)];
-    r.g[2 * c] = x.x;
-    r.g[2 * c + 1] = x.y;
-  }
-  r.g[8] = p[swz<8>(j, 7)].x;
-}
 
 // field-wise sum of two cells' viscous records in shared memory
 __device__ __forceinline__ void smem_V_sum(const int4* sm, int a, int b, VRec& r) {

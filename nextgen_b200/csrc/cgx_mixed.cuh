@@ -25,31 +25,6 @@ struct FluxF {
   float rho, ru[3], rE;
 };
 
-// 256-bit read-only load of eight floats (sm_100)
-__device__ __forceinline__ void ld8f(const void* p, float4& x, float4& y) {
-  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-      : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(y.x), "=f"(y.y), "=f"(y.z), "=f"(y.w)
-      : "l"(p));
-}
-
-__device__ __forceinline__ void load_LF(const LRecF* base, int j, LRecF& r) {
-  float4 a, b;
-  ld8f(base + j, a, b);
-  r.u[0] = a.x; r.u[1] = a.y; r.u[2] = a.z; r.sp_vol = a.w;
-  r.pp = b.x; r.hh = b.y; r.rho = b.z; r.sos = b.w;
-}
-
-// properties and dudx of one cell (the whole 64 B record)
-__device__ __forceinline__ void load_VF(const VRecF* base, int j, VRecF& r) {
-  float4 a, b, c, d;
-  ld8f(base + j, a, b);
-  ld8f(reinterpret_cast<const float*>(base + j) + 8, c, d);
-  r.mu_total = a.x; r.loc_total = a.y; r.a_sgs = a.z; r.fgr = a.w;
-  r.symh = b.x; r.symp = b.y; r.g[0] = b.z; r.g[1] = b.w;
-  r.g[2] = c.x; r.g[3] = c.y; r.g[4] = c.z; r.g[5] = c.w;
-  r.g[6] = d.x; r.g[7] = d.y; r.g[8] = d.z;
-}
-
 // FP32 records in the swizzled shared arrays
 __device__ __forceinline__ void smem_LF(const int4* sm, int j, LRecF& r) {
   const float4* p = reinterpret_cast<const float4*>(sm);
@@ -68,15 +43,6 @@ __device__ __forceinline__ void smem_VF_sum(const int4* sm, int a, int b, VRecF&
   r.g[2] = x.x + y.x; r.g[3] = x.y + y.y; r.g[4] = x.z + y.z; r.g[5] = x.w + y.w;
   x = p[swz<4>(a, 3)]; y = p[swz<4>(b, 3)];
   r.g[6] = x.x + y.x; r.g[7] = x.y + y.y; r.g[8] = x.z + y.z;
-}
-
-__device__ __forceinline__ void smem_VF(const int4* sm, int j, VRecF& r) {
-  const float4* p = reinterpret_cast<const float4*>(sm);
-  const float4 a = p[swz<4>(j, 0)], b = p[swz<4>(j, 1)], c = p[swz<4>(j, 2)], d = p[swz<4>(j, 3)];
-  r.mu_total = a.x; r.loc_total = a.y; r.a_sgs = a.z; r.fgr = a.w;
-  r.symh = b.x; r.symp = b.y; r.g[0] = b.z; r.g[1] = b.w;
-  r.g[2] = c.x; r.g[3] = c.y; r.g[4] = c.z; r.g[5] = c.w;
-  r.g[6] = d.x; r.g[7] = d.y; r.g[8] = d.z;
 }
 
 // the once-per-step kernel's streams, mixed form
