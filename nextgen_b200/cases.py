@@ -1,5 +1,6 @@
-"""Canonical periodic-box cases: Taylor-Green vortex and decaying isotropic
-turbulence initial states, with the solver parameters they run with.
+"""Canonical periodic-box cases: Taylor-Green vortex, decaying isotropic
+turbulence and the inviscid (isentropic) vortex, with the solver parameters
+they run with.
 
 All fields are evaluated in the caller's (lattice) cell order.
 """
@@ -87,3 +88,58 @@ def hit_state(n, prm, Mt=0.3, k0=4.0, seed=4321):
     rho = np.full(ncv, prm.rho_ref)
     p = np.full(ncv, prm.p_ref)
     return rho, u, p
+
+
+def vortex_params(gamma=1.4, cfl=0.8):
+    """The reference's inviscid vortex harness (IdealGasEulerSolver,
+    src/charles/charles_ig.cpp:170-290): rho_inf = p_inf = 1, no viscosity and
+    no SGS model, CFL time step."""
+    prm = Params()
+    prm.gamma = gamma
+    prm.rho_ref = 1.0
+    prm.p_ref = 1.0
+    prm.T_ref = 1.0
+    prm.mu_ref = 0.0
+    prm.sgs_model = 0
+    prm.dt_mode = 1
+    prm.dt_data[0] = cfl
+    return prm
+
+
+def vortex_state(x_cv, prm, t=0.0, u_inf=0.5, Lx=10.0, Ly=10.0 * np.sqrt(3.0) / 2.0, periodic=True,
+                 x0=-2.5, y0=-2.5, theta=np.pi / 3.0, e_twopi=0.32, rc=1.0):
+    """calcInviscidVortexLocal (src/charles/charles_ig.cpp:88-168): the exact
+    isentropic vortex at time t, of circulation parameter e_twopi (0.32, the
+    reference's "strong" setting) and radius rc, started at (x0, y0) and
+    advected at u_inf along theta.  On a periodic box [-Lx, Lx] x [-Ly, Ly] the
+    vortex offset is wrapped into the box.  Defaults are the reference's
+    (EULER_UINF 0.5, EULER_LX 10, EULER_LY 10 sqrt(3)/2).  Returns rho, u, p."""
+    gamma = prm.gamma
+    Ma_inf = u_inf / np.sqrt(gamma * prm.p_ref / prm.rho_ref)
+    coeff = 0.5 * e_twopi * e_twopi * (gamma - 1.0) * Ma_inf * Ma_inf
+    dx = x_cv[:, 0] - x0 - u_inf * np.cos(theta) * t
+    dy = x_cv[:, 1] - y0 - u_inf * np.sin(theta) * t
+    if periodic:
+        dx = (dx + Lx) % (2.0 * Lx) - Lx
+        dy = (dy + Ly) % (2.0 * Ly) - Ly
+    f0 = 1.0 - (dx * dx + dy * dy) / (rc * rc)
+    rho = prm.rho_ref * (1.0 - coeff * np.exp(f0)) ** (1.0 / (gamma - 1.0))
+    u = np.zeros((len(dx), 3))
+    u[:, 0] = u_inf * (np.cos(theta) - e_twopi * dy / rc * np.exp(f0 / 2.0))
+    u[:, 1] = u_inf * (np.sin(theta) + e_twopi * dx / rc * np.exp(f0 / 2.0))
+    p = prm.p_ref * (1.0 - coeff * np.exp(f0)) ** (gamma / (gamma - 1.0))
+    return np.ascontiguousarray(rho), np.ascontiguousarray(u), np.ascontiguousarray(p)
+
+
+def vortex_errors(x_cv, vol_cv, rho, u, rhoE, prm, t, **vortex_kw):
+    """The error norms IdealGasEulerSolver::temporalHook reports
+    (src/charles/charles_ig.cpp:224-288): volume-weighted L2 and Linf of
+    rho - rho_exact, u - u_exact (3) and rhoE - rhoE_exact against the exact
+    vortex at time t.  Returns (l2[5], linf[5])."""
+    re, ue, pe = vortex_state(x_cv, prm, t=t, **vortex_kw)
+    rEe = pe / (prm.gamma - 1.0) + 0.5 * re * (ue * ue).sum(1)
+    d = np.column_stack([rho - re, u - ue, rhoE - rEe])
+    vol = np.asarray(vol_cv)
+    l2 = np.sqrt((vol[:, None] * d * d).sum(0) / vol.sum())
+    linf = np.abs(d).max(0)
+    return l2, linf
