@@ -1,6 +1,6 @@
 """Build the package's native libraries in-tree (nextgen_b200/lib/).
 
-  libcgx.so          CUDA kernels + C ABI (include/cgx.h), sm_100a only
+  libcgx.so          CUDA kernels + C ABI (include/cgx.h, include/cgx_ops.h), sm_100a only
   libcgx_meshgen.so  host mesh/operator generator (include/cgx_meshgen.h)
 
 `python -m nextgen_b200.build` rebuilds whatever is out of date.
@@ -52,7 +52,7 @@ def _run(cmd):
 def build_meshgen(force=False):
     out = os.path.join(LIB, "libcgx_meshgen.so")
     src = os.path.join(CSRC, "meshgen.cpp")
-    if force or _stale(out, [src, os.path.join(INC, "cgx_meshgen.h")]):
+    if force or _stale(out, [src, os.path.join(CSRC, "svd33.h"), os.path.join(INC, "cgx_meshgen.h")]):
         os.makedirs(LIB, exist_ok=True)
         _run([_cxx(), "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out, src])
     return out
@@ -60,15 +60,21 @@ def build_meshgen(force=False):
 
 def build_cgx(force=False, verbose=False):
     out = os.path.join(LIB, "libcgx.so")
-    srcs = [os.path.join(CSRC, f) for f in ("cgx.cu", "cgx_kernels.cuh", "cgx_mixed.cuh")] + [os.path.join(INC, "cgx.h")]
+    ops_obj = os.path.join(LIB, "cgx_ops.o")
+    srcs = [os.path.join(CSRC, f) for f in ("cgx.cu", "cgx_kernels.cuh", "cgx_mixed.cuh", "cgx_ops.cu", "svd33.h")] + \
+        [os.path.join(INC, h) for h in ("cgx.h", "cgx_ops.h", "cgx_meshgen.h")]
     if force or _stale(out, srcs):
         os.makedirs(LIB, exist_ok=True)
-        cmd = [_nvcc(), "-O3", "-std=c++17"] + NVCC_ARCH + [
-            "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", _cxx(),
-            "-shared", "-o", out, os.path.join(CSRC, "cgx.cu"), "-lgomp"]
+        common = [_nvcc(), "-O3", "-std=c++17"] + NVCC_ARCH + ["-lineinfo", "-ccbin", _cxx()]
         if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        log = _run(cmd)
+            common.insert(1, "-Xptxas=-v")
+        # the operator build reproduces the host generator's arithmetic bit
+        # for bit, so it is compiled without multiply-add contraction
+        log = _run(common + ["-fmad=false", "-Xcompiler", "-fPIC", "-c", "-o", ops_obj,
+                             os.path.join(CSRC, "cgx_ops.cu")])
+        log += _run(common + ["-Xcompiler", "-fPIC,-fopenmp", "-shared", "-o", out,
+                              os.path.join(CSRC, "cgx.cu"), ops_obj, "-lgomp"])
+        os.remove(ops_obj)
         if verbose:
             sys.stdout.write(log)
     return out

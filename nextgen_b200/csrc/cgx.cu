@@ -1770,6 +1770,11 @@ int check_nan(cgx_solver* s, bool* got) {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+namespace cgx {
+// error text for calls implemented in other translation units of this library
+void set_last_error(const std::string& s) { g_err = s; }
+}  // namespace cgx
+
 extern "C" const char* cgx_last_error(void) { return g_err.c_str(); }
 
 extern "C" void cgx_params_default(cgx_params* p) {

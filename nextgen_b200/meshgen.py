@@ -85,11 +85,15 @@ class PeriodicBoxMesh:
                                             ctypes.byref(out))
         if rc != 0:
             raise RuntimeError("meshgen failed (%d): %s" % (rc, lib().cgx_meshgen_last_error().decode()))
+        self._free = lib().cgx_meshgen_free
+        self._attach(out, (int(nx), int(ny), int(nz)), Ls, float(jitter), int(seed))
+
+    def _attach(self, out, dims, Ls, jitter, seed):
         self.ptr = out
-        self.dims = (int(nx), int(ny), int(nz))
+        self.dims = dims
         self.L = Ls
-        self.jitter = float(jitter)
-        self.seed = int(seed)
+        self.jitter = jitter
+        self.seed = seed
         m = out.contents
         self.ncv, self.ncv_g, self.ncv_g2 = m.ncv, m.ncv_g, m.ncv_g2
         self.nfa, self.nfa_i, self.nef, self.nef_i = m.nfa, m.nfa_i, m.nef, m.nef_i
@@ -102,7 +106,7 @@ class PeriodicBoxMesh:
         self.area_over_delta_fa = _view(m.area_over_delta_fa, (self.nfa,), np.float64)
         self.vol_cv = _view(m.vol_cv, (self.ncv,), np.float64)
         self.x_cv = _view(m.x_cv, (self.ncv_g2, 3), np.float64)
-        self.x_vv = _view(m.x_vv, (self.ncv, 3), np.float64)
+        self.x_vv = _view(m.x_vv, (self.ncv, 3), np.float64) if m.x_vv else None
         self.cvocv_i = _view(m.cvocv_i, (self.ncv + 1,), np.int32)
         ncoc = int(self.cvocv_i[-1])
         self.cvocv_v = _view(m.cvocv_v, (ncoc,), np.int32)
@@ -135,8 +139,8 @@ class PeriodicBoxMesh:
         return (self.nfa_i + 0.5 * (self.nfa - self.nfa_i)) / self.ncv
 
     def close(self):
-        if self.ptr:
-            lib().cgx_meshgen_free(self.ptr)
+        if getattr(self, "ptr", None):
+            self._free(self.ptr)
             self.ptr = None
 
     def __del__(self):
@@ -144,3 +148,74 @@ class PeriodicBoxMesh:
             self.close()
         except Exception:
             pass
+
+
+class CompactDesc(ctypes.Structure):
+    """cgx_compact_desc (include/cgx_ops.h)."""
+    _fields_ = [
+        ("ncv", ctypes.c_int), ("ncv_g", ctypes.c_int), ("nfa", ctypes.c_int), ("nfa_i", ctypes.c_int),
+        ("L", ctypes.c_double * 3), ("h", ctypes.c_double),
+        ("cvofa", c_int_p), ("n_fa", c_dbl_p), ("x_fa", c_dbl_p), ("vol_cv", c_dbl_p),
+        ("x_cv", c_dbl_p), ("x_vv", c_dbl_p), ("icv_owner_g", c_int_p), ("shift_g", c_int_p),
+    ]
+
+
+def _ops_lib():
+    from . import cgx
+    L = cgx.lib()
+    if not getattr(L, "_ops_bound", False):
+        L.cgx_operators_build.restype = ctypes.c_int
+        L.cgx_operators_build.argtypes = [ctypes.POINTER(CompactDesc), ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, ctypes.POINTER(ctypes.POINTER(MeshgenOut)),
+                                          ctypes.POINTER(ctypes.c_float)]
+        L.cgx_operators_free.restype = None
+        L.cgx_operators_free.argtypes = [ctypes.POINTER(MeshgenOut)]
+        L._ops_bound = True
+    return L
+
+
+def compact_desc(mesh):
+    """The compact part of a mesh (cells, compact faces, level-1 ghosts) as a
+    cgx_compact_desc.  The arrays stay owned by `mesh`."""
+    ng1 = mesh.ncv_g - mesh.ncv
+    d = CompactDesc()
+    d.ncv, d.ncv_g, d.nfa, d.nfa_i = mesh.ncv, mesh.ncv_g, mesh.nfa, mesh.nfa_i
+    d.L[:] = [float(v) for v in mesh.L]
+    d.h = mesh.h
+    keep = []
+
+    def ptr(a, ct, n=None):
+        a = np.ascontiguousarray(a if n is None else a[:n])
+        keep.append(a)
+        return a.ctypes.data_as(ctypes.POINTER(ct))
+    d.cvofa = ptr(mesh.cvofa, ctypes.c_int)
+    d.n_fa = ptr(mesh.n_fa, ctypes.c_double)
+    d.x_fa = ptr(mesh.x_fa, ctypes.c_double)
+    d.vol_cv = ptr(mesh.vol_cv, ctypes.c_double)
+    d.x_cv = ptr(mesh.x_cv, ctypes.c_double, mesh.ncv)
+    d.x_vv = ptr(mesh.x_vv, ctypes.c_double) if mesh.x_vv is not None else None
+    d.icv_owner_g = ptr(mesh.icv_owner_g, ctypes.c_int, ng1)
+    d.shift_g = ptr(mesh.shift_g, ctypes.c_int, ng1)
+    d._keep = keep
+    return d
+
+
+class DeviceOperatorMesh(PeriodicBoxMesh):
+    """A mesh whose operators (gradient coefficients, extended faces, level-2
+    ghosts, per-cell factors) were built on the GPU by cgx_operators_build
+    from another mesh's compact part.  Same attributes as PeriodicBoxMesh;
+    `device_ms` is the device time of the build."""
+
+    def __init__(self, source, device=0, interp_factor=1.0 / 3.0, sigma_thresh=0.45):
+        L = _ops_lib()
+        desc = compact_desc(source)
+        out = ctypes.POINTER(MeshgenOut)()
+        ms = ctypes.c_float()
+        rc = L.cgx_operators_build(ctypes.byref(desc), float(interp_factor), float(sigma_thresh), int(device),
+                                   ctypes.byref(out), ctypes.byref(ms))
+        if rc != 0:
+            from . import cgx
+            raise cgx.CgxError(rc, L.cgx_last_error().decode())
+        self.device_ms = ms.value
+        self._free = L.cgx_operators_free
+        self._attach(out, source.dims, source.L, source.jitter, source.seed)

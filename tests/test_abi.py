@@ -28,6 +28,31 @@ def test_cgx_exports_every_declared_symbol(built):
     assert set(cgx.EXPORTS) <= set(names)
 
 
+def test_cgx_exports_every_operator_build_symbol(built):
+    from nextgen_b200 import _lib
+    names = declared("include/cgx_ops.h")
+    assert names == ["cgx_operators_build", "cgx_operators_free"]
+    L = ctypes.CDLL(_lib.path("libcgx.so"))
+    assert all(hasattr(L, n) for n in names)
+
+
+def test_operator_build_checks_arguments_before_the_device(built):
+    """Invalid descriptors fail on the host with CGX_E_ARG (no GPU needed)."""
+    from nextgen_b200 import meshgen
+    L = meshgen._ops_lib()
+    out = ctypes.POINTER(meshgen.MeshgenOut)()
+    assert L.cgx_operators_build(None, 1.0 / 3.0, 0.45, 0, ctypes.byref(out), None) == -1
+    d = meshgen.CompactDesc()  # ncv = 0, no arrays
+    assert L.cgx_operators_build(ctypes.byref(d), 1.0 / 3.0, 0.45, 0, ctypes.byref(out), None) == -1
+    assert b"invalid argument" in L.cgx_last_error()
+    m = meshgen.PeriodicBoxMesh(6, jitter=0.1)
+    d = meshgen.compact_desc(m)
+    assert L.cgx_operators_build(ctypes.byref(d), 1.0 / 3.0, 0.45, 0, None, None) == -1
+    d.L[1] = 0.0
+    assert L.cgx_operators_build(ctypes.byref(d), 1.0 / 3.0, 0.45, 0, ctypes.byref(out), None) == -1
+    assert not out
+
+
 def test_meshgen_exports_every_declared_symbol(built):
     from nextgen_b200 import _lib
     names = declared("include/cgx_meshgen.h")
