@@ -563,6 +563,78 @@ def run_batch64(args, seed=64):
     return 0
 
 
+def _host_phases(fn):
+    """Run fn() with the host generator's phase timer on; returns (fn(),
+    {phase: seconds}) parsed from what the generator writes to stderr."""
+    import tempfile
+    os.environ["CGX_MESHGEN_VERBOSE"] = "1"
+    sys.stderr.flush()
+    saved = os.dup(2)
+    with tempfile.TemporaryFile(mode="w+") as tf:
+        os.dup2(tf.fileno(), 2)
+        try:
+            res = fn()
+        finally:
+            os.dup2(saved, 2)
+            os.close(saved)
+            del os.environ["CGX_MESHGEN_VERBOSE"]
+        tf.seek(0)
+        phases = {}
+        for line in tf.read().splitlines():
+            if line.startswith("meshgen "):
+                name, sec = line[len("meshgen "):].rsplit(None, 2)[0].strip(), float(line.split()[-2])
+                phases[name] = phases.get(name, 0.0) + sec
+    return res, phases
+
+
+def run_opbuild(args):
+    """The operator build (gradient coefficients, extended faces, level-2
+    ghosts, per-cell factors) of the jittered n^3 periodic Voronoi mesh
+    (128^3, about 2.1M cells, by default): the host generator's operator
+    phases on all host cores against cgx_operators_build on the GPU from the
+    same compact mesh.  Checks that every array is bit-identical and prints
+    one JSON line with the times."""
+    from nextgen_b200 import cgx
+    from nextgen_b200.meshgen import DeviceOperatorMesh, PeriodicBoxMesh
+    n = args.opbuild_n
+    threads = os.cpu_count() or 1
+    DeviceOperatorMesh(PeriodicBoxMesh(8, jitter=JITTER, seed=SEED)).close()  # context + module load
+    t0 = time.perf_counter()
+    host, ph = _host_phases(lambda: PeriodicBoxMesh(n, jitter=JITTER, seed=SEED, nthreads=threads))
+    host_total = time.perf_counter() - t0
+    mesher = ("seeds", "voronoi", "compact faces")
+    host_ops = sum(v for k, v in ph.items() if k not in mesher)
+    runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        dev = DeviceOperatorMesh(host)
+        runs.append((time.perf_counter() - t0, dev.device_ms))
+        if len(runs) < 3:
+            dev.close()
+    fields = ["cvocv_i", "cvocv_v", "cvocv_grad_coeff", "cvoef", "n_ef", "c_ef", "area_over_delta_fa", "cmag_cv",
+              "dcmag_hat_cv", "sa_to_vol_ratio", "x_cv", "icv_owner_g", "shift_g"]
+    same = all(np.array_equal(getattr(dev, f), getattr(host, f)) for f in fields) and dev.nef == host.nef
+    t0 = time.perf_counter()
+    gm = cgx.Mesh(dev)
+    mesh_create = time.perf_counter() - t0
+    gm.close()
+    wall = min(r[0] for r in runs)
+    dms = min(r[1] for r in runs)
+    out = {"metric": "operator build time", "unit": "s", "cells": host.ncv, "extended_faces": host.nef,
+           "config": {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3, EF_OPS DEFAULT "
+                                  "(interp 1/3), SIGMA_THRESH 0.45" % n},
+           "host_operator_s": host_ops, "host_threads": threads,
+           "host_phases_s": {k: round(v, 4) for k, v in ph.items()},
+           "host_mesher_s": sum(v for k, v in ph.items() if k in mesher), "host_generator_total_s": host_total,
+           "device_build_s": dms / 1e3, "device_build_with_copies_s": wall,
+           "speedup_device_vs_host": host_ops / (dms / 1e3),
+           "speedup_with_copies_vs_host": host_ops / wall,
+           "cgx_mesh_create_s": mesh_create, "bit_identical": bool(same), "data": "synthetic"}
+    print(json.dumps(out), flush=True)
+    dev.close()
+    return 0 if same else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -588,6 +660,9 @@ def main():
                     help="instead of the throughput bench: FP64 GPU vs CPU oracle over many steps")
     ap.add_argument("--validate-n", type=int, default=128)
     ap.add_argument("--validate-steps", type=int, default=200)
+    ap.add_argument("--opbuild", action="store_true",
+                    help="instead of the throughput bench: operator build on the GPU vs the host generator")
+    ap.add_argument("--opbuild-n", type=int, default=128)
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         sys.exit("steps >= 1, warmup >= 0")
@@ -599,6 +674,8 @@ def main():
         return run_batch64(args)
     if args.validate:
         return run_validate(args)
+    if args.opbuild:
+        return run_opbuild(args)
     return run_cgx(args)
 
 

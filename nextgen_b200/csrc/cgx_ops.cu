@@ -57,7 +57,7 @@ constexpr int kRowWarps = 4;  // rows (warps) per block of the row kernels
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
-enum { ERR_INPUT = 0, ERR_ROW = 1, ERR_THIN = 2, ERR_SLOTS = 4 };
+enum { ERR_INPUT = 0, ERR_ROW = 1, ERR_THIN = 2, ERR_INTERNAL = 3, ERR_SLOTS = 4 };
 
 __device__ __forceinline__ i64 img_key(int cell, int sx, int sy, int sz) {
   return i64(cell) * 343 + (sx + 3) * 49 + (sy + 3) * 7 + (sz + 3);
@@ -385,79 +385,188 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_row_count(Mesh M, i64* rcnt)
   }
 }
 
+// Row values, one lane per image: each lane walks the row's whole term list
+// and adds the terms that hit its image.  Used for rows too long for the
+// shared-memory accumulators of row_values_by_term.
+__device__ void row_values_by_image(const Mesh& M, int r, const i64* sk, int n, double* dv, int lane) {
+  const double f = M.f_int;
+  const i64 self = img_key(r, 0, 0, 0);
+  const double xr[3] = {M.xcv[3 * size_t(r)], M.xcv[3 * size_t(r) + 1], M.xcv[3 * size_t(r) + 2]};
+  const int fb = M.faocv_i[r], fe = M.faocv_i[r + 1];
+  const int rb = M.cvocv_i[r], re = M.cvocv_i[r + 1];
+  for (int kb = 0; kb < n; kb += 32) {
+    const int e = kb + lane;
+    const i64 K = e < n ? sk[e] : -2;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int foc = fb; foc < fe; ++foc) {
+      LF lf;
+      local_face(M, r, foc, lf);
+      // (i) own terms
+      if (K == img_key(lf.cell, lf.sx, lf.sy, lf.sz)) {
+        acc0 += 0.5 * lf.n[0];
+        acc1 += 0.5 * lf.n[1];
+        acc2 += 0.5 * lf.n[2];
+      }
+      double xk[3];
+      image_pos(M, lf.cell, lf.sx, lf.sy, lf.sz, xk);
+      double dx[3];
+      for (int i = 0; i < 3; ++i) dx[i] = 0.5 * lf.xf[i] - (0.5 - 0.25 * f) * xr[i] - 0.25 * f * xk[i];
+      for (int coc = rb; coc < re; ++coc) {
+        int c2, s2x, s2y, s2z;
+        nbr_image(M, M.cvocv_v[coc], c2, s2x, s2y, s2z);
+        const i64 k2 = img_key(c2, s2x, s2y, s2z);
+        if (k2 != self && K == k2) {
+          const double* g = &M.gc[3 * size_t(coc)];
+          const double dp = g[0] * dx[0] + g[1] * dx[1] + g[2] * dx[2];
+          acc0 += dp * lf.n[0];
+          acc1 += dp * lf.n[1];
+          acc2 += dp * lf.n[2];
+        }
+      }
+      // (ii) terms the neighbour k adds to row r
+      const int k = lf.cell;
+      const int bf = back_face(M, k, r, lf.sx, lf.sy, lf.sz, lane);
+      if (bf < 0) continue;
+      LF bk;
+      local_face(M, k, bf, bk);
+      const double xkk[3] = {M.xcv[3 * size_t(k)], M.xcv[3 * size_t(k) + 1], M.xcv[3 * size_t(k) + 2]};
+      double xri[3];
+      image_pos(M, r, -lf.sx, -lf.sy, -lf.sz, xri);
+      double dxb[3];
+      for (int i = 0; i < 3; ++i) dxb[i] = 0.5 * bk.xf[i] - (0.5 - 0.25 * f) * xkk[i] - 0.25 * f * xri[i];
+      const int cb = M.cvocv_i[k], ce = M.cvocv_i[k + 1];
+      for (int coc = cb; coc < ce; ++coc) {
+        int c2, s2x, s2y, s2z;
+        nbr_image(M, M.cvocv_v[coc], c2, s2x, s2y, s2z);
+        if (c2 == r && s2x == -lf.sx && s2y == -lf.sy && s2z == -lf.sz) continue;
+        if (K == img_key(c2, s2x + lf.sx, s2y + lf.sy, s2z + lf.sz)) {
+          const double* g = &M.gc[3 * size_t(coc)];
+          const double dp = g[0] * dxb[0] + g[1] * dxb[1] + g[2] * dxb[2];
+          acc0 -= dp * bk.n[0];
+          acc1 -= dp * bk.n[1];
+          acc2 -= dp * bk.n[2];
+        }
+      }
+    }
+    if (e < n) {
+      dv[3 * size_t(e)] = acc0;
+      dv[3 * size_t(e) + 1] = acc1;
+      dv[3 * size_t(e) + 2] = acc2;
+    }
+  }
+}
+
+// Add one chunk of up to 32 consecutive terms (lane order = term order) into
+// the shared accumulators acc[3 * image].  Terms that hit the same image are
+// added in rounds, lowest lane first, so each image receives its terms in
+// term order, exactly as a sequential loop would add them.
+__device__ __forceinline__ void add_terms(const Mesh& M, const i64* sk, int n, double* acc, bool active, i64 key,
+                                          double v0, double v1, double v2, int lane) {
+  int idx = -1;
+  if (active) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (sk[mid] < key) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < n && sk[lo] == key) idx = lo;
+    else atomicExch(&M.err[ERR_INTERNAL], 1);
+  }
+  const unsigned grp = __match_any_sync(kFull, idx);
+  const int rank = __popc(grp & ((1u << lane) - 1));
+  const int rounds = __reduce_max_sync(kFull, idx >= 0 ? unsigned(__popc(grp)) : 0u);
+  for (int t = 0; t < rounds; ++t) {
+    if (idx >= 0 && rank == t) {
+      acc[3 * idx] += v0;
+      acc[3 * idx + 1] += v1;
+      acc[3 * idx + 2] += v2;
+    }
+    __syncwarp();
+  }
+}
+
+// Row values, lanes over terms: each chunk of 32 consecutive terms is
+// evaluated in parallel and added by add_terms.  acc holds 3 * n doubles.
+__device__ void row_values_by_term(const Mesh& M, int r, const i64* sk, int n, double* acc, int lane) {
+  const double f = M.f_int;
+  const i64 self = img_key(r, 0, 0, 0);
+  for (int i = lane; i < 3 * n; i += 32) acc[i] = 0.0;
+  __syncwarp();
+  const double xr[3] = {M.xcv[3 * size_t(r)], M.xcv[3 * size_t(r) + 1], M.xcv[3 * size_t(r) + 2]};
+  const int fb = M.faocv_i[r], fe = M.faocv_i[r + 1];
+  const int rb = M.cvocv_i[r], re = M.cvocv_i[r + 1];
+  for (int foc = fb; foc < fe; ++foc) {
+    LF lf;
+    local_face(M, r, foc, lf);
+    // (i) own terms: the face's half normal, then the gradient correction
+    add_terms(M, sk, n, acc, lane == 0, img_key(lf.cell, lf.sx, lf.sy, lf.sz), 0.5 * lf.n[0], 0.5 * lf.n[1],
+              0.5 * lf.n[2], lane);
+    double xk[3];
+    image_pos(M, lf.cell, lf.sx, lf.sy, lf.sz, xk);
+    double dx[3];
+    for (int i = 0; i < 3; ++i) dx[i] = 0.5 * lf.xf[i] - (0.5 - 0.25 * f) * xr[i] - 0.25 * f * xk[i];
+    for (int base = rb; base < re; base += 32) {
+      const int coc = base + lane;
+      bool act = coc < re;
+      i64 k2 = -3;
+      double dp = 0.0;
+      if (act) {
+        int c2, s2x, s2y, s2z;
+        nbr_image(M, M.cvocv_v[coc], c2, s2x, s2y, s2z);
+        k2 = img_key(c2, s2x, s2y, s2z);
+        act = k2 != self;
+        const double* g = &M.gc[3 * size_t(coc)];
+        dp = g[0] * dx[0] + g[1] * dx[1] + g[2] * dx[2];
+      }
+      add_terms(M, sk, n, acc, act, k2, dp * lf.n[0], dp * lf.n[1], dp * lf.n[2], lane);
+    }
+    // (ii) terms the neighbour k adds to row r (subtracted: added negated)
+    const int k = lf.cell;
+    const int bf = back_face(M, k, r, lf.sx, lf.sy, lf.sz, lane);
+    if (bf < 0) continue;
+    LF bk;
+    local_face(M, k, bf, bk);
+    const double xkk[3] = {M.xcv[3 * size_t(k)], M.xcv[3 * size_t(k) + 1], M.xcv[3 * size_t(k) + 2]};
+    double xri[3];
+    image_pos(M, r, -lf.sx, -lf.sy, -lf.sz, xri);
+    double dxb[3];
+    for (int i = 0; i < 3; ++i) dxb[i] = 0.5 * bk.xf[i] - (0.5 - 0.25 * f) * xkk[i] - 0.25 * f * xri[i];
+    const int cb = M.cvocv_i[k], ce = M.cvocv_i[k + 1];
+    for (int base = cb; base < ce; base += 32) {
+      const int coc = base + lane;
+      bool act = coc < ce;
+      i64 key = -3;
+      double dp = 0.0;
+      if (act) {
+        int c2, s2x, s2y, s2z;
+        nbr_image(M, M.cvocv_v[coc], c2, s2x, s2y, s2z);
+        act = !(c2 == r && s2x == -lf.sx && s2y == -lf.sy && s2z == -lf.sz);
+        key = img_key(c2, s2x + lf.sx, s2y + lf.sy, s2z + lf.sz);
+        const double* g = &M.gc[3 * size_t(coc)];
+        dp = g[0] * dxb[0] + g[1] * dxb[1] + g[2] * dxb[2];
+      }
+      add_terms(M, sk, n, acc, act, key, -(dp * bk.n[0]), -(dp * bk.n[1]), -(dp * bk.n[2]), lane);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kRowWarps * 32) k_row_fill(Mesh M, const i64* drow_i, i64* dkey, double* dval) {
   extern __shared__ i64 smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   i64* hs = smem + size_t(w) * 2 * kHash;
   i64* sk = hs + kHash;
-  const double f = M.f_int;
+  double* acc = reinterpret_cast<double*>(hs);  // the hash set is done with once sk is sorted
   for (int r = blockIdx.x * kRowWarps + w; r < M.ncv; r += gridDim.x * kRowWarps) {
     const int n = row_images(M, r, hs, sk, lane);
-    if (n < 0) continue;
-    const i64 off = drow_i[r];
-    for (int i = lane; i < n; i += 32) dkey[off + i] = sk[i];
-    const i64 self = img_key(r, 0, 0, 0);
-    const double xr[3] = {M.xcv[3 * size_t(r)], M.xcv[3 * size_t(r) + 1], M.xcv[3 * size_t(r) + 2]};
-    const int fb = M.faocv_i[r], fe = M.faocv_i[r + 1];
-    const int rb = M.cvocv_i[r], re = M.cvocv_i[r + 1];
-    for (int kb = 0; kb < n; kb += 32) {
-      const int e = kb + lane;
-      const i64 K = e < n ? sk[e] : -2;
-      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-      for (int foc = fb; foc < fe; ++foc) {
-        LF lf;
-        local_face(M, r, foc, lf);
-        // (i) own terms
-        if (K == img_key(lf.cell, lf.sx, lf.sy, lf.sz)) {
-          acc0 += 0.5 * lf.n[0];
-          acc1 += 0.5 * lf.n[1];
-          acc2 += 0.5 * lf.n[2];
-        }
-        double xk[3];
-        image_pos(M, lf.cell, lf.sx, lf.sy, lf.sz, xk);
-        double dx[3];
-        for (int i = 0; i < 3; ++i) dx[i] = 0.5 * lf.xf[i] - (0.5 - 0.25 * f) * xr[i] - 0.25 * f * xk[i];
-        for (int coc = rb; coc < re; ++coc) {
-          int c2, s2x, s2y, s2z;
-          nbr_image(M, M.cvocv_v[coc], c2, s2x, s2y, s2z);
-          const i64 k2 = img_key(c2, s2x, s2y, s2z);
-          if (k2 != self && K == k2) {
-            const double* g = &M.gc[3 * size_t(coc)];
-            const double dp = g[0] * dx[0] + g[1] * dx[1] + g[2] * dx[2];
-            acc0 += dp * lf.n[0];
-            acc1 += dp * lf.n[1];
-            acc2 += dp * lf.n[2];
-          }
-        }
-        // (ii) terms the neighbour k adds to row r
-        const int k = lf.cell;
-        const int bf = back_face(M, k, r, lf.sx, lf.sy, lf.sz, lane);
-        if (bf < 0) continue;
-        LF bk;
-        local_face(M, k, bf, bk);
-        const double xkk[3] = {M.xcv[3 * size_t(k)], M.xcv[3 * size_t(k) + 1], M.xcv[3 * size_t(k) + 2]};
-        double xri[3];
-        image_pos(M, r, -lf.sx, -lf.sy, -lf.sz, xri);
-        double dxb[3];
-        for (int i = 0; i < 3; ++i) dxb[i] = 0.5 * bk.xf[i] - (0.5 - 0.25 * f) * xkk[i] - 0.25 * f * xri[i];
-        const int cb = M.cvocv_i[k], ce = M.cvocv_i[k + 1];
-        for (int coc = cb; coc < ce; ++coc) {
-          int c2, s2x, s2y, s2z;
-          nbr_image(M, M.cvocv_v[coc], c2, s2x, s2y, s2z);
-          if (c2 == r && s2x == -lf.sx && s2y == -lf.sy && s2z == -lf.sz) continue;
-          if (K == img_key(c2, s2x + lf.sx, s2y + lf.sy, s2z + lf.sz)) {
-            const double* g = &M.gc[3 * size_t(coc)];
-            const double dp = g[0] * dxb[0] + g[1] * dxb[1] + g[2] * dxb[2];
-            acc0 -= dp * bk.n[0];
-            acc1 -= dp * bk.n[1];
-            acc2 -= dp * bk.n[2];
-          }
-        }
-      }
-      if (e < n) {
-        dval[3 * size_t(off + e)] = acc0;
-        dval[3 * size_t(off + e) + 1] = acc1;
-        dval[3 * size_t(off + e) + 2] = acc2;
+    if (n >= 0) {
+      const i64 off = drow_i[r];
+      for (int i = lane; i < n; i += 32) dkey[off + i] = sk[i];
+      if (3 * n <= kHash) {
+        row_values_by_term(M, r, sk, n, acc, lane);
+        for (int i = lane; i < 3 * n; i += 32) dval[3 * size_t(off) + i] = acc[i];
+      } else {
+        row_values_by_image(M, r, sk, n, dval + 3 * size_t(off), lane);
       }
     }
     __syncwarp();
@@ -843,6 +952,7 @@ void check_err(const int* d_err, cudaStream_t s) {
   if (e[ERR_INPUT]) throw Failure{CGX_E_ARG, "cgx_operators_build: inconsistent compact mesh (cell or ghost index out of range)"};
   if (e[ERR_THIN]) throw Failure{CGX_E_ARG, "cgx_operators_build: box too thin (extended stencil reaches a cell's own image)"};
   if (e[ERR_ROW]) throw Failure{CGX_E_ARG, "cgx_operators_build: operator row longer than 768 entries"};
+  if (e[ERR_INTERNAL]) throw Failure{CGX_E_CUDA, "cgx_operators_build: internal error (operator term without an image)"};
 }
 
 int build(const cgx_compact_desc* in, double f_int, double sigma_thresh, int device, cgx_meshgen_out** out,
