@@ -90,6 +90,17 @@ int cgx_meshgen_periodic_box(int nx, int ny, int nz,
                              double interp_factor, double sigma_thresh,
                              int nthreads, cgx_meshgen_out** out);
 
+/*
+ * The mesher's part only: cells, compact faces and the level-1 ghosts of the
+ * same mesh (identical arrays), with every operator array NULL, nef = 0 and
+ * ncv_g2 = ncv_g (x_cv, icv_owner_g and shift_g cover the level-1 ghosts).
+ * This is the input of the GPU operator build (include/cgx_ops.h).
+ */
+int cgx_meshgen_periodic_box_compact(int nx, int ny, int nz,
+                                     double Lx, double Ly, double Lz,
+                                     double jitter, unsigned long long seed,
+                                     int nthreads, cgx_meshgen_out** out);
+
 void cgx_meshgen_free(cgx_meshgen_out* m);
 
 /* Error text for the last failing call on this thread. */

@@ -364,10 +364,30 @@ extern "C" void cgx_meshgen_free(cgx_meshgen_out* m) {
   std::free(m);
 }
 
+namespace {
+int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jitter,
+             unsigned long long seed, double interp_factor, double sigma_thresh, int nthreads,
+             bool compact_only, cgx_meshgen_out** out);
+}  // namespace
+
 extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, double Ly,
                                         double Lz, double jitter, unsigned long long seed,
                                         double interp_factor, double sigma_thresh,
                                         int nthreads, cgx_meshgen_out** out) {
+  return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, interp_factor, sigma_thresh, nthreads,
+                  false, out);
+}
+
+extern "C" int cgx_meshgen_periodic_box_compact(int nx, int ny, int nz, double Lx, double Ly,
+                                                double Lz, double jitter, unsigned long long seed,
+                                                int nthreads, cgx_meshgen_out** out) {
+  return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, 1.0 / 3.0, 0.45, nthreads, true, out);
+}
+
+namespace {
+int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jitter,
+             unsigned long long seed, double interp_factor, double sigma_thresh, int nthreads,
+             bool compact_only, cgx_meshgen_out** out) {
   if (!out || nx < 4 || ny < 4 || nz < 4 || !(Lx > 0) || !(Ly > 0) || !(Lz > 0) ||
       !(jitter >= 0.0) || jitter > 0.3 || int64_t(nx) * ny * nz > (int64_t(1) << 30)) {
     g_err = "cgx_meshgen_periodic_box: invalid argument";
@@ -625,6 +645,45 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
     raw.shrink_to_fit();
     PT.mark("compact faces");
     const int ncv_g = ncv + int(g_owner.size());
+    if (compact_only) {
+      // what a mesher hands over: cells, compact faces, level-1 ghosts
+      std::vector<double> xg(3 * size_t(ncv_g));
+      for (int a = 0; a < ncv; ++a) {
+        xg[3 * size_t(a)] = xcv[a].x;
+        xg[3 * size_t(a) + 1] = xcv[a].y;
+        xg[3 * size_t(a) + 2] = xcv[a].z;
+      }
+      for (int g = 0; g < ncv_g - ncv; ++g) {
+        const int b = g_owner[g];
+        xg[3 * size_t(ncv + g)] = xcv[b].x + g_shift[3 * g] * L[0];
+        xg[3 * size_t(ncv + g) + 1] = xcv[b].y + g_shift[3 * g + 1] * L[1];
+        xg[3 * size_t(ncv + g) + 2] = xcv[b].z + g_shift[3 * g + 2] * L[2];
+      }
+      std::vector<double> xv(3 * size_t(ncv));
+      for (int a = 0; a < ncv; ++a) {
+        xv[3 * size_t(a)] = xvv[a].x;
+        xv[3 * size_t(a) + 1] = xvv[a].y;
+        xv[3 * size_t(a) + 2] = xvv[a].z;
+      }
+      cgx_meshgen_out* m = static_cast<cgx_meshgen_out*>(std::calloc(1, sizeof(cgx_meshgen_out)));
+      if (!m) throw std::bad_alloc();
+      m->ncv = ncv;
+      m->ncv_g = ncv_g;
+      m->ncv_g2 = ncv_g;
+      m->nfa = nfa;
+      m->nfa_i = nfa_i;
+      m->h = hx;
+      m->cvofa = reinterpret_cast<int(*)[2]>(dup_array(cvofa));
+      m->n_fa = reinterpret_cast<double(*)[3]>(dup_array(n_fa));
+      m->x_fa = reinterpret_cast<double(*)[3]>(dup_array(x_fa));
+      m->vol_cv = dup_array(vol);
+      m->x_cv = reinterpret_cast<double(*)[3]>(dup_array(xg));
+      m->x_vv = reinterpret_cast<double(*)[3]>(dup_array(xv));
+      m->icv_owner_g = dup_array(g_owner);
+      m->shift_g = reinterpret_cast<int(*)[3]>(dup_array(g_shift));
+      *out = m;
+      return CGX_MG_OK;
+    }
 
     auto image_pos = [&](int cell, int sx, int sy, int sz) -> V3 {
       return {xcv[cell].x + sx * Lx, xcv[cell].y + sy * Ly, xcv[cell].z + sz * Lz};
@@ -1147,3 +1206,4 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
     return CGX_MG_E_ARG;
   }
 }
+}  // namespace

@@ -40,6 +40,11 @@ def _load():
         ctypes.c_double, ctypes.c_double, ctypes.c_double,
         ctypes.c_double, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_double,
         ctypes.c_int, ctypes.POINTER(ctypes.POINTER(MeshgenOut))]
+    lib.cgx_meshgen_periodic_box_compact.restype = ctypes.c_int
+    lib.cgx_meshgen_periodic_box_compact.argtypes = [
+        ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double,
+        ctypes.c_double, ctypes.c_ulonglong, ctypes.c_int, ctypes.POINTER(ctypes.POINTER(MeshgenOut))]
     lib.cgx_meshgen_free.restype = None
     lib.cgx_meshgen_free.argtypes = [ctypes.POINTER(MeshgenOut)]
     lib.cgx_meshgen_last_error.restype = ctypes.c_char_p
@@ -58,6 +63,8 @@ def lib():
 
 
 def _view(ptr, shape, dtype):
+    if not ptr:
+        return None
     n = int(np.prod(shape))
     if n == 0:
         return np.zeros(shape, dtype=dtype)
@@ -74,15 +81,21 @@ class PeriodicBoxMesh:
     """
 
     def __init__(self, nx, ny=None, nz=None, L=2.0 * np.pi, jitter=0.0, seed=1234,
-                 interp_factor=1.0 / 3.0, sigma_thresh=0.45, nthreads=0):
+                 interp_factor=1.0 / 3.0, sigma_thresh=0.45, nthreads=0, compact_only=False):
         ny = nx if ny is None else ny
         nz = nx if nz is None else nz
         Ls = (L, L, L) if np.isscalar(L) else tuple(L)
         out = ctypes.POINTER(MeshgenOut)()
-        rc = lib().cgx_meshgen_periodic_box(int(nx), int(ny), int(nz), Ls[0], Ls[1], Ls[2],
-                                            float(jitter), int(seed), float(interp_factor),
-                                            float(sigma_thresh), int(nthreads),
-                                            ctypes.byref(out))
+        if compact_only:
+            # the mesher's part only (operators None): input of DeviceOperatorMesh
+            rc = lib().cgx_meshgen_periodic_box_compact(int(nx), int(ny), int(nz), Ls[0], Ls[1], Ls[2],
+                                                        float(jitter), int(seed), int(nthreads),
+                                                        ctypes.byref(out))
+        else:
+            rc = lib().cgx_meshgen_periodic_box(int(nx), int(ny), int(nz), Ls[0], Ls[1], Ls[2],
+                                                float(jitter), int(seed), float(interp_factor),
+                                                float(sigma_thresh), int(nthreads),
+                                                ctypes.byref(out))
         if rc != 0:
             raise RuntimeError("meshgen failed (%d): %s" % (rc, lib().cgx_meshgen_last_error().decode()))
         self._free = lib().cgx_meshgen_free
@@ -108,7 +121,7 @@ class PeriodicBoxMesh:
         self.x_cv = _view(m.x_cv, (self.ncv_g2, 3), np.float64)
         self.x_vv = _view(m.x_vv, (self.ncv, 3), np.float64) if m.x_vv else None
         self.cvocv_i = _view(m.cvocv_i, (self.ncv + 1,), np.int32)
-        ncoc = int(self.cvocv_i[-1])
+        ncoc = int(self.cvocv_i[-1]) if self.cvocv_i is not None else 0
         self.cvocv_v = _view(m.cvocv_v, (ncoc,), np.int32)
         self.cvocv_grad_coeff = _view(m.cvocv_grad_coeff, (ncoc, 3), np.float64)
         self.cvoef = _view(m.cvoef, (self.nef, 2), np.int32)

@@ -49,6 +49,18 @@ def test_device_build_equals_host(built, kw):
     dev.close()
 
 
+def test_from_the_mesher_alone(built):
+    """The pipeline a served mesh takes: the mesher's compact output
+    (cgx_meshgen_periodic_box_compact) -> cgx_operators_build gives the full
+    host generator's mesh."""
+    kw = dict(nx=18, ny=14, nz=12, L=(1.2, 0.9, 0.8), jitter=0.25, seed=21)
+    full = PeriodicBoxMesh(**kw)
+    dev = DeviceOperatorMesh(PeriodicBoxMesh(compact_only=True, **kw))
+    assert (dev.ncv_g2, dev.nef, dev.nef_i) == (full.ncv_g2, full.nef, full.nef_i)
+    for f in FIELDS:
+        assert np.array_equal(getattr(dev, f), getattr(full, f)), f
+
+
 def test_solver_on_device_built_mesh(built):
     host = PeriodicBoxMesh(14, jitter=0.25, seed=5)
     dev = DeviceOperatorMesh(host)

@@ -155,3 +155,19 @@ def test_grad_coeff_with_reference_svd(built):
             gc[k] = g + Vm.T @ tmp
         worst = max(worst, np.abs(gc - m.cvocv_grad_coeff[s:e]).max() / np.abs(gc).max())
     assert worst < 1e-12, worst
+
+
+def test_compact_only_is_the_generators_compact_part(built):
+    """cgx_meshgen_periodic_box_compact returns the full generator's cells,
+    compact faces and level-1 ghosts unchanged, and no operator arrays."""
+    a = PeriodicBoxMesh(10, 9, 8, L=(1.0, 0.9, 0.8), jitter=0.3, seed=11)
+    b = PeriodicBoxMesh(10, 9, 8, L=(1.0, 0.9, 0.8), jitter=0.3, seed=11, compact_only=True)
+    assert (b.ncv, b.ncv_g, b.ncv_g2, b.nfa, b.nfa_i, b.nef) == (a.ncv, a.ncv_g, a.ncv_g, a.nfa, a.nfa_i, 0)
+    for f in ("cvofa", "n_fa", "x_fa", "vol_cv", "x_vv"):
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
+    ng1 = a.ncv_g - a.ncv
+    assert np.array_equal(a.x_cv[: a.ncv_g], b.x_cv)
+    assert np.array_equal(a.icv_owner_g[:ng1], b.icv_owner_g)
+    assert np.array_equal(a.shift_g[:ng1], b.shift_g)
+    for f in ("cvocv_i", "cvocv_grad_coeff", "cvoef", "n_ef", "c_ef", "area_over_delta_fa", "dcmag_hat_cv"):
+        assert getattr(b, f) is None, f
