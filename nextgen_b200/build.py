@@ -70,7 +70,7 @@ def build_cgx(force=False, verbose=False):
             common.insert(1, "-Xptxas=-v")
         # the operator build reproduces the host generator's arithmetic bit
         # for bit, so it is compiled without multiply-add contraction
-        log = _run(common + ["-fmad=false", "-Xcompiler", "-fPIC", "-c", "-o", ops_obj,
+        log = _run(common + ["-fmad=false", "-Xcompiler", "-fPIC,-fopenmp", "-c", "-o", ops_obj,
                              os.path.join(CSRC, "cgx_ops.cu")])
         log += _run(common + ["-Xcompiler", "-fPIC,-fopenmp", "-shared", "-o", out,
                               os.path.join(CSRC, "cgx.cu"), ops_obj, "-lgomp"])

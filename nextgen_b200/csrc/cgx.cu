@@ -28,6 +28,7 @@
 
 #include "../../include/cgx.h"
 #include "cgx_kernels.cuh"
+#include "host_staging.h"
 
 #include <cuda_runtime.h>
 
@@ -42,6 +43,8 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1223,11 +1226,42 @@ int dalloc(T** p, size_t n, size_t* acc) {
   return CGX_OK;
 }
 
+// std::vector whose elements start uninitialised (for large set-up arrays
+// that are written in full in parallel: no serial zero fill)
 template <class T>
-int dupload(T** p, const std::vector<T>& v, size_t* acc) {
+struct DefaultInit : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = DefaultInit<U>;
+  };
+  DefaultInit() = default;
+  template <class U>
+  DefaultInit(const DefaultInit<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <class T>
+using uvec = std::vector<T, DefaultInit<T>>;
+
+// device copy of a host vector; large ones go through the pinned staging
+// buffers (asynchronous on the legacy default stream, which the set-up
+// kernels also use)
+template <class T, class A>
+int dupload(T** p, const std::vector<T, A>& v, size_t* acc, cgx_staging::Staging* st = nullptr) {
   int rc = dalloc(p, v.size(), acc);
   if (rc) return rc;
-  if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  const size_t bytes = v.size() * sizeof(T);
+  if (st && bytes >= (size_t(8) << 20)) {
+    CK(st->put(*p, v.data(), bytes));
+  } else if (!v.empty()) {
+    CK(cudaMemcpy(*p, v.data(), bytes, cudaMemcpyHostToDevice));
+  }
   return CGX_OK;
 }
 
@@ -1856,18 +1890,32 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
 
     PT.mark("renumbering");
     // ---- match compact faces to extended faces (FlowSolver.hpp:1833-1900)
-    std::vector<int> ef_i(N + 1, 0);
+    int bad_ef = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_ef)
     for (int f = 0; f < nef; ++f) {
-      const int a = d->cvoef[2 * size_t(f)];
-      if (a < 0 || a >= N || d->cvoef[2 * size_t(f) + 1] < 0 || d->cvoef[2 * size_t(f) + 1] >= ncv_g2)
-        return bail(fail(CGX_E_ARG, "cvoef out of range"));
-      ++ef_i[a + 1];
+      const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
+      bad_ef |= (a < 0 || a >= N || b < 0 || b >= ncv_g2);
+    }
+    if (bad_ef) return bail(fail(CGX_E_ARG, "cvoef out of range"));
+    std::vector<int> ef_i(N + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int f = 0; f < nef; ++f) {
+#pragma omp atomic
+      ++ef_i[d->cvoef[2 * size_t(f)] + 1];
     }
     for (int a = 0; a < N; ++a) ef_i[a + 1] += ef_i[a];
-    std::vector<int> ef_v(nef);
+    uvec<int> ef_v(nef);
     {
       std::vector<int> fill(ef_i.begin(), ef_i.end() - 1);
-      for (int f = 0; f < nef; ++f) ef_v[fill[d->cvoef[2 * size_t(f)]]++] = f;
+#pragma omp parallel for schedule(static)
+      for (int f = 0; f < nef; ++f) {
+        int k;
+#pragma omp atomic capture
+        k = fill[d->cvoef[2 * size_t(f)]]++;
+        ef_v[k] = f;
+      }
+#pragma omp parallel for schedule(dynamic, 4096)
+      for (int a = 0; a < N; ++a) std::sort(ef_v.begin() + ef_i[a], ef_v.begin() + ef_i[a + 1]);
     }
     auto find_ef = [&](int a, int b) -> int {
       if (a < 0 || a >= N) return -1;
@@ -1877,43 +1925,92 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     };
     std::vector<int> cf_of_ef(nef, -1);
     std::vector<signed char> cf_rev(nef, 0);
-    for (int fa = 0; fa < nfa; ++fa) {
-      const int a = d->cvofa[2 * size_t(fa)], b = d->cvofa[2 * size_t(fa) + 1];
-      if (a < 0 || a >= N || b < 0 || b >= ncv_g2) return bail(fail(CGX_E_ARG, "cvofa out of range"));
-      int f = find_ef(a, b);
-      signed char rev = 0;
-      if (f < 0) {
-        f = find_ef(b, a);
-        rev = 1;
+    {
+      uvec<int> ef_of_fa(nfa);
+      uvec<signed char> rev_of_fa(nfa);
+      int bad_fa = 0, unmatched = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_fa, unmatched)
+      for (int fa = 0; fa < nfa; ++fa) {
+        const int a = d->cvofa[2 * size_t(fa)], b = d->cvofa[2 * size_t(fa) + 1];
+        int f = -1;
+        signed char rev = 0;
+        if (a < 0 || a >= N || b < 0 || b >= ncv_g2) {
+          bad_fa = 1;
+        } else {
+          f = find_ef(a, b);
+          if (f < 0) {
+            f = find_ef(b, a);
+            rev = 1;
+          }
+          unmatched |= (f < 0);
+        }
+        ef_of_fa[fa] = f;
+        rev_of_fa[fa] = rev;
       }
-      if (f < 0) return bail(fail(CGX_E_ARG, "compact face without extended face"));
-      if (cf_of_ef[f] >= 0) return bail(fail(CGX_E_ARG, "two compact faces on one extended face"));
-      cf_of_ef[f] = fa;
-      cf_rev[f] = rev;
+      if (bad_fa) return bail(fail(CGX_E_ARG, "cvofa out of range"));
+      if (unmatched) return bail(fail(CGX_E_ARG, "compact face without extended face"));
+      for (int fa = 0; fa < nfa; ++fa) {
+        const int f = ef_of_fa[fa];
+        if (cf_of_ef[f] >= 0) return bail(fail(CGX_E_ARG, "two compact faces on one extended face"));
+        cf_of_ef[f] = fa;
+        cf_rev[f] = rev_of_fa[fa];
+      }
     }
     PT.mark("compact/extended match");
     // ---- face numbering: compact faces first, each group ordered by the
-    // first cell (new numbering) that reads the face
-    // (counting sort on the bucket 2*first + (extended only))
-    std::vector<int> fbucket(nef);
-    std::vector<long long> bstart(2 * size_t(N) + 1, 0);
-    for (int f = 0; f < nef; ++f) {
-      const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
-      const int na = iperm[a];
-      const int first = (b < N) ? std::min(na, iperm[b]) : na;
-      const int bk = (cf_of_ef[f] >= 0) ? first : N + first;
-      fbucket[f] = bk;
-      ++bstart[bk + 1];
+    // first cell (new numbering) that reads the face, then by input face
+    // order: a stable counting sort on the bucket 2*first + (extended only),
+    // in parallel over fixed chunks of faces (per-chunk bucket counts), so
+    // the numbering does not depend on the thread count
+    uvec<int> fnew(nef);
+    {
+      uvec<int> fbucket(nef);
+#pragma omp parallel for schedule(static)
+      for (int f = 0; f < nef; ++f) {
+        const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
+        const int na = iperm[a];
+        const int first = (b < N) ? std::min(na, iperm[b]) : na;
+        fbucket[f] = (cf_of_ef[f] >= 0) ? first : N + first;
+      }
+      const size_t NB = 2 * size_t(N);
+      const int nchunk = int(std::min<long long>(16, std::max<long long>(1, nef / 65536)));
+      auto chunk_lo = [&](int c) { return int((long long)nef * c / nchunk); };
+      uvec<int> ccnt(size_t(nchunk) * NB);
+#pragma omp parallel for schedule(static, 1)
+      for (int c = 0; c < nchunk; ++c) {
+        int* cc = ccnt.data() + size_t(c) * NB;
+        std::fill(cc, cc + NB, 0);
+        for (int f = chunk_lo(c); f < chunk_lo(c + 1); ++f) ++cc[fbucket[f]];
+      }
+      // per bucket: the buckets before it, then the chunks before this one
+      std::vector<long long> btot(NB + 1, 0);
+#pragma omp parallel for schedule(static)
+      for (long long k = 0; k < (long long)NB; ++k) {
+        long long t = 0;
+        for (int c = 0; c < nchunk; ++c) t += ccnt[size_t(c) * NB + k];
+        btot[k + 1] = t;
+      }
+      for (size_t k = 0; k < NB; ++k) btot[k + 1] += btot[k];
+#pragma omp parallel for schedule(static)
+      for (long long k = 0; k < (long long)NB; ++k) {
+        long long run = btot[k];
+        for (int c = 0; c < nchunk; ++c) {
+          const int n = ccnt[size_t(c) * NB + k];
+          ccnt[size_t(c) * NB + k] = int(run);
+          run += n;
+        }
+      }
+#pragma omp parallel for schedule(static, 1)
+      for (int c = 0; c < nchunk; ++c) {
+        int* cc = ccnt.data() + size_t(c) * NB;
+        for (int f = chunk_lo(c); f < chunk_lo(c + 1); ++f) fnew[f] = cc[fbucket[f]]++;
+      }
     }
-    for (size_t k = 0; k < 2 * size_t(N); ++k) bstart[k + 1] += bstart[k];
-    std::vector<int> fnew(nef);
-    for (int f = 0; f < nef; ++f) fnew[f] = int(bstart[fbucket[f]]++);
-    std::vector<int>().swap(fbucket);
-    std::vector<long long>().swap(bstart);
     int ncf = 0;
+#pragma omp parallel for schedule(static) reduction(+ : ncf)
     for (int f = 0; f < nef; ++f) ncf += (cf_of_ef[f] >= 0);
-    std::vector<EFRec> efr(nef);
-    std::vector<CFRec> cfr(std::max(ncf, 1));
+    uvec<EFRec> efr(nef);
+    uvec<CFRec> cfr(std::max(ncf, 1));
 #pragma omp parallel for schedule(static)
     for (int f = 0; f < nef; ++f) {
       EFRec& r = efr[fnew[f]];
@@ -1965,7 +2062,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     }
     std::vector<long long> cell_off(N + 1, 0);
     for (int i = 0; i < N; ++i) cell_off[i + 1] = cell_off[i] + deg[i];
-    std::vector<int> e_nbr(cell_off[N]), e_fid(cell_off[N]);
+    uvec<int> e_nbr(cell_off[N]), e_fid(cell_off[N]);
     {
       std::vector<long long> fill(cell_off.begin(), cell_off.end() - 1);
 #pragma omp parallel for schedule(static)
@@ -2014,8 +2111,8 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       if (cd < 0) return bail(fail(CGX_E_ARG, "cvocv without diagonal"));
       coff[i + 1] = coff[i] + cd;
     }
-    std::vector<int> c_nbr(coff[N]);
-    std::vector<double> gx(coff[N]), gy(coff[N]), gz(coff[N]);
+    uvec<int> c_nbr(coff[N]);
+    uvec<double> gx(coff[N]), gy(coff[N]), gz(coff[N]);
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < N; ++i) {
       const int coc0 = d->cvocv_i[perm[i]] + 1;
@@ -2156,8 +2253,15 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     double *d_gx, *d_gy, *d_gz, *d_vol, *d_ivol, *d_en, *d_qg;
     double4* d_cc;
     Item* d_items;
-#define UP(ptr, vec)                                   \
-  if ((rc = dupload(&ptr, vec, acc))) return bail(rc); \
+    cgx_staging::Staging stage(0);
+    {
+      const cudaError_t se = stage.init();
+      if (se != cudaSuccess)
+        return bail(fail(se == cudaErrorMemoryAllocation ? CGX_E_OOM : CGX_E_CUDA,
+                         std::string("pinned staging buffers: ") + cudaGetErrorString(se)));
+    }
+#define UP(ptr, vec)                                           \
+  if ((rc = dupload(&ptr, vec, acc, &stage))) return bail(rc); \
   M->allocs.push_back(ptr);
     UP(d_items, items);
     UP(d_hcell, hcell);
@@ -2196,8 +2300,8 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         cudaFree(t_cf);
         cudaFree(t_eofq);
       };
-      if ((rc = dupload(&t_fid, e_fid, nullptr)) || (rc = dupload(&t_ef, efr, nullptr)) ||
-          (rc = dupload(&t_cf, cfr, nullptr)) || (rc = dupload(&t_eofq, eofq, nullptr))) {
+      if ((rc = dupload(&t_fid, e_fid, nullptr, &stage)) || (rc = dupload(&t_ef, efr, nullptr, &stage)) ||
+          (rc = dupload(&t_cf, cfr, nullptr, &stage)) || (rc = dupload(&t_eofq, eofq, nullptr, &stage))) {
         free_tmp();
         return bail(rc);
       }

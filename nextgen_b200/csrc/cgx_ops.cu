@@ -31,6 +31,7 @@
 
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <cstdlib>
@@ -41,6 +42,7 @@
 
 #include "../../include/cgx.h"
 #include "../../include/cgx_ops.h"
+#include "host_staging.h"
 #include "svd33.h"
 
 namespace cgx {
@@ -894,18 +896,27 @@ struct Pool {
   }
 };
 
+
+// staged copies (csrc/host_staging.h) with this file's error handling
+struct Staging {
+  cgx_staging::Staging st;
+  explicit Staging(cudaStream_t s) : st(s) { ck(st.init(), "pinned staging buffers"); }
+  void put(void* dst, const void* src, size_t bytes, const char* what) { ck(st.put(dst, src, bytes), what); }
+  void get(void* dst, const void* src, size_t bytes, const char* what) { ck(st.get(dst, src, bytes), what); }
+};
+
 template <class T>
-T* upload(Pool& P, const T* h, size_t n, cudaStream_t s, const char* what) {
+T* upload(Pool& P, Staging& st, const T* h, size_t n, const char* what) {
   T* d = P.get<T>(n, what);
-  if (n) ck(cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, s), what);
+  st.put(d, h, sizeof(T) * n, what);
   return d;
 }
 
 template <class T>
-T* download(const T* d, size_t n, cudaStream_t s, const char* what) {
+T* download(Staging& st, const T* d, size_t n, const char* what) {
   T* h = static_cast<T*>(std::malloc(sizeof(T) * (n ? n : 1)));
   if (!h) throw std::bad_alloc();
-  if (n) ck(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, s), what);
+  st.get(h, d, sizeof(T) * n, what);
   return h;
 }
 
@@ -913,7 +924,7 @@ template <class T>
 T* host_copy(const T* src, size_t n) {
   T* h = static_cast<T*>(std::malloc(sizeof(T) * (n ? n : 1)));
   if (!h) throw std::bad_alloc();
-  if (n) std::memcpy(h, src, sizeof(T) * n);
+  cgx_staging::par_memcpy(h, src, sizeof(T) * n);
   return h;
 }
 
@@ -977,6 +988,7 @@ int build(const cgx_compact_desc* in, double f_int, double sigma_thresh, int dev
     }
   } eg{ev0, ev1};
   Pool P;
+  Staging st(s);
 
   Mesh M;
   M.ncv = ncv;
@@ -987,13 +999,13 @@ int build(const cgx_compact_desc* in, double f_int, double sigma_thresh, int dev
   M.L1 = in->L[1];
   M.L2 = in->L[2];
   M.f_int = f_int;
-  M.cvofa = upload(P, in->cvofa, 2 * size_t(nfa), s, "cvofa");
-  M.n_fa = upload(P, in->n_fa, 3 * size_t(nfa), s, "n_fa");
-  M.x_fa = upload(P, in->x_fa, 3 * size_t(nfa), s, "x_fa");
-  M.vol = upload(P, in->vol_cv, size_t(ncv), s, "vol_cv");
-  M.xcv = upload(P, in->x_cv, 3 * size_t(ncv), s, "x_cv");
-  M.g_owner = upload(P, in->icv_owner_g, size_t(ng1), s, "icv_owner_g");
-  M.g_shift = upload(P, in->shift_g, 3 * size_t(ng1), s, "shift_g");
+  M.cvofa = upload(P, st, in->cvofa, 2 * size_t(nfa), "cvofa");
+  M.n_fa = upload(P, st, in->n_fa, 3 * size_t(nfa), "n_fa");
+  M.x_fa = upload(P, st, in->x_fa, 3 * size_t(nfa), "x_fa");
+  M.vol = upload(P, st, in->vol_cv, size_t(ncv), "vol_cv");
+  M.xcv = upload(P, st, in->x_cv, 3 * size_t(ncv), "x_cv");
+  M.g_owner = upload(P, st, in->icv_owner_g, size_t(ng1), "icv_owner_g");
+  M.g_shift = upload(P, st, in->shift_g, 3 * size_t(ng1), "shift_g");
   int* d_err = P.get<int>(ERR_SLOTS, "flags");
   ck(cudaMemsetAsync(d_err, 0, sizeof(int) * ERR_SLOTS, s), "memset");
   M.err = d_err;
@@ -1198,19 +1210,19 @@ int build(const cgx_compact_desc* in, double f_int, double sigma_thresh, int dev
   m->x_fa = reinterpret_cast<double(*)[3]>(host_copy(in->x_fa, 3 * size_t(nfa)));
   m->vol_cv = host_copy(in->vol_cv, size_t(ncv));
   if (in->x_vv) m->x_vv = reinterpret_cast<double(*)[3]>(host_copy(in->x_vv, 3 * size_t(ncv)));
-  m->area_over_delta_fa = download(aod, size_t(nfa), s, "aod");
-  m->x_cv = reinterpret_cast<double(*)[3]>(download(x_cv, 3 * size_t(ncv_g2), s, "x_cv"));
-  m->cvocv_i = download(cvocv_i, size_t(ncv) + 1, s, "cvocv_i");
-  m->cvocv_v = download(cvocv_v, ncoc, s, "cvocv_v");
-  m->cvocv_grad_coeff = reinterpret_cast<double(*)[3]>(download(gc, 3 * ncoc, s, "grad coeff"));
-  m->cvoef = reinterpret_cast<int(*)[2]>(download(cvoef, 2 * size_t(nef), s, "cvoef"));
-  m->n_ef = reinterpret_cast<double(*)[3]>(download(n_ef, 3 * size_t(nef), s, "n_ef"));
-  m->c_ef = reinterpret_cast<double(*)[3]>(download(c_ef, 3 * size_t(nef), s, "c_ef"));
-  m->cmag_cv = download(cmag, size_t(ncv), s, "cmag");
-  m->dcmag_hat_cv = download(dcmag, size_t(ncv), s, "dcmag_hat");
-  m->sa_to_vol_ratio = download(sav, size_t(ncv), s, "sa_to_vol");
-  m->icv_owner_g = download(g_owner, size_t(ncv_g2 - ncv), s, "icv_owner_g");
-  m->shift_g = reinterpret_cast<int(*)[3]>(download(g_shift, 3 * size_t(ncv_g2 - ncv), s, "shift_g"));
+  m->area_over_delta_fa = download(st, aod, size_t(nfa), "aod");
+  m->x_cv = reinterpret_cast<double(*)[3]>(download(st, x_cv, 3 * size_t(ncv_g2), "x_cv"));
+  m->cvocv_i = download(st, cvocv_i, size_t(ncv) + 1, "cvocv_i");
+  m->cvocv_v = download(st, cvocv_v, ncoc, "cvocv_v");
+  m->cvocv_grad_coeff = reinterpret_cast<double(*)[3]>(download(st, gc, 3 * ncoc, "grad coeff"));
+  m->cvoef = reinterpret_cast<int(*)[2]>(download(st, cvoef, 2 * size_t(nef), "cvoef"));
+  m->n_ef = reinterpret_cast<double(*)[3]>(download(st, n_ef, 3 * size_t(nef), "n_ef"));
+  m->c_ef = reinterpret_cast<double(*)[3]>(download(st, c_ef, 3 * size_t(nef), "c_ef"));
+  m->cmag_cv = download(st, cmag, size_t(ncv), "cmag");
+  m->dcmag_hat_cv = download(st, dcmag, size_t(ncv), "dcmag_hat");
+  m->sa_to_vol_ratio = download(st, sav, size_t(ncv), "sa_to_vol");
+  m->icv_owner_g = download(st, g_owner, size_t(ncv_g2 - ncv), "icv_owner_g");
+  m->shift_g = reinterpret_cast<int(*)[3]>(download(st, g_shift, 3 * size_t(ncv_g2 - ncv), "shift_g"));
   ck(cudaStreamSynchronize(s), "download");
   if (device_ms) ck(cudaEventElapsedTime(device_ms, ev0, ev1), "elapsed");
   *out = m;
