@@ -1,7 +1,8 @@
 """Build the package's native libraries in-tree (nextgen_b200/lib/).
 
   libcgx.so          CUDA kernels + C ABI (include/cgx.h, include/cgx_ops.h), sm_100a only
-  libcgx_meshgen.so  host mesh/operator generator (include/cgx_meshgen.h)
+  libcgx_meshgen.so  host mesh/operator generator and .mles reader
+                     (include/cgx_meshgen.h, include/cgx_mles.h)
 
 `python -m nextgen_b200.build` rebuilds whatever is out of date.
 """
@@ -51,10 +52,11 @@ def _run(cmd):
 
 def build_meshgen(force=False):
     out = os.path.join(LIB, "libcgx_meshgen.so")
-    src = os.path.join(CSRC, "meshgen.cpp")
-    if force or _stale(out, [src, os.path.join(CSRC, "svd33.h"), os.path.join(INC, "cgx_meshgen.h")]):
+    srcs = [os.path.join(CSRC, f) for f in ("meshgen.cpp", "mles.cpp")]
+    deps = srcs + [os.path.join(CSRC, "svd33.h"), os.path.join(INC, "cgx_meshgen.h"), os.path.join(INC, "cgx_mles.h")]
+    if force or _stale(out, deps):
         os.makedirs(LIB, exist_ok=True)
-        _run([_cxx(), "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out, src])
+        _run([_cxx(), "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out] + srcs)
     return out
 
 

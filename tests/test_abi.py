@@ -60,6 +60,14 @@ def test_meshgen_exports_every_declared_symbol(built):
     assert names and all(hasattr(L, n) for n in names)
 
 
+def test_meshgen_exports_every_mles_symbol(built):
+    from nextgen_b200 import _lib
+    names = declared("include/cgx_mles.h")
+    assert names == ["cgx_mles_free", "cgx_mles_last_error", "cgx_mles_read"]
+    L = ctypes.CDLL(_lib.path("libcgx_meshgen.so"))
+    assert all(hasattr(L, n) for n in names)
+
+
 def test_oracle_exports_every_declared_symbol(built):
     names = declared("oracle/oracle.h")
     L = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
