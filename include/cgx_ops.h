@@ -56,7 +56,8 @@ typedef struct cgx_compact_desc {
  * device time from the end of the upload to the start of the download.
  * Returns 0, CGX_E_ARG for an inconsistent mesh, a box too thin for the
  * extended stencil (a cell reaching its own image) or an operator row longer
- * than 768 entries, CGX_E_OOM or CGX_E_CUDA; cgx_last_error() says which.
+ * than 384 entries (the host generator's limit), CGX_E_OOM or CGX_E_CUDA;
+ * cgx_last_error() says which.
  */
 int cgx_operators_build(const cgx_compact_desc* in, double interp_factor, double sigma_thresh,
                         int device, cgx_meshgen_out** out, float* device_ms);

@@ -16,9 +16,10 @@
 //   1. local faces of each cell (faocv), ifa ascending; cvocv            thread/face, thread/cell
 //   2. gradient coefficients (3x3 SVD pseudo-inverse per cell)           thread/cell
 //   3. operator rows D(r, image): the row's distinct images collected in a
-//      shared-memory hash set and bitonic-sorted by one warp; then each lane
-//      owns one image and adds the row's terms that hit it in the host's
-//      term order (no atomics on values, so sums are order-exact)          warp/row
+//      shared-memory hash set and bitonic-sorted by one warp; then the row's
+//      terms, 32 at a time in the host's term order, are added to per-image
+//      shared-memory accumulators in rounds that keep that order per image
+//      (no floating-point atomics, so sums are order-exact)               warp/row
 //   4. extended faces: n = D_ij - D_ji, c = D_ij + D_ji per canonical pair,
 //      bucketed by the smaller cell, ordered by (cell, image); periodic
 //      pairs split into one side per owner; level-2 ghosts numbered by
@@ -53,8 +54,8 @@ namespace {
 
 typedef long long i64;
 
-constexpr int kRowMax = 768;  // distinct entries of one operator row
-constexpr int kHash = 1024;   // hash slots per row (power of two above kRowMax)
+constexpr int kRowMax = 384;  // distinct entries of one operator row (the host generator's limit)
+constexpr int kHash = 512;    // hash slots per row (power of two above kRowMax)
 constexpr int kRowWarps = 4;  // rows (warps) per block of the row kernels
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
@@ -962,7 +963,7 @@ void check_err(const int* d_err, cudaStream_t s) {
   ck(cudaStreamSynchronize(s), "sync");
   if (e[ERR_INPUT]) throw Failure{CGX_E_ARG, "cgx_operators_build: inconsistent compact mesh (cell or ghost index out of range)"};
   if (e[ERR_THIN]) throw Failure{CGX_E_ARG, "cgx_operators_build: box too thin (extended stencil reaches a cell's own image)"};
-  if (e[ERR_ROW]) throw Failure{CGX_E_ARG, "cgx_operators_build: operator row longer than 768 entries"};
+  if (e[ERR_ROW]) throw Failure{CGX_E_ARG, "cgx_operators_build: operator row longer than 384 entries"};
   if (e[ERR_INTERNAL]) throw Failure{CGX_E_CUDA, "cgx_operators_build: internal error (operator term without an image)"};
 }
 
