@@ -186,12 +186,18 @@ int cgx_calc_cfl(cgx_solver* s, double dt, double* cfl_max, double* cfl);
  * CGX_E_NAN after restoring the stored state and scaling dt_data[0] by 0.8. */
 int cgx_advance_solution(cgx_solver* s);
 /* nsteps of {setDt; advanceSolution}, dt and time kept on the device, the
- * step replayed from a CUDA graph.  NaNs are checked every check_interval
- * steps and after the last one (CGX_E_NAN as above). */
+ * step replayed from a CUDA graph.  NaNs are checked whenever the global step
+ * count reaches a multiple of check_interval and after the last step, and the
+ * restore point is stored at multiples of 20 check_intervals
+ * (IdealGasSolver.hpp:807-811; CGX_E_NAN as above). */
 int cgx_step(cgx_solver* s, int nsteps);
 
 /* time, dt of the last completed step (0 before the first) and step count */
 int cgx_get_time(cgx_solver* s, double* time, double* dt, int* step);
+/* Restart: set the solver's time and step count, as a host solver does after
+ * reading them from a restart file.  After cgx_init_complete the current
+ * state becomes the restore point. */
+int cgx_set_time(cgx_solver* s, double time, int step);
 /* report(): {sum rho V, sum rho u V (3), sum rhoE V}, fixed-order reduction. */
 int cgx_totals(cgx_solver* s, double out[5]);
 

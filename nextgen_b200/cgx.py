@@ -137,7 +137,7 @@ EXPORTS = [
     "cgx_calc_rhs", "cgx_rk3_step", "cgx_calc_cfl", "cgx_advance_solution", "cgx_step",
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
-    "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled",
+    "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
 ]
 
 _LIB = None
@@ -169,6 +169,7 @@ def lib():
         "cgx_advance_solution": (ctypes.c_int, [vp]),
         "cgx_step": (ctypes.c_int, [vp, ctypes.c_int]),
         "cgx_get_time": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_int_p]),
+        "cgx_set_time": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "cgx_totals": (ctypes.c_int, [vp, c_dbl_p]),
         "cgx_get_primitive": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p, c_dbl_p]),
         "cgx_get_grad": (ctypes.c_int, [vp, c_dbl_p]),
@@ -335,6 +336,10 @@ class Solver:
         t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         _check(lib().cgx_get_time(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))
         return t.value, dt.value, st.value
+
+    def set_time(self, time, step):
+        """Restart at (time, step): cgx_set_time."""
+        _check(lib().cgx_set_time(self.h, float(time), int(step)))
 
     def totals(self):
         out = np.empty(5)

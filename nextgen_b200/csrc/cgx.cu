@@ -2788,25 +2788,44 @@ extern "C" int cgx_step(cgx_solver* s, int nsteps) {
   int rc;
   if ((rc = ensure_graph(s))) return rc;
   const int ci = std::max(1, s->prm.check_interval);
+  // checks fall on global step numbers (IdealGasSolver.hpp:807-811): each
+  // batch ends at the next multiple of check_interval, so a run restarted at
+  // any step (cgx_set_time) checks and stores where the reference does
+  Ctl c;
+  if ((rc = read_ctl(s, &c))) return rc;
   int done = 0;
   while (done < nsteps) {
-    const int batch = std::min(ci, nsteps - done);
+    const int batch = std::min(ci - c.step % ci, nsteps - done);
     for (int k = 0; k < batch; ++k) {
       CK(cudaGraphLaunch(s->graph, s->stream));
       s->launches += launches_per_step(s->run);
     }
     done += batch;
-    bool nan = false;
-    if ((rc = check_nan(s, &nan))) return rc;
-    if (nan) {
+    if ((rc = read_ctl(s, &c))) return rc;
+    if (c.nan) {
       if ((rc = restore_state(s))) return rc;
       return fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8");
     }
-    Ctl c;
-    if ((rc = read_ctl(s, &c))) return rc;
     if (c.step % (ci * 20) == 0 && (rc = store_state(s))) return rc;
   }
   return CGX_OK;
+}
+
+extern "C" int cgx_set_time(cgx_solver* s, double time, int step) {
+  if (!s) return fail(CGX_E_ARG, "null solver");
+  if (step < 0 || !std::isfinite(time)) return fail(CGX_E_ARG, "cgx_set_time: step < 0 or time not finite");
+  CK(cudaSetDevice(s->mesh->device));
+  Ctl c;
+  int rc = read_ctl(s, &c);
+  if (rc) return rc;
+  c.time = time;
+  c.step = step;
+  c.dt_last = 0.0;
+  CK(cudaMemcpyAsync(s->sd.ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (!s->inited) return CGX_OK;
+  s->have_store = false;  // the restart is the first restore point
+  return store_state(s);
 }
 
 static int ensure_graph(cgx_solver* s) {
