@@ -27,6 +27,8 @@ MESHES = [
     dict(nx=20, jitter=0.0),
     dict(nx=32, ny=32, nz=6, L=(10.0, 10.0, 1.875), jitter=0.25, seed=1234),
     dict(nx=24, jitter=0.3, seed=7, interp_factor=0.25, sigma_thresh=0.9),  # 9111 cells thresholded
+    dict(nx=8, ny=8, nz=4, L=(1.0, 1.0, 0.5), jitter=0.25, seed=3),  # thinnest box the generator makes
+    dict(nx=4, jitter=0.2, seed=5),  # 64 cells: most faces periodic
 ]
 
 
