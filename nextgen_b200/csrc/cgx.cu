@@ -41,6 +41,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <type_traits>
@@ -1343,6 +1344,7 @@ struct cgx_solver {
   cudaGraphExec_t graph = nullptr;
   cudaGraphExec_t pgraph = nullptr;  // the step with face-kernel timing events (cgx_step_profiled)
   cudaEvent_t pev[9] = {};
+  std::unique_ptr<cgx_staging::Staging> staging;  // for pageable caller arrays, made on first use
   std::atomic<long long> launches{0};
 };
 
@@ -2540,18 +2542,71 @@ extern "C" int cgx_solver_destroy(cgx_solver* s) {
   for (cudaEvent_t e : s->pev)
     if (e) cudaEventDestroy(e);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  s->staging.reset();
   for (void* q : s->allocs) cudaFree(q);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return CGX_OK;
 }
 
+// Copies between the caller's host arrays and the device.  Page-locked
+// (cudaMallocHost or registered) arrays go straight to the copy engine;
+// pageable ones, such as a host solver's new[] arrays, go through the
+// solver's two pinned staging chunks with the host-side copy on all threads,
+// which is several times faster than a pageable cudaMemcpy.
+static bool page_locked(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+static int staging_of(cgx_solver* s, cgx_staging::Staging** st) {
+  if (!s->staging) {
+    std::unique_ptr<cgx_staging::Staging> n(new cgx_staging::Staging(s->stream));
+    const cudaError_t e = n->init();
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? CGX_E_OOM : CGX_E_CUDA,
+                  std::string("pinned staging buffers: ") + cudaGetErrorString(e));
+    s->staging = std::move(n);
+  }
+  *st = s->staging.get();
+  return CGX_OK;
+}
+
+static int host_to_device(cgx_solver* s, void* dst, const void* src, size_t bytes) {
+  if (bytes < (size_t(4) << 20) || page_locked(src)) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream));
+    return CGX_OK;
+  }
+  cgx_staging::Staging* st;
+  int rc = staging_of(s, &st);
+  if (rc) return rc;
+  CK(st->put(dst, src, bytes));
+  return CGX_OK;
+}
+
+// complete when it returns for staged copies; queued on the stream otherwise
+static int device_to_host(cgx_solver* s, void* dst, const void* src, size_t bytes) {
+  if (bytes < (size_t(4) << 20) || page_locked(dst)) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream));
+    return CGX_OK;
+  }
+  cgx_staging::Staging* st;
+  int rc = staging_of(s, &st);
+  if (rc) return rc;
+  CK(st->get(dst, src, bytes));
+  return CGX_OK;
+}
+
 static int upload_stage(cgx_solver* s, const double* a, const double* u, const double* b) {
   const size_t N = s->mesh->N;
-  CK(cudaMemcpyAsync(s->d_stage, a, N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemcpyAsync(s->d_stage + N, u, 3 * N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemcpyAsync(s->d_stage + 4 * N, b, N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-  return CGX_OK;
+  int rc;
+  if ((rc = host_to_device(s, s->d_stage, a, N * sizeof(double)))) return rc;
+  if ((rc = host_to_device(s, s->d_stage + N, u, 3 * N * sizeof(double)))) return rc;
+  return host_to_device(s, s->d_stage + 4 * N, b, N * sizeof(double));
 }
 
 extern "C" int cgx_set_state(cgx_solver* s, const double* rho, const double* u, const double* rhoE) {
@@ -2587,9 +2642,9 @@ extern "C" int cgx_get_state(cgx_solver* s, double* rho, double* u, double* rhoE
   k_state_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd);
   int rc = launch_check(s->run, 1);
   if (rc) return rc;
-  if (rho) CK(cudaMemcpyAsync(rho, s->d_stage, N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-  if (u) CK(cudaMemcpyAsync(u, s->d_stage + N, 3 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-  if (rhoE) CK(cudaMemcpyAsync(rhoE, s->d_stage + 4 * size_t(N), N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if (rho && (rc = device_to_host(s, rho, s->d_stage, N * sizeof(double)))) return rc;
+  if (u && (rc = device_to_host(s, u, s->d_stage + N, 3 * size_t(N) * sizeof(double)))) return rc;
+  if (rhoE && (rc = device_to_host(s, rhoE, s->d_stage + 4 * size_t(N), N * sizeof(double)))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
@@ -2640,10 +2695,10 @@ extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
   }
   if (nsc > 0) {
     if (size_t(nsc) * N > 9 * N) return fail(CGX_E_ARG, "cgx_set_scalars: staging too small");
-    CK(cudaMemcpyAsync(s->d_stage, sc, size_t(nsc) * N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-    k_scalars_io<<<int((N + 255) / 256), 256, 0, s->stream>>>(int(N), nsc, s->mesh->d_perm, s->d_stage, sd, 0, 0);
-    int rc = launch_check(s->run, 1);
+    int rc = host_to_device(s, s->d_stage, sc, size_t(nsc) * N * sizeof(double));
     if (rc) return rc;
+    k_scalars_io<<<int((N + 255) / 256), 256, 0, s->stream>>>(int(N), nsc, s->mesh->d_perm, s->d_stage, sd, 0, 0);
+    if ((rc = launch_check(s->run, 1))) return rc;
   }
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -2658,7 +2713,7 @@ extern "C" int cgx_get_scalars(cgx_solver* s, double* sc) {
   k_scalars_io<<<(N + 255) / 256, 256, 0, s->stream>>>(N, nsc, s->mesh->d_perm, s->d_stage, s->sd, 1, 0);
   int rc = launch_check(s->run, 1);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(sc, s->d_stage, size_t(nsc) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if ((rc = device_to_host(s, sc, s->d_stage, size_t(nsc) * N * sizeof(double)))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
@@ -2674,7 +2729,7 @@ extern "C" int cgx_get_rhs_sc(cgx_solver* s, int rk_stage, double* rhs_sc) {
                                                        rk_stage - 1);
   int rc = launch_check(s->run, 1);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(rhs_sc, s->d_stage, size_t(nsc) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if ((rc = device_to_host(s, rhs_sc, s->d_stage, size_t(nsc) * N * sizeof(double)))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
@@ -2726,7 +2781,7 @@ extern "C" int cgx_calc_rhs(cgx_solver* s, double* rhs_out, double time, int rk_
     const int N = s->mesh->N;
     k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, 0, rk_stage - 1, s->ph.R, s->ph.p_ref);
     if ((rc = launch_check(s->run, 1))) return rc;
-    CK(cudaMemcpyAsync(rhs_out, s->d_stage, 5 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    if ((rc = device_to_host(s, rhs_out, s->d_stage, 5 * size_t(N) * sizeof(double)))) return rc;
   }
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -2995,7 +3050,7 @@ static int diag(cgx_solver* s, int what, int k, double* out) {
   k_diag_out<<<(N + 255) / 256, 256, 0, s->stream>>>(N, s->mesh->d_perm, s->d_stage, s->sd, what, 0, s->ph.R, s->ph.p_ref);
   int rc = launch_check(s->run, 1);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(out, s->d_stage, size_t(k) * N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if ((rc = device_to_host(s, out, s->d_stage, size_t(k) * N * sizeof(double)))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
