@@ -377,6 +377,10 @@ def run_cgx(args):
             kernels[kname] = {"launch_ms": ktimes[key], "algorithmic_bytes_per_cell": split_bytes[kname],
                               "achieved_gbs": split_bytes[kname] * N / (ktimes[key] * 1e-3) / 1e9,
                               "dram_bytes_per_cell": per_kernel_dram.get(kname)}
+            if per_kernel_dram.get(kname):
+                # the kernel's actual DRAM traffic over its in-step launch time
+                kernels[kname]["traffic_gbs"] = per_kernel_dram[kname] * N / (ktimes[key] * 1e-3) / 1e9
+                kernels[kname]["traffic_frac"] = kernels[kname]["traffic_gbs"] / peak
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -398,6 +402,8 @@ def run_cgx(args):
         "roofline": {"bound": "hbm", "kernel": "k_rhs_ext + k_rhs_comp (calcRhsBase)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_cell": rhs_bytes,
+                     "traffic_achieved": achieved * traffic / (rhs_bytes * N) if traffic else None,
+                     "traffic_frac": achieved * traffic / (rhs_bytes * N) / peak if traffic else None,
                      "launch_ms": ktimes["rhs"], "kernels": kernels},
         "step_roofline": {"bytes_per_cell_step": step_bytes, "achieved": value / world * step_bytes / 1e9,
                           "frac": value / world * step_bytes / 1e9 / peak, "unit": "GB/s"},
