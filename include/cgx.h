@@ -144,7 +144,12 @@ int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision prec,
                       cgx_solver** out);
 int cgx_solver_destroy(cgx_solver* s);
 
-/* Conserved state in reference order (host arrays). */
+/* Conserved state in reference order (host arrays).  Host arrays may be
+ * page-locked (copied directly) or pageable, such as a host solver's new[]
+ * arrays: pageable arrays of 4 MiB or more are staged through the solver's
+ * two pinned 64 MiB chunks (allocated at first use), which is several times
+ * faster than a pageable copy.  The same holds for every call below that
+ * takes or fills a host array of cells. */
 int cgx_set_state(cgx_solver* s, const double* rho, const double* u, const double* rhoE);
 /* rho, u, p; rhoE = p/(gamma-1) + 0.5 rho |u|^2 (IdealGasSolver.hpp:275-301). */
 int cgx_set_state_primitive(cgx_solver* s, const double* rho, const double* u,
