@@ -31,7 +31,9 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <unordered_map>
+#include <utility>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -329,11 +331,42 @@ struct RowAcc {
   }
 };
 
+// std::vector whose elements start uninitialised, for large arrays that are
+// written in full (in parallel) before they are read: no serial zero fill
 template <class T>
-T* dup_array(const std::vector<T>& v) {
+struct DefaultInit : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = DefaultInit<U>;
+  };
+  DefaultInit() = default;
+  template <class U>
+  DefaultInit(const DefaultInit<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <class T>
+using uvec = std::vector<T, DefaultInit<T>>;
+
+// malloc'd copy for the C ABI output, copied on all threads
+template <class T, class A>
+T* dup_array(const std::vector<T, A>& v) {
   T* p = static_cast<T*>(std::malloc(sizeof(T) * std::max<size_t>(v.size(), 1)));
   if (!p) throw std::bad_alloc();
-  if (!v.empty()) std::memcpy(p, v.data(), sizeof(T) * v.size());
+  const size_t bytes = sizeof(T) * v.size(), blk = size_t(1) << 20;
+  const long long nb = (long long)((bytes + blk - 1) / blk);
+  const char* src = reinterpret_cast<const char*>(v.data());
+#pragma omp parallel for schedule(static)
+  for (long long b = 0; b < nb; ++b) {
+    const size_t off = size_t(b) * blk;
+    std::memcpy(reinterpret_cast<char*>(p) + off, src + off, std::min(blk, bytes - off));
+  }
   return p;
 }
 
@@ -703,18 +736,28 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
 
     // ---------------- faocv + local faces ----------------
     std::vector<int> faocv_i(ncv + 1, 0);
+#pragma omp parallel for schedule(static)
     for (int ifa = 0; ifa < nfa; ++ifa) {
+#pragma omp atomic
       ++faocv_i[cvofa[2 * size_t(ifa)] + 1];
-      if (ifa < nfa_i) ++faocv_i[cvofa[2 * size_t(ifa) + 1] + 1];
+      if (ifa < nfa_i) {
+#pragma omp atomic
+        ++faocv_i[cvofa[2 * size_t(ifa) + 1] + 1];
+      }
     }
     for (int a = 0; a < ncv; ++a) faocv_i[a + 1] += faocv_i[a];
-    std::vector<LocFace> loc(faocv_i[ncv]);
+    uvec<LocFace> loc(faocv_i[ncv]);
     {
+      // filled in any order, then each cell's faces ordered by face id
       std::vector<int> fill(faocv_i.begin(), faocv_i.end() - 1);
+#pragma omp parallel for schedule(static)
       for (int ifa = 0; ifa < nfa; ++ifa) {
         const int c0 = cvofa[2 * size_t(ifa)], c1 = cvofa[2 * size_t(ifa) + 1];
         {
-          LocFace& lf = loc[fill[c0]++];
+          int k;
+#pragma omp atomic capture
+          k = fill[c0]++;
+          LocFace& lf = loc[k];
           lf.ifa = ifa;
           lf.nbr_idx = c1;
           nbr_image(c1, lf.nbr_cell, lf.sx, lf.sy, lf.sz);
@@ -724,7 +767,10 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
           }
         }
         if (ifa < nfa_i) {
-          LocFace& lf = loc[fill[c1]++];
+          int k;
+#pragma omp atomic capture
+          k = fill[c1]++;
+          LocFace& lf = loc[k];
           lf.ifa = ifa;
           lf.nbr_idx = c0;
           lf.nbr_cell = c0;
@@ -735,6 +781,10 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
           }
         }
       }
+#pragma omp parallel for schedule(dynamic, 1024)
+      for (int a = 0; a < ncv; ++a)
+        std::sort(loc.begin() + faocv_i[a], loc.begin() + faocv_i[a + 1],
+                  [](const LocFace& p, const LocFace& q) { return p.ifa < q.ifa; });
     }
 
     PT.mark("faocv/local");
@@ -742,6 +792,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     std::vector<int> cvocv_i(ncv + 1);
     for (int a = 0; a <= ncv; ++a) cvocv_i[a] = faocv_i[a] + a;
     std::vector<int> cvocv_v(cvocv_i[ncv]);
+#pragma omp parallel for schedule(static)
     for (int a = 0; a < ncv; ++a) {
       int coc = cvocv_i[a];
       cvocv_v[coc++] = a;
@@ -908,7 +959,8 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
       }
     }
     for (int a = 0; a < ncv; ++a) drow_i[a + 1] += drow_i[a];
-    std::vector<DEnt> dent(size_t(drow_i[ncv]));
+    uvec<DEnt> dent(size_t(drow_i[ncv]));
+#pragma omp parallel for schedule(dynamic, 1)
     for (int ch = 0; ch < nch; ++ch) {
       const int a0 = ch * CH;
       std::copy(dchunks[ch].begin(), dchunks[ch].end(), dent.begin() + drow_i[a0]);
@@ -988,7 +1040,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
       });
     std::vector<int64_t> ooff(ncv + 1, 0);
     for (int a = 0; a < ncv; ++a) ooff[a + 1] = ooff[a] + ocnt[a];
-    std::vector<EFace> efs(size_t(ooff[ncv]));
+    uvec<EFace> efs(size_t(ooff[ncv]));
     std::fill(ocnt.begin(), ocnt.end(), 0);
 #pragma omp parallel for schedule(dynamic, 1024)
     for (int r = 0; r < ncv; ++r)
@@ -998,7 +1050,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
         pos = ocnt[f.a]++;
         efs[size_t(ooff[f.a] + pos)] = f;
       });
-    std::vector<DEnt>().swap(dent);
+    uvec<DEnt>().swap(dent);
     auto efkey = [](const EFace& p) { return img_key(p.b, p.sx, p.sy, p.sz); };
     std::vector<int> ni(ncv + 1, 0), np(ncv, 0);
 #pragma omp parallel for schedule(dynamic, 1024)
@@ -1010,11 +1062,14 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
       ni[a + 1] = c;
     }
     // per-side periodic entries: both cells of a periodic pair
+#pragma omp parallel for schedule(dynamic, 1024)
     for (int a = 0; a < ncv; ++a) {
       for (int64_t k = ooff[a]; k < ooff[a + 1]; ++k) {
         const EFace& f = efs[k];
         if (f.sx || f.sy || f.sz) {
+#pragma omp atomic
           ++np[f.a];
+#pragma omp atomic
           ++np[f.b];
         }
       }
@@ -1029,8 +1084,8 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     }
     const int nef_i = int(nef_i64);
     const int nef = int(nef_i64 + nper_ef);
-    std::vector<int> cvoef(2 * size_t(nef));
-    std::vector<double> n_ef(3 * size_t(nef)), c_ef(3 * size_t(nef));
+    uvec<int> cvoef(2 * size_t(nef));
+    uvec<double> n_ef(3 * size_t(nef)), c_ef(3 * size_t(nef));
     {
 #pragma omp parallel for schedule(dynamic, 1024)
       for (int a = 0; a < ncv; ++a) {
@@ -1053,16 +1108,24 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
         int64_t key;
         double n[3], c[3];
       };
-      std::vector<PSide> ps(static_cast<size_t>(nper_ef));
+      uvec<PSide> ps(static_cast<size_t>(nper_ef));
       std::fill(np.begin(), np.end(), 0);
+      // filled in any order: each owner's sides are sorted by their (unique)
+      // image key below
+#pragma omp parallel for schedule(dynamic, 1024)
       for (int a = 0; a < ncv; ++a) {
         for (int64_t k = ooff[a]; k < ooff[a + 1]; ++k) {
           const EFace& f = efs[k];
           if (!(f.sx || f.sy || f.sz)) continue;
           PSide p0{img_key(f.b, f.sx, f.sy, f.sz), {f.n[0], f.n[1], f.n[2]}, {f.c[0], f.c[1], f.c[2]}};
           PSide p1{img_key(f.a, -f.sx, -f.sy, -f.sz), {-f.n[0], -f.n[1], -f.n[2]}, {f.c[0], f.c[1], f.c[2]}};
-          ps[size_t(poff[f.a] + np[f.a]++)] = p0;
-          ps[size_t(poff[f.b] + np[f.b]++)] = p1;
+          int k0, k1;
+#pragma omp atomic capture
+          k0 = np[f.a]++;
+#pragma omp atomic capture
+          k1 = np[f.b]++;
+          ps[size_t(poff[f.a] + k0)] = p0;
+          ps[size_t(poff[f.b] + k1)] = p1;
         }
       }
 #pragma omp parallel for schedule(dynamic, 1024)
@@ -1086,12 +1149,12 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
       }
     }
     PT.mark("ef assembly");
-    std::vector<EFace>().swap(efs);
+    uvec<EFace>().swap(efs);
     const int ncv_g2 = ncv + int(g_owner.size());
     // ghosts reachable by compact faces were numbered first
     // (all periodic compact faces were processed before any extended face)
 
-    std::vector<double> x_cv(3 * size_t(ncv_g2));
+    uvec<double> x_cv(3 * size_t(ncv_g2));
     for (int a = 0; a < ncv; ++a) {
       x_cv[3 * size_t(a)] = xcv[a].x;
       x_cv[3 * size_t(a) + 1] = xcv[a].y;
@@ -1127,35 +1190,49 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     auto dist3 = [](const double* a, const double* b) {
       return std::sqrt(std::pow(a[0] - b[0], 2) + std::pow(a[1] - b[1], 2) + std::pow(a[2] - b[2], 2));
     };
+    // Each cell sums in the order a loop over the faces adds to it: the
+    // internal faces where it is the second cell (they belong to lower cells'
+    // groups, so they come first), its own internal faces, its periodic
+    // sides; sa_to_vol and the dcmag_hat area over its compact faces in face
+    // order.  The incoming faces are gathered per cell first.
+    std::vector<int> in_i(ncv + 1, 0);
+#pragma omp parallel for schedule(static)
     for (int ief = 0; ief < nef_i; ++ief) {
-      const double cm = mag3(&c_ef[3 * size_t(ief)]);
-      const int c0 = cvoef[2 * size_t(ief)], c1 = cvoef[2 * size_t(ief) + 1];
-      cmag[c0] += cm;
-      cmag[c1] += cm;
-      const double delta = dist3(&x_cv[3 * size_t(c1)], &x_cv[3 * size_t(c0)]);
-      dcmag[c0] += delta * cm;
-      dcmag[c1] += delta * cm;
+#pragma omp atomic
+      ++in_i[cvoef[2 * size_t(ief) + 1] + 1];
     }
-    for (int ief = nef_i; ief < nef; ++ief) {
-      const double cm = mag3(&c_ef[3 * size_t(ief)]);
-      const int c0 = cvoef[2 * size_t(ief)], c1 = cvoef[2 * size_t(ief) + 1];
-      cmag[c0] += cm;
-      const double delta = dist3(&x_cv[3 * size_t(c1)], &x_cv[3 * size_t(c0)]);
-      dcmag[c0] += delta * cm;
+    for (int a = 0; a < ncv; ++a) in_i[a + 1] += in_i[a];
+    uvec<int> in_v(size_t(in_i[ncv]));
+    {
+      std::vector<int> fill(in_i.begin(), in_i.end() - 1);
+#pragma omp parallel for schedule(static)
+      for (int ief = 0; ief < nef_i; ++ief) {
+        int k;
+#pragma omp atomic capture
+        k = fill[cvoef[2 * size_t(ief) + 1]]++;
+        in_v[size_t(k)] = ief;
+      }
     }
+#pragma omp parallel for schedule(dynamic, 1024)
     for (int a = 0; a < ncv; ++a) {
+      std::sort(in_v.begin() + in_i[a], in_v.begin() + in_i[a + 1]);
+      double cm_sum = 0.0, dc = 0.0;
+      auto add = [&](size_t ief) {
+        const double cm = mag3(&c_ef[3 * ief]);
+        const int c0 = cvoef[2 * ief], c1 = cvoef[2 * ief + 1];
+        cm_sum += cm;
+        const double delta = dist3(&x_cv[3 * size_t(c1)], &x_cv[3 * size_t(c0)]);
+        dc += delta * cm;
+      };
+      for (int k = in_i[a]; k < in_i[a + 1]; ++k) add(size_t(in_v[size_t(k)]));
+      for (int ief = ni[a]; ief < ni[a + 1]; ++ief) add(size_t(ief));
+      for (int64_t k = poff[a]; k < poff[a + 1]; ++k) add(size_t(nef_i64 + k));
       double area_sum = 0.0;
-      for (int foc = faocv_i[a]; foc < faocv_i[a + 1]; ++foc)
-        area_sum += mag3(&n_fa[3 * size_t(loc[foc].ifa)]);
-      dcmag[a] /= area_sum;
+      for (int foc = faocv_i[a]; foc < faocv_i[a + 1]; ++foc) area_sum += mag3(&n_fa[3 * size_t(loc[foc].ifa)]);
+      cmag[a] = cm_sum;
+      dcmag[a] = dc / area_sum;
+      sav[a] = area_sum / vol[a];
     }
-    for (int ifa = 0; ifa < nfa; ++ifa) {
-      const int c0 = cvofa[2 * size_t(ifa)], c1 = cvofa[2 * size_t(ifa) + 1];
-      const double nm = mag3(&n_fa[3 * size_t(ifa)]);
-      sav[c0] += nm;
-      if (c1 < ncv) sav[c1] += nm;
-    }
-    for (int a = 0; a < ncv; ++a) sav[a] = sav[a] / vol[a];
 
     PT.mark("factors");
     // ---------------- output ----------------
