@@ -171,3 +171,9 @@ def test_compact_only_is_the_generators_compact_part(built):
     assert np.array_equal(a.shift_g[:ng1], b.shift_g)
     for f in ("cvocv_i", "cvocv_grad_coeff", "cvoef", "n_ef", "c_ef", "area_over_delta_fa", "dcmag_hat_cv"):
         assert getattr(b, f) is None, f
+
+
+def test_compact_only_checks_arguments(built):
+    for kw in (dict(nx=3), dict(nx=8, jitter=0.5), dict(nx=8, L=(1.0, 0.0, 1.0))):
+        with pytest.raises(RuntimeError):
+            PeriodicBoxMesh(compact_only=True, **kw)

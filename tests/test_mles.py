@@ -128,6 +128,15 @@ def test_errors(built, tmp_path):
     with pytest.raises(MlesError) as e:
         MlesMesh(str(cut))
     assert e.value.code == -1
+    # the same file with its first two words in the other byte order
+    raw = bytearray(open(ASSET, "rb").read(1 << 16))
+    for o in (0, 4):
+        raw[o:o + 4] = raw[o:o + 4][::-1]
+    swapped = tmp_path / "swapped.mles"
+    swapped.write_bytes(bytes(raw))
+    with pytest.raises(MlesError) as e:
+        MlesMesh(str(swapped))
+    assert e.value.code == -3 and "byte-swapped" in str(e.value)
     if os.path.exists(V3_LES):
         with pytest.raises(MlesError) as e:
             MlesMesh(V3_LES)
