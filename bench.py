@@ -255,7 +255,16 @@ def run_cgx(args):
     device = local
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    m = PeriodicBoxMesh(args.n, jitter=JITTER, seed=SEED, nthreads=max(1, cores // world))
+    if args.device_ops:
+        # the mesher's compact output, operators built on this rank's GPU
+        # (bit-identical to the host generator's)
+        from nextgen_b200.meshgen import DeviceOperatorMesh
+        compact = PeriodicBoxMesh(args.n, jitter=JITTER, seed=SEED, nthreads=max(1, cores // world),
+                                  compact_only=True)
+        m = DeviceOperatorMesh(compact, device=device)
+        compact.close()
+    else:
+        m = PeriodicBoxMesh(args.n, jitter=JITTER, seed=SEED, nthreads=max(1, cores // world))
     t_mesh = time.perf_counter() - t0
     prm = cases.tgv_params()
     rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
@@ -392,7 +401,8 @@ def run_cgx(args):
                    "cells": N, "e_per_cell": e, "f_per_cell": f,
                    "l2": "inputs larger than L2 (%.1f GB mesh on device)" % (st.device_bytes / 1e9),
                    "parallelism": "replicas x%d" % world, "precision": "fp64",
-                   "mesh_build_s": round(t_mesh, 2), "mesh_upload_s": round(t_up, 2)},
+                   "mesh_build_s": round(t_mesh, 2), "mesh_upload_s": round(t_up, 2),
+                   "mesh_operators": "gpu (cgx_operators_build)" if args.device_ops else "host generator"},
         "e2e_pageable_host_arrays": {"value": e2e_pageable, "unit": UNIT},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 40 * N, "d2h_bytes_per_step": 40 * N,
                 "steps": ke, "how": "per step: cgx_set_state (pinned host -> device), cgx_step(1), "
@@ -688,6 +698,8 @@ def main():
                     help="instead of the throughput bench: FP64 GPU vs CPU oracle over many steps")
     ap.add_argument("--validate-n", type=int, default=128)
     ap.add_argument("--validate-steps", type=int, default=200)
+    ap.add_argument("--device-ops", action="store_true",
+                    help="build the bench mesh's operators on the GPU from the compact mesh")
     ap.add_argument("--opbuild", action="store_true",
                     help="instead of the throughput bench: operator build on the GPU vs the host generator")
     ap.add_argument("--opbuild-n", type=int, default=128)
