@@ -107,3 +107,19 @@ def test_product_never_imports_the_oracle():
                 txt = open(os.path.join(dp, f)).read()
                 assert "import oracle" not in txt and "from oracle" not in txt, f
                 assert "liboracle" not in txt and "libref" not in txt, f
+
+
+def test_gpu_paths_fail_loudly_without_a_gpu(built):
+    """No CPU fallback: without a CUDA device the mesh upload and the operator
+    build return CGX_E_CUDA (-3) instead of computing anything on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from nextgen_b200 import cgx, meshgen
+    m = meshgen.PeriodicBoxMesh(6, jitter=0.1)
+    with pytest.raises(cgx.CgxError) as e:
+        meshgen.DeviceOperatorMesh(m)
+    assert e.value.code == -3
+    with pytest.raises(cgx.CgxError) as e:
+        cgx.Mesh(m, device=0)
+    assert e.value.code == -3
