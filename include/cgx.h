@@ -238,6 +238,11 @@ int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]);
 int cgx_get_tuning(const cgx_solver* s, int out[4]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
+/* Self-test of the device reciprocal that the flux kernels use for the face
+ * density 2/(v0+v1) and the face Mach number |u_n|/c (no counterpart in the
+ * reference, which divides in IEEE FP64): out[i] = that reciprocal of x[i]
+ * for n host values, evaluated on `device`. */
+int cgx_selftest_rcp(int device, const double* x, double* out, int n);
 
 /*
  * Batched and served form (no single reference counterpart: the reference
@@ -286,7 +291,11 @@ long long cgx_batch_launch_count(const cgx_batch* b);
  * (320 KiB, held by every GPU that loads this library until the process
  * exits); n is limited to 16,777,216 cells (8192 blocks of 2048) and larger
  * n is rejected with CGX_E_ARG.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
+ * array's device address and keeps it for the life of the process; make that
+ * first call before any stream capture.  cudaDeviceReset (or any other
+ * teardown of the device's primary context) reloads the module and leaves
+ * the kept address stale: do not call this entry point on a device after
+ * resetting it.
  * All calls share the array: calls that overlap on the GPU (other streams,
  * other host threads) race, so serialise them.  Returns without waiting for
  * the GPU.

@@ -70,9 +70,11 @@ constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) 
 // device helpers
 // ===========================================================================
 
-// 1/x by Newton-Raphson refinement (two steps, r <- r + r(1 - x r)) of the
-// hardware reciprocal approximation (PTX rcp.approx.ftz.f64); within 1 ulp of
-// the correctly rounded quotient for the normal, O(1) arguments used here.
+// 1/x by the Newton-Raphson reciprocal iteration r <- r + r(1 - x r), two
+// steps (each squares the relative error), started from the hardware
+// approximation (PTX rcp.approx.ftz.f64).  Within 1 ulp of the correctly
+// rounded 1.0/x for the normal arguments used here (sums of specific volumes,
+// mean sound speeds); cgx_selftest_rcp exposes it for a direct check.
 __device__ __forceinline__ double rcp_nr(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -3096,6 +3098,30 @@ extern "C" int cgx_get_tuning(const cgx_solver* s, int out[4]) {
 }
 
 extern "C" long long cgx_launch_count(const cgx_solver* s) { return s ? s->launches.load() : 0; }
+
+namespace {
+__global__ void k_rcp_selftest(const double* __restrict__ x, double* __restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = rcp_nr(x[i]);
+}
+}  // namespace
+
+extern "C" int cgx_selftest_rcp(int device, const double* x, double* out, int n) {
+  if (!x || !out || n < 0) return fail(CGX_E_ARG, "cgx_selftest_rcp: null argument or negative size");
+  if (n == 0) return CGX_OK;
+  CK(cudaSetDevice(device));
+  double* d = nullptr;
+  CK(cudaMalloc(&d, 2 * size_t(n) * sizeof(double)));
+  cudaError_t e = cudaMemcpy(d, x, size_t(n) * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_rcp_selftest<<<(n + 255) / 256, 256>>>(d, d + n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + n, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(CGX_E_CUDA, std::string("cgx_selftest_rcp: ") + cudaGetErrorString(e));
+  return CGX_OK;
+}
 
 // ===========================================================================
 // batched / served form

@@ -76,8 +76,16 @@ struct Error {
 
 struct File {
   FILE* f = nullptr;
+  int64_t size = 0;  // bytes in the file
   ~File() {
     if (f) std::fclose(f);
+  }
+  // a record's data range [off, off + n*elem) must lie inside the file; checked
+  // before anything of that size is allocated, so a small file cannot make the
+  // reader allocate for counts it does not hold
+  void need(int64_t off, int64_t n, int64_t elem, const char* what) const {
+    if (off < 0 || n < 0 || n > (size - off) / elem)
+      fail(CGX_MLES_E_IO, std::string(what) + " record runs past the end of the file (truncated?)");
   }
   void read_at(int64_t off, void* dst, size_t bytes) {
     if (bytes == 0) return;
@@ -95,6 +103,7 @@ T* alloc(size_t n) {
 
 // int8 indices in the file -> int, each checked against [0, limit)
 int* read_indices(File& F, int64_t off, int64_t n, int64_t limit, const char* what) {
+  F.need(off, n, int64_t(sizeof(int64_t)), what);
   std::vector<int64_t> tmp(static_cast<size_t>(n));
   F.read_at(off, tmp.data(), sizeof(int64_t) * size_t(n));
   int* out = alloc<int>(size_t(n));
@@ -111,6 +120,7 @@ int* read_indices(File& F, int64_t off, int64_t n, int64_t limit, const char* wh
 // counts (n ints) then values (int8): CSR offsets [n+1] and int values
 void read_i_and_v(File& F, int64_t off, int64_t n, int64_t total, int64_t limit, int** csr, int** val,
                   const char* what) {
+  F.need(off, n, int64_t(sizeof(int32_t)), what);
   std::vector<int32_t> cnt(static_cast<size_t>(n));
   F.read_at(off, cnt.data(), sizeof(int32_t) * size_t(n));
   int* c = alloc<int>(size_t(n) + 1);
@@ -138,6 +148,7 @@ void read_i_and_v(File& F, int64_t off, int64_t n, int64_t total, int64_t limit,
 
 template <class T>
 T* read_array(File& F, int64_t off, int64_t n) {
+  F.need(off, n, int64_t(sizeof(T)), "array");
   T* p = alloc<T>(size_t(n));
   try {
     F.read_at(off, p, sizeof(T) * size_t(n));
@@ -154,6 +165,8 @@ void read_file(const char* path, cgx_mles* m) {
   File F;
   F.f = std::fopen(path, "rb");
   if (!F.f) fail(CGX_MLES_E_IO, std::string("cannot open ") + path);
+  if (fseeko(F.f, 0, SEEK_END) != 0 || (F.size = int64_t(ftello(F.f))) < 0)
+    fail(CGX_MLES_E_IO, std::string("cannot size ") + path);
   int32_t head[2];
   F.read_at(0, head, sizeof(head));
   if (head[0] != kMagic) {
@@ -180,6 +193,8 @@ void read_file(const char* path, cgx_mles* m) {
     if (needs_counts && !have_counts) fail(CGX_MLES_E_FORMAT, "data record before the counts record");
     switch (h.id) {
       case ID_NO_FA_BF_CV_COUNTS: {
+        // one counts record only: the arrays already read are sized by it
+        if (have_counts) fail(CGX_MLES_E_FORMAT, "a second counts record");
         m->nno = pair64(h.idata + 0);
         m->nbf = pair64(h.idata + 2);
         m->nfa = pair64(h.idata + 4);

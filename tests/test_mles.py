@@ -19,8 +19,9 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ASSET = "/root/reference/src/core/common/tests/assets/orifice.mles"
-V3_LES = "/root/reference/grids/result.lam_chan.les"
+REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+ASSET = os.path.join(REFERENCE_ROOT, "src/core/common/tests/assets/orifice.mles")
+V3_LES = os.path.join(REFERENCE_ROOT, "grids/result.lam_chan.les")
 
 pytestmark = pytest.mark.skipif(not os.path.exists(ASSET), reason="reference tree not present")
 
@@ -113,6 +114,20 @@ def test_zone_totals(mesh):
         assert abs(m.area_over_delta_bf[sl].sum() - z["area_over_delta"]) <= 1e-12 * z["area_over_delta"]
 
 
+def _records(data):
+    """(offset, id, skip) of each record of a UGP record file: a 256-byte
+    header per record, id at byte 52, skip (int64) at byte 56."""
+    out, off = [], 8
+    while off + 256 <= len(data):
+        rid = int(np.frombuffer(data, np.int32, 1, off + 52)[0])
+        skip = int(np.frombuffer(data, np.int64, 1, off + 56)[0])
+        out.append((off, rid, skip))
+        if rid == 51 or skip < 256:
+            break
+        off += skip
+    return out
+
+
 def test_errors(built, tmp_path):
     from nextgen_b200.mles import MlesError, MlesMesh
     with pytest.raises(MlesError) as e:
@@ -137,6 +152,26 @@ def test_errors(built, tmp_path):
     with pytest.raises(MlesError) as e:
         MlesMesh(str(swapped))
     assert e.value.code == -3 and "byte-swapped" in str(e.value)
+    # a second counts record after the cell-face records were read at the
+    # first one's sizes is refused
+    data = open(ASSET, "rb").read()
+    recs = _records(data)
+    cnt = next(r for r in recs if r[1] == 10001)
+    after = next(r for r in recs if r[1] == 2006)  # cvofa
+    dup = data[:after[0] + after[2]] + data[cnt[0]:cnt[0] + cnt[2]] + data[after[0] + after[2]:]
+    twice = tmp_path / "two_counts.mles"
+    twice.write_bytes(dup)
+    with pytest.raises(MlesError) as e:
+        MlesMesh(str(twice))
+    assert e.value.code == -2 and "second counts" in str(e.value)
+    # a record whose count reaches past the end of the file is refused before
+    # anything of that size is allocated: the x_no record cut after its header
+    xno = next(r for r in recs if r[1] == 31)
+    short = tmp_path / "short_x_no.mles"
+    short.write_bytes(data[:xno[0] + 256 + 64])
+    with pytest.raises(MlesError) as e:
+        MlesMesh(str(short))
+    assert e.value.code == -1 and "past the end" in str(e.value)
     if os.path.exists(V3_LES):
         with pytest.raises(MlesError) as e:
             MlesMesh(V3_LES)

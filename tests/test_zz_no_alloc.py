@@ -58,3 +58,27 @@ def test_totals_noalloc_matches_allocating_totals(built):
     # sizes beyond the stated maximum are refused before any GPU work
     rc = f(16_777_217, d_rho.data_ptr(), d_u.data_ptr(), d_e.data_ptr(), d_v.data_ptr(), out.data_ptr(), None)
     assert rc == -1 and b"exceed the maximum" in L.cgx_last_error()
+    # a null array is refused too
+    rc = f(m.ncv, None, d_u.data_ptr(), d_e.data_ptr(), d_v.data_ptr(), out.data_ptr(), None)
+    assert rc == -1 and b"null" in L.cgx_last_error()
+
+    # n = 0: one block of zero partials, totals zero (the scratch still holds
+    # the previous call's partials, which must not leak into the result)
+    out.fill_(7.0)
+    assert f(0, None, None, None, None, out.data_ptr(), ctypes.c_void_p(stream.cuda_stream)) == 0
+    torch.cuda.synchronize(dev)
+    assert (out.cpu().numpy() == 0.0).all()
+
+    # n = 2049: one cell past a whole block of 2048, against a numpy sum
+    n = 2049
+    rng = np.random.default_rng(3)
+    hr, hu, he, hv = rng.uniform(0.5, 2, n), rng.uniform(-1, 1, (n, 3)), rng.uniform(1, 3, n), rng.uniform(0.1, 1, n)
+    tr, tu, te, tv = (torch.tensor(a.reshape(-1), device=dev) for a in (hr, hu, he, hv))
+    want = np.array([(hr * hv).sum()] + [(hr * hu[:, k] * hv).sum() for k in range(3)] + [(he * hv).sum()])
+    wnorm = np.array([(hr * hv).sum()] + [(hr * np.abs(hu[:, k]) * hv).sum() for k in range(3)] + [(he * hv).sum()])
+    for _ in range(2):
+        out.zero_()
+        assert f(n, tr.data_ptr(), tu.data_ptr(), te.data_ptr(), tv.data_ptr(), out.data_ptr(),
+                 ctypes.c_void_p(stream.cuda_stream)) == 0
+        torch.cuda.synchronize(dev)
+        assert (np.abs(out.cpu().numpy() - want) / wnorm).max() <= 1e-13
