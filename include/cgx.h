@@ -172,6 +172,50 @@ int cgx_get_scalars(cgx_solver* s, double* sc);
  * [ncv][nsc] in reference order (unscaled face sums). */
 int cgx_get_rhs_sc(cgx_solver* s, int rk_stage, double* rhs_sc);
 
+/*
+ * Source terms: the counterpart of the user hook addSourceHook(rhs, time,
+ * rk_stage) (IdealGasSolver.hpp:713), which calcRhs calls after calcRhsBase
+ * and calcRhsScalars (IdealGasSolver.hpp:697-705) to add to the stage's rhs.
+ * Two forms, which may be combined; both apply to single-case solvers (not
+ * to batch cases), in every stage of cgx_calc_rhs, cgx_advance_solution and
+ * cgx_step.
+ *
+ * cgx_set_source: evaluated on the device inside the step graph.
+ *   force: per cell f = vol rho (A u + g) (unscaled, like every rhs term)
+ *          added as rhs.rhou += f, rhs.rhoE += f.u.  g alone is a body force
+ *          (gravity), A = -1/tau with g = u_target/tau the relaxation force
+ *          of the reference's example hooks (quiver/charles/charles.sphere.cpp
+ *          :166-173), A alone linear forcing of isotropic turbulence.
+ *   field: optional host array [ncv][5] (reference order and rhs layout),
+ *          copied once and added as is to every stage's rhs.
+ * A NULL source, or one with A = 0, g = 0 and field = NULL, removes it.
+ */
+typedef struct cgx_source {
+  double A;             /* 1/time: coefficient of u in the force */
+  double g[3];          /* acceleration */
+  const double* field;  /* [ncv][5] or NULL */
+} cgx_source;
+int cgx_set_source(cgx_solver* s, const cgx_source* src);
+
+/*
+ * cgx_set_source_hook: a host callback with the reference hook's contract,
+ * for sources that need host code.  In each stage, after the face sums, the
+ * library copies the stage's conserved state to page-locked host memory and
+ * calls
+ *   fn(user, ncv, rho, u, rhoE, rhs, time, rk_stage)
+ * with rho[ncv], u[ncv][3], rhoE[ncv] in reference order, rhs[ncv][5] zero
+ * on entry, time the stage's time (t, t + dt, t + dt/2 for stages 1, 2, 3,
+ * IdealGasSolver.hpp:488,528,569; the caller's time for cgx_calc_rhs), and
+ * rk_stage 1..3.  What fn leaves in rhs is added to the stage's rhs.  fn runs
+ * on a CUDA-owned host thread, as a host node of the step graph: it must not
+ * call CUDA (or this library), and must not block on the thread that called
+ * cgx_step.  The copies cost 80 bytes per cell per stage over PCIe, so this
+ * form is for sources the device form cannot express.  fn = NULL removes it.
+ */
+typedef void (*cgx_source_hook)(void* user, int ncv, const double* rho, const double* u,
+                                const double* rhoE, double* rhs, double time, int rk_stage);
+int cgx_set_source_hook(cgx_solver* s, cgx_source_hook fn, void* user);
+
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */
 int cgx_init_complete(cgx_solver* s);
@@ -218,24 +262,29 @@ int cgx_synchronize(cgx_solver* s);
  * step, FlowSolver.hpp:2596-2605): run nsteps as cgx_step does and return
  * their device time from CUDA events on the solver's stream. */
 int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms);
-/* As cgx_step_timed, with the two face-flux kernels of calcRhs timed inside
- * the steps by CUDA events recorded in the step graph around them:
- * face_ms = {average launch time of the pair (extended faces + compact
- * closures), of the extended-face kernel, of the compact-closure kernel}
- * over the 3 x nsteps stages.  The host waits for each step before the next
+/* As cgx_step_timed, with the face-flux kernels of calcRhs timed inside the
+ * steps by CUDA events recorded in the step graph around them:
+ * face_ms = {average launch time of calcRhs's face kernels (extended faces +
+ * compact closures), of the extended-face kernel (or the one-pass kernel),
+ * of the compact-closure kernel (0 with the one-pass kernel)} over the
+ * 3 x nsteps stages.  The host waits for each step before the next
  * one (the marks are reused), which device_ms includes. */
 int cgx_step_profiled(cgx_solver* s, int nsteps, float* device_ms, double face_ms[3]);
 /* Average device time of one launch of each step kernel, measured with CUDA
- * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs, both
- * kernels), ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is
- * kept), ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/CFL,
- * ms[4] the extended-face flux kernel alone, ms[5] the compact-closure kernel
- * alone.  Overwrites the stage-0 rhs. */
+ * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs, all
+ * its face kernels), ms[1] rk3Step + packed state (3 weights, dt = 0 so the
+ * state is kept), ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/
+ * CFL, ms[4] the extended-face flux kernel alone (the one-pass face kernel
+ * when the tuner picked it), ms[5] the compact-closure kernel alone (0 with
+ * the one-pass kernel).  Overwrites the stage-0 rhs. */
 int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]);
 /* Lanes per cell chosen by the autotuner that cgx_init_complete runs (timed
  * candidates per kernel, cached per mesh-size bucket and precision):
- * out = {face fluxes, compact closures, gradient, once-per-step kernel}. */
-int cgx_get_tuning(const cgx_solver* s, int out[4]);
+ * out = {extended-face kernel, compact closures, gradient, once-per-step
+ * kernel, one-pass face kernel}; out[4] = 0 when the two-kernel face pair
+ * was faster than every one-pass candidate, else the one-pass kernel's lanes
+ * (it then replaces the pair). */
+int cgx_get_tuning(const cgx_solver* s, int out[5]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
 /* Self-test of the device reciprocal that the flux kernels use for the face

@@ -138,7 +138,19 @@ EXPORTS = [
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
+    "cgx_set_source", "cgx_set_source_hook",
 ]
+
+
+class Source(ctypes.Structure):
+    """cgx_source: per-cell force f = vol rho (A u + g) and an optional field."""
+    _fields_ = [("A", ctypes.c_double), ("g", ctypes.c_double * 3), ("field", ctypes.POINTER(ctypes.c_double))]
+
+
+# cgx_source_hook: (user, ncv, rho, u, rhoE, rhs, time, rk_stage)
+SOURCE_HOOK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int)
 
 _LIB = None
 
@@ -182,6 +194,8 @@ def lib():
         "cgx_step_profiled": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), c_dbl_p]),
         "cgx_get_tuning": (ctypes.c_int, [vp, c_int_p]),
         "cgx_set_scalars": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
+        "cgx_set_source": (ctypes.c_int, [vp, ctypes.POINTER(Source)]),
+        "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
         "cgx_get_rhs_sc": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
@@ -291,6 +305,39 @@ class Solver:
         _check(lib().cgx_get_rhs_sc(self.h, int(rk_stage), _dp(out)))
         return out
 
+    # -- source terms (addSourceHook) ----------------------------------------
+    def set_source(self, A=0.0, g=(0.0, 0.0, 0.0), field=None):
+        """Device-side source of every stage: f = vol rho (A u + g) into rhou,
+        f.u into rhoE, plus field[ncv][5] (reference order) if given.  All
+        zero / None removes it."""
+        src = Source()
+        src.A = float(A)
+        src.g = (ctypes.c_double * 3)(*[float(x) for x in g])
+        f = None
+        if field is not None:
+            f = np.ascontiguousarray(field, dtype=np.float64).reshape(self.ncv, 5)
+            src.field = _dp(f)
+        _check(lib().cgx_set_source(self.h, ctypes.byref(src)))
+
+    def set_source_hook(self, fn):
+        """Host hook of every stage with addSourceHook's contract:
+        fn(rho[ncv], u[ncv,3], rhoE[ncv], rhs[ncv,5], time, rk_stage) adds to
+        rhs (zero on entry); the arrays are views of the library's
+        page-locked copies, valid during the call.  fn runs on a CUDA host
+        thread and must not call the library.  None removes it."""
+        if fn is None:
+            _check(lib().cgx_set_source_hook(self.h, SOURCE_HOOK(), None))
+            self._hook = None
+            return
+
+        def thunk(user, ncv, rho, u, rhoE, rhs, time, stage):
+            n = int(ncv)
+            fn(np.ctypeslib.as_array(rho, (n,)), np.ctypeslib.as_array(u, (n, 3)),
+               np.ctypeslib.as_array(rhoE, (n,)), np.ctypeslib.as_array(rhs, (n, 5)), float(time), int(stage))
+        cb = SOURCE_HOOK(thunk)
+        _check(lib().cgx_set_source_hook(self.h, cb, None))
+        self._hook = cb  # the callback must outlive the solver's use of it
+
     # -- reference calls ----------------------------------------------------
     def initComplete(self):
         _check(lib().cgx_init_complete(self.h))
@@ -384,10 +431,12 @@ class Solver:
         return dict(zip(("rhs", "rk_prim", "grad", "step_end", "ext", "comp"), ms.tolist()))
 
     def tuning(self):
-        """Lanes per cell picked by the autotuner: ext, comp, grad, step_end."""
-        t = (ctypes.c_int * 4)()
+        """Lanes per cell picked by the autotuner: ext, comp, grad, step_end,
+        fused (0: the two-kernel face pair runs; else the one-pass face
+        kernel's lanes)."""
+        t = (ctypes.c_int * 5)()
         _check(lib().cgx_get_tuning(self.h, t))
-        return dict(zip(("ext", "comp", "grad", "step_end"), list(t)))
+        return dict(zip(("ext", "comp", "grad", "step_end", "fused"), list(t)))
 
     def set_state_ptr(self, rho_ptr, u_ptr, rhoE_ptr):
         """cgx_set_state from raw host pointers (e.g. pinned buffers)."""

@@ -176,6 +176,26 @@ __device__ __forceinline__ void prefetch_round(const MeshDev& m, const TB* plane
                    __ldg(o + it.cell0 + b));
 }
 
+// The streams of the one-pass face kernel in round `sub` of item `it`: the
+// extended entries' six planes and local indices (threads 0..6) and the
+// compact entries' six planes and compact-union indices (threads 7..13).
+template <class TB>
+__device__ __forceinline__ void prefetch_fused(const MeshDev& m, const TB* en, const TB* qg, const Item& it,
+                                               int sub, int cpr) {
+  const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
+  const int t = threadIdx.x;
+  if (a >= b || t >= 14) return;
+  if (t < 7) {
+    prefetch_entries(en, m.E, m.lidx, __ldg(m.off + it.cell0 + a), __ldg(m.off + it.cell0 + b));
+    return;
+  }
+  const long long q0 = __ldg(m.qoff + it.cell0 + a), q1 = __ldg(m.qoff + it.cell0 + b);
+  if (t < 13)
+    prefetch_l2(qg + (t - 7) * m.Q + q0, (q1 - q0) * static_cast<long long>(sizeof(TB)));
+  else
+    prefetch_l2(m.clidx + q0, (q1 - q0) * 2);
+}
+
 // The streams the once-per-step kernel reads in round `sub` of item `it`:
 // the extended entries' local indices, the compact entries' local indices,
 // unit normals and areas.
@@ -574,6 +594,86 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
   STAGED_ROUNDS_END
   STAGED_LOOP_END
 #undef PF_COMP
+}
+
+// calcRhsBase in one pass over each cell's extended entries (the closures of
+// IdealGasSolverFlux.hpp:93-215 evaluated on the first ncomp entries, which
+// are the cell's compact faces): rhs[i] = -sum over the entries of the skew
+// + symmetric flux plus, on compact entries, the closure.  The item's
+// extended-face union of packed states and its compact-face union of
+// property/gradient records are staged once; rhs is written once.  A group
+// of G lanes per cell (lane l takes entries l, l+G, ...), partial sums
+// combined by the fixed butterfly.  The compact entries all fall in the first
+// sweeps of the lanes, so the closure work is spread over the group.
+template <int G, bool DIRECT>
+__global__ void __launch_bounds__(256, 2) k_rhs_fused(CASE_ARGS, int stage) {
+  extern __shared__ int4 smem[];
+#define PF_FUSED(it, mm, r) prefetch_fused(mm, mm.en, mm.qg, it, r, 256 / G)
+  STAGED_LOOP_BEGIN(PF_FUSED)
+  int4* sV = smem + swz_chunks<4>(it_.ncell + it_.nh);
+  stage_records<4>(smem, s.L, it_, m.hcell + it_.hoff, it_.nh);
+  stage_records<8>(sV, s.V, it_, m.chcell + it_.choff, it_.nch);
+  stage_wait();
+  const long long E = m.E, Q = m.Q;
+  STAGED_ROUNDS_BEGIN(G, PF_FUSED)
+  long long b = 0, e = 0, q0 = 0;
+  int ncomp = 0;
+  LRec Li;
+  if (valid) {
+    b = m.off[i];
+    e = m.off[i + 1];
+    q0 = m.qoff[i];
+    ncomp = int(m.qoff[i + 1] - q0);
+    smem_L(smem, loc_, Li);
+  }
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long k = b + lane; k < e; k += G) {
+    const int jl = __ldg(m.lidx + k);
+    const double* g = m.en + k;
+    const double n[3] = {__ldg(g), __ldg(g + E), __ldg(g + 2 * E)};
+    const double c[3] = {__ldg(g + 3 * E), __ldg(g + 4 * E), __ldg(g + 5 * E)};
+    LRec Lj;
+    smem_L(smem, jl, Lj);
+    double F[5];
+    ext_flux(F, n, c, Li, Lj);
+    const int t = int(k - b);
+    if (t < ncomp) {
+      const long long q = q0 + t;
+      const int jc = __ldg(m.clidx + q);
+      const double* h = m.qg + q;
+      const double un[3] = {__ldg(h), __ldg(h + Q), __ldg(h + 2 * Q)};
+      const double area = __ldg(h + 3 * Q), aod = __ldg(h + 4 * Q), delta = __ldg(h + 5 * Q);
+      VRec Vs;
+      smem_V_sum(sV, loc_, jc, Vs);
+      double uf[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) uf[d] = 0.5 * (Li.u[d] + Lj.u[d]);
+      const double uaub = Li.u[0] * Lj.u[0] + Li.u[1] * Lj.u[1] + Li.u[2] * Lj.u[2];
+      const double h_f = 0.5 * ((Lj.h + Li.h) + uaub);
+      Flux Fc;
+      Fc.rho = 0.0; Fc.ru[0] = Fc.ru[1] = Fc.ru[2] = 0.0; Fc.rE = 0.0;
+      compact_flux_add(Fc, un, area, aod, delta, Li, Lj, Vs, uf, h_f);
+      F[0] += Fc.rho;
+      F[1] += Fc.ru[0];
+      F[2] += Fc.ru[1];
+      F[3] += Fc.ru[2];
+      F[4] += Fc.rE;
+    }
+    if (s.mf) s.mf[k] = F[0];  // mf[ief] of calcRhsBase, for calcRhsScalars
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc[q] -= F[q];
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
+  if (valid) {
+    double* r = s.rhs + size_t(stage) * 5 * m.N;
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+      if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
+  }
+  STAGED_ROUNDS_END
+  STAGED_LOOP_END
+#undef PF_FUSED
 }
 
 // calcRhsScalars (IdealGasSolver.cpp:537-693), cell-centric over each
@@ -1107,6 +1207,51 @@ __global__ void k_diag_out(int N, const int* __restrict__ perm, double* __restri
   }
 }
 
+// addSourceHook's device form (IdealGasSolver.hpp:702,713), added to one
+// stage's rhs after the face sums: f = vol rho (A u + g) into rhs.rhou and
+// f.u into rhs.rhoE (force != 0), then a per-cell field [5][N] in cell
+// order (field != null).
+__global__ void k_source(int N, double* __restrict__ rhs, StateDev s, const double* __restrict__ vol, int force,
+                         double A, double g0, double g1, double g2, const double* __restrict__ field) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const size_t n = size_t(N);
+  if (force) {
+    const double Vr = vol[i] * s.rho[i];
+    const double u0 = s.u0[i], u1 = s.u1[i], u2 = s.u2[i];
+    const double f0 = Vr * (A * u0 + g0), f1 = Vr * (A * u1 + g1), f2 = Vr * (A * u2 + g2);
+    rhs[n + i] += f0;
+    rhs[2 * n + i] += f1;
+    rhs[3 * n + i] += f2;
+    double e = rhs[4 * n + i];
+    e += f0 * u0;
+    e += f1 * u1;
+    e += f2 * u2;
+    rhs[4 * n + i] = e;
+  }
+  if (field)
+    for (int c = 0; c < 5; ++c) rhs[c * n + i] += field[c * n + i];
+}
+
+// a host hook's source [ncv][5] (reference order, in the staging buffer)
+// added to one stage's rhs
+__global__ void k_source_ref(int N, const int* __restrict__ perm, const double* __restrict__ src,
+                             double* __restrict__ rhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int o = perm[i];
+  for (int c = 0; c < 5; ++c) rhs[size_t(c) * N + i] += src[5 * size_t(o) + c];
+}
+
+// [ncv][5] reference order -> [5][N] cell order
+__global__ void k_field_in(int N, const int* __restrict__ perm, const double* __restrict__ src,
+                           double* __restrict__ field) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int o = perm[i];
+  for (int c = 0; c < 5; ++c) field[size_t(c) * N + i] = src[5 * size_t(o) + c];
+}
+
 // Per-entry geometry planes from the per-face records: entry k of the
 // extended CSR reads face fid[k] (bit 31: the cell is the face's second cell,
 // normal negated); compact entry q = qoff[i] + t mirrors extended entry
@@ -1296,8 +1441,36 @@ struct cgx_mesh {
   cgx_mesh_stats stats{};
 };
 
+// Lanes per cell of each face/gradient/step kernel.  g_fused > 0 selects the
+// one-pass face kernel (k_rhs_fused) with that many lanes in place of the
+// k_rhs_ext + k_rhs_comp pair.
 struct Tune {
-  int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4;
+  int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4, g_fused = 0;
+};
+
+// The source terms of a single-case solver (cgx_set_source,
+// cgx_set_source_hook); see enqueue_source.
+struct SourceCfg {
+  bool force = false;
+  double A = 0.0, g[3] = {0.0, 0.0, 0.0};
+  double* field = nullptr;  // device [5][N] in cell order, or null
+  cgx_source_hook fn = nullptr;
+  void* user = nullptr;
+  int N = 0;
+  const int* perm = nullptr;  // device, cell -> reference index
+  double* d_stage = nullptr;  // device staging, >= 5N
+  double* h_state = nullptr;  // page-locked [5N]: rho, u[N][3], rhoE in reference order
+  double* h_src = nullptr;    // page-locked [5N]: the hook's rhs
+  Ctl* h_ctl = nullptr;       // page-locked copy of the control block
+  // what the host node of stage `stage` needs (ctx[3]: an explicit time)
+  struct Hook {
+    SourceCfg* cfg;
+    int stage;
+    bool explicit_time;
+    double time;
+  } ctx[4] = {};
+  bool device_form() const { return force || field; }
+  bool any() const { return force || field || fn; }
 };
 
 // What a launch needs: the case table and work list on the device, the grid,
@@ -1317,6 +1490,7 @@ struct Runner {
   int max_union = 0;            // staging sizes: largest unions over the cases
   int max_cunion = 0;
   std::atomic<long long>* launches = nullptr;
+  SourceCfg* src = nullptr;     // source terms (single-case solvers only)
 };
 
 struct cgx_solver {
@@ -1348,6 +1522,7 @@ struct cgx_solver {
   cudaEvent_t pev[9] = {};
   std::unique_ptr<cgx_staging::Staging> staging;  // for pageable caller arrays, made on first use
   std::atomic<long long> launches{0};
+  SourceCfg src;
 };
 
 namespace {
@@ -1382,6 +1557,11 @@ inline size_t smem_grad(const Runner& R) {
 inline size_t smem_end(const Runner& R) {
   return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_union) + swz_chunks<2>(R.max_cunion)
                                     : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) *
+         16;
+}
+inline size_t smem_fused(const Runner& R) {
+  return size_t(R.prec == CGX_MIXED ? swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)
+                                    : swz_chunks<4>(R.max_union) + swz_chunks<8>(R.max_cunion)) *
          16;
 }
 inline size_t smem_comp(const Runner& R) {
@@ -1424,6 +1604,13 @@ void launch_comp_d(const Runner& R, int st) {
     k_rhs_comp<G, DIRECT><<<grid_staged(R), 256, smem_comp(R), R.stream>>>(RARGS, st);
 }
 template <int G, bool MIX, bool DIRECT>
+void launch_fused_d(const Runner& R, int st) {
+  if (MIX)
+    k_rhs_fused_f<G, DIRECT><<<grid_staged(R), 256, smem_fused(R), R.stream>>>(RARGS, st);
+  else
+    k_rhs_fused<G, DIRECT><<<grid_staged(R), 256, smem_fused(R), R.stream>>>(RARGS, st);
+}
+template <int G, bool MIX, bool DIRECT>
 void launch_end_d(const Runner& R, int mode) {
   if (MIX)
     k_step_end_f<G, DIRECT><<<grid_staged(R), 256, smem_end(R), R.stream>>>(RARGS, mode);
@@ -1446,6 +1633,11 @@ template <int G, bool DIRECT>
 void allow_smem_ext() {
   allow_dyn_smem(k_rhs_ext<G, DIRECT>);
   allow_dyn_smem(k_rhs_ext_f<G, DIRECT>);
+}
+template <int G, bool DIRECT>
+void allow_smem_fused() {
+  allow_dyn_smem(k_rhs_fused<G, DIRECT>);
+  allow_dyn_smem(k_rhs_fused_f<G, DIRECT>);
 }
 template <int G, bool DIRECT>
 void allow_smem_end() {
@@ -1484,6 +1676,12 @@ int prepare_kernels(int device) {
   allow_smem_comp<8, false>();
   allow_smem_comp<16, true>();
   allow_smem_comp<16, false>();
+  allow_smem_fused<8, true>();
+  allow_smem_fused<8, false>();
+  allow_smem_fused<16, true>();
+  allow_smem_fused<16, false>();
+  allow_smem_fused<32, true>();
+  allow_smem_fused<32, false>();
   allow_smem_grad<1, true>();
   allow_smem_grad<1, false>();
   allow_smem_grad<2, true>();
@@ -1520,6 +1718,10 @@ void launch_comp(const Runner& R, int st) {
   R.direct ? launch_comp_d<G, MIX, true>(R, st) : launch_comp_d<G, MIX, false>(R, st);
 }
 template <int G, bool MIX>
+void launch_fused(const Runner& R, int st) {
+  R.direct ? launch_fused_d<G, MIX, true>(R, st) : launch_fused_d<G, MIX, false>(R, st);
+}
+template <int G, bool MIX>
 void launch_end(const Runner& R, int mode) {
   R.direct ? launch_end_d<G, MIX, true>(R, mode) : launch_end_d<G, MIX, false>(R, mode);
 }
@@ -1553,6 +1755,14 @@ void comp_g(const Runner& R, int G, int st) {
   }
 }
 template <bool MIX>
+void fused_g(const Runner& R, int G, int st) {
+  switch (G) {
+    case 8: launch_fused<8, MIX>(R, st); break;
+    case 32: launch_fused<32, MIX>(R, st); break;
+    default: launch_fused<16, MIX>(R, st); break;
+  }
+}
+template <bool MIX>
 void end_g(const Runner& R, int G, int mode) {
   switch (G) {
     case 1: launch_end<1, MIX>(R, mode); break;
@@ -1576,6 +1786,10 @@ int comp_var(const Runner& R, int G, int st) {
   is_mixed(R) ? comp_g<true>(R, G, st) : comp_g<false>(R, G, st);
   return launch_check(R, 1);
 }
+int fused_var(const Runner& R, int G, int st) {
+  is_mixed(R) ? fused_g<true>(R, G, st) : fused_g<false>(R, G, st);
+  return launch_check(R, 1);
+}
 int end_var(const Runner& R, int G, int mode) {
   is_mixed(R) ? end_g<true>(R, G, mode) : end_g<false>(R, G, mode);
   return launch_check(R, 1);
@@ -1596,17 +1810,76 @@ int enqueue_rhs_sc(const Runner& R, int stage0) {
   }
 }
 
-int enqueue_rhs(const Runner& R, int stage0) {
+// the face fluxes of one stage: the one-pass kernel or the two-kernel pair
+int enqueue_faces(const Runner& R, int stage0) {
+  if (R.tune.g_fused > 0) return fused_var(R, R.tune.g_fused, stage0);
   int rc = ext_var(R, R.tune.g_ext, stage0);
   if (rc) return rc;
-  if ((rc = comp_var(R, R.tune.g_comp, stage0))) return rc;
-  if (R.direct && R.dcase.s.nsc > 0) return enqueue_rhs_sc(R, stage0);
+  return comp_var(R, R.tune.g_comp, stage0);
+}
+
+// The host node of a stage with a source hook: zero the hook's rhs, call the
+// hook on the page-locked state copy at the stage's time.
+void CUDART_CB source_hook_thunk(void* p) {
+  const SourceCfg::Hook* h = static_cast<const SourceCfg::Hook*>(p);
+  const SourceCfg* c = h->cfg;
+  const size_t N = size_t(c->N);
+  std::memset(c->h_src, 0, 5 * N * sizeof(double));
+  double t = h->time;
+  if (!h->explicit_time) {
+    // stage times t, t + dt, t + dt/2 (IdealGasSolver.hpp:488,528,569)
+    const Ctl& k = *c->h_ctl;
+    t = k.time + (h->stage == 1 ? k.dt : (h->stage == 2 ? 0.5 * k.dt : 0.0));
+  }
+  c->fn(c->user, c->N, c->h_state, c->h_state + N, c->h_state + 4 * N, c->h_src, t, h->stage + 1);
+}
+
+// addSourceHook (IdealGasSolver.hpp:702): the solver's source terms into the
+// rhs of stage0, after the face sums.  `time`: an explicit stage time for
+// the host hook (cgx_calc_rhs), else the control block's.
+int enqueue_source(const Runner& R, int stage0, const double* time) {
+  SourceCfg* c = R.src;
+  if (!c || !c->any()) return CGX_OK;
+  const StateDev& s = R.dcase.s;
+  const int N = R.dcase.m.N;
+  double* rhs = s.rhs + size_t(stage0) * 5 * N;
+  int rc;
+  if (c->device_form()) {
+    k_source<<<(N + 255) / 256, 256, 0, R.stream>>>(N, rhs, s, R.dcase.m.vol, c->force ? 1 : 0, c->A, c->g[0],
+                                                     c->g[1], c->g[2], c->field);
+    if ((rc = launch_check(R, 1))) return rc;
+  }
+  if (c->fn) {
+    k_state_out<<<(N + 255) / 256, 256, 0, R.stream>>>(N, c->perm, c->d_stage, s);
+    if ((rc = launch_check(R, 1))) return rc;
+    CK(cudaMemcpyAsync(c->h_state, c->d_stage, 5 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
+    CK(cudaMemcpyAsync(c->h_ctl, s.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, R.stream));
+    SourceCfg::Hook* h = &c->ctx[time ? 3 : stage0];
+    h->cfg = c;
+    h->stage = stage0;
+    h->explicit_time = time != nullptr;
+    h->time = time ? *time : 0.0;
+    CK(cudaLaunchHostFunc(R.stream, source_hook_thunk, h));
+    CK(cudaMemcpyAsync(c->d_stage, c->h_src, 5 * size_t(N) * sizeof(double), cudaMemcpyHostToDevice, R.stream));
+    k_source_ref<<<(N + 255) / 256, 256, 0, R.stream>>>(N, c->perm, c->d_stage, rhs);
+    if ((rc = launch_check(R, 1))) return rc;
+  }
   return CGX_OK;
 }
 
-// kernel launches of one RK3 step (three more with transport scalars)
+int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
+  int rc = enqueue_faces(R, stage0);
+  if (rc) return rc;
+  if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, stage0))) return rc;
+  return enqueue_source(R, stage0, time);
+}
+
+// kernel launches of one RK3 step (more with transport scalars and sources);
+// with the one-pass face kernel, one fewer per stage
 inline int launches_per_step(const Runner& R) {
-  return kLaunchesPerStep + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0);
+  int n = kLaunchesPerStep - (R.tune.g_fused > 0 ? 3 : 0) + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0);
+  if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0));
+  return n;
 }
 
 int enqueue_step_end(const Runner& R, int mode) { return end_var(R, R.tune.g_end, mode); }
@@ -1624,21 +1897,24 @@ int tune_bucket(long long ncells, cgx_precision prec) {
 // keep the fastest; results are cached per size bucket (log2 of the cell
 // count) and precision.  All candidates compute the same values (only the
 // order of the per-cell sums changes), and none changes the state.
-// CGX_TUNE="ext,comp,grad,end" (lanes per cell) skips the timing and fixes
-// the lane counts, e.g. to profile one variant.
+// CGX_TUNE="ext,comp,grad,end[,fused]" (lanes per cell; fused 0 = the
+// two-kernel face pair) skips the timing and fixes the lane counts, e.g. to
+// profile one variant.
 bool fixed_tune(Tune* t) {
   const char* e = std::getenv("CGX_TUNE");
   if (!e) return false;
-  int a, b, c, d;
-  if (std::sscanf(e, "%d,%d,%d,%d", &a, &b, &c, &d) != 4) return false;
+  int a, b, c, d, f = 0;
+  const int got = std::sscanf(e, "%d,%d,%d,%d,%d", &a, &b, &c, &d, &f);
+  if (got != 4 && got != 5) return false;
   auto ok = [](int g, std::initializer_list<int> allowed) {
     for (int x : allowed)
       if (g == x) return true;
     return false;
   };
-  if (!ok(a, {4, 8, 16, 32}) || !ok(b, {2, 4, 8, 16}) || !ok(c, {1, 2, 4, 8, 16}) || !ok(d, {1, 4, 8, 16}))
+  if (!ok(a, {4, 8, 16, 32}) || !ok(b, {2, 4, 8, 16}) || !ok(c, {1, 2, 4, 8, 16}) || !ok(d, {1, 4, 8, 16}) ||
+      !ok(f, {0, 8, 16, 32}))
     return false;
-  *t = Tune{a, b, c, d};
+  *t = Tune{a, b, c, d, f};
   return true;
 }
 
@@ -1670,19 +1946,31 @@ int autotune(Runner& R, long long ncells) {
   float bt;
   int rc = CGX_OK;
   const int ext_c[] = {4, 8, 16, 32}, comp_c[] = {2, 4, 8, 16}, grad_c[] = {1, 2, 4, 8, 16},
-            end_c[] = {1, 4, 8, 16};
+            end_c[] = {1, 4, 8, 16}, fused_c[] = {8, 16, 32};
   bt = 1e30f;
+  float pair_ms = 0.f;
   for (int G : ext_c) {
     float ms;
     if ((rc = time_it([&] { return ext_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_ext = G; }
   }
+  pair_ms += bt;
   bt = 1e30f;
   for (int G : comp_c) {
     if (rc) break;
     float ms;
     if ((rc = time_it([&] { return comp_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_comp = G; }
+  }
+  pair_ms += bt;
+  // the one-pass face kernel against the best pair (same stage-0 rhs)
+  best.g_fused = 0;
+  bt = pair_ms;
+  for (int G : fused_c) {
+    if (rc) break;
+    float ms;
+    if ((rc = time_it([&] { return fused_var(R, G, 0); }, &ms))) break;
+    if (ms < bt) { bt = ms; best.g_fused = G; }
   }
   bt = 1e30f;
   for (int G : grad_c) {
@@ -1721,12 +2009,14 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
   for (int st = 0; st < 3; ++st) {
     if (marks) {
       // external records: captured into a graph they become event-record nodes
+      // (with the one-pass face kernel the second interval is empty)
       CK(cudaEventRecordWithFlags(marks[3 * st], R.stream, cudaEventRecordExternal));
-      if ((rc = ext_var(R, R.tune.g_ext, st))) return rc;
+      if ((rc = (R.tune.g_fused > 0 ? fused_var(R, R.tune.g_fused, st) : ext_var(R, R.tune.g_ext, st)))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 1], R.stream, cudaEventRecordExternal));
-      if ((rc = comp_var(R, R.tune.g_comp, st))) return rc;
+      if (R.tune.g_fused == 0 && (rc = comp_var(R, R.tune.g_comp, st))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 2], R.stream, cudaEventRecordExternal));
       if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, st))) return rc;
+      if ((rc = enqueue_source(R, st, nullptr))) return rc;
     } else if ((rc = enqueue_rhs(R, st))) {
       return rc;
     }
@@ -2524,6 +2814,10 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     R.max_union = m->max_union;
     R.max_cunion = m->max_cunion;
     R.launches = &s->launches;
+    s->src.N = int(N);
+    s->src.perm = m->d_perm;
+    s->src.d_stage = s->d_stage;
+    R.src = &s->src;
   }
   s->bytes = bytes;
   Ctl c{};
@@ -2546,6 +2840,9 @@ extern "C" int cgx_solver_destroy(cgx_solver* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   s->staging.reset();
   for (void* q : s->allocs) cudaFree(q);
+  if (s->src.h_state) cudaFreeHost(s->src.h_state);
+  if (s->src.h_src) cudaFreeHost(s->src.h_src);
+  if (s->src.h_ctl) cudaFreeHost(s->src.h_ctl);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return CGX_OK;
@@ -2736,6 +3033,76 @@ extern "C" int cgx_get_rhs_sc(cgx_solver* s, int rk_stage, double* rhs_sc) {
   return CGX_OK;
 }
 
+// a new source configuration changes what the step graphs hold
+static void drop_graphs(cgx_solver* s) {
+  if (s->pgraph) {
+    cudaGraphExecDestroy(s->pgraph);
+    s->pgraph = nullptr;
+  }
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+}
+
+extern "C" int cgx_set_source(cgx_solver* s, const cgx_source* src) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_source: null solver");
+  CK(cudaSetDevice(s->mesh->device));
+  CK(cudaStreamSynchronize(s->stream));
+  SourceCfg& c = s->src;
+  const cgx_source none{};
+  const cgx_source& q = src ? *src : none;
+  if (!std::isfinite(q.A) || !std::isfinite(q.g[0]) || !std::isfinite(q.g[1]) || !std::isfinite(q.g[2]))
+    return fail(CGX_E_ARG, "cgx_set_source: A and g must be finite");
+  const size_t N = size_t(s->mesh->N);
+  if (q.field) {
+    if (!c.field) {
+      int rc = dalloc(&c.field, 5 * N, &s->bytes);
+      if (rc) return rc;
+      s->allocs.push_back(c.field);
+    }
+    int rc = host_to_device(s, s->d_stage, q.field, 5 * N * sizeof(double));
+    if (rc) return rc;
+    k_field_in<<<int((N + 255) / 256), 256, 0, s->stream>>>(int(N), s->mesh->d_perm, s->d_stage, c.field);
+    if ((rc = launch_check(s->run, 1))) return rc;
+  } else if (c.field) {
+    cudaFree(c.field);
+    s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), static_cast<void*>(c.field)), s->allocs.end());
+    c.field = nullptr;
+  }
+  c.A = q.A;
+  for (int k = 0; k < 3; ++k) c.g[k] = q.g[k];
+  c.force = q.A != 0.0 || q.g[0] != 0.0 || q.g[1] != 0.0 || q.g[2] != 0.0;
+  drop_graphs(s);
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
+extern "C" int cgx_set_source_hook(cgx_solver* s, cgx_source_hook fn, void* user) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_source_hook: null solver");
+  CK(cudaSetDevice(s->mesh->device));
+  CK(cudaStreamSynchronize(s->stream));
+  SourceCfg& c = s->src;
+  if (fn && !c.h_state) {
+    const size_t bytes = 5 * size_t(s->mesh->N) * sizeof(double);
+    cudaError_t e = cudaMallocHost(&c.h_state, bytes);
+    if (e == cudaSuccess) e = cudaMallocHost(&c.h_src, bytes);
+    if (e == cudaSuccess) e = cudaMallocHost(&c.h_ctl, sizeof(Ctl));
+    if (e != cudaSuccess) {
+      if (c.h_state) cudaFreeHost(c.h_state);
+      if (c.h_src) cudaFreeHost(c.h_src);
+      c.h_state = c.h_src = nullptr;
+      c.h_ctl = nullptr;
+      return fail(e == cudaErrorMemoryAllocation ? CGX_E_OOM : CGX_E_CUDA,
+                  std::string("cgx_set_source_hook: page-locked buffers: ") + cudaGetErrorString(e));
+    }
+  }
+  c.fn = fn;
+  c.user = user;
+  drop_graphs(s);
+  return CGX_OK;
+}
+
 extern "C" int cgx_update_primitive(cgx_solver* s) {
   if (!s) return fail(CGX_E_ARG, "null solver");
   if (!s->state_set) return fail(CGX_E_STATE, "state not set");
@@ -2772,12 +3139,11 @@ extern "C" int cgx_init_complete(cgx_solver* s) {
 }
 
 extern "C" int cgx_calc_rhs(cgx_solver* s, double* rhs_out, double time, int rk_stage) {
-  (void)time;
   if (!s) return fail(CGX_E_ARG, "null solver");
   if (rk_stage < 1 || rk_stage > 3) return fail(CGX_E_ARG, "rk_stage must be 1..3");
   if (!s->inited) return fail(CGX_E_STATE, "cgx_init_complete not called");
   CK(cudaSetDevice(s->mesh->device));
-  int rc = enqueue_rhs(s->run, rk_stage - 1);
+  int rc = enqueue_rhs(s->run, rk_stage - 1, &time);
   if (rc) return rc;
   if (rhs_out) {
     const int N = s->mesh->N;
@@ -3007,8 +3373,11 @@ extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]) {
       else if (which == 1) rc = enqueue_prim(s->run, 3, kRkW[2], 0.0, true);
       else if (which == 2) rc = enqueue_grad(s->run);
       else if (which == 3) rc = enqueue_step_end(s->run, 0);
-      else if (which == 4) rc = ext_var(s->run, s->run.tune.g_ext, 0);
-      else rc = comp_var(s->run, s->run.tune.g_comp, 0);
+      else if (which == 4)
+        rc = s->run.tune.g_fused > 0 ? fused_var(s->run, s->run.tune.g_fused, 0)
+                                     : ext_var(s->run, s->run.tune.g_ext, 0);
+      else if (s->run.tune.g_fused == 0)
+        rc = comp_var(s->run, s->run.tune.g_comp, 0);
     }
     CK(cudaEventRecord(e1, s->stream));
     CK(cudaEventSynchronize(e1));
@@ -3088,12 +3457,13 @@ extern "C" int cgx_synchronize(cgx_solver* s) {
   return CGX_OK;
 }
 
-extern "C" int cgx_get_tuning(const cgx_solver* s, int out[4]) {
+extern "C" int cgx_get_tuning(const cgx_solver* s, int out[5]) {
   if (!s || !out) return fail(CGX_E_ARG, "null argument");
   out[0] = s->run.tune.g_ext;
   out[1] = s->run.tune.g_comp;
   out[2] = s->run.tune.g_grad;
   out[3] = s->run.tune.g_end;
+  out[4] = s->run.tune.g_fused;
   return CGX_OK;
 }
 
@@ -3382,7 +3752,7 @@ extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
       if ((rc = autotune(b->run, b->active_cells))) return rc;
       const Tune& t = b->run.tune;
       if (b->tuned_bucket < 0 || t.g_ext != old.g_ext || t.g_comp != old.g_comp || t.g_grad != old.g_grad ||
-          t.g_end != old.g_end) {
+          t.g_end != old.g_end || t.g_fused != old.g_fused) {
         if ((rc = enqueue_grad(b->run))) return rc;  // dudx summed in the new grouping
         batch_free_graph(b);
       }
@@ -3408,7 +3778,7 @@ extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
     run = std::max(run, 1);
     for (int k = 0; k < run; ++k) {
       CK(cudaGraphLaunch(b->graph, b->stream));
-      b->launches += kLaunchesPerStep;
+      b->launches += launches_per_step(b->run);
     }
     left -= run;
     for (BatchCase& c : b->slots) {

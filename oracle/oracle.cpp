@@ -125,6 +125,9 @@ struct orc_solver {
   int nsc = 0;
   std::vector<double> sc, rhs_sc[3], scale_sc;
   bool want_scale = false;
+  // source terms (the addSourceHook of a subclass)
+  double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
+  std::vector<double> src_field;  // [ncv][5] or empty
   // time
   int step = 0;
   double time = 0.0, dt = 0.0;
@@ -400,18 +403,43 @@ void rhs_sc_part(orc_solver* o, int ip, double* rhs_sc) {
 
 // calcRhs (IdealGasSolver.hpp:697-705): calcRhsBase, then calcRhsScalars
 // into rhs_sc (when the solver carries transport scalars)
+// addSourceHook of a subclass that adds the force f = vol rho (A u + g)
+// per cell, in the form of quiver/charles/charles.sphere.cpp:166-173
+// (rhs.rhou += f; rhs.rhoE += f.u, component by component), then a fixed
+// per-cell field
+void add_source(orc_solver* o, IdealGasRhs* rhs) {
+  const bool force = o->src_A != 0.0 || o->src_g[0] != 0.0 || o->src_g[1] != 0.0 || o->src_g[2] != 0.0;
+  if (force)
+    for (int icv = 0; icv < o->ncv; ++icv) {
+      const double* uu = &o->u[3 * size_t(icv)];
+      for (int i = 0; i < 3; ++i) {
+        const double fi = o->vol_cv[icv] * o->rho[icv] * (o->src_A * uu[i] + o->src_g[i]);
+        rhs[icv].rhou[i] += fi;
+        rhs[icv].rhoE += fi * uu[i];
+      }
+    }
+  if (!o->src_field.empty())
+    for (int icv = 0; icv < o->ncv; ++icv) {
+      const double* f = &o->src_field[5 * size_t(icv)];
+      rhs[icv].rho += f[0];
+      for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] += f[1 + i];
+      rhs[icv].rhoE += f[4];
+    }
+}
+
 void calc_rhs(orc_solver* o, IdealGasRhs* rhs, double* rhs_sc = nullptr) {
   const bool sc = o->nsc > 0 && rhs_sc;
   if (o->nparts == 1) {
     rhs_part(o, 0, rhs);
     if (sc) rhs_sc_part(o, 0, rhs_sc);
-    return;
-  }
+  } else {
 #pragma omp parallel for schedule(static, 1) num_threads(o->nparts)
-  for (int ip = 0; ip < o->nparts; ++ip) {
-    rhs_part(o, ip, rhs);
-    if (sc) rhs_sc_part(o, ip, rhs_sc);
+    for (int ip = 0; ip < o->nparts; ++ip) {
+      rhs_part(o, ip, rhs);
+      if (sc) rhs_sc_part(o, ip, rhs_sc);
+    }
   }
+  add_source(o, rhs);
 }
 
 // computeSgsVreman (IdealGasSolverSgs.cpp:207-296) over [b, e)
@@ -956,6 +984,15 @@ extern "C" void orc_get_aux(const orc_solver* o, double* aux) {
     a[4] = A.symh_fax;
     a[5] = A.symp_fax;
   }
+}
+
+extern "C" void orc_set_source(orc_solver* o, double A, const double g[3], const double* field) {
+  o->src_A = A;
+  for (int i = 0; i < 3; ++i) o->src_g[i] = g ? g[i] : 0.0;
+  if (field)
+    o->src_field.assign(field, field + 5 * size_t(o->ncv));
+  else
+    o->src_field.clear();
 }
 
 extern "C" void orc_poison(orc_solver* o, int icv) {

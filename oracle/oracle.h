@@ -62,6 +62,13 @@ void orc_get_time(const orc_solver* o, double* time, double* dt, int* step);
 void orc_get_primitive(const orc_solver* o, double* p, double* T, double* sos);
 void orc_get_grad(const orc_solver* o, double* dudx);
 void orc_get_aux(const orc_solver* o, double* aux);
+/* Source terms added by calc_rhs after the face sums, where the reference's
+ * calcRhs calls addSourceHook (IdealGasSolver.hpp:697-705): per cell
+ * f = vol rho (A u + g) into rhs.rhou and f.u into rhs.rhoE (the body and
+ * relaxation forces of the reference's example hooks,
+ * quiver/charles/charles.sphere.cpp:166-173), plus field[ncv][5] if non-NULL.
+ * A = 0, g = 0 and field = NULL remove them. */
+void orc_set_source(orc_solver* o, double A, const double g[3], const double* field);
 /* write a NaN into rho[icv] (host-side fault injection for the NaN path) */
 void orc_poison(orc_solver* o, int icv);
 

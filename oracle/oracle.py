@@ -56,6 +56,7 @@ def _load(path):
         "orc_get_grad": (None, [vp, c_dbl_p]),
         "orc_get_aux": (None, [vp, c_dbl_p]),
         "orc_poison": (None, [vp, ctypes.c_int]),
+        "orc_set_source": (None, [vp, ctypes.c_double, c_dbl_p, c_dbl_p]),
         "orc_uses_reference_flux": (ctypes.c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -178,6 +179,13 @@ class Oracle:
         a = np.empty((self.ncv, 6))
         self.L.orc_get_aux(self.h, _dp(a))
         return a
+
+    def set_source(self, A=0.0, g=(0.0, 0.0, 0.0), field=None):
+        """Source terms after the face sums (a subclass's addSourceHook):
+        f = vol rho (A u + g) into rhou, f.u into rhoE, plus field[ncv][5]."""
+        gg = np.ascontiguousarray(g, dtype=np.float64)
+        f = None if field is None else np.ascontiguousarray(field, dtype=np.float64).reshape(self.ncv, 5)
+        self.L.orc_set_source(self.h, float(A), _dp(gg), _dp(f))
 
     def poison(self, icv):
         self.L.orc_poison(self.h, int(icv))

@@ -1,7 +1,8 @@
 """Every lane-count variant the autotuner can choose gives calcRhs within
 the face-sum tolerance of the oracle, so the variant picked on any mesh is
 a correct one.  Lane counts per kernel are forced through CGX_TUNE
-(extended faces, compact closures, gradient, once-per-step)."""
+(extended faces, compact closures, gradient, once-per-step, one-pass face
+kernel; 0 for the last selects the two-kernel face pair)."""
 import os
 
 import numpy as np
@@ -13,7 +14,8 @@ from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-TUNES = [(4, 16, 1, 1), (8, 8, 2, 4), (16, 4, 8, 8), (32, 2, 16, 16)]
+TUNES = [(4, 16, 1, 1, 0), (8, 8, 2, 4, 0), (16, 4, 8, 8, 0), (32, 2, 16, 16, 0),
+         (16, 2, 4, 4, 8), (16, 2, 4, 4, 16), (16, 2, 4, 4, 32)]
 
 
 @pytest.fixture(scope="module")
@@ -28,12 +30,12 @@ def case(built):
     return m, prm, (rho, u, p), cgx.Mesh(m, device=0), ref, scale
 
 
-@pytest.mark.parametrize("tune", TUNES, ids=lambda t: "%d-%d-%d-%d" % t)
+@pytest.mark.parametrize("tune", TUNES, ids=lambda t: "%d-%d-%d-%d-%d" % t)
 @pytest.mark.parametrize("prec", [cgx.CGX_FP64, cgx.CGX_MIXED], ids=["fp64", "mixed"])
 def test_lane_variant(case, tune, prec):
     m, prm, (rho, u, p), gm, ref, scale = case
     old = os.environ.get("CGX_TUNE")
-    os.environ["CGX_TUNE"] = "%d,%d,%d,%d" % tune
+    os.environ["CGX_TUNE"] = "%d,%d,%d,%d,%d" % tune
     try:
         s = cgx.Solver(gm, prm, prec)
         s.set_state_primitive(rho, u, p)
@@ -44,10 +46,17 @@ def test_lane_variant(case, tune, prec):
         else:
             os.environ["CGX_TUNE"] = old
     t = s.tuning()
-    assert (t["ext"], t["comp"], t["grad"], t["step_end"]) == tune
+    assert (t["ext"], t["comp"], t["grad"], t["step_end"], t["fused"]) == tune
     r = s.calcRhs(2)
     err = (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max()
     tol = 1e-12 if prec == cgx.CGX_FP64 else 2e-5  # FP32 flux arithmetic in the mixed form
     assert err <= tol, err
+    # the mass flux each variant leaves for the scalars: a unit scalar's
+    # rhs_sc is the continuity rhs (-sum of the entries' mass fluxes)
+    s.set_scalars(np.ones((m.ncv, 1)))
+    r = s.calcRhs(2)
+    rsc = s.rhs_sc(2)[:, 0]
+    assert (np.abs(rsc - r[:, 0]) / np.maximum(np.abs(ref[:, 0]), scale[:, 0])).max() <= 1e-12
+    s.set_scalars(np.zeros((m.ncv, 0)))
     assert s.step(3) == 0
     s.close()
