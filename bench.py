@@ -424,7 +424,11 @@ def run_cgx(args):
     for k in list(solvers):
         solvers[k].close()
     solvers = {}
+    if rank == 0 and world == 1 and args.accuracy_steps > 0:
+        out["accuracy"] = accuracy_block(gm, args.n, vol_cv, (rho, u, p), args.accuracy_steps)
     gm.close()
+    if rank == 0 and world == 1 and args.batch_steps > 0:
+        out["batch64"] = batch64_block(args.batch_steps)
     if rank == 0 and world == 1 and not args.no_served:
         out["served"] = served_stream(nreq=args.served_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -435,7 +439,7 @@ def run_cgx(args):
     return 0
 
 
-def _errors(m, vol, ref, got, init):
+def _errors(vol, ref, got, init):
     """Velocity, pressure (fluctuation) and kinetic-energy errors of `got`
     against `ref`: (rho, u, p) triples on the same mesh."""
     r64, u64, p64 = ref
@@ -454,26 +458,25 @@ def _errors(m, vol, ref, got, init):
             "ke_decay_rel_err": float(abs(ke32 - ke64) / max(abs(ke0 - ke64), 1e-300))}
 
 
-def run_accuracy(args):
-    """The mixed-precision form against the FP64 path on the jittered n^3 mesh
-    (200^3 = 8M cells by default): the Ma 0.1 Taylor-Green state and the
-    Mt 0.3 random-solenoidal state, each advanced `--accuracy-steps` RK3 steps
-    (500 by default) at CFL 0.8 by both precisions from the same initial state.
-    Prints one JSON line with the L2/L-inf errors of velocity and pressure and
-    the kinetic-energy (decay) error of the mixed form."""
+KE_DECAY_BOUND = 1e-5  # the mixed form's kinetic-energy (decay) error bound against FP64
+
+
+def accuracy_block(gm, n, vol, tgv, K):
+    """The mixed-precision form against the FP64 path on the device mesh `gm`
+    of the jittered n^3 lattice: the Ma 0.1 Taylor-Green state `tgv` = (rho,
+    u, p) and the Mt 0.3 random-solenoidal state, each advanced K RK3 steps
+    at CFL 0.8 by both precisions from the same initial state.  Returns the
+    L2/L-inf errors of velocity and pressure and the kinetic-energy (decay)
+    error of the mixed form, with the step times."""
     from nextgen_b200 import cases, cgx
-    from nextgen_b200.meshgen import PeriodicBoxMesh
-    n, K = args.n, args.accuracy_steps
-    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED, nthreads=os.cpu_count() or 1)
-    gm = cgx.Mesh(m)
-    vol = np.array(m.vol_cv)
-    out = {"metric": "mixed-precision error vs FP64 after %d RK3 steps" % K, "cells": m.ncv,
-           "config": {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3, CFL 0.8, Vreman" % n},
-           "data": "synthetic", "cases": {}}
+    out = {"metric": "mixed-precision error vs FP64 after %d RK3 steps" % K, "steps": K,
+           "cells": gm.ncv, "ke_decay_rel_err_bound": KE_DECAY_BOUND,
+           "workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3, CFL 0.8, Vreman" % n, "cases": {}}
+    ok = True
     for kind in ("tgv", "solenoidal"):
         if kind == "tgv":
             prm = cases.tgv_params()
-            rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
+            rho, u, p = tgv
         else:
             prm = cases.hit_params(Mt=0.3)
             rho, u, p = cases.hit_state(n, prm, Mt=0.3, k0=4.0, seed=4321)
@@ -487,10 +490,27 @@ def run_accuracy(args):
             r1, u1, _ = s.get_state()
             res[name] = (r1, u1, s.primitive()[0])
             s.close()
-        e = _errors(m, vol, res["fp64"], res["mixed"], (rho, u))
+        e = _errors(vol, res["fp64"], res["mixed"], (rho, u))
         e.update({"fp64_ms_per_step": ms["fp64"] / K, "mixed_ms_per_step": ms["mixed"] / K,
                   "speedup": ms["fp64"] / ms["mixed"]})
+        ok = ok and e["ke_rel"] <= KE_DECAY_BOUND and e["ke_decay_rel_err"] <= KE_DECAY_BOUND
         out["cases"][kind] = e
+    out["within_bound"] = bool(ok)
+    return out
+
+
+def run_accuracy(args):
+    """accuracy_block on the jittered n^3 mesh (200^3 = 8M cells by default)
+    for `--accuracy-steps` steps (500 by default), as one JSON line."""
+    from nextgen_b200 import cases, cgx
+    from nextgen_b200.meshgen import PeriodicBoxMesh
+    n, K = args.n, args.accuracy_steps
+    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED, nthreads=os.cpu_count() or 1)
+    gm = cgx.Mesh(m)
+    vol = np.array(m.vol_cv)
+    prm = cases.tgv_params()
+    out = accuracy_block(gm, n, vol, cases.tgv_state(m.x_cv[: m.ncv], prm), K)
+    out.update({"config": {"workload": out["workload"]}, "data": "synthetic"})
     print(json.dumps(out), flush=True)
     return 0
 
@@ -541,13 +561,13 @@ def run_validate(args):
     return 0
 
 
-def run_batch64(args, seed=64):
+def batch64_block(K, seed=64):
     """64 independent Taylor-Green cases of uneven size in one batch: edges
     log-uniform in [8, 64] (512 to 262,144 cells, +/-0.25h jitter), Mach
-    uniform in [0.1, 0.5], Re uniform in [400, 3200], advanced together for
-    `--batch-steps` steps (300 by default) in FP64 and in mixed precision; the
-    same cases one at a time on the plain FP64 path for comparison.  Prints one
-    JSON line with the cell-steps/s of each."""
+    uniform in [0.1, 0.5], Re uniform in [400, 3200], advanced together for K
+    steps in FP64 and in mixed precision; the same cases one at a time on the
+    plain FP64 path and at their own precision for comparison.  Returns the
+    cell-steps/s of each."""
     from nextgen_b200 import cases, cgx
     rng = np.random.default_rng(seed)
     edges = [int(round(np.exp(x))) for x in rng.uniform(np.log(8), np.log(64), size=64)]
@@ -562,7 +582,6 @@ def run_batch64(args, seed=64):
         prm = cases.tgv_params(Ma=float(rng.uniform(0.1, 0.5)), Re=float(rng.uniform(400, 3200)))
         prm.check_interval = 50
         cs.append((gm, prm) + tuple(cases.tgv_state(hm.x_cv[: hm.ncv], prm)))
-    K = args.batch_steps
     total = float(sum(gm.ncv for gm, *_ in cs)) * K
     out = {"metric": "batched uneven instances: cell-steps/s", "unit": UNIT, "cases": len(cs),
            "cells": int(sum(gm.ncv for gm, *_ in cs)), "steps": K, "edges": edges, "data": "synthetic"}
@@ -576,18 +595,34 @@ def run_batch64(args, seed=64):
         el = time.perf_counter() - t0
         out["batch_" + name] = {"cell_steps_per_s": total / el, "seconds": el}
         b.close()
-    t0 = time.perf_counter()
-    for gm, prm, rho, u, p in cs:
-        s = cgx.Solver(gm, prm)
-        s.set_state_primitive(rho, u, p)
-        s.initComplete()
-        s.step(K)
-        s.synchronize()
-        s.close()
-    el = time.perf_counter() - t0
-    out["sequential_plain_fp64"] = {"cell_steps_per_s": total / el, "seconds": el}
-    out["speedup_batch_fp64_vs_sequential"] = out["batch_fp64"]["cell_steps_per_s"] / (total / el)
-    out["speedup_batch_mixed_vs_sequential"] = out["batch_mixed"]["cell_steps_per_s"] / (total / el)
+    for name, prec in (("fp64", cgx.CGX_FP64), ("mixed", cgx.CGX_MIXED)):
+        t0 = time.perf_counter()
+        for gm, prm, rho, u, p in cs:
+            s = cgx.Solver(gm, prm, prec)
+            s.set_state_primitive(rho, u, p)
+            s.initComplete()
+            s.step(K)
+            s.synchronize()
+            s.close()
+        el = time.perf_counter() - t0
+        out["sequential_" + name] = {"cell_steps_per_s": total / el, "seconds": el}
+    seq64 = out["sequential_fp64"]["cell_steps_per_s"]
+    out["speedup_batch_fp64_vs_sequential_fp64"] = out["batch_fp64"]["cell_steps_per_s"] / seq64
+    out["speedup_batch_mixed_vs_sequential_fp64"] = out["batch_mixed"]["cell_steps_per_s"] / seq64
+    out["speedup_batch_mixed_vs_sequential_mixed"] = (out["batch_mixed"]["cell_steps_per_s"] /
+                                                      out["sequential_mixed"]["cell_steps_per_s"])
+    out["how"] = ("batch: host wall clock around K steps of one cgx_batch (graph replays) after a 2-step "
+                  "warm-up; sequential: each case alone (solver create, initComplete, K steps) one after another")
+    for hm, gm in meshes.values():
+        gm.close()
+        hm.close()
+    return out
+
+
+def run_batch64(args):
+    """batch64_block for `--batch-steps` steps (300 by default), as one JSON
+    line."""
+    out = batch64_block(args.batch_steps)
     print(json.dumps(out), flush=True)
     return 0
 
@@ -690,10 +725,12 @@ def main():
     ap.add_argument("--served-requests", type=int, default=16)
     ap.add_argument("--accuracy", action="store_true",
                     help="instead of the throughput bench: mixed vs FP64 errors (TGV and solenoidal)")
-    ap.add_argument("--accuracy-steps", type=int, default=500)
+    ap.add_argument("--accuracy-steps", type=int, default=500,
+                    help="steps of the mixed-vs-FP64 accuracy block of the default run (0: skip it)")
     ap.add_argument("--batch64", action="store_true",
                     help="instead of the throughput bench: 64 uneven cases in one batch vs one at a time")
-    ap.add_argument("--batch-steps", type=int, default=300)
+    ap.add_argument("--batch-steps", type=int, default=300,
+                    help="steps of the 64-case batch block of the default run (0: skip it)")
     ap.add_argument("--validate", action="store_true",
                     help="instead of the throughput bench: FP64 GPU vs CPU oracle over many steps")
     ap.add_argument("--validate-n", type=int, default=128)

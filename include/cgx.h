@@ -121,6 +121,17 @@ typedef struct cgx_mesh_desc {
   const double* sa_to_vol_ratio;    /* [ncv] */
   const int*    icv_owner_g;        /* [ncv_g2-ncv] */
   const double* x_cv;               /* [ncv][3] or NULL */
+  /* Boundary faces (nbf = 0 for a periodic box), as StaticSolver holds them
+   * (cvobf, n_bf outward, area_over_delta_bf), with each face's boundary
+   * zone in [0, nbf_zones); every zone needs a boundary condition
+   * (cgx_set_bc) before cgx_init_complete.  The gradient coefficients given
+   * above must include the faces' Gij_bf term, as calcCvGradCoeff forms them
+   * (StaticSolver.cpp:5642-5650). */
+  int nbf, nbf_zones;
+  const int*    cvobf;              /* [nbf] owned cell */
+  const double* n_bf;               /* [nbf][3] */
+  const double* area_over_delta_bf; /* [nbf] */
+  const int*    zone_bf;            /* [nbf] */
 } cgx_mesh_desc;
 
 typedef struct cgx_mesh cgx_mesh;
@@ -215,6 +226,25 @@ int cgx_set_source(cgx_solver* s, const cgx_source* src);
 typedef void (*cgx_source_hook)(void* user, int ncv, const double* rho, const double* u,
                                 const double* rhoE, double* rhs, double time, int rk_stage);
 int cgx_set_source_hook(cgx_solver* s, cgx_source_hook fn, void* user);
+
+/*
+ * Boundary conditions of a mesh's boundary zones (registerBoundaryConditions,
+ * IdealGasSolver.hpp:170-231).  Their fluxes enter each stage's rhs as
+ * addBoundaryFlux does (IdealGasSolver.cpp:261-262) and their faces enter
+ * calcCfl (IdealGasSolver.cpp:1068-1074):
+ *   CGX_BC_SLIP            SLIP / SYMMETRY: rhs.rhou -= p n_bf
+ *                          (SlipWallBc::addBoundaryFlux, IdealGasSolverBcs.cpp:14-23)
+ *   CGX_BC_WALL_ADIABATIC  WALL_ADIABATIC [TRANSLATE u_wall]: tau = mu_lam
+ *                          area_over_delta_bf (u - u_wall), rhs.rhou -= p n_bf +
+ *                          tau, rhs.rhoE -= u_wall.tau
+ *                          (WallAdiabatic::addBoundaryFlux, IdealGasSolverBcs.cpp:25-48;
+ *                          u_wall = 0 by default, IdealGasSolverBcs.cpp:450-475)
+ * u_wall may be NULL (zero).  Single-case solvers only: a batch refuses
+ * meshes with boundary faces.
+ */
+#define CGX_BC_SLIP            1
+#define CGX_BC_WALL_ADIABATIC  2
+int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */

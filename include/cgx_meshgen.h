@@ -74,6 +74,19 @@ typedef struct cgx_meshgen_out {
   /* ghosts */
   int     *icv_owner_g;            /* [ncv_g2-ncv] */
   int    (*shift_g)[3];            /* [ncv_g2-ncv] periodic shift, box lengths */
+  /* boundary faces (a channel; nbf = 0 and NULL arrays for a periodic box),
+   * ordered by cell, a cell's faces by zone */
+  int nbf;
+  int nbf_zones;                   /* zone 0: the wall y = 0, zone 1: y = Ly */
+  int     *cvobf;                  /* [nbf] owning cell */
+  int     *zone_bf;                /* [nbf] */
+  double (*n_bf)[3];               /* [nbf][3] outward area vector */
+  double (*x_bf)[3];               /* [nbf][3] centroid */
+  double  *area_bf;                /* [nbf] |n_bf| */
+  double  *area_over_delta_bf;     /* [nbf] src/core/common/StripedMesh.hpp:2781-2792 */
+  double (*Gij_bf)[3][3];          /* [nbf] Gij = -dx[j] n_bf[i], dx = x_bf - x_vv
+                                      (StripedMesh.hpp:2794), the boundary term of
+                                      calcCvGradCoeff (StaticSolver.cpp:5642-5650) */
 } cgx_meshgen_out;
 
 /*
@@ -100,6 +113,24 @@ int cgx_meshgen_periodic_box_compact(int nx, int ny, int nz,
                                      double Lx, double Ly, double Lz,
                                      double jitter, unsigned long long seed,
                                      int nthreads, cgx_meshgen_out** out);
+
+/*
+ * A channel: the same Voronoi construction periodic in x and z, bounded by
+ * walls at y = 0 (boundary zone 0) and y = Ly (zone 1).  Each cell next to a
+ * wall is clipped by the wall plane; the clipped polygon is its boundary
+ * face.  The gradient coefficients include the boundary faces' Gij term.
+ */
+int cgx_meshgen_channel(int nx, int ny, int nz,
+                        double Lx, double Ly, double Lz,
+                        double jitter, unsigned long long seed,
+                        double interp_factor, double sigma_thresh,
+                        int nthreads, cgx_meshgen_out** out);
+/* the mesher's part of the channel (boundary faces included), as
+ * cgx_meshgen_periodic_box_compact */
+int cgx_meshgen_channel_compact(int nx, int ny, int nz,
+                                double Lx, double Ly, double Lz,
+                                double jitter, unsigned long long seed,
+                                int nthreads, cgx_meshgen_out** out);
 
 void cgx_meshgen_free(cgx_meshgen_out* m);
 

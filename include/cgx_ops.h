@@ -48,6 +48,18 @@ typedef struct cgx_compact_desc {
   const double* x_vv;       /* [ncv][3] Voronoi seeds, passed through, or NULL */
   const int*    icv_owner_g;/* [ncv_g-ncv] owner of each level-1 ghost */
   const int*    shift_g;    /* [ncv_g-ncv][3] its periodic shift, in box lengths, |s| <= 1 */
+  /* boundary faces (0 for a triply periodic box).  Gij_bf enters the
+   * gradient coefficients (calcCvGradCoeff's boundary term,
+   * StaticSolver.cpp:5642-5650), each cell's faces in increasing index; the
+   * rest is passed through to the output. */
+  int nbf, nbf_zones;
+  const int*    cvobf;              /* [nbf] */
+  const int*    zone_bf;            /* [nbf] or NULL */
+  const double* n_bf;               /* [nbf][3] or NULL */
+  const double* x_bf;               /* [nbf][3] or NULL */
+  const double* area_bf;            /* [nbf] or NULL */
+  const double* area_over_delta_bf; /* [nbf] or NULL */
+  const double* Gij_bf;             /* [nbf][3][3] */
 } cgx_compact_desc;
 
 /*

@@ -88,6 +88,8 @@ class MeshDesc(ctypes.Structure):
         ("cvocv_grad_coeff", c_dbl_p), ("cvoef", c_int_p), ("n_ef", c_dbl_p), ("c_ef", c_dbl_p),
         ("dcmag_hat_cv", c_dbl_p), ("sa_to_vol_ratio", c_dbl_p), ("icv_owner_g", c_int_p),
         ("x_cv", c_dbl_p),
+        ("nbf", ctypes.c_int), ("nbf_zones", ctypes.c_int), ("cvobf", c_int_p), ("n_bf", c_dbl_p),
+        ("area_over_delta_bf", c_dbl_p), ("zone_bf", c_int_p),
     ]
 
 
@@ -120,6 +122,13 @@ def mesh_desc(mesh, with_x=True):
     d.sa_to_vol_ratio = _p(arr(mesh.sa_to_vol_ratio, np.float64), ctypes.c_double)
     d.icv_owner_g = _p(arr(mesh.icv_owner_g, np.int32), ctypes.c_int)
     d.x_cv = _p(arr(mesh.x_cv[: mesh.ncv], np.float64), ctypes.c_double) if with_x else None
+    nbf = int(getattr(mesh, "nbf", 0) or 0)
+    if nbf > 0:
+        d.nbf, d.nbf_zones = nbf, int(mesh.nbf_zones)
+        d.cvobf = _p(arr(mesh.cvobf, np.int32), ctypes.c_int)
+        d.n_bf = _p(arr(mesh.n_bf, np.float64), ctypes.c_double)
+        d.area_over_delta_bf = _p(arr(mesh.area_over_delta_bf, np.float64), ctypes.c_double)
+        d.zone_bf = _p(arr(mesh.zone_bf, np.int32), ctypes.c_int)
     d._keep = keep
     return d
 
@@ -138,8 +147,11 @@ EXPORTS = [
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
-    "cgx_set_source", "cgx_set_source_hook",
+    "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc",
 ]
+
+CGX_BC_SLIP = 1
+CGX_BC_WALL_ADIABATIC = 2
 
 
 class Source(ctypes.Structure):
@@ -195,6 +207,7 @@ def lib():
         "cgx_get_tuning": (ctypes.c_int, [vp, c_int_p]),
         "cgx_set_scalars": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_set_source": (ctypes.c_int, [vp, ctypes.POINTER(Source)]),
+        "cgx_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
         "cgx_get_rhs_sc": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
@@ -304,6 +317,13 @@ class Solver:
         out = _out(self.ncv, getattr(self, "nsc", 0))
         _check(lib().cgx_get_rhs_sc(self.h, int(rk_stage), _dp(out)))
         return out
+
+    # -- boundary conditions (registerBoundaryConditions) ----------------------
+    def set_bc(self, zone, kind, u_wall=None):
+        """Boundary condition of boundary zone `zone`: CGX_BC_SLIP or
+        CGX_BC_WALL_ADIABATIC (u_wall: the wall velocity, zero if None)."""
+        uw = None if u_wall is None else np.ascontiguousarray(u_wall, dtype=np.float64)
+        _check(lib().cgx_set_bc(self.h, int(zone), int(kind), _dp(uw)))
 
     # -- source terms (addSourceHook) ----------------------------------------
     def set_source(self, A=0.0, g=(0.0, 0.0, 0.0), field=None):

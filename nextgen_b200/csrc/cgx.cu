@@ -972,7 +972,23 @@ __device__ __forceinline__ int cell_props(const Phys& ph, const MeshDev& m, cons
   double* P = reinterpret_cast<double*>(s.V + i);
   st4(P, mu_lam + mu_sgs, loc_lam + loc_sgs, a_sgs, fgr);
   reinterpret_cast<double2*>(P)[2] = make_double2(symh, symp);
+  P[15] = mu_lam;
   return (rho != rho) || (Li.p != Li.p) || (T != T);
+}
+
+// calcCfl's boundary-face terms of cell i (IdealGasSolver.cpp:1068-1074):
+// the sum over its boundary faces of |u.n_bf| + |n_bf| sos
+__device__ __forceinline__ double cfl_bf(const MeshDev& m, int i, double u0, double u1, double u2, double sos) {
+  double c = 0.0;
+  if (m.nbf == 0) return c;
+  const int f1 = __ldg(m.bfc + i + 1);
+  for (int f = __ldg(m.bfc + i); f < f1; ++f) {
+    const double n0 = __ldg(m.bf_n + f), n1 = __ldg(m.bf_n + m.nbf + f), n2 = __ldg(m.bf_n + 2 * m.nbf + f);
+    const double area = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    const double undA = u0 * n0 + u1 * n1 + u2 * n2;
+    c += fabs(undA) + area * sos;
+  }
+  return c;
 }
 
 // Once per step: cell_props + calcCfl(NULL, 1.0) for the next step's dt +
@@ -1037,6 +1053,7 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   cfl = group_sum<G>(cfl);
   if (valid && lane == 0) {
     anynan |= cell_props(ph, m, s, i, Li, vv2);
+    cfl += cfl_bf(m, i, Li.u[0], Li.u[1], Li.u[2], Li.sos);
     cmax = fmax(cmax, cfl * (0.5 * 1.0 * __ldg(m.inv_vol + i)));
   }
   STAGED_ROUNDS_END
@@ -1069,6 +1086,53 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
 }
 
 #include "cgx_mixed.cuh"
+
+// addBoundaryFlux of the boundary zones (IdealGasSolverBcs.cpp:14-48), one
+// thread per cell with boundary faces, added to one stage's rhs after the
+// face sums:
+//   SLIP            rhs.rhou -= p n_bf
+//   WALL_ADIABATIC  tau = mu_lam aod (u - u_wall); rhs.rhou -= p n_bf + tau;
+//                   rhs.rhoE -= u_wall.tau
+// p from the FP64 state (updateExtendedState's formula), mu_lam from the
+// cell's property record (the last calcSgsAndMaterialProperties).
+template <bool MIX>
+__global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
+  const MeshDev& m = c.m;
+  const StateDev& s = c.s;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.nbc) return;
+  const int i = m.bcell[t];
+  const double rho = s.rho[i], rhoE = s.rhoE[i];
+  const double u[3] = {s.u0[i], s.u1[i], s.u2[i]};
+  const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const double p = (c.ph.gamma - 1.0) * (rhoE - 0.5 * rho * usq);
+  const double mu_lam = MIX ? double(s.VF[i].mu_lam) : s.V[i].mu_lam;
+  double fr[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int f = m.bfc[i]; f < m.bfc[i + 1]; ++f) {
+    const double n[3] = {m.bf_n[f], m.bf_n[m.nbf + f], m.bf_n[2 * m.nbf + f]};
+    const double4 bc = s.bc[m.bf_zone[f]];
+    if (int(bc.x) == CGX_BC_WALL_ADIABATIC) {
+      const double visc = mu_lam * m.bf_aod[f];
+      const double uw[3] = {bc.y, bc.z, bc.w};
+      double work = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double tau = visc * (u[d] - uw[d]);
+        fr[d] -= p * n[d] + tau;
+        work += uw[d] * tau;
+      }
+      fr[3] -= work;
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) fr[d] -= p * n[d];
+    }
+  }
+  const size_t N = size_t(m.N);
+  double* r = s.rhs + size_t(stage) * 5 * N;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) r[(1 + d) * N + i] += fr[d];
+  r[4 * N + i] += fr[3];
+}
 
 // report() totals: per-block partial sums in a fixed tree, then one block
 // sums the partials in block order (deterministic).
@@ -1326,6 +1390,7 @@ __global__ void k_cfl_cells(MeshDev m, StateDev s, const int* __restrict__ perm,
                                       (uj[0] * un[0] + uj[1] * un[1] + uj[2] * un[2]));
     cfl += fabs(undA) + area * (0.5 * (si + sj));
   }
+  cfl += cfl_bf(m, i, ui[0], ui[1], ui[2], si);
   out[perm[i]] = cfl * (0.5 * dt * m.inv_vol[i]);
 }
 
@@ -1436,6 +1501,7 @@ struct cgx_mesh {
   std::vector<Item> items;  // work items (host copy of md.items)
   int max_union = 0;        // largest extended-face union of an item (records)
   int max_cunion = 0;       // largest compact-face union of an item
+  int nbf_zones = 0;        // boundary zones (0: periodic)
   std::vector<void*> allocs;
   size_t bytes = 0;
   cgx_mesh_stats stats{};
@@ -1523,6 +1589,7 @@ struct cgx_solver {
   std::unique_ptr<cgx_staging::Staging> staging;  // for pageable caller arrays, made on first use
   std::atomic<long long> launches{0};
   SourceCfg src;
+  std::vector<double4> bc;  // boundary conditions per zone (host copy of sd.bc)
 };
 
 namespace {
@@ -1867,9 +1934,21 @@ int enqueue_source(const Runner& R, int stage0, const double* time) {
   return CGX_OK;
 }
 
+// the boundary zones' fluxes into the rhs of stage0 (single-case solvers)
+int enqueue_bf(const Runner& R, int stage0) {
+  const int nbc = R.dcase.m.nbc;
+  if (!R.direct || nbc == 0) return CGX_OK;
+  if (R.prec == CGX_MIXED)
+    k_rhs_bf<true><<<(nbc + 127) / 128, 128, 0, R.stream>>>(R.dcase, stage0);
+  else
+    k_rhs_bf<false><<<(nbc + 127) / 128, 128, 0, R.stream>>>(R.dcase, stage0);
+  return launch_check(R, 1);
+}
+
 int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
   int rc = enqueue_faces(R, stage0);
   if (rc) return rc;
+  if ((rc = enqueue_bf(R, stage0))) return rc;
   if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, stage0))) return rc;
   return enqueue_source(R, stage0, time);
 }
@@ -1877,7 +1956,8 @@ int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
 // kernel launches of one RK3 step (more with transport scalars and sources);
 // with the one-pass face kernel, one fewer per stage
 inline int launches_per_step(const Runner& R) {
-  int n = kLaunchesPerStep - (R.tune.g_fused > 0 ? 3 : 0) + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0);
+  int n = kLaunchesPerStep - (R.tune.g_fused > 0 ? 3 : 0) + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
+          ((R.direct && R.dcase.m.nbc > 0) ? 3 : 0);
   if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0));
   return n;
 }
@@ -2015,6 +2095,7 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
       CK(cudaEventRecordWithFlags(marks[3 * st + 1], R.stream, cudaEventRecordExternal));
       if (R.tune.g_fused == 0 && (rc = comp_var(R, R.tune.g_comp, st))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 2], R.stream, cudaEventRecordExternal));
+      if ((rc = enqueue_bf(R, st))) return rc;
       if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, st))) return rc;
       if ((rc = enqueue_source(R, st, nullptr))) return rc;
     } else if ((rc = enqueue_rhs(R, st))) {
@@ -2139,6 +2220,12 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       !d->vol_cv || !d->cvocv_i || !d->cvocv_v || !d->cvocv_grad_coeff || !d->cvoef || !d->n_ef ||
       !d->c_ef || !d->dcmag_hat_cv || !d->sa_to_vol_ratio || (ncv_g2 > N && !d->icv_owner_g))
     return fail(CGX_E_ARG, "cgx_mesh_create: incomplete mesh description");
+  if (d->nbf < 0 || (d->nbf > 0 && (d->nbf_zones < 1 || !d->cvobf || !d->n_bf || !d->area_over_delta_bf ||
+                                    !d->zone_bf)))
+    return fail(CGX_E_ARG, "cgx_mesh_create: incomplete boundary-face description");
+  for (int f = 0; f < d->nbf; ++f)
+    if (d->cvobf[f] < 0 || d->cvobf[f] >= N || d->zone_bf[f] < 0 || d->zone_bf[f] >= d->nbf_zones)
+      return fail(CGX_E_ARG, "cgx_mesh_create: boundary face cell or zone out of range");
   CK(cudaSetDevice(device));
   cgx_mesh* M = new cgx_mesh();
   M->device = device;
@@ -2431,6 +2518,25 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
                            d->sa_to_vol_ratio[o]);
     }
     PT.mark("cell constants");
+    // ---- boundary faces by cell (new numbering), each cell's in input order
+    const int nbf = d->nbf;
+    std::vector<int> bfc(size_t(N) + 1, 0), bcell;
+    std::vector<int> bf_zone(std::max(nbf, 1), 0);
+    std::vector<double> bf_n(3 * size_t(std::max(nbf, 1)), 0.0), bf_aod(std::max(nbf, 1), 0.0);
+    if (nbf > 0) {
+      for (int f = 0; f < nbf; ++f) ++bfc[size_t(iperm[d->cvobf[f]]) + 1];
+      for (int i = 0; i < N; ++i) bfc[size_t(i) + 1] += bfc[size_t(i)];
+      std::vector<int> fill(bfc.begin(), bfc.end() - 1);
+      for (int f = 0; f < nbf; ++f) {
+        const int k = fill[size_t(iperm[d->cvobf[f]])]++;
+        for (int c = 0; c < 3; ++c) bf_n[size_t(c) * nbf + k] = d->n_bf[3 * size_t(f) + c];
+        bf_aod[k] = d->area_over_delta_bf[f];
+        bf_zone[k] = d->zone_bf[f];
+      }
+      for (int i = 0; i < N; ++i)
+        if (bfc[size_t(i) + 1] > bfc[size_t(i)]) bcell.push_back(i);
+    }
+    M->nbf_zones = nbf > 0 ? d->nbf_zones : 0;
     // ---- work items (runs of consecutive cells) and their halos; an item
     // whose neighbour unions exceed the shared-memory budget is split
     std::vector<Item> items;
@@ -2575,6 +2681,15 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     UP(d_ivol, inv_vol);
     UP(d_cc, cc);
     UP(M->d_perm, perm);
+    int *d_bfc = nullptr, *d_bcell = nullptr, *d_bfz = nullptr;
+    double *d_bfn = nullptr, *d_bfa = nullptr;
+    if (nbf > 0) {
+      UP(d_bfc, bfc);
+      UP(d_bcell, bcell);
+      UP(d_bfz, bf_zone);
+      UP(d_bfn, bf_n);
+      UP(d_bfa, bf_aod);
+    }
 #undef UP
     if ((rc = dalloc(&d_en, 6 * size_t(std::max(E, 1LL)), acc))) return bail(rc);
     M->allocs.push_back(d_en);
@@ -2634,6 +2749,13 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     md.vol = d_vol;
     md.inv_vol = d_ivol;
     md.cc = d_cc;
+    md.nbf = nbf;
+    md.nbc = int(bcell.size());
+    md.bfc = d_bfc;
+    md.bcell = d_bcell;
+    md.bf_n = d_bfn;
+    md.bf_aod = d_bfa;
+    md.bf_zone = d_bfz;
     md.en32 = nullptr;
     md.qg32 = nullptr;
     md.gcx32 = md.gcy32 = md.gcz32 = nullptr;
@@ -2781,6 +2903,15 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   AL(s->d_part, 5 * size_t(s->nblocks) + 5);
   AL(s->d_store[0], 5 * N);
   AL(s->d_store[1], 5 * N);
+  {
+    double4* d_bc = nullptr;
+    AL(d_bc, size_t(std::max(m->nbf_zones, 1)));
+    sd.bc = d_bc;
+    s->bc.assign(std::max(m->nbf_zones, 1), make_double4(0.0, 0.0, 0.0, 0.0));
+    if (cudaMemcpyAsync(d_bc, s->bc.data(), s->bc.size() * sizeof(double4), cudaMemcpyHostToDevice, s->stream) !=
+        cudaSuccess)
+      return bail(fail(CGX_E_CUDA, "boundary condition table upload failed"));
+  }
 #undef AL
   const bool zero_ok =
       cudaMemsetAsync(sd.rhs, 0, 15 * N * sizeof(double), s->stream) == cudaSuccess &&
@@ -3124,7 +3255,29 @@ extern "C" int cgx_calc_sgs_props(cgx_solver* s) {
   return CGX_OK;
 }
 
+extern "C" int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_bc: null solver");
+  if (zone < 0 || zone >= s->mesh->nbf_zones)
+    return fail(CGX_E_ARG, "cgx_set_bc: zone " + std::to_string(zone) + " not in [0, " +
+                               std::to_string(s->mesh->nbf_zones) + ")");
+  if (kind != CGX_BC_SLIP && kind != CGX_BC_WALL_ADIABATIC)
+    return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition");
+  CK(cudaSetDevice(s->mesh->device));
+  const double uw[3] = {u_wall ? u_wall[0] : 0.0, u_wall ? u_wall[1] : 0.0, u_wall ? u_wall[2] : 0.0};
+  s->bc[size_t(zone)] = make_double4(double(kind), kind == CGX_BC_SLIP ? 0.0 : uw[0],
+                                     kind == CGX_BC_SLIP ? 0.0 : uw[1], kind == CGX_BC_SLIP ? 0.0 : uw[2]);
+  CK(cudaMemcpyAsync(const_cast<double4*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(double4),
+                     cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
 extern "C" int cgx_init_complete(cgx_solver* s) {
+  if (s)
+    for (int z = 0; z < s->mesh->nbf_zones; ++z)
+      if (s->bc[size_t(z)].x == 0.0)
+        return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
+                                     " has no boundary condition (cgx_set_bc)");
   int rc = cgx_update_primitive(s);
   if (rc) return rc;
   if ((rc = cgx_calc_sgs_props(s))) return rc;
@@ -3697,6 +3850,7 @@ extern "C" int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, 
   if (!b || !mesh || !p || !rho || !u || !pres || nsteps < 0)
     return fail(CGX_E_ARG, "cgx_batch_add: invalid argument");
   if (mesh->device != b->device) return fail(CGX_E_ARG, "cgx_batch_add: mesh on another device");
+  if (mesh->md.nbf > 0) return fail(CGX_E_ARG, "cgx_batch_add: meshes with boundary faces run as single cases");
   int slot = -1;
   for (int k = 0; k < b->max_cases; ++k)
     if (!b->slots[k].s) {

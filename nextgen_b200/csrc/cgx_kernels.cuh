@@ -48,7 +48,8 @@ struct alignas(32) LRec {
   double sos;
 };
 
-// per-cell viscous record: lagged properties then dudx[i][j] at g[3*i+j]
+// per-cell viscous record: lagged properties then dudx[i][j] at g[3*i+j];
+// mu_lam (the laminar viscosity of the wall boundary flux) in the last slot
 struct alignas(128) VRec {
   double mu_total;
   double loc_total;
@@ -57,7 +58,7 @@ struct alignas(128) VRec {
   double symh;
   double symp;
   double g[9];
-  double pad;
+  double mu_lam;
 };
 
 struct alignas(32) QRec {
@@ -96,7 +97,7 @@ struct alignas(32) LRecF {
 struct alignas(64) VRecF {
   float mu_total, loc_total, a_sgs, fgr, symh, symp;
   float g[9];
-  float pad;
+  float mu_lam;
 };
 
 struct alignas(16) QRecF {
@@ -165,6 +166,14 @@ struct MeshDev {
   const double* vol;
   const double* inv_vol;
   const double4* cc;            // {pow(vol,1/3), pow(vol,2/3), dcmag_hat, sa_to_vol}
+  // boundary faces, ordered by cell (none: nbf = 0, pointers null)
+  int nbf;
+  int nbc;                      // cells with boundary faces
+  const int* bfc;               // [N+1] each cell's faces in the bf arrays
+  const int* bcell;             // [nbc] the cells with boundary faces, ascending
+  const double* bf_n;           // [3][nbf] outward area vector
+  const double* bf_aod;         // [nbf] area_over_delta_bf
+  const int* bf_zone;           // [nbf]
   // FP32 copies for the mixed-precision form (null until a mixed solver exists)
   const float* en32;            // [6][E]
   const float* qg32;            // [6][Q]
@@ -194,6 +203,8 @@ struct StateDev {
   double* sc;      // [nsc][N]
   double* rhs_sc;  // [3][nsc][N]
   double* mf;      // [E] mass flux of each extended entry, entry direction
+  // boundary conditions per boundary zone: {kind (CGX_BC_*), u_wall[3]}
+  const double4* bc;
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

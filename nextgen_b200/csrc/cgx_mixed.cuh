@@ -454,6 +454,7 @@ __device__ __forceinline__ int cell_props_f(const Phys& ph, const MeshDev& m, co
   float* P = reinterpret_cast<float*>(s.VF + i);
   reinterpret_cast<float4*>(P)[0] = make_float4(mu_lam + mu_sgs, loc_lam + loc_sgs, a_sgs, fgr);
   reinterpret_cast<float2*>(P)[2] = make_float2(symh, symp);
+  P[15] = mu_lam;
   return (rho != rho) || (p != p) || (T != T);
 }
 
@@ -514,6 +515,7 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   cfl = group_sum<G>(cfl);
   if (valid && lane == 0) {
     anynan |= cell_props_f(ph, m, s, i, Li, vv2);
+    cfl += cfl_bf(m, i, double(Li.u[0]), double(Li.u[1]), double(Li.u[2]), double(Li.sos));
     cmax = fmax(cmax, cfl * (0.5 * 1.0 * __ldg(m.inv_vol + i)));
   }
   STAGED_ROUNDS_END

@@ -90,6 +90,9 @@ struct Mesh {
   const int* cvocv_i;
   const int* cvocv_v;
   const double* gc;       // [ncoc][3]
+  const int* bfocv_i;     // [ncv+1] boundary faces of each cell
+  const int* bfocv_v;     // boundary face ids, ascending per cell
+  const double* Gij;      // [nbf][3][3]
   int* err;
 };
 
@@ -208,6 +211,12 @@ __global__ void k_grad_coeff(Mesh M, double sigma_thresh, double* gc, int* n_thr
     const int coc_l = M.cvocv_i[a + 1] - 1;
     double A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = 0; i < 3; ++i) A[i * 3 + i] = M.vol[a];
+    // boundary faces first, as the reference loops them
+    for (int boc = M.bfocv_i[a]; boc < M.bfocv_i[a + 1]; ++boc) {
+      const double* G = M.Gij + 9 * size_t(M.bfocv_v[boc]);
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) A[j * 3 + i] += G[3 * i + j];
+    }
     double g0[3] = {0.0, 0.0, 0.0};
     const double xc[3] = {M.xcv[3 * size_t(a)], M.xcv[3 * size_t(a) + 1], M.xcv[3 * size_t(a) + 2]};
     const int fb = M.faocv_i[a], fe = M.faocv_i[a + 1];
@@ -1007,6 +1016,23 @@ int build(const cgx_compact_desc* in, double f_int, double sigma_thresh, int dev
   M.xcv = upload(P, st, in->x_cv, 3 * size_t(ncv), "x_cv");
   M.g_owner = upload(P, st, in->icv_owner_g, size_t(ng1), "icv_owner_g");
   M.g_shift = upload(P, st, in->shift_g, 3 * size_t(ng1), "shift_g");
+  {
+    // boundary faces per cell (host counting sort, stable in face index)
+    const int nbf = in->nbf;
+    std::vector<int> bi(size_t(ncv) + 1, 0), bv(size_t(std::max(nbf, 1)), 0);
+    for (int f = 0; f < nbf; ++f) {
+      const int c = in->cvobf[f];
+      if (c < 0 || c >= ncv) throw Failure{CGX_E_ARG, "cgx_operators_build: cvobf out of range"};
+      ++bi[size_t(c) + 1];
+    }
+    for (int a = 0; a < ncv; ++a) bi[size_t(a) + 1] += bi[size_t(a)];
+    std::vector<int> fill(bi.begin(), bi.end() - 1);
+    for (int f = 0; f < nbf; ++f) bv[size_t(fill[size_t(in->cvobf[f])]++)] = f;
+    M.bfocv_i = upload(P, st, bi.data(), size_t(ncv) + 1, "bfocv_i");
+    M.bfocv_v = upload(P, st, bv.data(), bv.size(), "bfocv_v");
+    static const double kNoG[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    M.Gij = upload(P, st, nbf > 0 ? in->Gij_bf : kNoG, nbf > 0 ? 9 * size_t(nbf) : size_t(9), "Gij_bf");
+  }
   int* d_err = P.get<int>(ERR_SLOTS, "flags");
   ck(cudaMemsetAsync(d_err, 0, sizeof(int) * ERR_SLOTS, s), "memset");
   M.err = d_err;
@@ -1224,6 +1250,18 @@ int build(const cgx_compact_desc* in, double f_int, double sigma_thresh, int dev
   m->sa_to_vol_ratio = download(st, sav, size_t(ncv), "sa_to_vol");
   m->icv_owner_g = download(st, g_owner, size_t(ncv_g2 - ncv), "icv_owner_g");
   m->shift_g = reinterpret_cast<int(*)[3]>(download(st, g_shift, 3 * size_t(ncv_g2 - ncv), "shift_g"));
+  m->nbf = in->nbf;
+  m->nbf_zones = in->nbf_zones;
+  if (in->nbf > 0) {
+    const size_t nb = size_t(in->nbf);
+    m->cvobf = host_copy(in->cvobf, nb);
+    if (in->zone_bf) m->zone_bf = host_copy(in->zone_bf, nb);
+    if (in->n_bf) m->n_bf = reinterpret_cast<double(*)[3]>(host_copy(in->n_bf, 3 * nb));
+    if (in->x_bf) m->x_bf = reinterpret_cast<double(*)[3]>(host_copy(in->x_bf, 3 * nb));
+    if (in->area_bf) m->area_bf = host_copy(in->area_bf, nb);
+    if (in->area_over_delta_bf) m->area_over_delta_bf = host_copy(in->area_over_delta_bf, nb);
+    m->Gij_bf = reinterpret_cast<double(*)[3][3]>(host_copy(in->Gij_bf, 9 * nb));
+  }
   ck(cudaStreamSynchronize(s), "download");
   if (device_ms) ck(cudaEventElapsedTime(device_ms, ev0, ev1), "elapsed");
   *out = m;
@@ -1253,6 +1291,13 @@ extern "C" void cgx_operators_free(cgx_meshgen_out* m) {
   std::free(m->sa_to_vol_ratio);
   std::free(m->icv_owner_g);
   std::free(m->shift_g);
+  std::free(m->cvobf);
+  std::free(m->zone_bf);
+  std::free(m->n_bf);
+  std::free(m->x_bf);
+  std::free(m->area_bf);
+  std::free(m->area_over_delta_bf);
+  std::free(m->Gij_bf);
   std::free(m);
 }
 
@@ -1266,7 +1311,8 @@ extern "C" int cgx_operators_build(const cgx_compact_desc* in, double interp_fac
   if (!in || in->ncv < 1 || in->ncv_g < in->ncv || in->nfa < 0 || in->nfa_i < 0 || in->nfa_i > in->nfa ||
       !in->cvofa || !in->n_fa || !in->x_fa || !in->vol_cv || !in->x_cv ||
       (in->ncv_g > in->ncv && (!in->icv_owner_g || !in->shift_g)) || !(in->L[0] > 0) || !(in->L[1] > 0) ||
-      !(in->L[2] > 0) || !(interp_factor >= 0.0) || !(sigma_thresh >= 0.0)) {
+      !(in->L[2] > 0) || !(interp_factor >= 0.0) || !(sigma_thresh >= 0.0) || in->nbf < 0 ||
+      (in->nbf > 0 && (!in->cvobf || !in->Gij_bf))) {
     cgx::set_last_error("cgx_operators_build: invalid argument");
     return CGX_E_ARG;
   }

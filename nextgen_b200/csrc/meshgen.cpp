@@ -394,13 +394,20 @@ extern "C" void cgx_meshgen_free(cgx_meshgen_out* m) {
   std::free(m->sa_to_vol_ratio);
   std::free(m->icv_owner_g);
   std::free(m->shift_g);
+  std::free(m->cvobf);
+  std::free(m->zone_bf);
+  std::free(m->n_bf);
+  std::free(m->x_bf);
+  std::free(m->area_bf);
+  std::free(m->area_over_delta_bf);
+  std::free(m->Gij_bf);
   std::free(m);
 }
 
 namespace {
 int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jitter,
              unsigned long long seed, double interp_factor, double sigma_thresh, int nthreads,
-             bool compact_only, cgx_meshgen_out** out);
+             bool compact_only, bool walls_y, cgx_meshgen_out** out);
 }  // namespace
 
 extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, double Ly,
@@ -408,19 +415,44 @@ extern "C" int cgx_meshgen_periodic_box(int nx, int ny, int nz, double Lx, doubl
                                         double interp_factor, double sigma_thresh,
                                         int nthreads, cgx_meshgen_out** out) {
   return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, interp_factor, sigma_thresh, nthreads,
-                  false, out);
+                  false, false, out);
+}
+
+extern "C" int cgx_meshgen_channel(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jitter,
+                                   unsigned long long seed, double interp_factor, double sigma_thresh,
+                                   int nthreads, cgx_meshgen_out** out) {
+  return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, interp_factor, sigma_thresh, nthreads, false, true,
+                  out);
+}
+
+extern "C" int cgx_meshgen_channel_compact(int nx, int ny, int nz, double Lx, double Ly, double Lz,
+                                           double jitter, unsigned long long seed, int nthreads,
+                                           cgx_meshgen_out** out) {
+  return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, 1.0 / 3.0, 0.45, nthreads, true, true, out);
 }
 
 extern "C" int cgx_meshgen_periodic_box_compact(int nx, int ny, int nz, double Lx, double Ly,
                                                 double Lz, double jitter, unsigned long long seed,
                                                 int nthreads, cgx_meshgen_out** out) {
-  return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, 1.0 / 3.0, 0.45, nthreads, true, out);
+  return generate(nx, ny, nz, Lx, Ly, Lz, jitter, seed, 1.0 / 3.0, 0.45, nthreads, true, false, out);
 }
 
 namespace {
+// a cell face created by a channel wall's clip plane (the Poly tag of the
+// wall y = 0 is kWallTag0, of y = Ly kWallTag0 - 1)
+constexpr int kWallTag0 = -10;
+
+// One boundary face of one cell as computed from that cell's polyhedron.
+struct RawBFace {
+  int zone;
+  double n[3];   // outward area vector
+  double xf[3];  // centroid, relative to the seed
+  double area;
+};
+
 int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jitter,
              unsigned long long seed, double interp_factor, double sigma_thresh, int nthreads,
-             bool compact_only, cgx_meshgen_out** out) {
+             bool compact_only, bool walls_y, cgx_meshgen_out** out) {
   if (!out || nx < 4 || ny < 4 || nz < 4 || !(Lx > 0) || !(Ly > 0) || !(Lz > 0) ||
       !(jitter >= 0.0) || jitter > 0.3 || int64_t(nx) * ny * nz > (int64_t(1) << 30)) {
     g_err = "cgx_meshgen_periodic_box: invalid argument";
@@ -453,6 +485,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     PT.mark("seeds");
     // ---------------- Voronoi cells ----------------
     std::vector<std::vector<RawFace>> raw(ncv);
+    std::vector<std::vector<RawBFace>> rawb(walls_y ? ncv : 0);
     std::vector<double> vol(ncv);
     std::vector<V3> xcv(ncv);
     int n_bad = 0;
@@ -471,6 +504,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
             for (int di = -2; di <= 2; ++di) {
               if (di == 0 && dj == 0 && dk == 0) continue;
               int ii = i + di, jj = j + dj, kk = k + dk;
+              if (walls_y && (jj < 0 || jj >= ny)) continue;  // beyond a wall
               int sx = 0, sy = 0, sz = 0;
               if (ii < 0) { ii += nx; sx = -1; } else if (ii >= nx) { ii -= nx; sx = 1; }
               if (jj < 0) { jj += ny; sy = -1; } else if (jj >= ny) { jj -= ny; sy = 1; }
@@ -484,6 +518,15 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
                   [](const Cand& a, const Cand& b) { return a.r2 < b.r2; });
         make_box(P, 2.0 * hmax);
         double R2 = 3.0 * 4.0 * hmax * hmax;
+        if (walls_y) {
+          // the channel's walls, half-spaces y >= 0 and y <= Ly in the seed's frame
+          bool ch = clip(P, V3{0.0, -1.0, 0.0}, xvv[c].y, kWallTag0, 1e-12 * hmax, S);
+          ch = clip(P, V3{0.0, 1.0, 0.0}, Ly - xvv[c].y, kWallTag0 - 1, 1e-12 * hmax, S) || ch;
+          if (ch) {
+            R2 = 0.0;
+            for (const V3& v : P.v) R2 = std::max(R2, dot(v, v));
+          }
+        }
         for (int ic = 0; ic < int(cand.size()); ++ic) {
           const Cand& cd = cand[ic];
           if (0.25 * cd.r2 > R2 * (1.0 + 1e-9)) break;
@@ -525,6 +568,20 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
             }
             fc = (1.0 / (3.0 * wsum)) * fc;
           }
+          if (walls_y && (P.ftag[f] == kWallTag0 || P.ftag[f] == kWallTag0 - 1)) {
+            if (area <= 1e-12 * hmax * hmax) continue;
+            RawBFace bf;
+            bf.zone = kWallTag0 - P.ftag[f];
+            bf.n[0] = nsum.x;
+            bf.n[1] = nsum.y;
+            bf.n[2] = nsum.z;
+            bf.xf[0] = fc.x;
+            bf.xf[1] = fc.y;
+            bf.xf[2] = fc.z;
+            bf.area = area;
+            rawb[c].push_back(bf);
+            continue;
+          }
           if (P.ftag[f] < 0) {
             bad = true;
             continue;
@@ -560,6 +617,65 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     }
 
     PT.mark("voronoi");
+    // ---------------- boundary faces (channel walls) ----------------
+    // Ordered by cell, a cell's faces by zone.  area_over_delta_bf and Gij_bf
+    // as the reference forms them from the mesher's faces and seeds
+    // (src/core/common/StripedMesh.hpp:2781-2794): dx = x_bf - x_vv, the
+    // distance to the wall along the unit normal clipped below at
+    // min(vol^(1/3), vol/area)/4, Gij = -dx[j] n_bf[i].
+    std::vector<int> bfoff(ncv + 1, 0);
+    if (walls_y) {
+      for (int a = 0; a < ncv; ++a) {
+        std::stable_sort(rawb[a].begin(), rawb[a].end(),
+                         [](const RawBFace& p, const RawBFace& q) { return p.zone < q.zone; });
+        bfoff[a + 1] = bfoff[a] + int(rawb[a].size());
+      }
+    }
+    const int nbf = bfoff[ncv];
+    std::vector<int> cvobf(nbf), zone_bf(nbf);
+    std::vector<double> n_bf(3 * size_t(nbf)), x_bf(3 * size_t(nbf)), area_bf(nbf), aod_bf(nbf),
+        Gij_bf(9 * size_t(nbf));
+#pragma omp parallel for schedule(static)
+    for (int a = 0; a < ncv; ++a) {
+      for (int ibf = bfoff[a]; ibf < bfoff[a + 1]; ++ibf) {
+        const RawBFace& r = rawb[a][ibf - bfoff[a]];
+        const double area_eps = 1.0E-20;
+        const double xv[3] = {xvv[a].x, xvv[a].y, xvv[a].z};
+        cvobf[ibf] = a;
+        zone_bf[ibf] = r.zone;
+        double* n = &n_bf[3 * size_t(ibf)];
+        double* x = &x_bf[3 * size_t(ibf)];
+        for (int i = 0; i < 3; ++i) {
+          n[i] = r.n[i];
+          x[i] = xv[i] + r.xf[i];
+        }
+        const double area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        area_bf[ibf] = area;
+        const double dx[3] = {x[0] - xv[0], x[1] - xv[1], x[2] - xv[2]};
+        const double ua = std::max(area, area_eps);
+        const double unit_n[3] = {n[0] / ua, n[1] / ua, n[2] / ua};
+        const double dp = dx[0] * unit_n[0] + dx[1] * unit_n[1] + dx[2] * unit_n[2];
+        const double dx_vol = std::pow(vol[a], 1.0 / 3.0);
+        const double dx_vol_area = vol[a] / ua;
+        const double dx_clip = std::min(0.25 * dx_vol, 0.25 * dx_vol_area);
+        aod_bf[ibf] = (dp < dx_clip) ? area / dx_clip : area / dp;
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) Gij_bf[9 * size_t(ibf) + 3 * i + j] = -dx[j] * n[i];
+      }
+    }
+    std::vector<std::vector<RawBFace>>().swap(rawb);
+    auto put_bf = [&](cgx_meshgen_out* m) {
+      m->nbf = nbf;
+      m->nbf_zones = walls_y ? 2 : 0;
+      if (nbf == 0) return;
+      m->cvobf = dup_array(cvobf);
+      m->zone_bf = dup_array(zone_bf);
+      m->n_bf = reinterpret_cast<double(*)[3]>(dup_array(n_bf));
+      m->x_bf = reinterpret_cast<double(*)[3]>(dup_array(x_bf));
+      m->area_bf = dup_array(area_bf);
+      m->area_over_delta_bf = dup_array(aod_bf);
+      m->Gij_bf = reinterpret_cast<double(*)[3][3]>(dup_array(Gij_bf));
+    };
     // ---------------- compact faces ----------------
     // A face between cell a and image (b,s) is owned by min(a,b); its
     // geometry is the owner's.  Internal faces (s == 0): one face, icv0 = a <
@@ -676,6 +792,39 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     perf.shrink_to_fit();
     raw.clear();
     raw.shrink_to_fit();
+    // every cell must close: its faces' outward area vectors sum to zero.  A
+    // face seen from one side only (a neighbour beyond the 5x5x5 candidate
+    // neighbourhood, which a strongly anisotropic lattice can produce) breaks
+    // this, and the mesh is refused.
+    {
+      std::vector<double> S(3 * size_t(ncv), 0.0), A(ncv, 0.0);
+      for (int ifa = 0; ifa < nfa; ++ifa) {
+        const int c0 = cvofa[2 * size_t(ifa)], c1 = cvofa[2 * size_t(ifa) + 1];
+        const double* n = &n_fa[3 * size_t(ifa)];
+        const double a = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        for (int d = 0; d < 3; ++d) S[3 * size_t(c0) + d] += n[d];
+        A[c0] += a;
+        if (c1 < ncv) {
+          for (int d = 0; d < 3; ++d) S[3 * size_t(c1) + d] -= n[d];
+          A[c1] += a;
+        }
+      }
+      for (int ibf = 0; ibf < nbf; ++ibf) {
+        const int c = cvobf[ibf];
+        for (int d = 0; d < 3; ++d) S[3 * size_t(c) + d] += n_bf[3 * size_t(ibf) + d];
+        A[c] += area_bf[ibf];
+      }
+      int n_open = 0;
+      for (int c = 0; c < ncv; ++c) {
+        const double* s = &S[3 * size_t(c)];
+        if (std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) > 1e-9 * A[c]) ++n_open;
+      }
+      if (n_open > 0) {
+        g_err = "cgx_meshgen: " + std::to_string(n_open) +
+                " cells do not close (the lattice spacings differ too much for the 5x5x5 neighbourhood)";
+        return CGX_MG_E_GEOM;
+      }
+    }
     PT.mark("compact faces");
     const int ncv_g = ncv + int(g_owner.size());
     if (compact_only) {
@@ -714,6 +863,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
       m->x_vv = reinterpret_cast<double(*)[3]>(dup_array(xv));
       m->icv_owner_g = dup_array(g_owner);
       m->shift_g = reinterpret_cast<int(*)[3]>(dup_array(g_shift));
+      put_bf(m);
       *out = m;
       return CGX_MG_OK;
     }
@@ -811,6 +961,10 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
       const int coc_l = cvocv_i[a + 1] - 1;
       double A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int i = 0; i < 3; ++i) A[i * 3 + i] = vol[a];
+      // boundary faces first, as the reference loops them
+      for (int ibf = bfoff[a]; ibf < bfoff[a + 1]; ++ibf)
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) A[j * 3 + i] += Gij_bf[9 * size_t(ibf) + 3 * i + j];
       for (int foc = faocv_i[a]; foc < faocv_i[a + 1]; ++foc) {
         const LocFace& lf = loc[foc];
         const int coc = coc_f + foc - faocv_i[a] + 1;
@@ -1273,6 +1427,7 @@ int generate(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jit
     m->sa_to_vol_ratio = dup_array(sav);
     m->icv_owner_g = dup_array(g_owner);
     m->shift_g = reinterpret_cast<int(*)[3]>(dup_array(g_shift));
+    put_bf(m);
     *out = m;
     return CGX_MG_OK;
   } catch (const std::bad_alloc&) {

@@ -29,6 +29,9 @@ class MeshgenOut(ctypes.Structure):
         ("cvoef", c_int_p), ("n_ef", c_dbl_p), ("c_ef", c_dbl_p),
         ("cmag_cv", c_dbl_p), ("dcmag_hat_cv", c_dbl_p), ("sa_to_vol_ratio", c_dbl_p),
         ("icv_owner_g", c_int_p), ("shift_g", c_int_p),
+        ("nbf", ctypes.c_int), ("nbf_zones", ctypes.c_int),
+        ("cvobf", c_int_p), ("zone_bf", c_int_p), ("n_bf", c_dbl_p), ("x_bf", c_dbl_p),
+        ("area_bf", c_dbl_p), ("area_over_delta_bf", c_dbl_p), ("Gij_bf", c_dbl_p),
     ]
 
 
@@ -45,6 +48,13 @@ def _load():
         ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_double, ctypes.c_double, ctypes.c_double,
         ctypes.c_double, ctypes.c_ulonglong, ctypes.c_int, ctypes.POINTER(ctypes.POINTER(MeshgenOut))]
+    for name in ("cgx_meshgen_channel", "cgx_meshgen_channel_compact"):
+        f = getattr(lib, name)
+        f.restype = ctypes.c_int
+        f.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                       ctypes.c_double, ctypes.c_ulonglong] +
+                      ([] if name.endswith("compact") else [ctypes.c_double, ctypes.c_double]) +
+                      [ctypes.c_int, ctypes.POINTER(ctypes.POINTER(MeshgenOut))])
     lib.cgx_meshgen_free.restype = None
     lib.cgx_meshgen_free.argtypes = [ctypes.POINTER(MeshgenOut)]
     lib.cgx_meshgen_last_error.restype = ctypes.c_char_p
@@ -132,6 +142,14 @@ class PeriodicBoxMesh:
         self.sa_to_vol_ratio = _view(m.sa_to_vol_ratio, (self.ncv,), np.float64)
         self.icv_owner_g = _view(m.icv_owner_g, (ng,), np.int32)
         self.shift_g = _view(m.shift_g, (ng, 3), np.int32)
+        self.nbf, self.nbf_zones = m.nbf, m.nbf_zones
+        self.cvobf = _view(m.cvobf, (self.nbf,), np.int32)
+        self.zone_bf = _view(m.zone_bf, (self.nbf,), np.int32)
+        self.n_bf = _view(m.n_bf, (self.nbf, 3), np.float64)
+        self.x_bf = _view(m.x_bf, (self.nbf, 3), np.float64)
+        self.area_bf = _view(m.area_bf, (self.nbf,), np.float64)
+        self.area_over_delta_bf = _view(m.area_over_delta_bf, (self.nbf,), np.float64)
+        self.Gij_bf = _view(m.Gij_bf, (self.nbf, 3, 3), np.float64)
 
     def owner(self, idx):
         """Owned cell of a cell-or-ghost index array."""
@@ -163,6 +181,29 @@ class PeriodicBoxMesh:
             pass
 
 
+class ChannelMesh(PeriodicBoxMesh):
+    """Voronoi mesh of an nx*ny*nz (jittered) lattice in a channel: periodic
+    in x and z, walls at y = 0 (boundary zone 0) and y = Ly (zone 1)."""
+
+    def __init__(self, nx, ny=None, nz=None, L=(2.0 * np.pi, 2.0, np.pi), jitter=0.0, seed=1234,
+                 interp_factor=1.0 / 3.0, sigma_thresh=0.45, nthreads=0, compact_only=False):
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        Ls = (L, L, L) if np.isscalar(L) else tuple(float(v) for v in L)
+        out = ctypes.POINTER(MeshgenOut)()
+        if compact_only:
+            rc = lib().cgx_meshgen_channel_compact(int(nx), int(ny), int(nz), Ls[0], Ls[1], Ls[2], float(jitter),
+                                                   int(seed), int(nthreads), ctypes.byref(out))
+        else:
+            rc = lib().cgx_meshgen_channel(int(nx), int(ny), int(nz), Ls[0], Ls[1], Ls[2], float(jitter), int(seed),
+                                           float(interp_factor), float(sigma_thresh), int(nthreads),
+                                           ctypes.byref(out))
+        if rc != 0:
+            raise RuntimeError("meshgen failed (%d): %s" % (rc, lib().cgx_meshgen_last_error().decode()))
+        self._free = lib().cgx_meshgen_free
+        self._attach(out, (int(nx), int(ny), int(nz)), Ls, float(jitter), int(seed))
+
+
 class CompactDesc(ctypes.Structure):
     """cgx_compact_desc (include/cgx_ops.h)."""
     _fields_ = [
@@ -170,6 +211,9 @@ class CompactDesc(ctypes.Structure):
         ("L", ctypes.c_double * 3), ("h", ctypes.c_double),
         ("cvofa", c_int_p), ("n_fa", c_dbl_p), ("x_fa", c_dbl_p), ("vol_cv", c_dbl_p),
         ("x_cv", c_dbl_p), ("x_vv", c_dbl_p), ("icv_owner_g", c_int_p), ("shift_g", c_int_p),
+        ("nbf", ctypes.c_int), ("nbf_zones", ctypes.c_int),
+        ("cvobf", c_int_p), ("zone_bf", c_int_p), ("n_bf", c_dbl_p), ("x_bf", c_dbl_p),
+        ("area_bf", c_dbl_p), ("area_over_delta_bf", c_dbl_p), ("Gij_bf", c_dbl_p),
     ]
 
 
@@ -209,6 +253,16 @@ def compact_desc(mesh):
     d.x_vv = ptr(mesh.x_vv, ctypes.c_double) if mesh.x_vv is not None else None
     d.icv_owner_g = ptr(mesh.icv_owner_g, ctypes.c_int, ng1)
     d.shift_g = ptr(mesh.shift_g, ctypes.c_int, ng1)
+    d.nbf = getattr(mesh, "nbf", 0) or 0
+    d.nbf_zones = getattr(mesh, "nbf_zones", 0) or 0
+    if d.nbf > 0:
+        d.cvobf = ptr(mesh.cvobf, ctypes.c_int)
+        d.Gij_bf = ptr(mesh.Gij_bf, ctypes.c_double)
+        for f, ct in (("zone_bf", ctypes.c_int), ("n_bf", ctypes.c_double), ("x_bf", ctypes.c_double),
+                      ("area_bf", ctypes.c_double), ("area_over_delta_bf", ctypes.c_double)):
+            a = getattr(mesh, f, None)
+            if a is not None:
+                setattr(d, f, ptr(a, ct))
     d._keep = keep
     return d
 

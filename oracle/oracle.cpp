@@ -26,6 +26,8 @@
 //   calcRhsScalars               src/charles/ideal_gas/IdealGasSolver.cpp:537-693
 //   advanceScalars               src/charles/ideal_gas/IdealGasSolver.cpp:874-892
 //   face records (FaHash/FaNC/FaCompact, c halved)  src/charles/FlowSolver.hpp:1748-2262
+//   addBoundaryFlux (SLIP, WALL_ADIABATIC)  src/charles/ideal_gas/IdealGasSolverBcs.cpp:14-48
+//   calcCfl boundary faces       src/charles/ideal_gas/IdealGasSolver.cpp:1068-1074
 // The geometry is taken with DISABLE_FA_GROUPING semantics
 // (FlowSolver.hpp:667): every face keeps its own geometry, so every face is
 // in the "with c" ranges.
@@ -33,6 +35,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -125,6 +128,12 @@ struct orc_solver {
   int nsc = 0;
   std::vector<double> sc, rhs_sc[3], scale_sc;
   bool want_scale = false;
+  // boundary faces (cvobf, n_bf, area_over_delta_bf, zone) and one boundary
+  // condition per zone {kind, u_wall[3]}
+  int nbf = 0, nbf_zones = 0;
+  std::vector<int> cvobf, zone_bf;
+  std::vector<double> n_bf, aod_bf;
+  std::vector<std::array<double, 4>> bc;
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
@@ -427,8 +436,36 @@ void add_source(orc_solver* o, IdealGasRhs* rhs) {
     }
 }
 
+// addBoundaryFlux of each zone's boundary condition, zone by zone, before
+// the face loops as calcRhsBase calls them (IdealGasSolver.cpp:261-262):
+// SlipWallBc (IdealGasSolverBcs.cpp:14-23) and WallAdiabatic (:25-48)
+void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
+  for (int z = 0; z < o->nbf_zones; ++z) {
+    const std::array<double, 4>& bc = o->bc[z];
+    const int kind = int(bc[0]);
+    for (int ibf = 0; ibf < o->nbf; ++ibf) {
+      if (o->zone_bf[ibf] != z) continue;
+      const int icv = o->cvobf[ibf];
+      const double* n = &o->n_bf[3 * size_t(ibf)];
+      if (kind == CGX_BC_SLIP) {
+        for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= o->p[icv] * n[i];
+      } else {
+        const double visc_coeff = o->mu_lam[icv] * o->aod_bf[ibf];
+        double visc_work = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          const double tauijnj = visc_coeff * (o->u[3 * size_t(icv) + i] - bc[1 + i]);
+          rhs[icv].rhou[i] -= o->p[icv] * n[i] + tauijnj;
+          visc_work += bc[1 + i] * tauijnj;
+        }
+        rhs[icv].rhoE -= visc_work;
+      }
+    }
+  }
+}
+
 void calc_rhs(orc_solver* o, IdealGasRhs* rhs, double* rhs_sc = nullptr) {
   const bool sc = o->nsc > 0 && rhs_sc;
+  add_boundary_flux(o, rhs);
   if (o->nparts == 1) {
     rhs_part(o, 0, rhs);
     if (sc) rhs_sc_part(o, 0, rhs_sc);
@@ -584,6 +621,15 @@ void rk3_step(orc_solver* o, const double w[3], double dt) {
 
 double calc_cfl(const orc_solver* o, double dt_, double* cfl_out) {
   std::vector<double> cfl(o->ncv, 0.0);
+  // boundary faces first (IdealGasSolver.cpp:1068-1074)
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    const int icv = o->cvobf[ibf];
+    const double* n = &o->n_bf[3 * size_t(ibf)];
+    const double* uu = &o->u[3 * size_t(icv)];
+    const double area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const double undA = uu[0] * n[0] + uu[1] * n[1] + uu[2] * n[2];
+    cfl[icv] += std::fabs(undA) + area * o->sos[icv];
+  }
   auto add = [&](int c0, int c1, int ifa, bool both) {
     const double* n = &o->n_fa[3 * size_t(ifa)];
     const double area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
@@ -696,6 +742,15 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
   o->cvocv_v.assign(m->cvocv_v, m->cvocv_v + m->cvocv_i[ncv]);
   o->gc.assign(m->cvocv_grad_coeff, m->cvocv_grad_coeff + 3 * size_t(m->cvocv_i[ncv]));
   o->owner.assign(m->icv_owner_g, m->icv_owner_g + (ncv_g2 - ncv));
+  if (m->nbf > 0) {
+    o->nbf = m->nbf;
+    o->nbf_zones = m->nbf_zones;
+    o->cvobf.assign(m->cvobf, m->cvobf + m->nbf);
+    o->zone_bf.assign(m->zone_bf, m->zone_bf + m->nbf);
+    o->n_bf.assign(m->n_bf, m->n_bf + 3 * size_t(m->nbf));
+    o->aod_bf.assign(m->area_over_delta_bf, m->area_over_delta_bf + m->nbf);
+    o->bc.assign(m->nbf_zones, {0.0, 0.0, 0.0, 0.0});
+  }
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
   for (int ifa = 0; ifa < nfa; ++ifa) ncv_g = std::max(ncv_g, m->cvofa[2 * size_t(ifa) + 1] + 1);
@@ -984,6 +1039,13 @@ extern "C" void orc_get_aux(const orc_solver* o, double* aux) {
     a[4] = A.symh_fax;
     a[5] = A.symp_fax;
   }
+}
+
+extern "C" int orc_set_bc(orc_solver* o, int zone, int kind, const double u_wall[3]) {
+  if (zone < 0 || zone >= o->nbf_zones || (kind != CGX_BC_SLIP && kind != CGX_BC_WALL_ADIABATIC)) return -1;
+  o->bc[zone] = {double(kind), kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[0],
+                 kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[1], kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[2]};
+  return 0;
 }
 
 extern "C" void orc_set_source(orc_solver* o, double A, const double g[3], const double* field) {

@@ -69,6 +69,11 @@ void orc_get_aux(const orc_solver* o, double* aux);
  * quiver/charles/charles.sphere.cpp:166-173), plus field[ncv][5] if non-NULL.
  * A = 0, g = 0 and field = NULL remove them. */
 void orc_set_source(orc_solver* o, double A, const double g[3], const double* field);
+/* Boundary condition of boundary zone `zone` (the mesh's zone_bf), as
+ * registerBoundaryConditions sets one per zone (IdealGasSolver.hpp:170-231):
+ * CGX_BC_SLIP or CGX_BC_WALL_ADIABATIC with the wall velocity u_wall (NULL:
+ * zero).  0, or -1 on a bad argument. */
+int orc_set_bc(orc_solver* o, int zone, int kind, const double u_wall[3]);
 /* write a NaN into rho[icv] (host-side fault injection for the NaN path) */
 void orc_poison(orc_solver* o, int icv);
 

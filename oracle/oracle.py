@@ -57,6 +57,7 @@ def _load(path):
         "orc_get_aux": (None, [vp, c_dbl_p]),
         "orc_poison": (None, [vp, ctypes.c_int]),
         "orc_set_source": (None, [vp, ctypes.c_double, c_dbl_p, c_dbl_p]),
+        "orc_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
         "orc_uses_reference_flux": (ctypes.c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -186,6 +187,13 @@ class Oracle:
         gg = np.ascontiguousarray(g, dtype=np.float64)
         f = None if field is None else np.ascontiguousarray(field, dtype=np.float64).reshape(self.ncv, 5)
         self.L.orc_set_source(self.h, float(A), _dp(gg), _dp(f))
+
+    def set_bc(self, zone, kind, u_wall=None):
+        """Boundary condition of a boundary zone (CGX_BC_SLIP = 1,
+        CGX_BC_WALL_ADIABATIC = 2; u_wall zero if None)."""
+        uw = None if u_wall is None else np.ascontiguousarray(u_wall, dtype=np.float64)
+        if self.L.orc_set_bc(self.h, int(zone), int(kind), _dp(uw)) != 0:
+            raise ValueError("orc_set_bc: bad zone or kind")
 
     def poison(self, icv):
         self.L.orc_poison(self.h, int(icv))
