@@ -408,6 +408,21 @@ class Solver:
         """Restart at (time, step): cgx_set_time."""
         _check(lib().cgx_set_time(self.h, float(time), int(step)))
 
+    def write_sles(self, path, params=""):
+        """The current state, step and time as a .sles result file
+        (writeSles, StaticSolver.hpp:2311-2321), cells in the mesh's order."""
+        from .mles import write_sles
+        rho, u, rhoE = self.get_state()
+        t, _, step = self.time()
+        write_sles(path, rho, u, rhoE, step, t, params)
+
+    def read_sles(self, path):
+        """Restart from a .sles file: its state, then its time and step."""
+        from .mles import read_sles
+        rho, u, rhoE, step, t = read_sles(path, self.ncv)
+        self.set_state(rho, u, rhoE)
+        self.set_time(t, step)
+
     def totals(self):
         out = np.empty(5)
         _check(lib().cgx_totals(self.h, _dp(out)))

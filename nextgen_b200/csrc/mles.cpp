@@ -28,6 +28,10 @@ thread_local std::string g_err;
 
 constexpr int32_t kMagic = 123581321;
 enum : int32_t {
+  ID_I0 = 11,
+  ID_D0 = 12,
+  ID_PARAMS = 91,
+  ID_HASHIDS = 94,
   ID_EOF = 51,
   ID_FA_D2 = 25,
   ID_X_NO = 31,
@@ -345,6 +349,158 @@ void read_file(const char* path, cgx_mles* m) {
 }  // namespace
 
 extern "C" const char* cgx_mles_last_error(void) { return g_err.c_str(); }
+
+namespace {
+
+constexpr int32_t kSlesMagic = kMagic + 1;  // data file, not a restart (StaticSolver.cpp:7575)
+
+// 64-bit count as the (lsw, msw) int pair pair64 reads
+void set_pair64(int32_t* p, int64_t n) {
+  p[0] = int32_t(n & 0x7fffffffLL);
+  p[1] = int32_t(n >> 31);
+}
+
+struct Out {
+  FILE* f = nullptr;
+  ~Out() {
+    if (f) std::fclose(f);
+  }
+  void put(const void* p, size_t bytes) {
+    if (bytes && std::fwrite(p, 1, bytes, f) != bytes) fail(CGX_MLES_E_IO, "short write");
+  }
+  void header(const char* name, int32_t id, int64_t data_bytes, Header h) {
+    std::memset(h.name, 0, sizeof(h.name));
+    std::strncpy(h.name, name, sizeof(h.name) - 1);
+    h.id = id;
+    h.skip = int64_t(sizeof(Header)) + data_bytes;
+    put(&h, sizeof(h));
+  }
+};
+
+Header blank() {
+  Header h;
+  std::memset(&h, 0, sizeof(h));
+  return h;
+}
+
+}  // namespace
+
+extern "C" int cgx_sles_write(const char* path, long long ncv, int step, double time, const double* rho,
+                              const double* u, const double* rhoE, const char* params) {
+  if (!path || ncv < 0 || (ncv > 0 && (!rho || !u || !rhoE))) {
+    g_err = "cgx_sles_write: null argument or negative size";
+    return CGX_MLES_E_IO;
+  }
+  // written to a temporary name, then renamed over the target, as the
+  // reference does (StaticSolver.cpp:7567-7569, 7632-7636)
+  const std::string tmp = std::string(path) + ".tmp";
+  try {
+    {
+      Out O;
+      O.f = std::fopen(tmp.c_str(), "wb");
+      if (!O.f) fail(CGX_MLES_E_IO, "cannot create " + tmp);
+      const int32_t head[2] = {kSlesMagic, 5};
+      O.put(head, sizeof(head));
+      {
+        Header h = blank();
+        h.idata[0] = h.idata[1] = 20;
+        O.header("UGP_IO_HASHIDS", ID_HASHIDS, 40, h);
+        const unsigned char zeros[40] = {};
+        O.put(zeros, sizeof(zeros));
+      }
+      {
+        const std::string p = params ? params : "";
+        Header h = blank();
+        h.idata[0] = int32_t(p.size());
+        O.header("UGP_IO_PARAMS", ID_PARAMS, int64_t(p.size()), h);
+        O.put(p.data(), p.size());
+      }
+      auto cv_record = [&](const char* name, int32_t id, const double* v, int comps) {
+        Header h = blank();
+        set_pair64(h.idata, ncv);
+        if (comps == 3) h.idata[2] = 3;
+        O.header(name, id, int64_t(ncv) * comps * int64_t(sizeof(double)), h);
+        O.put(v, size_t(ncv) * comps * sizeof(double));
+      };
+      cv_record("rho", ID_CV_D1, rho, 1);
+      cv_record("rhoE", ID_CV_D1, rhoE, 1);
+      {
+        Header h = blank();
+        h.idata[0] = step;
+        O.header("step", ID_I0, 0, h);
+      }
+      {
+        Header h = blank();
+        h.rdata[0] = time;
+        O.header("time", ID_D0, 0, h);
+      }
+      cv_record("u", ID_CV_D2, u, 3);
+      O.header("EOF", ID_EOF, 0, blank());
+      if (std::fflush(O.f) != 0) fail(CGX_MLES_E_IO, "cannot flush " + tmp);
+    }
+    if (std::rename(tmp.c_str(), path) != 0) fail(CGX_MLES_E_IO, std::string("cannot rename to ") + path);
+  } catch (const Error& e) {
+    std::remove(tmp.c_str());
+    g_err = "cgx_sles_write: " + e.what;
+    return e.code;
+  }
+  return CGX_MLES_OK;
+}
+
+extern "C" int cgx_sles_read(const char* path, long long ncv, int* step, double* time, double* rho, double* u,
+                             double* rhoE) {
+  if (!path || ncv < 0) {
+    g_err = "cgx_sles_read: null argument or negative size";
+    return CGX_MLES_E_IO;
+  }
+  try {
+    File F;
+    F.f = std::fopen(path, "rb");
+    if (!F.f) fail(CGX_MLES_E_IO, std::string("cannot open ") + path);
+    if (fseeko(F.f, 0, SEEK_END) != 0 || (F.size = int64_t(ftello(F.f))) < 0)
+      fail(CGX_MLES_E_IO, std::string("cannot size ") + path);
+    int32_t head[2];
+    F.read_at(0, head, sizeof(head));
+    if (head[0] != kSlesMagic) fail(CGX_MLES_E_FORMAT, "not a .sles data file (magic number)");
+    if (head[1] != 5) fail(CGX_MLES_E_UNSUPPORTED, "io version " + std::to_string(head[1]) + " (5 is read)");
+    bool got[5] = {false, false, false, false, false};  // rho, rhoE, u, step, time
+    int64_t off = 8;
+    for (int nrec = 0;; ++nrec) {
+      if (nrec > 100000) fail(CGX_MLES_E_FORMAT, "no end-of-file record");
+      Header h;
+      F.read_at(off, &h, sizeof(h));
+      const int64_t data = off + int64_t(sizeof(Header));
+      if (h.id == ID_CV_D1 && (is(h, "rho") || is(h, "rhoE"))) {
+        if (pair64(h.idata) != ncv) fail(CGX_MLES_E_FORMAT, "cell record size differs from the mesh");
+        const bool e = is(h, "rhoE");
+        F.need(data, ncv, 8, e ? "rhoE" : "rho");
+        double* dst = e ? rhoE : rho;
+        if (dst) F.read_at(data, dst, size_t(ncv) * sizeof(double));
+        got[e ? 1 : 0] = true;
+      } else if (h.id == ID_CV_D2 && is(h, "u")) {
+        if (pair64(h.idata) != ncv || h.idata[2] != 3) fail(CGX_MLES_E_FORMAT, "u record size differs from the mesh");
+        F.need(data, 3 * ncv, 8, "u");
+        if (u) F.read_at(data, u, 3 * size_t(ncv) * sizeof(double));
+        got[2] = true;
+      } else if (h.id == ID_I0 && is(h, "step")) {
+        if (step) *step = h.idata[0];
+        got[3] = true;
+      } else if (h.id == ID_D0 && is(h, "time")) {
+        if (time) *time = h.rdata[0];
+        got[4] = true;
+      }
+      if (h.id == ID_EOF) break;
+      if (h.skip < int64_t(sizeof(Header))) fail(CGX_MLES_E_FORMAT, "record with a bad skip");
+      off += h.skip;
+    }
+    if (!(got[0] && got[1] && got[2] && got[3] && got[4]))
+      fail(CGX_MLES_E_FORMAT, "missing rho, rhoE, u, step or time");
+  } catch (const Error& e) {
+    g_err = "cgx_sles_read: " + e.what;
+    return e.code;
+  }
+  return CGX_MLES_OK;
+}
 
 extern "C" void cgx_mles_free(cgx_mles* m) {
   if (!m) return;

@@ -51,6 +51,12 @@ class MlesError(RuntimeError):
 def _lib():
     L = _meshgen_lib()
     if not getattr(L, "_mles_bound", False):
+        L.cgx_sles_write.restype = ctypes.c_int
+        L.cgx_sles_write.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, c_dbl_p,
+                                     c_dbl_p, c_dbl_p, ctypes.c_char_p]
+        L.cgx_sles_read.restype = ctypes.c_int
+        L.cgx_sles_read.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_double), c_dbl_p, c_dbl_p, c_dbl_p]
         L.cgx_mles_read.restype = ctypes.c_int
         L.cgx_mles_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(Mles))]
         L.cgx_mles_free.restype = None
@@ -121,3 +127,83 @@ class MlesMesh:
             self.close()
         except Exception:
             pass
+
+
+def write_sles(path, rho, u, rhoE, step=0, time=0.0, params=""):
+    """Write a .sles result file (cgx_sles_write): rho[ncv], u[ncv][3],
+    rhoE[ncv] in the mesh's cell order, the step and the time."""
+    rho, rhoE = (np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, rhoE))
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
+    dp = lambda a: a.ctypes.data_as(c_dbl_p)
+    rc = _lib().cgx_sles_write(str(path).encode(), rho.size, int(step), float(time), dp(rho), dp(u), dp(rhoE),
+                               (params or "").encode())
+    if rc != 0:
+        raise MlesError(rc, _lib().cgx_mles_last_error().decode())
+
+
+def read_sles(path, ncv):
+    """(rho, u, rhoE, step, time) of a .sles result file of ncv cells."""
+    rho, u, rhoE = np.empty(ncv), np.empty((ncv, 3)), np.empty(ncv)
+    st, t = ctypes.c_int(), ctypes.c_double()
+    dp = lambda a: a.ctypes.data_as(c_dbl_p)
+    rc = _lib().cgx_sles_read(str(path).encode(), int(ncv), ctypes.byref(st), ctypes.byref(t), dp(rho), dp(u),
+                              dp(rhoE))
+    if rc != 0:
+        raise MlesError(rc, _lib().cgx_mles_last_error().decode())
+    return rho, u, rhoE, st.value, t.value
+
+
+class CompactMesh:
+    """The mesher's part of a non-periodic mesh -- cells, internal faces and
+    boundary faces with their zones -- in the form the GPU operator build
+    takes (meshgen.compact_desc): from an MlesMesh (`from_mles`) or from the
+    arrays saved by `save` (`load`).  Internal faces are ordered by their
+    first cell (cvofa[:,0] < cvofa[:,1]); boundary faces keep the file's
+    order, each with the index of its zone in `zone_names`."""
+
+    FIELDS = ("cvofa", "n_fa", "x_fa", "vol_cv", "x_cv", "x_vv", "cvobf", "zone_bf", "n_bf", "x_bf", "area_bf",
+              "area_over_delta_bf", "Gij_bf")
+
+    def __init__(self, arrays, zone_names):
+        for k in self.FIELDS:
+            setattr(self, k, np.ascontiguousarray(arrays[k]))
+        self.zone_names = list(zone_names)
+        self.ncv = self.ncv_g = self.ncv_g2 = int(self.vol_cv.size)
+        self.nfa = self.nfa_i = int(self.cvofa.shape[0])
+        self.nbf = int(self.cvobf.size)
+        self.nbf_zones = len(self.zone_names)
+        self.nef = self.nef_i = 0
+        self.icv_owner_g = np.zeros(0, np.int32)
+        self.shift_g = np.zeros((0, 3), np.int32)
+        # no periodic images: the box lengths only have to be positive
+        self.L = (1.0, 1.0, 1.0)
+        self.h = float(np.cbrt(self.vol_cv.mean()))
+        self.dims, self.jitter, self.seed = (self.ncv, 1, 1), 0.0, 0
+
+    @classmethod
+    def from_mles(cls, m):
+        if m.nfa_p != 0 or m.nno_p != 0:
+            raise ValueError("periodic meshes are not handled")
+        c = np.asarray(m.cvofa)
+        n, x = np.asarray(m.n_fa), np.asarray(m.x_fa)
+        # each face from its lower cell, faces ordered by (lower cell, upper)
+        flip = c[:, 0] > c[:, 1]
+        c = np.where(flip[:, None], c[:, ::-1], c)
+        n = np.where(flip[:, None], -n, n)
+        order = np.lexsort((c[:, 1], c[:, 0]))
+        zone = np.zeros(m.nbf, np.int32)
+        for k, z in enumerate(m.bf_zones):
+            zone[z["ibf_f"]:z["ibf_f"] + z["nbf"]] = k
+        arrays = dict(cvofa=c[order].astype(np.int32), n_fa=n[order], x_fa=x[order], vol_cv=m.vol_cv,
+                      x_cv=m.x_cv, x_vv=m.x_vv if m.x_vv is not None else m.x_cv, cvobf=m.cvobf, zone_bf=zone,
+                      n_bf=m.n_bf, x_bf=m.x_bf, area_bf=m.area_bf, area_over_delta_bf=m.area_over_delta_bf,
+                      Gij_bf=m.Gij_bf)
+        return cls({k: np.array(v) for k, v in arrays.items()}, [z["name"] for z in m.bf_zones])
+
+    def save(self, path):
+        np.savez_compressed(path, zone_names=np.array(self.zone_names), **{k: getattr(self, k) for k in self.FIELDS})
+
+    @classmethod
+    def load(cls, path):
+        d = np.load(path)
+        return cls({k: d[k] for k in cls.FIELDS}, [str(s) for s in d["zone_names"]])
