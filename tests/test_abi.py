@@ -63,7 +63,7 @@ def test_meshgen_exports_every_declared_symbol(built):
 def test_meshgen_exports_every_mles_symbol(built):
     from nextgen_b200 import _lib
     names = declared("include/cgx_mles.h")
-    assert names == ["cgx_mles_free", "cgx_mles_last_error", "cgx_mles_read"]
+    assert names == ["cgx_mles_free", "cgx_mles_last_error", "cgx_mles_read", "cgx_sles_read", "cgx_sles_write"]
     L = ctypes.CDLL(_lib.path("libcgx_meshgen.so"))
     assert all(hasattr(L, n) for n in names)
 
