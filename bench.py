@@ -151,32 +151,32 @@ def cpu_baseline(seconds=12.0, n=48, lib_kind="reference"):
                       "%d OpenMP ranks over contiguous cell ranges" % (steps, what, n, m.ncv, cores)}
 
 
-def served_stream(nreq=16, seed=4242, budget_gb=60):
+def served_stream(nreq=64, seed=4242, budget_gb=60):
     """The served configuration: requests arrive as a seeded Poisson process;
-    each is a jittered-lattice periodic Voronoi box with edge uniform in
-    [16, 96] (rounded to a multiple of 8 so that requests share device
-    meshes), Taylor-Green or random-solenoidal (k0 = 4) initial state, Mach
-    uniform in [0.1, 0.5], steps uniform in [200, 2000], FP64 or mixed.  The
-    rate is set to twice the GPU's estimated throughput so the device stays
-    saturated.  Also runs the same cases one at a time on the plain FP64
+    each is its own jittered-lattice periodic Voronoi box (seed per request)
+    with edge uniform in [16, 96], Taylor-Green or random-solenoidal (k0 = 4)
+    initial state, Mach uniform in [0.1, 0.5], steps uniform in [200, 2000],
+    FP64 or mixed.  Requests bring the mesher's compact mesh (made before the
+    stream starts, as a mesher upstream would); admission builds the
+    operators on the GPU, uploads the device mesh and prepares the case on a
+    preparer thread while the GPU steps the resident cases.  The rate is twice
+    the GPU's estimated service rate, so the device stays saturated.  The same
+    requests also run one at a time (operator build, upload, initComplete,
+    steps, state read-back) at their own precision and on the plain FP64
     path."""
     from nextgen_b200 import cases, cgx, serve
     from nextgen_b200.meshgen import PeriodicBoxMesh
     rng = np.random.default_rng(seed)
-    edges = [int(8 * round(e / 8)) for e in rng.uniform(16, 96, size=nreq)]
-    meshes = {}
+    edges = [int(e) for e in rng.integers(16, 97, size=nreq)]
+    cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    for n in sorted(set(edges)):
-        hm = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED + n)
-        meshes[n] = (hm, cgx.Mesh(hm))
-    t_mesh = time.perf_counter() - t0
     reqs = []
     for k, n in enumerate(edges):
-        hm, gm = meshes[n]
+        compact = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED + 7919 * (k + 1), nthreads=cores, compact_only=True)
         Ma = float(rng.uniform(0.1, 0.5))
         if rng.random() < 0.5:
             prm = cases.tgv_params(Ma=Ma, Re=float(rng.uniform(400, 3200)))
-            rho, u, p = cases.tgv_state(hm.x_cv[: hm.ncv], prm)
+            rho, u, p = cases.tgv_state(compact.x_cv[: compact.ncv], prm)
             kind = "tgv"
         else:
             prm = cases.hit_params(Mt=Ma)
@@ -184,25 +184,50 @@ def served_stream(nreq=16, seed=4242, budget_gb=60):
             kind = "solenoidal"
         prm.check_interval = 20
         prec = cgx.CGX_FP64 if rng.random() < 0.5 else cgx.CGX_MIXED
-        reqs.append(serve.Request(k, gm, prm, rho, u, p, int(rng.integers(200, 2001)), prec))
-        reqs[-1].kind = kind
+        r = serve.Request(k, None, prm, rho, u, p, int(rng.integers(200, 2001)), prec, compact=compact)
+        r.kind = kind
+        reqs.append(r)
+    t_mesh = time.perf_counter() - t0
     total_cs = sum(r.cell_steps for r in reqs)
-    rate = 2.0 * 1.5e8 / (total_cs / nreq)  # requests/s: twice the estimated service rate
+    rate = 2.0 * 2.0e8 / (total_cs / nreq)  # requests/s: twice the estimated service rate
     for r, a in zip(reqs, serve.poisson_arrivals(nreq, rate, seed=seed + 1)):
         r.arrival = float(a)
     out = serve.serve(reqs, hbm_budget=int(budget_gb * (1 << 30)), chunk=16, keep_state=False)
-    seq, _ = serve.run_sequential(reqs, precision=cgx.CGX_FP64)
-    out.update({"sequential_plain_fp64_cell_steps_per_s": seq["cell_steps_per_s"],
-                "sequential_plain_fp64_seconds": seq["seconds"],
-                "speedup_vs_sequential_plain_fp64": out["cell_steps_per_s"] / seq["cell_steps_per_s"],
-                "poisson_rate_per_s": rate, "mesh_build_s": round(t_mesh, 2),
+    own, _ = serve.run_sequential(reqs, precision=None)
+    plain, _ = serve.run_sequential(reqs, precision=cgx.CGX_FP64)
+    for r in reqs:
+        r.compact.close()
+    out.update({"sequential_own_precision_cell_steps_per_s": own["cell_steps_per_s"],
+                "sequential_own_precision_seconds": own["seconds"],
+                "sequential_plain_fp64_cell_steps_per_s": plain["cell_steps_per_s"],
+                "sequential_plain_fp64_seconds": plain["seconds"],
+                "speedup_vs_sequential_own_precision": out["cell_steps_per_s"] / own["cell_steps_per_s"],
+                "speedup_vs_sequential_plain_fp64": out["cell_steps_per_s"] / plain["cell_steps_per_s"],
+                "poisson_rate_per_s": rate, "compact_mesh_build_s": round(t_mesh, 2),
+                "how": "host wall clock; admission (GPU operator build, device mesh, case set-up) inside the "
+                       "served window and inside each sequential run; the mesher's compact meshes made before",
                 "mix": {"fp64": sum(r.precision == cgx.CGX_FP64 for r in reqs),
                         "mixed": sum(r.precision == cgx.CGX_MIXED for r in reqs),
-                        "edges": edges, "steps_total": int(sum(r.nsteps for r in reqs))}})
+                        "distinct_meshes": nreq, "edges": edges,
+                        "steps_total": int(sum(r.nsteps for r in reqs))}})
     return out
 
 
+def workload_config(n, cells, e, f):
+    """The `config` object of both arms: what the workload is, nothing about
+    how it was run."""
+    return {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3 = %d cells per GPU, "
+                        "Taylor-Green Ma 0.1 Re 1600 Pr 0.71, Vreman SGS, FP64 RK3 at CFL 0.8" % (n, cells),
+            "cells": int(cells), "e_per_cell": float(e), "f_per_cell": float(f), "precision": "fp64"}
+
+
 def run_reference(args):
+    """The reference's CPU path on this arm's workload: the oracle built on the
+    reference's own flux, state and RK headers (the reference binary stops at
+    its licence check), on all host threads as contiguous cell ranges like
+    MPI ranks, stepping the same 200^3 mesh and state W + K RK3 steps; K
+    timed.  A 1-core leg times one step of the single-range oracle on a
+    jittered 64^3 sample.  Rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -211,33 +236,54 @@ def run_reference(args):
     from nextgen_b200 import cases
     from nextgen_b200.meshgen import PeriodicBoxMesh
     cores = os.cpu_count() or 1
-    n = args.ref_n
-    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED)
+    n = args.n
+    t0 = time.perf_counter()
+    m = PeriodicBoxMesh(n, jitter=JITTER, seed=SEED, nthreads=cores)
+    t_mesh = time.perf_counter() - t0
     prm = cases.tgv_params()
     rho, u, p = cases.tgv_state(m.x_cv[: m.ncv], prm)
     use_ref = ref_available()
     o = Oracle(m, prm, nparts=cores, reference=use_ref)
     o.set_state_primitive(rho, u, p)
     o.init_complete()
+    config = workload_config(n, m.ncv, m.e_per_cell, m.f_per_cell)
+    del rho, u, p
     if args.warmup:
         o.step(args.warmup)
     t0 = time.perf_counter()
     o.step(args.steps)
     el = time.perf_counter() - t0
     v = m.ncv * args.steps / el
+    o.close()
+    m.close()
+    # one core, the single-range oracle (the reference's serial order)
+    s1 = PeriodicBoxMesh(64, jitter=JITTER, seed=SEED, nthreads=cores)
+    prm1 = cases.tgv_params()
+    o1 = Oracle(s1, prm1, nparts=1, reference=use_ref)
+    o1.set_state_primitive(*cases.tgv_state(s1.x_cv[: s1.ncv], prm1))
+    o1.init_complete()
+    try:
+        os.sched_setaffinity(0, {sorted(os.sched_getaffinity(0))[0]})
+    except (AttributeError, OSError):
+        pass
+    t1 = time.perf_counter()
+    o1.step(1)
+    el1 = time.perf_counter() - t1
+    one_core = {"value": s1.ncv / el1, "unit": UNIT, "cores": 1,
+                "sample": "1 RK3 step of the single-range oracle on a jittered 64^3 box (%d cells)" % s1.ncv}
     what = ("oracle built on the reference's own IdealGasSolverFlux.hpp/States.hpp/RkWeights.hpp compiled in place"
             if use_ref else "oracle port of the reference hot path")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic",
-           "config": {"workload": "jittered-lattice periodic Voronoi %d^3 sample of the %d^3 (%d-cell) case, "
-                                  "TGV Ma 0.1 Re 1600, FP64 RK3 CFL 0.8" % (n, args.n, args.n ** 3),
-                      "cells": m.ncv, "e_per_cell": m.e_per_cell, "f_per_cell": m.f_per_cell,
-                      "parallelism": "cpu %d threads" % cores},
+           "data": "synthetic", "config": config,
+           "setup": {"parallelism": "cpu %d threads (cell ranges as MPI ranks)" % cores,
+                     "mesh_build_s": round(t_mesh, 2)},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference" if use_ref else "port",
-                            "sample": "%d RK3 steps of the %s on a jittered %d^3 box (%d cells) per run, "
-                                      "%d OpenMP ranks" % (args.steps, what, n, m.ncv, cores)},
+                            "sample": "%d timed RK3 steps (after %d warm-up) of the %s on the same %d-cell "
+                                      "mesh and state as the GPU arm, %d OpenMP ranks"
+                                      % (args.steps, args.warmup, what, config["cells"], cores)},
+           "cpu_1core": one_core,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -395,14 +441,12 @@ def run_cgx(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "jittered-lattice (+/-0.25h) periodic Voronoi %d^3 = %d cells per GPU, "
-                               "Taylor-Green Ma 0.1 Re 1600 Pr 0.71, Vreman SGS, FP64 RK3 at CFL 0.8"
-                               % (args.n, N),
-                   "cells": N, "e_per_cell": e, "f_per_cell": f,
-                   "l2": "inputs larger than L2 (%.1f GB mesh on device)" % (st.device_bytes / 1e9),
-                   "parallelism": "replicas x%d" % world, "precision": "fp64",
-                   "mesh_build_s": round(t_mesh, 2), "mesh_upload_s": round(t_up, 2),
-                   "mesh_operators": "gpu (cgx_operators_build)" if args.device_ops else "host generator"},
+        "config": workload_config(args.n, N, e, f),
+        "setup": {"l2": "inputs larger than L2 (%.1f GB mesh on device)" % (st.device_bytes / 1e9),
+                  "device_bytes_per_cell": st.device_bytes / N,
+                  "parallelism": "replicas x%d" % world,
+                  "mesh_build_s": round(t_mesh, 2), "mesh_upload_s": round(t_up, 2),
+                  "mesh_operators": "gpu (cgx_operators_build)" if args.device_ops else "host generator"},
         "e2e_pageable_host_arrays": {"value": e2e_pageable, "unit": UNIT},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 40 * N, "d2h_bytes_per_step": 40 * N,
                 "steps": ke, "how": "per step: cgx_set_state (pinned host -> device), cgx_step(1), "
@@ -718,11 +762,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--cpu-n", type=int, default=48)
-    ap.add_argument("--ref-n", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--served-requests", type=int, default=16)
+    ap.add_argument("--served-requests", type=int, default=64)
+    ap.add_argument("--served-only", action="store_true",
+                    help="instead of the throughput bench: only the served stream, as one JSON line")
     ap.add_argument("--accuracy", action="store_true",
                     help="instead of the throughput bench: mixed vs FP64 errors (TGV and solenoidal)")
     ap.add_argument("--accuracy-steps", type=int, default=500,
@@ -753,6 +798,9 @@ def main():
         return run_validate(args)
     if args.opbuild:
         return run_opbuild(args)
+    if args.served_only:
+        print(json.dumps(served_stream(nreq=args.served_requests)), flush=True)
+        return 0
     return run_cgx(args)
 
 

@@ -346,6 +346,19 @@ int cgx_batch_destroy(cgx_batch* b);
  * CGX_E_OOM, allocating nothing, when the case would exceed the budget. */
 int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
                   const double* u, const double* pres, int nsteps, int* case_id);
+/* cgx_batch_add in two parts, so that a server can build new cases while the
+ * batch steps.  cgx_batch_prepare creates the case's solver on its own
+ * stream, sets its state and runs initComplete (with the batch's lane counts:
+ * no tuning); it reads only the batch's device and precision, so another
+ * host thread may call it while cgx_batch_step runs.  cgx_batch_admit joins a
+ * prepared case between steps (a slot, its descriptor, the budget check:
+ * CGX_E_OOM leaves the case prepared, to be admitted later or released) and
+ * takes ownership of it on success.  The mesh must outlive the case. */
+typedef struct cgx_batch_case cgx_batch_case;
+int cgx_batch_prepare(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
+                      const double* u, const double* pres, int nsteps, cgx_batch_case** out);
+int cgx_batch_admit(cgx_batch* b, cgx_batch_case* c, int* case_id);
+int cgx_batch_case_release(cgx_batch_case* c);
 /* Advance every active case by up to nsteps steps (a case stops at its own
  * step count); *n_done = cases that have finished and not been removed. */
 int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done);

@@ -217,6 +217,10 @@ def lib():
         "cgx_batch_add": (ctypes.c_int, [vp, vp, ctypes.POINTER(Params), c_dbl_p, c_dbl_p, c_dbl_p,
                                           ctypes.c_int, c_int_p]),
         "cgx_batch_step": (ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
+        "cgx_batch_prepare": (ctypes.c_int, [vp, vp, ctypes.POINTER(Params), c_dbl_p, c_dbl_p, c_dbl_p,
+                                              ctypes.c_int, ctypes.POINTER(vp)]),
+        "cgx_batch_admit": (ctypes.c_int, [vp, vp, c_int_p]),
+        "cgx_batch_case_release": (ctypes.c_int, [vp]),
         "cgx_batch_done": (ctypes.c_int, [vp, c_int_p, ctypes.c_int, c_int_p]),
         "cgx_batch_get_state": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]),
         "cgx_batch_get_time": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_int_p]),
@@ -500,6 +504,25 @@ class Solver:
             pass
 
 
+class PreparedCase:
+    """A case built by Batch.prepare(), not yet admitted."""
+
+    def __init__(self, h, mesh):
+        self.h = h
+        self.mesh = mesh
+
+    def release(self):
+        if self.h:
+            lib().cgx_batch_case_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
 class Batch:
     """Resident cases advanced together (cgx_batch_*): continuous batching.
 
@@ -526,6 +549,29 @@ class Batch:
         _check(rc)
         self.ncv[cid.value] = mesh.ncv
         self._meshes[cid.value] = mesh
+        return cid.value
+
+    def prepare(self, mesh, params, rho, u, p, nsteps):
+        """A case built for this batch but not in it yet (cgx_batch_prepare):
+        safe to call from another thread while the batch steps.  Returns a
+        handle for admit()."""
+        rho, u, p = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, p))
+        h = ctypes.c_void_p()
+        _check(lib().cgx_batch_prepare(self.h, mesh.h, ctypes.byref(params), _dp(rho), _dp(u), _dp(p),
+                                       int(nsteps), ctypes.byref(h)))
+        return PreparedCase(h, mesh)
+
+    def admit(self, case):
+        """Join a prepared case between steps; its id, or None (and the case
+        stays prepared) when the HBM budget or the slots are full."""
+        cid = ctypes.c_int()
+        rc = lib().cgx_batch_admit(self.h, case.h, ctypes.byref(cid))
+        if rc == -2:
+            return None
+        _check(rc)
+        case.h = None  # owned by the batch now
+        self.ncv[cid.value] = case.mesh.ncv
+        self._meshes[cid.value] = case.mesh
         return cid.value
 
     def step(self, nsteps):

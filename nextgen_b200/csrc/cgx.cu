@@ -1094,7 +1094,10 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
 //   WALL_ADIABATIC  tau = mu_lam aod (u - u_wall); rhs.rhou -= p n_bf + tau;
 //                   rhs.rhoE -= u_wall.tau
 // p from the FP64 state (updateExtendedState's formula), mu_lam from the
-// cell's property record (the last calcSgsAndMaterialProperties).
+// cell's property record (the last calcSgsAndMaterialProperties).  The
+// mixed-precision face sums leave out p_ref sum(n_ef), which on a cell with
+// boundary faces is -p_ref sum(n_bf) (the extended-face GCL), so its
+// boundary term takes p - p_ref.
 template <bool MIX>
 __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
   const MeshDev& m = c.m;
@@ -1105,7 +1108,7 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
   const double rho = s.rho[i], rhoE = s.rhoE[i];
   const double u[3] = {s.u0[i], s.u1[i], s.u2[i]};
   const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-  const double p = (c.ph.gamma - 1.0) * (rhoE - 0.5 * rho * usq);
+  const double p = (c.ph.gamma - 1.0) * (rhoE - 0.5 * rho * usq) - (MIX ? c.ph.p_ref : 0.0);
   const double mu_lam = MIX ? double(s.VF[i].mu_lam) : s.V[i].mu_lam;
   double fr[4] = {0.0, 0.0, 0.0, 0.0};
   for (int f = m.bfc[i]; f < m.bfc[i + 1]; ++f) {
@@ -1877,9 +1880,16 @@ int enqueue_rhs_sc(const Runner& R, int stage0) {
   }
 }
 
+// The one-pass face kernel runs when the tuner picked it and its staged
+// unions fit the shared memory of one CTA (lane counts are cached per size
+// bucket, and another mesh of the bucket may have larger unions).
+inline bool use_fused(const Runner& R) {
+  return R.tune.g_fused > 0 && smem_fused(R) <= size_t(g_smem_optin);
+}
+
 // the face fluxes of one stage: the one-pass kernel or the two-kernel pair
 int enqueue_faces(const Runner& R, int stage0) {
-  if (R.tune.g_fused > 0) return fused_var(R, R.tune.g_fused, stage0);
+  if (use_fused(R)) return fused_var(R, R.tune.g_fused, stage0);
   int rc = ext_var(R, R.tune.g_ext, stage0);
   if (rc) return rc;
   return comp_var(R, R.tune.g_comp, stage0);
@@ -1956,7 +1966,7 @@ int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
 // kernel launches of one RK3 step (more with transport scalars and sources);
 // with the one-pass face kernel, one fewer per stage
 inline int launches_per_step(const Runner& R) {
-  int n = kLaunchesPerStep - (R.tune.g_fused > 0 ? 3 : 0) + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
+  int n = kLaunchesPerStep - (use_fused(R) ? 3 : 0) + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
           ((R.direct && R.dcase.m.nbc > 0) ? 3 : 0);
   if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0));
   return n;
@@ -2047,7 +2057,7 @@ int autotune(Runner& R, long long ncells) {
   best.g_fused = 0;
   bt = pair_ms;
   for (int G : fused_c) {
-    if (rc) break;
+    if (rc || smem_fused(R) > size_t(g_smem_optin)) break;
     float ms;
     if ((rc = time_it([&] { return fused_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_fused = G; }
@@ -2091,9 +2101,9 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
       // external records: captured into a graph they become event-record nodes
       // (with the one-pass face kernel the second interval is empty)
       CK(cudaEventRecordWithFlags(marks[3 * st], R.stream, cudaEventRecordExternal));
-      if ((rc = (R.tune.g_fused > 0 ? fused_var(R, R.tune.g_fused, st) : ext_var(R, R.tune.g_ext, st)))) return rc;
+      if ((rc = (use_fused(R) ? fused_var(R, R.tune.g_fused, st) : ext_var(R, R.tune.g_ext, st)))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 1], R.stream, cudaEventRecordExternal));
-      if (R.tune.g_fused == 0 && (rc = comp_var(R, R.tune.g_comp, st))) return rc;
+      if (!use_fused(R) && (rc = comp_var(R, R.tune.g_comp, st))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 2], R.stream, cudaEventRecordExternal));
       if ((rc = enqueue_bf(R, st))) return rc;
       if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, st))) return rc;
@@ -3272,24 +3282,30 @@ extern "C" int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall
   return CGX_OK;
 }
 
-extern "C" int cgx_init_complete(cgx_solver* s) {
-  if (s)
-    for (int z = 0; z < s->mesh->nbf_zones; ++z)
-      if (s->bc[size_t(z)].x == 0.0)
-        return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
-                                     " has no boundary condition (cgx_set_bc)");
+// initComplete; `tune`: pick the lane counts (a case prepared for a batch
+// runs with the batch's own lane counts and skips it)
+static int init_complete(cgx_solver* s, bool tune) {
+  if (!s) return fail(CGX_E_ARG, "null solver");
+  for (int z = 0; z < s->mesh->nbf_zones; ++z)
+    if (s->bc[size_t(z)].x == 0.0)
+      return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
+                                   " has no boundary condition (cgx_set_bc)");
   int rc = cgx_update_primitive(s);
   if (rc) return rc;
   if ((rc = cgx_calc_sgs_props(s))) return rc;
-  if ((rc = autotune(s->run, s->mesh->N))) return rc;
-  // recompute with the tuned lane counts so that the initial packed state,
-  // gradient and properties do not depend on whether tuning ran or was cached
-  if ((rc = cgx_update_primitive(s))) return rc;
-  if ((rc = cgx_calc_sgs_props(s))) return rc;
+  if (tune) {
+    if ((rc = autotune(s->run, s->mesh->N))) return rc;
+    // recompute with the tuned lane counts so that the initial packed state,
+    // gradient and properties do not depend on whether tuning ran or was cached
+    if ((rc = cgx_update_primitive(s))) return rc;
+    if ((rc = cgx_calc_sgs_props(s))) return rc;
+  }
   s->inited = true;
   s->have_store = false;
   return store_state(s);
 }
+
+extern "C" int cgx_init_complete(cgx_solver* s) { return init_complete(s, true); }
 
 extern "C" int cgx_calc_rhs(cgx_solver* s, double* rhs_out, double time, int rk_stage) {
   if (!s) return fail(CGX_E_ARG, "null solver");
@@ -3412,7 +3428,11 @@ static int ensure_graph(cgx_solver* s) {
   int rc = enqueue_step(s->run);
   cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
   s->launches = before;  // capturing launches nothing
-  if (rc) return rc;
+  if (rc || ec != cudaSuccess) cudaGetLastError();  // a failed capture leaves no error behind
+  if (rc) {
+    if (ec == cudaSuccess) cudaGraphDestroy(g);
+    return rc;
+  }
   if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
   ec = cudaGraphInstantiate(&s->graph, g, 0);
   cudaGraphDestroy(g);
@@ -3460,7 +3480,11 @@ static int ensure_pgraph(cgx_solver* s) {
   int rc = enqueue_step(s->run, s->pev);
   cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
   s->launches = before;
-  if (rc) return rc;
+  if (rc || ec != cudaSuccess) cudaGetLastError();  // a failed capture leaves no error behind
+  if (rc) {
+    if (ec == cudaSuccess) cudaGraphDestroy(g);
+    return rc;
+  }
   if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
   ec = cudaGraphInstantiate(&s->pgraph, g, 0);
   cudaGraphDestroy(g);
@@ -3527,9 +3551,8 @@ extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]) {
       else if (which == 2) rc = enqueue_grad(s->run);
       else if (which == 3) rc = enqueue_step_end(s->run, 0);
       else if (which == 4)
-        rc = s->run.tune.g_fused > 0 ? fused_var(s->run, s->run.tune.g_fused, 0)
-                                     : ext_var(s->run, s->run.tune.g_ext, 0);
-      else if (s->run.tune.g_fused == 0)
+        rc = use_fused(s->run) ? fused_var(s->run, s->run.tune.g_fused, 0) : ext_var(s->run, s->run.tune.g_ext, 0);
+      else if (!use_fused(s->run))
         rc = comp_var(s->run, s->run.tune.g_comp, 0);
     }
     CK(cudaEventRecord(e1, s->stream));
@@ -3616,7 +3639,7 @@ extern "C" int cgx_get_tuning(const cgx_solver* s, int out[5]) {
   out[1] = s->run.tune.g_comp;
   out[2] = s->run.tune.g_grad;
   out[3] = s->run.tune.g_end;
-  out[4] = s->run.tune.g_fused;
+  out[4] = use_fused(s->run) ? s->run.tune.g_fused : 0;
   return CGX_OK;
 }
 
@@ -3845,49 +3868,105 @@ extern "C" int cgx_batch_destroy(cgx_batch* b) {
   return CGX_OK;
 }
 
-extern "C" int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
-                             const double* u, const double* pres, int nsteps, int* case_id) {
-  if (!b || !mesh || !p || !rho || !u || !pres || nsteps < 0)
-    return fail(CGX_E_ARG, "cgx_batch_add: invalid argument");
-  if (mesh->device != b->device) return fail(CGX_E_ARG, "cgx_batch_add: mesh on another device");
-  if (mesh->md.nbf > 0) return fail(CGX_E_ARG, "cgx_batch_add: meshes with boundary faces run as single cases");
+// A case built for a batch but not yet in it (cgx_batch_prepare).
+struct cgx_batch_case {
+  cgx_solver* s = nullptr;
+  cgx_mesh* mesh = nullptr;
+  int target = 0;
+  int device = 0;
+  cgx_precision prec = CGX_FP64;
+};
+
+extern "C" int cgx_batch_prepare(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
+                                 const double* u, const double* pres, int nsteps, cgx_batch_case** out) {
+  if (!b || !mesh || !p || !rho || !u || !pres || nsteps < 0 || !out)
+    return fail(CGX_E_ARG, "cgx_batch_prepare: invalid argument");
+  *out = nullptr;
+  if (mesh->device != b->device) return fail(CGX_E_ARG, "cgx_batch_prepare: mesh on another device");
+  if (mesh->md.nbf > 0) return fail(CGX_E_ARG, "cgx_batch_prepare: meshes with boundary faces run as single cases");
+  CK(cudaSetDevice(b->device));
+  cgx_solver* s = nullptr;
+  int rc = cgx_solver_create(mesh, p, b->prec, &s);
+  if (rc) return rc;
+  if ((rc = cgx_set_state_primitive(s, rho, u, pres)) || (rc = init_complete(s, false)) ||
+      (rc = (cudaStreamSynchronize(s->stream) == cudaSuccess ? CGX_OK : fail(CGX_E_CUDA, "prepare sync")))) {
+    cgx_solver_destroy(s);
+    return rc;
+  }
+  cgx_batch_case* c = new cgx_batch_case();
+  c->s = s;
+  c->mesh = mesh;
+  c->target = nsteps;
+  c->device = b->device;
+  c->prec = b->prec;
+  *out = c;
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_case_release(cgx_batch_case* c) {
+  if (!c) return CGX_OK;
+  cgx_solver_destroy(c->s);
+  delete c;
+  return CGX_OK;
+}
+
+extern "C" int cgx_batch_admit(cgx_batch* b, cgx_batch_case* pc, int* case_id) {
+  if (!b || !pc) return fail(CGX_E_ARG, "cgx_batch_admit: null argument");
+  if (pc->device != b->device || pc->prec != b->prec)
+    return fail(CGX_E_ARG, "cgx_batch_admit: case prepared for another device or precision");
   int slot = -1;
   for (int k = 0; k < b->max_cases; ++k)
     if (!b->slots[k].s) {
       slot = k;
       break;
     }
-  if (slot < 0) return fail(CGX_E_OOM, "cgx_batch_add: all case slots in use");
-  size_t need = solver_bytes(mesh->N, mesh->md.nitems, b->prec);
-  if (!b->mesh_refs.count(mesh)) need += mesh->bytes;
-  if (b->prec == CGX_MIXED && !mesh->have32) need += mesh32_bytes(mesh);
-  if (b->used + need > b->budget) return fail(CGX_E_OOM, "cgx_batch_add: HBM budget exceeded");
+  if (slot < 0) return fail(CGX_E_OOM, "cgx_batch_admit: all case slots in use");
+  cgx_mesh* mesh = pc->mesh;
+  cgx_solver* s = pc->s;
+  const size_t need = s->bytes + (b->mesh_refs.count(mesh) ? 0 : mesh->bytes);
+  if (b->used + need > b->budget) return fail(CGX_E_OOM, "cgx_batch_admit: HBM budget exceeded");
   CK(cudaSetDevice(b->device));
-  const size_t mesh_before = mesh->bytes;
-  cgx_solver* s = nullptr;
-  int rc = cgx_solver_create(mesh, p, b->prec, &s);
-  if (rc) return rc;
-  if ((rc = cgx_set_state_primitive(s, rho, u, pres)) || (rc = cgx_init_complete(s))) {
-    cgx_solver_destroy(s);
-    return rc;
-  }
+  // the case's descriptor into the table (mesh records as of now), ordered
+  // before the next step on the batch's stream
+  s->hcase.m = mesh->md;
+  CK(cudaMemcpyAsync(b->d_cases + slot, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
   BatchCase& c = b->slots[slot];
   c.id = b->next_id++;
   c.s = s;
   c.mesh = mesh;
-  c.target = nsteps;
-  c.finished = (nsteps == 0);
+  c.target = pc->target;
+  c.steps = 0;
+  c.finished = (pc->target == 0);
   c.bytes = s->bytes;
-  b->used += s->bytes + (mesh->bytes - mesh_before);
-  if (b->mesh_refs[mesh]++ == 0) b->used += mesh_before;
+  b->used += need;
+  b->mesh_refs[mesh]++;
   b->slot_of[c.id] = slot;
-  // the case's descriptor into the table (mesh records as of now)
-  s->hcase.m = mesh->md;
-  CK(cudaMemcpyAsync(b->d_cases + slot, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream));
-  CK(cudaStreamSynchronize(b->stream));
   b->dirty = true;
+  delete pc;
   if (case_id) *case_id = c.id;
   return CGX_OK;
+}
+
+extern "C" int cgx_batch_add(cgx_batch* b, cgx_mesh* mesh, const cgx_params* p, const double* rho,
+                             const double* u, const double* pres, int nsteps, int* case_id) {
+  if (!b || !mesh || !p || !rho || !u || !pres || nsteps < 0)
+    return fail(CGX_E_ARG, "cgx_batch_add: invalid argument");
+  if (mesh->device != b->device) return fail(CGX_E_ARG, "cgx_batch_add: mesh on another device");
+  if (mesh->md.nbf > 0) return fail(CGX_E_ARG, "cgx_batch_add: meshes with boundary faces run as single cases");
+  bool free_slot = false;
+  for (int k = 0; k < b->max_cases && !free_slot; ++k) free_slot = !b->slots[k].s;
+  if (!free_slot) return fail(CGX_E_OOM, "cgx_batch_add: all case slots in use");
+  // the footprint checked before anything is allocated
+  size_t need = solver_bytes(mesh->N, mesh->md.nitems, b->prec);
+  if (!b->mesh_refs.count(mesh)) need += mesh->bytes;
+  if (b->prec == CGX_MIXED && !mesh->have32) need += mesh32_bytes(mesh);
+  if (b->used + need > b->budget) return fail(CGX_E_OOM, "cgx_batch_add: HBM budget exceeded");
+  cgx_batch_case* pc = nullptr;
+  int rc = cgx_batch_prepare(b, mesh, p, rho, u, pres, nsteps, &pc);
+  if (rc) return rc;
+  if ((rc = cgx_batch_admit(b, pc, case_id))) cgx_batch_case_release(pc);
+  return rc;
 }
 
 extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
@@ -3919,7 +3998,11 @@ extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
       rc = enqueue_step(b->run);
       cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
       b->launches = before;
-      if (rc) return rc;
+      if (rc || ec != cudaSuccess) cudaGetLastError();  // a failed capture leaves no error behind
+      if (rc) {
+        if (ec == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+      }
       if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
       ec = cudaGraphInstantiate(&b->graph, g, 0);
       cudaGraphDestroy(g);
