@@ -311,12 +311,10 @@ int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]);
 /* Lanes per cell chosen by the autotuner that cgx_init_complete runs (timed
  * candidates per kernel, cached per mesh-size bucket and precision):
  * out = {extended-face kernel, compact closures, gradient, once-per-step
- * kernel, one-pass face kernel, copy-ring depth}; out[4] = 0 when the
- * two-kernel face pair was faster than every one-pass candidate, else the
- * one-pass kernel's lanes (it then replaces the pair); out[5] = 0 when the
- * extended-face kernel loads its geometry directly, else the depth of the
- * per-lane asynchronous copy ring it streams the geometry through. */
-int cgx_get_tuning(const cgx_solver* s, int out[6]);
+ * kernel, one-pass face kernel}; out[4] = 0 when the two-kernel face pair
+ * was faster than every one-pass candidate, else the one-pass kernel's lanes
+ * (it then replaces the pair). */
+int cgx_get_tuning(const cgx_solver* s, int out[5]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
 /* Self-test of the device reciprocal that the flux kernels use for the face

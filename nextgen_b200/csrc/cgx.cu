@@ -142,16 +142,6 @@ __device__ __forceinline__ void cp_async16(int4* dst, const void* src) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// wait until at most N of this thread's copy groups are in flight
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // Asynchronous prefetch of a byte range into L2 by the bulk-copy engine
 // (start rounded down, end rounded up to 16 bytes).
@@ -541,77 +531,6 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
   STAGED_ROUNDS_END
   STAGED_LOOP_END
 #undef PF_EXT
-}
-
-// k_rhs_ext with each lane's geometry streamed through a ring of D entries in
-// shared memory: every lane keeps its next D-1 entries' six FP64 values in
-// flight with per-thread asynchronous copies (cp.async, one commit group per
-// entry, waited per thread: no barrier) while it evaluates the current one,
-// so the entry stream's latency is covered without holding the values in
-// registers.  The ring (D x 6 x 256 doubles, [slot][plane][thread]: a warp
-// reads 256 contiguous bytes per plane) sits before the staged records.
-template <int G, bool DIRECT, int D>
-__global__ void __launch_bounds__(256, 3) k_rhs_ext_ring(CASE_ARGS, int stage) {
-  extern __shared__ int4 smem[];
-  double* ring = reinterpret_cast<double*>(smem);
-  int4* sL = smem + D * 6 * 256 * 8 / 16;
-#define PF_EXTR(it, mm, r) prefetch_round<false>(mm, mm.en, it, r, 256 / G)
-  STAGED_LOOP_BEGIN(PF_EXTR)
-  stage_records<4>(sL, s.L, it_, m.hcell + it_.hoff, it_.nh);
-  stage_wait();
-  const long long E = m.E;
-  STAGED_ROUNDS_BEGIN(G, PF_EXTR)
-  long long b = 0, e = 0;
-  LRec Li;
-  if (valid) {
-    b = m.off[i];
-    e = m.off[i + 1];
-    smem_L(sL, loc_, Li);
-  }
-  // entry j of this lane is k = b + lane + j*G
-  const long long k0 = b + lane;
-  const int J = (e > k0) ? int((e - k0 + G - 1) / G) : 0;
-  double* my = ring + threadIdx.x;
-  auto issue = [&](int j) {
-    if (j < J) {
-      const double* g = m.en + (k0 + (long long)j * G);
-      double* slot = my + (j % D) * 6 * 256;
-#pragma unroll
-      for (int p = 0; p < 6; ++p) cp_async8(slot + p * 256, g + p * E);
-    }
-    cp_async_commit();
-  };
-#pragma unroll
-  for (int j = 0; j < D - 1; ++j) issue(j);
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int j = 0; j < J; ++j) {
-    issue(j + D - 1);
-    cp_async_wait<D - 1>();
-    const long long k = k0 + (long long)j * G;
-    const int jl = __ldg(m.lidx + k);
-    const double* slot = my + (j % D) * 6 * 256;
-    const double n[3] = {slot[0], slot[256], slot[512]};
-    const double c[3] = {slot[768], slot[1024], slot[1280]};
-    LRec Lj;
-    smem_L(sL, jl, Lj);
-    double F[5];
-    ext_flux(F, n, c, Li, Lj);
-    if (s.mf) s.mf[k] = F[0];  // mf[ief] of calcRhsBase, for calcRhsScalars
-#pragma unroll
-    for (int q = 0; q < 5; ++q) acc[q] -= F[q];
-  }
-  cp_async_wait<0>();
-#pragma unroll
-  for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  if (valid) {
-    double* r = s.rhs + size_t(stage) * 5 * m.N;
-#pragma unroll
-    for (int c = 0; c < 5; ++c)
-      if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
-  }
-  STAGED_ROUNDS_END
-  STAGED_LOOP_END
-#undef PF_EXTR
 }
 
 // Two CTAs per SM: the closure needs about 126 registers per thread, and at
@@ -1596,7 +1515,6 @@ struct cgx_mesh {
 // k_rhs_ext + k_rhs_comp pair.
 struct Tune {
   int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4, g_fused = 0;
-  int ext_ring = 0;  // FP64 extended-face kernel: depth of its per-lane copy ring (0: plain loads)
 };
 
 // The source terms of a single-case solver (cgx_set_source,
@@ -1711,9 +1629,6 @@ inline size_t smem_end(const Runner& R) {
                                     : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) *
          16;
 }
-inline size_t smem_ext_ring(const Runner& R, int D) {
-  return size_t(D) * 6 * 256 * sizeof(double) + size_t(swz_chunks<4>(R.max_union)) * 16;
-}
 inline size_t smem_fused(const Runner& R) {
   return size_t(R.prec == CGX_MIXED ? swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)
                                     : swz_chunks<4>(R.max_union) + swz_chunks<8>(R.max_cunion)) *
@@ -1758,10 +1673,6 @@ void launch_comp_d(const Runner& R, int st) {
   else
     k_rhs_comp<G, DIRECT><<<grid_staged(R), 256, smem_comp(R), R.stream>>>(RARGS, st);
 }
-template <int G, bool DIRECT, int D>
-void launch_ext_ring_d(const Runner& R, int st) {
-  k_rhs_ext_ring<G, DIRECT, D><<<grid_staged(R), 256, smem_ext_ring(R, D), R.stream>>>(RARGS, st);
-}
 template <int G, bool MIX, bool DIRECT>
 void launch_fused_d(const Runner& R, int st) {
   if (MIX)
@@ -1792,11 +1703,6 @@ template <int G, bool DIRECT>
 void allow_smem_ext() {
   allow_dyn_smem(k_rhs_ext<G, DIRECT>);
   allow_dyn_smem(k_rhs_ext_f<G, DIRECT>);
-}
-template <int G, bool DIRECT>
-void allow_smem_ext_ring() {
-  allow_dyn_smem(k_rhs_ext_ring<G, DIRECT, 2>);
-  allow_dyn_smem(k_rhs_ext_ring<G, DIRECT, 3>);
 }
 template <int G, bool DIRECT>
 void allow_smem_fused() {
@@ -1840,12 +1746,6 @@ int prepare_kernels(int device) {
   allow_smem_comp<8, false>();
   allow_smem_comp<16, true>();
   allow_smem_comp<16, false>();
-  allow_smem_ext_ring<8, true>();
-  allow_smem_ext_ring<8, false>();
-  allow_smem_ext_ring<16, true>();
-  allow_smem_ext_ring<16, false>();
-  allow_smem_ext_ring<32, true>();
-  allow_smem_ext_ring<32, false>();
   allow_smem_fused<8, true>();
   allow_smem_fused<8, false>();
   allow_smem_fused<16, true>();
@@ -1906,14 +1806,6 @@ void grad_g(const Runner& R, int G) {
     default: launch_grad<16, MIX>(R); break;
   }
 }
-template <int D>
-void ext_ring_g(const Runner& R, int G, int st) {
-  switch (G) {
-    case 8: R.direct ? launch_ext_ring_d<8, true, D>(R, st) : launch_ext_ring_d<8, false, D>(R, st); break;
-    case 32: R.direct ? launch_ext_ring_d<32, true, D>(R, st) : launch_ext_ring_d<32, false, D>(R, st); break;
-    default: R.direct ? launch_ext_ring_d<16, true, D>(R, st) : launch_ext_ring_d<16, false, D>(R, st); break;
-  }
-}
 template <bool MIX>
 void ext_g(const Runner& R, int G, int st) {
   switch (G) {
@@ -1956,18 +1848,8 @@ int grad_var(const Runner& R, int G) {
   is_mixed(R) ? grad_g<true>(R, G) : grad_g<false>(R, G);
   return launch_check(R, 1);
 }
-// the ring variants fit when their copy ring and staged records fit one CTA
-inline bool ring_fits(const Runner& R, int D) { return smem_ext_ring(R, D) <= size_t(g_smem_optin); }
-
-// the extended-face kernel with G lanes per cell; `ring` > 0: the FP64
-// variant with a per-lane copy ring of that depth (where it fits)
-int ext_var(const Runner& R, int G, int st, int ring) {
-  if (!is_mixed(R) && ring == 2 && ring_fits(R, 2))
-    ext_ring_g<2>(R, G, st);
-  else if (!is_mixed(R) && ring == 3 && ring_fits(R, 3))
-    ext_ring_g<3>(R, G, st);
-  else
-    is_mixed(R) ? ext_g<true>(R, G, st) : ext_g<false>(R, G, st);
+int ext_var(const Runner& R, int G, int st) {
+  is_mixed(R) ? ext_g<true>(R, G, st) : ext_g<false>(R, G, st);
   return launch_check(R, 1);
 }
 int comp_var(const Runner& R, int G, int st) {
@@ -2008,7 +1890,7 @@ inline bool use_fused(const Runner& R) {
 // the face fluxes of one stage: the one-pass kernel or the two-kernel pair
 int enqueue_faces(const Runner& R, int stage0) {
   if (use_fused(R)) return fused_var(R, R.tune.g_fused, stage0);
-  int rc = ext_var(R, R.tune.g_ext, stage0, R.tune.ext_ring);
+  int rc = ext_var(R, R.tune.g_ext, stage0);
   if (rc) return rc;
   return comp_var(R, R.tune.g_comp, stage0);
 }
@@ -2105,25 +1987,24 @@ int tune_bucket(long long ncells, cgx_precision prec) {
 // keep the fastest; results are cached per size bucket (log2 of the cell
 // count) and precision.  All candidates compute the same values (only the
 // order of the per-cell sums changes), and none changes the state.
-// CGX_TUNE="ext,comp,grad,end[,fused[,ring]]" (lanes per cell; fused 0 =
-// the two-kernel face pair; ring = the depth of the extended-face kernel's
-// copy ring, 0 = plain loads) skips the timing and fixes the lane counts,
-// e.g. to profile one variant.
+// CGX_TUNE="ext,comp,grad,end[,fused]" (lanes per cell; fused 0 = the
+// two-kernel face pair) skips the timing and fixes the lane counts, e.g. to
+// profile one variant.
 bool fixed_tune(Tune* t) {
   const char* e = std::getenv("CGX_TUNE");
   if (!e) return false;
-  int a, b, c, d, f = 0, ring = 0;
-  const int got = std::sscanf(e, "%d,%d,%d,%d,%d,%d", &a, &b, &c, &d, &f, &ring);
-  if (got < 4) return false;
+  int a, b, c, d, f = 0;
+  const int got = std::sscanf(e, "%d,%d,%d,%d,%d", &a, &b, &c, &d, &f);
+  if (got != 4 && got != 5) return false;
   auto ok = [](int g, std::initializer_list<int> allowed) {
     for (int x : allowed)
       if (g == x) return true;
     return false;
   };
   if (!ok(a, {4, 8, 16, 32}) || !ok(b, {2, 4, 8, 16}) || !ok(c, {1, 2, 4, 8, 16}) || !ok(d, {1, 4, 8, 16}) ||
-      !ok(f, {0, 8, 16, 32}) || !ok(ring, {0, 2, 3}) || (ring > 0 && a == 4))
+      !ok(f, {0, 8, 16, 32}))
     return false;
-  *t = Tune{a, b, c, d, f, ring};
+  *t = Tune{a, b, c, d, f};
   return true;
 }
 
@@ -2156,21 +2037,12 @@ int autotune(Runner& R, long long ncells) {
   int rc = CGX_OK;
   const int ext_c[] = {4, 8, 16, 32}, comp_c[] = {2, 4, 8, 16}, grad_c[] = {1, 2, 4, 8, 16},
             end_c[] = {1, 4, 8, 16}, fused_c[] = {8, 16, 32};
-  const int ring_c[][2] = {{8, 2}, {8, 3}, {16, 2}, {16, 3}, {32, 2}};
   bt = 1e30f;
   float pair_ms = 0.f;
-  best.ext_ring = 0;
   for (int G : ext_c) {
     float ms;
-    if ((rc = time_it([&] { return ext_var(R, G, 0, 0); }, &ms))) break;
-    if (ms < bt) { bt = ms; best.g_ext = G; best.ext_ring = 0; }
-  }
-  // the copy-ring variants (FP64)
-  for (const int (&v)[2] : ring_c) {
-    if (rc || is_mixed(R) || !ring_fits(R, v[1])) break;
-    float ms;
-    if ((rc = time_it([&] { return ext_var(R, v[0], 0, v[1]); }, &ms))) break;
-    if (ms < bt) { bt = ms; best.g_ext = v[0]; best.ext_ring = v[1]; }
+    if ((rc = time_it([&] { return ext_var(R, G, 0); }, &ms))) break;
+    if (ms < bt) { bt = ms; best.g_ext = G; }
   }
   pair_ms += bt;
   bt = 1e30f;
@@ -2229,7 +2101,7 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
       // external records: captured into a graph they become event-record nodes
       // (with the one-pass face kernel the second interval is empty)
       CK(cudaEventRecordWithFlags(marks[3 * st], R.stream, cudaEventRecordExternal));
-      if ((rc = (use_fused(R) ? fused_var(R, R.tune.g_fused, st) : ext_var(R, R.tune.g_ext, st, R.tune.ext_ring)))) return rc;
+      if ((rc = (use_fused(R) ? fused_var(R, R.tune.g_fused, st) : ext_var(R, R.tune.g_ext, st)))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 1], R.stream, cudaEventRecordExternal));
       if (!use_fused(R) && (rc = comp_var(R, R.tune.g_comp, st))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 2], R.stream, cudaEventRecordExternal));
@@ -3679,7 +3551,7 @@ extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]) {
       else if (which == 2) rc = enqueue_grad(s->run);
       else if (which == 3) rc = enqueue_step_end(s->run, 0);
       else if (which == 4)
-        rc = use_fused(s->run) ? fused_var(s->run, s->run.tune.g_fused, 0) : ext_var(s->run, s->run.tune.g_ext, 0, s->run.tune.ext_ring);
+        rc = use_fused(s->run) ? fused_var(s->run, s->run.tune.g_fused, 0) : ext_var(s->run, s->run.tune.g_ext, 0);
       else if (!use_fused(s->run))
         rc = comp_var(s->run, s->run.tune.g_comp, 0);
     }
@@ -3761,16 +3633,13 @@ extern "C" int cgx_synchronize(cgx_solver* s) {
   return CGX_OK;
 }
 
-extern "C" int cgx_get_tuning(const cgx_solver* s, int out[6]) {
+extern "C" int cgx_get_tuning(const cgx_solver* s, int out[5]) {
   if (!s || !out) return fail(CGX_E_ARG, "null argument");
   out[0] = s->run.tune.g_ext;
   out[1] = s->run.tune.g_comp;
   out[2] = s->run.tune.g_grad;
   out[3] = s->run.tune.g_end;
   out[4] = use_fused(s->run) ? s->run.tune.g_fused : 0;
-  out[5] = (s->prec == CGX_FP64 && s->run.tune.ext_ring > 0 && ring_fits(s->run, s->run.tune.ext_ring))
-               ? s->run.tune.ext_ring
-               : 0;
   return CGX_OK;
 }
 
@@ -4116,7 +3985,7 @@ extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
       if ((rc = autotune(b->run, b->active_cells))) return rc;
       const Tune& t = b->run.tune;
       if (b->tuned_bucket < 0 || t.g_ext != old.g_ext || t.g_comp != old.g_comp || t.g_grad != old.g_grad ||
-          t.g_end != old.g_end || t.g_fused != old.g_fused || t.ext_ring != old.ext_ring) {
+          t.g_end != old.g_end || t.g_fused != old.g_fused) {
         if ((rc = enqueue_grad(b->run))) return rc;  // dudx summed in the new grouping
         batch_free_graph(b);
       }
