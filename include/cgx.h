@@ -292,29 +292,24 @@ int cgx_synchronize(cgx_solver* s);
  * step, FlowSolver.hpp:2596-2605): run nsteps as cgx_step does and return
  * their device time from CUDA events on the solver's stream. */
 int cgx_step_timed(cgx_solver* s, int nsteps, float* device_ms);
-/* As cgx_step_timed, with the face-flux kernels of calcRhs timed inside the
- * steps by CUDA events recorded in the step graph around them:
- * face_ms = {average launch time of calcRhs's face kernels (extended faces +
- * compact closures), of the extended-face kernel (or the one-pass kernel),
- * of the compact-closure kernel (0 with the one-pass kernel)} over the
- * 3 x nsteps stages.  The host waits for each step before the next
+/* As cgx_step_timed, with the two face-flux kernels of calcRhs timed inside
+ * the steps by CUDA events recorded in the step graph around them:
+ * face_ms = {average launch time of the pair (extended faces + compact
+ * closures), of the extended-face kernel, of the compact-closure kernel}
+ * over the 3 x nsteps stages.  The host waits for each step before the next
  * one (the marks are reused), which device_ms includes. */
 int cgx_step_profiled(cgx_solver* s, int nsteps, float* device_ms, double face_ms[3]);
 /* Average device time of one launch of each step kernel, measured with CUDA
- * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs, all
- * its face kernels), ms[1] rk3Step + packed state (3 weights, dt = 0 so the
- * state is kept), ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/
- * CFL, ms[4] the extended-face flux kernel alone (the one-pass face kernel
- * when the tuner picked it), ms[5] the compact-closure kernel alone (0 with
- * the one-pass kernel).  Overwrites the stage-0 rhs. */
+ * events over `reps` back-to-back launches: ms[0] face fluxes (calcRhs, both
+ * kernels), ms[1] rk3Step + packed state (3 weights, dt = 0 so the state is
+ * kept), ms[2] gradient, ms[3] once-per-step SGS/properties/sensor/CFL,
+ * ms[4] the extended-face flux kernel alone, ms[5] the compact-closure kernel
+ * alone.  Overwrites the stage-0 rhs. */
 int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]);
 /* Lanes per cell chosen by the autotuner that cgx_init_complete runs (timed
  * candidates per kernel, cached per mesh-size bucket and precision):
- * out = {extended-face kernel, compact closures, gradient, once-per-step
- * kernel, one-pass face kernel}; out[4] = 0 when the two-kernel face pair
- * was faster than every one-pass candidate, else the one-pass kernel's lanes
- * (it then replaces the pair). */
-int cgx_get_tuning(const cgx_solver* s, int out[5]);
+ * out = {face fluxes, compact closures, gradient, once-per-step kernel}. */
+int cgx_get_tuning(const cgx_solver* s, int out[4]);
 /* Number of this library's kernels launched by the handle so far. */
 long long cgx_launch_count(const cgx_solver* s);
 /* Self-test of the device reciprocal that the flux kernels use for the face

@@ -470,12 +470,10 @@ class Solver:
         return dict(zip(("rhs", "rk_prim", "grad", "step_end", "ext", "comp"), ms.tolist()))
 
     def tuning(self):
-        """Lanes per cell picked by the autotuner: ext, comp, grad, step_end,
-        fused (0: the two-kernel face pair runs; else the one-pass face
-        kernel's lanes)."""
-        t = (ctypes.c_int * 5)()
+        """Lanes per cell picked by the autotuner: ext, comp, grad, step_end."""
+        t = (ctypes.c_int * 4)()
         _check(lib().cgx_get_tuning(self.h, t))
-        return dict(zip(("ext", "comp", "grad", "step_end", "fused"), list(t)))
+        return dict(zip(("ext", "comp", "grad", "step_end"), list(t)))
 
     def set_state_ptr(self, rho_ptr, u_ptr, rhoE_ptr):
         """cgx_set_state from raw host pointers (e.g. pinned buffers)."""

@@ -176,26 +176,6 @@ __device__ __forceinline__ void prefetch_round(const MeshDev& m, const TB* plane
                    __ldg(o + it.cell0 + b));
 }
 
-// The streams of the one-pass face kernel in round `sub` of item `it`: the
-// extended entries' six planes and local indices (threads 0..6) and the
-// compact entries' six planes and compact-union indices (threads 7..13).
-template <class TB>
-__device__ __forceinline__ void prefetch_fused(const MeshDev& m, const TB* en, const TB* qg, const Item& it,
-                                               int sub, int cpr) {
-  const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
-  const int t = threadIdx.x;
-  if (a >= b || t >= 14) return;
-  if (t < 7) {
-    prefetch_entries(en, m.E, m.lidx, __ldg(m.off + it.cell0 + a), __ldg(m.off + it.cell0 + b));
-    return;
-  }
-  const long long q0 = __ldg(m.qoff + it.cell0 + a), q1 = __ldg(m.qoff + it.cell0 + b);
-  if (t < 13)
-    prefetch_l2(qg + (t - 7) * m.Q + q0, (q1 - q0) * static_cast<long long>(sizeof(TB)));
-  else
-    prefetch_l2(m.clidx + q0, (q1 - q0) * 2);
-}
-
 // The streams the once-per-step kernel reads in round `sub` of item `it`:
 // the extended entries' local indices, the compact entries' local indices,
 // unit normals and areas.
@@ -594,86 +574,6 @@ __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
   STAGED_ROUNDS_END
   STAGED_LOOP_END
 #undef PF_COMP
-}
-
-// calcRhsBase in one pass over each cell's extended entries (the closures of
-// IdealGasSolverFlux.hpp:93-215 evaluated on the first ncomp entries, which
-// are the cell's compact faces): rhs[i] = -sum over the entries of the skew
-// + symmetric flux plus, on compact entries, the closure.  The item's
-// extended-face union of packed states and its compact-face union of
-// property/gradient records are staged once; rhs is written once.  A group
-// of G lanes per cell (lane l takes entries l, l+G, ...), partial sums
-// combined by the fixed butterfly.  The compact entries all fall in the first
-// sweeps of the lanes, so the closure work is spread over the group.
-template <int G, bool DIRECT>
-__global__ void __launch_bounds__(256, 2) k_rhs_fused(CASE_ARGS, int stage) {
-  extern __shared__ int4 smem[];
-#define PF_FUSED(it, mm, r) prefetch_fused(mm, mm.en, mm.qg, it, r, 256 / G)
-  STAGED_LOOP_BEGIN(PF_FUSED)
-  int4* sV = smem + swz_chunks<4>(it_.ncell + it_.nh);
-  stage_records<4>(smem, s.L, it_, m.hcell + it_.hoff, it_.nh);
-  stage_records<8>(sV, s.V, it_, m.chcell + it_.choff, it_.nch);
-  stage_wait();
-  const long long E = m.E, Q = m.Q;
-  STAGED_ROUNDS_BEGIN(G, PF_FUSED)
-  long long b = 0, e = 0, q0 = 0;
-  int ncomp = 0;
-  LRec Li;
-  if (valid) {
-    b = m.off[i];
-    e = m.off[i + 1];
-    q0 = m.qoff[i];
-    ncomp = int(m.qoff[i + 1] - q0);
-    smem_L(smem, loc_, Li);
-  }
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (long long k = b + lane; k < e; k += G) {
-    const int jl = __ldg(m.lidx + k);
-    const double* g = m.en + k;
-    const double n[3] = {__ldg(g), __ldg(g + E), __ldg(g + 2 * E)};
-    const double c[3] = {__ldg(g + 3 * E), __ldg(g + 4 * E), __ldg(g + 5 * E)};
-    LRec Lj;
-    smem_L(smem, jl, Lj);
-    double F[5];
-    ext_flux(F, n, c, Li, Lj);
-    const int t = int(k - b);
-    if (t < ncomp) {
-      const long long q = q0 + t;
-      const int jc = __ldg(m.clidx + q);
-      const double* h = m.qg + q;
-      const double un[3] = {__ldg(h), __ldg(h + Q), __ldg(h + 2 * Q)};
-      const double area = __ldg(h + 3 * Q), aod = __ldg(h + 4 * Q), delta = __ldg(h + 5 * Q);
-      VRec Vs;
-      smem_V_sum(sV, loc_, jc, Vs);
-      double uf[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) uf[d] = 0.5 * (Li.u[d] + Lj.u[d]);
-      const double uaub = Li.u[0] * Lj.u[0] + Li.u[1] * Lj.u[1] + Li.u[2] * Lj.u[2];
-      const double h_f = 0.5 * ((Lj.h + Li.h) + uaub);
-      Flux Fc;
-      Fc.rho = 0.0; Fc.ru[0] = Fc.ru[1] = Fc.ru[2] = 0.0; Fc.rE = 0.0;
-      compact_flux_add(Fc, un, area, aod, delta, Li, Lj, Vs, uf, h_f);
-      F[0] += Fc.rho;
-      F[1] += Fc.ru[0];
-      F[2] += Fc.ru[1];
-      F[3] += Fc.ru[2];
-      F[4] += Fc.rE;
-    }
-    if (s.mf) s.mf[k] = F[0];  // mf[ief] of calcRhsBase, for calcRhsScalars
-#pragma unroll
-    for (int q = 0; q < 5; ++q) acc[q] -= F[q];
-  }
-#pragma unroll
-  for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  if (valid) {
-    double* r = s.rhs + size_t(stage) * 5 * m.N;
-#pragma unroll
-    for (int c = 0; c < 5; ++c)
-      if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
-  }
-  STAGED_ROUNDS_END
-  STAGED_LOOP_END
-#undef PF_FUSED
 }
 
 // calcRhsScalars (IdealGasSolver.cpp:537-693), cell-centric over each
@@ -1510,11 +1410,9 @@ struct cgx_mesh {
   cgx_mesh_stats stats{};
 };
 
-// Lanes per cell of each face/gradient/step kernel.  g_fused > 0 selects the
-// one-pass face kernel (k_rhs_fused) with that many lanes in place of the
-// k_rhs_ext + k_rhs_comp pair.
+// Lanes per cell of each face/gradient/step kernel.
 struct Tune {
-  int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4, g_fused = 0;
+  int g_ext = 16, g_comp = 16, g_grad = 4, g_end = 4;
 };
 
 // The source terms of a single-case solver (cgx_set_source,
@@ -1629,11 +1527,6 @@ inline size_t smem_end(const Runner& R) {
                                     : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) *
          16;
 }
-inline size_t smem_fused(const Runner& R) {
-  return size_t(R.prec == CGX_MIXED ? swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)
-                                    : swz_chunks<4>(R.max_union) + swz_chunks<8>(R.max_cunion)) *
-         16;
-}
 inline size_t smem_comp(const Runner& R) {
   return size_t(R.prec == CGX_MIXED ? swz_chunks<2>(R.max_cunion) + swz_chunks<4>(R.max_cunion)
                                     : swz_chunks<4>(R.max_cunion) + swz_chunks<8>(R.max_cunion)) *
@@ -1674,13 +1567,6 @@ void launch_comp_d(const Runner& R, int st) {
     k_rhs_comp<G, DIRECT><<<grid_staged(R), 256, smem_comp(R), R.stream>>>(RARGS, st);
 }
 template <int G, bool MIX, bool DIRECT>
-void launch_fused_d(const Runner& R, int st) {
-  if (MIX)
-    k_rhs_fused_f<G, DIRECT><<<grid_staged(R), 256, smem_fused(R), R.stream>>>(RARGS, st);
-  else
-    k_rhs_fused<G, DIRECT><<<grid_staged(R), 256, smem_fused(R), R.stream>>>(RARGS, st);
-}
-template <int G, bool MIX, bool DIRECT>
 void launch_end_d(const Runner& R, int mode) {
   if (MIX)
     k_step_end_f<G, DIRECT><<<grid_staged(R), 256, smem_end(R), R.stream>>>(RARGS, mode);
@@ -1703,11 +1589,6 @@ template <int G, bool DIRECT>
 void allow_smem_ext() {
   allow_dyn_smem(k_rhs_ext<G, DIRECT>);
   allow_dyn_smem(k_rhs_ext_f<G, DIRECT>);
-}
-template <int G, bool DIRECT>
-void allow_smem_fused() {
-  allow_dyn_smem(k_rhs_fused<G, DIRECT>);
-  allow_dyn_smem(k_rhs_fused_f<G, DIRECT>);
 }
 template <int G, bool DIRECT>
 void allow_smem_end() {
@@ -1746,12 +1627,6 @@ int prepare_kernels(int device) {
   allow_smem_comp<8, false>();
   allow_smem_comp<16, true>();
   allow_smem_comp<16, false>();
-  allow_smem_fused<8, true>();
-  allow_smem_fused<8, false>();
-  allow_smem_fused<16, true>();
-  allow_smem_fused<16, false>();
-  allow_smem_fused<32, true>();
-  allow_smem_fused<32, false>();
   allow_smem_grad<1, true>();
   allow_smem_grad<1, false>();
   allow_smem_grad<2, true>();
@@ -1788,10 +1663,6 @@ void launch_comp(const Runner& R, int st) {
   R.direct ? launch_comp_d<G, MIX, true>(R, st) : launch_comp_d<G, MIX, false>(R, st);
 }
 template <int G, bool MIX>
-void launch_fused(const Runner& R, int st) {
-  R.direct ? launch_fused_d<G, MIX, true>(R, st) : launch_fused_d<G, MIX, false>(R, st);
-}
-template <int G, bool MIX>
 void launch_end(const Runner& R, int mode) {
   R.direct ? launch_end_d<G, MIX, true>(R, mode) : launch_end_d<G, MIX, false>(R, mode);
 }
@@ -1825,14 +1696,6 @@ void comp_g(const Runner& R, int G, int st) {
   }
 }
 template <bool MIX>
-void fused_g(const Runner& R, int G, int st) {
-  switch (G) {
-    case 8: launch_fused<8, MIX>(R, st); break;
-    case 32: launch_fused<32, MIX>(R, st); break;
-    default: launch_fused<16, MIX>(R, st); break;
-  }
-}
-template <bool MIX>
 void end_g(const Runner& R, int G, int mode) {
   switch (G) {
     case 1: launch_end<1, MIX>(R, mode); break;
@@ -1856,10 +1719,6 @@ int comp_var(const Runner& R, int G, int st) {
   is_mixed(R) ? comp_g<true>(R, G, st) : comp_g<false>(R, G, st);
   return launch_check(R, 1);
 }
-int fused_var(const Runner& R, int G, int st) {
-  is_mixed(R) ? fused_g<true>(R, G, st) : fused_g<false>(R, G, st);
-  return launch_check(R, 1);
-}
 int end_var(const Runner& R, int G, int mode) {
   is_mixed(R) ? end_g<true>(R, G, mode) : end_g<false>(R, G, mode);
   return launch_check(R, 1);
@@ -1880,16 +1739,8 @@ int enqueue_rhs_sc(const Runner& R, int stage0) {
   }
 }
 
-// The one-pass face kernel runs when the tuner picked it and its staged
-// unions fit the shared memory of one CTA (lane counts are cached per size
-// bucket, and another mesh of the bucket may have larger unions).
-inline bool use_fused(const Runner& R) {
-  return R.tune.g_fused > 0 && smem_fused(R) <= size_t(g_smem_optin);
-}
-
-// the face fluxes of one stage: the one-pass kernel or the two-kernel pair
+// the face fluxes of one stage
 int enqueue_faces(const Runner& R, int stage0) {
-  if (use_fused(R)) return fused_var(R, R.tune.g_fused, stage0);
   int rc = ext_var(R, R.tune.g_ext, stage0);
   if (rc) return rc;
   return comp_var(R, R.tune.g_comp, stage0);
@@ -1963,10 +1814,10 @@ int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
   return enqueue_source(R, stage0, time);
 }
 
-// kernel launches of one RK3 step (more with transport scalars and sources);
-// with the one-pass face kernel, one fewer per stage
+// kernel launches of one RK3 step (more with transport scalars, boundary
+// zones and sources)
 inline int launches_per_step(const Runner& R) {
-  int n = kLaunchesPerStep - (use_fused(R) ? 3 : 0) + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
+  int n = kLaunchesPerStep + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
           ((R.direct && R.dcase.m.nbc > 0) ? 3 : 0);
   if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0));
   return n;
@@ -1987,24 +1838,21 @@ int tune_bucket(long long ncells, cgx_precision prec) {
 // keep the fastest; results are cached per size bucket (log2 of the cell
 // count) and precision.  All candidates compute the same values (only the
 // order of the per-cell sums changes), and none changes the state.
-// CGX_TUNE="ext,comp,grad,end[,fused]" (lanes per cell; fused 0 = the
-// two-kernel face pair) skips the timing and fixes the lane counts, e.g. to
-// profile one variant.
+// CGX_TUNE="ext,comp,grad,end" (lanes per cell) skips the timing and fixes
+// the lane counts, e.g. to profile one variant.
 bool fixed_tune(Tune* t) {
   const char* e = std::getenv("CGX_TUNE");
   if (!e) return false;
-  int a, b, c, d, f = 0;
-  const int got = std::sscanf(e, "%d,%d,%d,%d,%d", &a, &b, &c, &d, &f);
-  if (got != 4 && got != 5) return false;
+  int a, b, c, d;
+  if (std::sscanf(e, "%d,%d,%d,%d", &a, &b, &c, &d) != 4) return false;
   auto ok = [](int g, std::initializer_list<int> allowed) {
     for (int x : allowed)
       if (g == x) return true;
     return false;
   };
-  if (!ok(a, {4, 8, 16, 32}) || !ok(b, {2, 4, 8, 16}) || !ok(c, {1, 2, 4, 8, 16}) || !ok(d, {1, 4, 8, 16}) ||
-      !ok(f, {0, 8, 16, 32}))
+  if (!ok(a, {4, 8, 16, 32}) || !ok(b, {2, 4, 8, 16}) || !ok(c, {1, 2, 4, 8, 16}) || !ok(d, {1, 4, 8, 16}))
     return false;
-  *t = Tune{a, b, c, d, f};
+  *t = Tune{a, b, c, d};
   return true;
 }
 
@@ -2036,31 +1884,19 @@ int autotune(Runner& R, long long ncells) {
   float bt;
   int rc = CGX_OK;
   const int ext_c[] = {4, 8, 16, 32}, comp_c[] = {2, 4, 8, 16}, grad_c[] = {1, 2, 4, 8, 16},
-            end_c[] = {1, 4, 8, 16}, fused_c[] = {8, 16, 32};
+            end_c[] = {1, 4, 8, 16};
   bt = 1e30f;
-  float pair_ms = 0.f;
   for (int G : ext_c) {
     float ms;
     if ((rc = time_it([&] { return ext_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_ext = G; }
   }
-  pair_ms += bt;
   bt = 1e30f;
   for (int G : comp_c) {
     if (rc) break;
     float ms;
     if ((rc = time_it([&] { return comp_var(R, G, 0); }, &ms))) break;
     if (ms < bt) { bt = ms; best.g_comp = G; }
-  }
-  pair_ms += bt;
-  // the one-pass face kernel against the best pair (same stage-0 rhs)
-  best.g_fused = 0;
-  bt = pair_ms;
-  for (int G : fused_c) {
-    if (rc || smem_fused(R) > size_t(g_smem_optin)) break;
-    float ms;
-    if ((rc = time_it([&] { return fused_var(R, G, 0); }, &ms))) break;
-    if (ms < bt) { bt = ms; best.g_fused = G; }
   }
   bt = 1e30f;
   for (int G : grad_c) {
@@ -2099,11 +1935,10 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
   for (int st = 0; st < 3; ++st) {
     if (marks) {
       // external records: captured into a graph they become event-record nodes
-      // (with the one-pass face kernel the second interval is empty)
       CK(cudaEventRecordWithFlags(marks[3 * st], R.stream, cudaEventRecordExternal));
-      if ((rc = (use_fused(R) ? fused_var(R, R.tune.g_fused, st) : ext_var(R, R.tune.g_ext, st)))) return rc;
+      if ((rc = ext_var(R, R.tune.g_ext, st))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 1], R.stream, cudaEventRecordExternal));
-      if (!use_fused(R) && (rc = comp_var(R, R.tune.g_comp, st))) return rc;
+      if ((rc = comp_var(R, R.tune.g_comp, st))) return rc;
       CK(cudaEventRecordWithFlags(marks[3 * st + 2], R.stream, cudaEventRecordExternal));
       if ((rc = enqueue_bf(R, st))) return rc;
       if (R.direct && R.dcase.s.nsc > 0 && (rc = enqueue_rhs_sc(R, st))) return rc;
@@ -3550,10 +3385,8 @@ extern "C" int cgx_kernel_times(cgx_solver* s, int reps, double ms[6]) {
       else if (which == 1) rc = enqueue_prim(s->run, 3, kRkW[2], 0.0, true);
       else if (which == 2) rc = enqueue_grad(s->run);
       else if (which == 3) rc = enqueue_step_end(s->run, 0);
-      else if (which == 4)
-        rc = use_fused(s->run) ? fused_var(s->run, s->run.tune.g_fused, 0) : ext_var(s->run, s->run.tune.g_ext, 0);
-      else if (!use_fused(s->run))
-        rc = comp_var(s->run, s->run.tune.g_comp, 0);
+      else if (which == 4) rc = ext_var(s->run, s->run.tune.g_ext, 0);
+      else rc = comp_var(s->run, s->run.tune.g_comp, 0);
     }
     CK(cudaEventRecord(e1, s->stream));
     CK(cudaEventSynchronize(e1));
@@ -3633,13 +3466,12 @@ extern "C" int cgx_synchronize(cgx_solver* s) {
   return CGX_OK;
 }
 
-extern "C" int cgx_get_tuning(const cgx_solver* s, int out[5]) {
+extern "C" int cgx_get_tuning(const cgx_solver* s, int out[4]) {
   if (!s || !out) return fail(CGX_E_ARG, "null argument");
   out[0] = s->run.tune.g_ext;
   out[1] = s->run.tune.g_comp;
   out[2] = s->run.tune.g_grad;
   out[3] = s->run.tune.g_end;
-  out[4] = use_fused(s->run) ? s->run.tune.g_fused : 0;
   return CGX_OK;
 }
 
@@ -3985,7 +3817,7 @@ extern "C" int cgx_batch_step(cgx_batch* b, int nsteps, int* n_done) {
       if ((rc = autotune(b->run, b->active_cells))) return rc;
       const Tune& t = b->run.tune;
       if (b->tuned_bucket < 0 || t.g_ext != old.g_ext || t.g_comp != old.g_comp || t.g_grad != old.g_grad ||
-          t.g_end != old.g_end || t.g_fused != old.g_fused) {
+          t.g_end != old.g_end) {
         if ((rc = enqueue_grad(b->run))) return rc;  // dudx summed in the new grouping
         batch_free_graph(b);
       }

@@ -271,83 +271,6 @@ __global__ void __launch_bounds__(256, 3) k_rhs_comp_f(CASE_ARGS, int stage) {
 #undef PF_COMPF
 }
 
-// k_rhs_fused (cgx.cu) in the mixed-precision form: one pass over each
-// cell's extended entries, the closure on the first ncomp (compact) entries,
-// FP32 flux arithmetic on the FP32 records, FP64 sums.
-template <int G, bool DIRECT>
-__global__ void __launch_bounds__(256, 3) k_rhs_fused_f(CASE_ARGS, int stage) {
-  extern __shared__ int4 smem[];
-#define PF_FUSEDF(it, mm, r) prefetch_fused(mm, mm.en32, mm.qg32, it, r, 256 / G)
-  STAGED_LOOP_BEGIN(PF_FUSEDF)
-  int4* sV = smem + swz_chunks<2>(it_.ncell + it_.nh);
-  stage_records<2>(smem, s.LF, it_, m.hcell + it_.hoff, it_.nh);
-  stage_records<4>(sV, s.VF, it_, m.chcell + it_.choff, it_.nch);
-  stage_wait();
-  const long long E = m.E, Q = m.Q;
-  const double h_ref = CASE_PH.h_ref;
-  const float p_ref = float(CASE_PH.p_ref);
-  STAGED_ROUNDS_BEGIN(G, PF_FUSEDF)
-  long long b = 0, e = 0, q0 = 0;
-  int ncomp = 0;
-  LRecF Li;
-  if (valid) {
-    b = m.off[i];
-    e = m.off[i + 1];
-    q0 = m.qoff[i];
-    ncomp = int(m.qoff[i + 1] - q0);
-    smem_LF(smem, loc_, Li);
-  }
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (long long k = b + lane; k < e; k += G) {
-    const int jl = __ldg(m.lidx + k);
-    const float* g = m.en32 + k;
-    const float n[3] = {__ldg(g), __ldg(g + E), __ldg(g + 2 * E)};
-    const float c[3] = {__ldg(g + 3 * E), __ldg(g + 4 * E), __ldg(g + 5 * E)};
-    LRecF Lj;
-    smem_LF(smem, jl, Lj);
-    float F[5];
-    ext_flux_f(F, n, c, Li, Lj);
-    const int t = int(k - b);
-    if (t < ncomp) {
-      const long long q = q0 + t;
-      const int jc = __ldg(m.clidx + q);
-      const float* h = m.qg32 + q;
-      const float un[3] = {__ldg(h), __ldg(h + Q), __ldg(h + 2 * Q)};
-      const float area = __ldg(h + 3 * Q), aod = __ldg(h + 4 * Q), delta = __ldg(h + 5 * Q);
-      VRecF Vs;
-      smem_VF_sum(sV, loc_, jc, Vs);
-      float uf[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) uf[d] = 0.5f * (Li.u[d] + Lj.u[d]);
-      const float uaub = Li.u[0] * Lj.u[0] + Li.u[1] * Lj.u[1] + Li.u[2] * Lj.u[2];
-      const float h_f = 0.5f * ((Lj.hh + Li.hh) + uaub);
-      FluxF Fc;
-      Fc.rho = 0.0f; Fc.ru[0] = Fc.ru[1] = Fc.ru[2] = 0.0f; Fc.rE = 0.0f;
-      compact_flux_add_f(Fc, un, area, aod, delta, Li, Lj, Vs, uf, h_f, p_ref);
-      F[0] += Fc.rho;
-      F[1] += Fc.ru[0];
-      F[2] += Fc.ru[1];
-      F[3] += Fc.ru[2];
-      F[4] += Fc.rE;
-    }
-    if (s.mf) s.mf[k] = double(F[0]);  // mass flux for calcRhsScalars
-#pragma unroll
-    for (int q = 0; q < 5; ++q) acc[q] -= double(F[q]);
-  }
-#pragma unroll
-  for (int c = 0; c < 5; ++c) acc[c] = group_sum<G>(acc[c]);
-  acc[4] += h_ref * acc[0];
-  if (valid) {
-    double* r = s.rhs + size_t(stage) * 5 * m.N;
-#pragma unroll
-    for (int c = 0; c < 5; ++c)
-      if (c % G == lane) r[size_t(c) * m.N + i] = acc[c];
-  }
-  STAGED_ROUNDS_END
-  STAGED_LOOP_END
-#undef PF_FUSEDF
-}
-
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256) k_grad_f(CASE_ARGS) {
   extern __shared__ int4 smem[];

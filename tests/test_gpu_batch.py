@@ -55,10 +55,9 @@ def test_batch_matches_alone(three, prec, tol):
     n0 = b.launch_count()
     b.step(100)
     assert sorted(b.done()) == sorted(ids)
-    # one graph replay per step of the longest case (13 kernels, or 10 when
-    # the tuner picked the one-pass face kernel), plus at most a re-tuning
-    # when the batch shrinks into another size bucket
-    assert 7 * 10 <= b.launch_count() - n0 < 7 * 13 + 30
+    # one graph replay (13 kernels) per step of the longest case, plus at most
+    # a re-tuning when the batch shrinks into another size bucket
+    assert 7 * 13 <= b.launch_count() - n0 < 7 * 13 + 30
     for cid, (m, gm, prm, rho, u, p), n in zip(ids, three, steps):
         got = b.get_state(cid)
         ref, (t_ref, dt_ref, st_ref) = alone(gm, prm, rho, u, p, n, prec)

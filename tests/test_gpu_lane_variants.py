@@ -1,8 +1,7 @@
 """Every lane-count variant the autotuner can choose gives calcRhs within
 the face-sum tolerance of the oracle, so the variant picked on any mesh is
 a correct one.  Lane counts per kernel are forced through CGX_TUNE
-(extended faces, compact closures, gradient, once-per-step, one-pass face
-kernel; 0 for the last selects the two-kernel face pair)."""
+(extended faces, compact closures, gradient, once-per-step)."""
 import os
 
 import numpy as np
@@ -14,8 +13,7 @@ from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-TUNES = [(4, 16, 1, 1, 0), (8, 8, 2, 4, 0), (16, 4, 8, 8, 0), (32, 2, 16, 16, 0),
-         (16, 2, 4, 4, 8), (16, 2, 4, 4, 16), (16, 2, 4, 4, 32)]
+TUNES = [(4, 16, 1, 1), (8, 8, 2, 4), (16, 4, 8, 8), (32, 2, 16, 16)]
 
 
 @pytest.fixture(scope="module")
@@ -30,12 +28,12 @@ def case(built):
     return m, prm, (rho, u, p), cgx.Mesh(m, device=0), ref, scale
 
 
-@pytest.mark.parametrize("tune", TUNES, ids=lambda t: "%d-%d-%d-%d-%d" % t)
+@pytest.mark.parametrize("tune", TUNES, ids=lambda t: "%d-%d-%d-%d" % t)
 @pytest.mark.parametrize("prec", [cgx.CGX_FP64, cgx.CGX_MIXED], ids=["fp64", "mixed"])
 def test_lane_variant(case, tune, prec):
     m, prm, (rho, u, p), gm, ref, scale = case
     old = os.environ.get("CGX_TUNE")
-    os.environ["CGX_TUNE"] = "%d,%d,%d,%d,%d" % tune
+    os.environ["CGX_TUNE"] = "%d,%d,%d,%d" % tune
     try:
         s = cgx.Solver(gm, prm, prec)
         s.set_state_primitive(rho, u, p)
@@ -46,7 +44,7 @@ def test_lane_variant(case, tune, prec):
         else:
             os.environ["CGX_TUNE"] = old
     t = s.tuning()
-    assert (t["ext"], t["comp"], t["grad"], t["step_end"], t["fused"]) == tune
+    assert (t["ext"], t["comp"], t["grad"], t["step_end"]) == tune
     r = s.calcRhs(2)
     err = (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max()
     tol = 1e-12 if prec == cgx.CGX_FP64 else 2e-5  # FP32 flux arithmetic in the mixed form

@@ -98,8 +98,7 @@ def test_mixed_deterministic_and_launches(built):
         s = solver(m, prm, rho, u, p, cgx.CGX_MIXED)
         n0 = s.launch_count()
         s.step(3)
-        # 13 kernels per step, 10 with the one-pass face kernel
-        assert s.launch_count() - n0 == 3 * (10 if s.tuning()["fused"] else 13)
+        assert s.launch_count() - n0 == 3 * 13
         outs.append(s.get_state())
     for a, b in zip(*outs):
         assert np.array_equal(a, b)

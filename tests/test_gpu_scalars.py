@@ -80,8 +80,7 @@ def test_steps_match_oracle(pair):
     o.init_complete()
     n0 = s.launch_count()
     assert s.step(20) == 0 and o.step(20) == 0
-    # 13 flow kernels (10 with the one-pass face kernel) + 3 scalar rhs per step
-    assert s.launch_count() - n0 >= 20 * (13 if s.tuning()["fused"] else 16)
+    assert s.launch_count() - n0 >= 20 * 16  # 13 flow kernels + 3 scalar rhs per step
     g, r = s.get_scalars(), o.get_scalars()
     assert (np.abs(g - r) / np.abs(r)).max() <= 1e-10
     r1, u1, e1 = s.get_state()
