@@ -788,25 +788,44 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->cf_geom[ifa].area_over_delta = m->area_over_delta_fa[ifa];
   }
   // link compact faces to extended faces (FlowSolver.hpp:1833-1900)
-  std::map<std::pair<int, int>, int> ef_of;
-  for (int ief = 0; ief < nef; ++ief) ef_of[{m->cvoef[2 * size_t(ief)], m->cvoef[2 * size_t(ief) + 1]}] = ief;
+  // extended faces grouped by their first cell and sorted by the second, so
+  // that a compact face's extended face is a binary search away
+  std::vector<int> efo_i(size_t(ncv) + 1, 0), efo_v(std::max(nef, 1));
+  for (int ief = 0; ief < nef; ++ief) ++efo_i[size_t(m->cvoef[2 * size_t(ief)]) + 1];
+  for (int i = 0; i < ncv; ++i) efo_i[size_t(i) + 1] += efo_i[size_t(i)];
+  {
+    std::vector<int> fill(efo_i.begin(), efo_i.end() - 1);
+    for (int ief = 0; ief < nef; ++ief) efo_v[size_t(fill[size_t(m->cvoef[2 * size_t(ief)])]++)] = ief;
+  }
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int i = 0; i < ncv; ++i)
+    std::sort(efo_v.begin() + efo_i[size_t(i)], efo_v.begin() + efo_i[size_t(i) + 1],
+              [&](int x, int y) { return m->cvoef[2 * size_t(x) + 1] < m->cvoef[2 * size_t(y) + 1]; });
+  auto find_ef = [&](int a, int b) -> int {
+    if (a < 0 || a >= ncv) return -1;
+    int lo = efo_i[size_t(a)], hi = efo_i[size_t(a) + 1];
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (m->cvoef[2 * size_t(efo_v[size_t(mid)]) + 1] < b) lo = mid + 1; else hi = mid;
+    }
+    return (lo < efo_i[size_t(a) + 1] && m->cvoef[2 * size_t(efo_v[size_t(lo)]) + 1] == b) ? efo_v[size_t(lo)] : -1;
+  };
   std::vector<int> icf_of(nef, -1);
   std::vector<signed char> cflip_of(nef, 0);
   for (int ifa = 0; ifa < nfa; ++ifa) {
     const int a = m->cvofa[2 * size_t(ifa)], b = m->cvofa[2 * size_t(ifa) + 1];
-    auto it = ef_of.find({a, b});
-    if (it != ef_of.end()) {
-      icf_of[it->second] = ifa;
-      cflip_of[it->second] = 0;
-    } else {
-      it = ef_of.find({b, a});
-      if (it == ef_of.end()) {
-        delete o;
-        return nullptr;
-      }
-      icf_of[it->second] = ifa;
-      cflip_of[it->second] = 1;
+    int ief = find_ef(a, b);
+    signed char flip = 0;
+    if (ief < 0) {
+      ief = find_ef(b, a);
+      flip = 1;
     }
+    if (ief < 0) {
+      delete o;
+      return nullptr;
+    }
+    icf_of[ief] = ifa;
+    cflip_of[ief] = flip;
   }
   // partitions: contiguous cell ranges ("ranks")
   o->parts.resize(o->nparts);
