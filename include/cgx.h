@@ -144,8 +144,6 @@ typedef struct cgx_mesh_stats {
   double e_per_cell;       /* extended faces per cell, each face once */
   double f_per_cell;       /* compact faces per cell, each face once */
   size_t device_bytes;     /* device memory held by the mesh */
-  long long n_ef_records;  /* extended-face geometry records: one per directed entry, less one
-                              per internal face whose two cells share a work item */
 } cgx_mesh_stats;
 
 /* Copy the mesh to device `device`, renumber it and build the CSR layouts. */

@@ -136,8 +136,7 @@ def mesh_desc(mesh, with_x=True):
 class MeshStats(ctypes.Structure):
     _fields_ = [("ncv", ctypes.c_int), ("n_ef_dir", ctypes.c_longlong),
                 ("n_cf_dir", ctypes.c_longlong), ("e_per_cell", ctypes.c_double),
-                ("f_per_cell", ctypes.c_double), ("device_bytes", ctypes.c_size_t),
-                ("n_ef_records", ctypes.c_longlong)]
+                ("f_per_cell", ctypes.c_double), ("device_bytes", ctypes.c_size_t)]
 
 
 EXPORTS = [

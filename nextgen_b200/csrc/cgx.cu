@@ -164,70 +164,17 @@ __device__ __forceinline__ void prefetch_entries(const TB* planes, long long str
     prefetch_l2(idx + k0, (k1 - k0) * 2);
 }
 
-// The compact entries a staged kernel reads in round `sub` of item `it`
-// (cells it.cell0 + [sub*cpr, (sub+1)*cpr)).
-template <class TB>
-__device__ __forceinline__ void prefetch_comp_round(const MeshDev& m, const TB* planes, const Item& it, int sub,
-                                                    int cpr) {
+// The entries a staged kernel reads in round `sub` of item `it` (cells
+// it.cell0 + [sub*cpr, (sub+1)*cpr)): extended (COMP false) or compact.
+template <bool COMP, class TB>
+__device__ __forceinline__ void prefetch_round(const MeshDev& m, const TB* planes, const Item& it, int sub,
+                                               int cpr) {
   const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
   if (a >= b || threadIdx.x >= 7) return;
-  prefetch_entries(planes, m.Q, m.clidx, __ldg(m.qoff + it.cell0 + a), __ldg(m.qoff + it.cell0 + b));
+  const long long* o = COMP ? m.qoff : m.off;
+  prefetch_entries(planes, COMP ? m.Q : m.E, COMP ? m.clidx : m.lidx, __ldg(o + it.cell0 + a),
+                   __ldg(o + it.cell0 + b));
 }
-
-// The streams the extended-face kernels read in round `sub` of item `it`:
-// the round's cells' own geometry records (six planes of TB-byte values,
-// threads 0..5), their entries' local indices (thread 6) and their
-// back-references (thread 7).
-template <class TB>
-__device__ __forceinline__ void prefetch_ext_round(const MeshDev& m, const TB* planes, const Item& it, int sub,
-                                                   int cpr) {
-  const int a = min(sub * cpr, it.ncell), b = min((sub + 1) * cpr, it.ncell);
-  const int t = threadIdx.x;
-  if (a >= b || t >= 8) return;
-  const int c0 = it.cell0 + a, c1 = it.cell0 + b;
-  if (t < 6) {
-    const long long r0 = __ldg(m.roff + c0), r1 = __ldg(m.roff + c1);
-    prefetch_l2(planes + t * m.R + r0, (r1 - r0) * static_cast<long long>(sizeof(TB)));
-  } else if (t == 6) {
-    const long long k0 = __ldg(m.off + c0), k1 = __ldg(m.off + c1);
-    prefetch_l2(m.lidx + k0, (k1 - k0) * 2);
-  } else {
-    const int q0 = __ldg(m.boff + c0), q1 = __ldg(m.boff + c1);
-    prefetch_l2(m.bref + q0, (long long)(q1 - q0) * 2);
-  }
-}
-
-// The geometry record of each of a cell's extended entries, as the cell's G
-// lanes take them sweep by sweep (entry k = b + j*G + lane in sweep j): an
-// entry of its own takes the cell's next record (its own records follow its
-// entries in order from roff[i]), a back-reference (bit 15 of its local
-// index) the record bref[] names within the item's records.  The positions
-// are counted with warp ballots over the group, so no per-entry record index
-// is stored.  Every lane of the warp calls next() in every sweep.
-template <int G>
-struct RecWalk {
-  long long ibase;  // the item's first record
-  int own, back;    // the cell's next own record (within the item), next back-reference
-  __device__ __forceinline__ RecWalk(const MeshDev& m, int item_cell0, bool valid, int cell) {
-    ibase = __ldg(m.roff + item_cell0);
-    own = valid ? int(__ldg(m.roff + cell) - ibase) : 0;
-    back = valid ? __ldg(m.boff + cell) : 0;
-  }
-  // w: this lane's local-index word, active: whether its entry exists
-  __device__ __forceinline__ long long next(const MeshDev& m, unsigned w, bool active, bool& is_back) {
-    const unsigned lw = threadIdx.x & 31u;
-    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lw & ~unsigned(G - 1)));
-    const unsigned below = (1u << lw) - 1u;
-    is_back = active && (w & 0x8000u);
-    const unsigned bm = __ballot_sync(0xffffffffu, is_back) & gmask;
-    const unsigned om = __ballot_sync(0xffffffffu, active && !is_back) & gmask;
-    const long long r = ibase + (is_back ? int(__ldg(m.bref + back + __popc(bm & below)))
-                                         : own + __popc(om & below));
-    own += __popc(om);
-    back += __popc(bm);
-    return r;
-  }
-};
 
 // The streams the once-per-step kernel reads in round `sub` of item `it`:
 // the extended entries' local indices, the compact entries' local indices,
@@ -526,11 +473,11 @@ __host__ __device__ constexpr int kRounds() {
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
   extern __shared__ int4 smem[];
-#define PF_EXT(it, mm, r) prefetch_ext_round(mm, mm.en, it, r, 256 / G)
+#define PF_EXT(it, mm, r) prefetch_round<false>(mm, mm.en, it, r, 256 / G)
   STAGED_LOOP_BEGIN(PF_EXT)
   stage_records<4>(smem, s.L, it_, m.hcell + it_.hoff, it_.nh);
   stage_wait();
-  const long long R = m.R;
+  const long long E = m.E;
   STAGED_ROUNDS_BEGIN(G, PF_EXT)
   long long b = 0, e = 0;
   LRec Li;
@@ -539,22 +486,14 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
     e = m.off[i + 1];
     smem_L(smem, loc_, Li);
   }
-  RecWalk<G> rw(m, it_.cell0, valid, i);
-  const int nsweep = __reduce_max_sync(0xffffffffu, int((e - b + G - 1) / G));
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int sw = 0; sw < nsweep; ++sw) {
-    const long long k = b + (long long)sw * G + lane;
-    const bool active = k < e;
-    const unsigned w = active ? __ldg(m.lidx + k) : 0u;
-    bool back;
-    const long long r = rw.next(m, w, active, back);
-    if (!active) continue;
-    const double* g = m.en + r;
-    const double sn = back ? -1.0 : 1.0;  // a back-reference reads its record from the other side
-    const double n[3] = {sn * __ldg(g), sn * __ldg(g + R), sn * __ldg(g + 2 * R)};
-    const double c[3] = {__ldg(g + 3 * R), __ldg(g + 4 * R), __ldg(g + 5 * R)};
+  for (long long k = b + lane; k < e; k += G) {
+    const int jl = __ldg(m.lidx + k);
+    const double* g = m.en + k;
+    const double n[3] = {__ldg(g), __ldg(g + E), __ldg(g + 2 * E)};
+    const double c[3] = {__ldg(g + 3 * E), __ldg(g + 4 * E), __ldg(g + 5 * E)};
     LRec Lj;
-    smem_L(smem, int(w & 0x7fffu), Lj);
+    smem_L(smem, jl, Lj);
     double F[5];
     ext_flux(F, n, c, Li, Lj);
     if (s.mf) s.mf[k] = F[0];  // mf[ief] of calcRhsBase, for calcRhsScalars
@@ -580,7 +519,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_ext(CASE_ARGS, int stage) {
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 2) k_rhs_comp(CASE_ARGS, int stage) {
   extern __shared__ int4 smem[];
-#define PF_COMP(it, mm, r) prefetch_comp_round(mm, mm.qg, it, r, 256 / G)
+#define PF_COMP(it, mm, r) prefetch_round<true>(mm, mm.qg, it, r, 256 / G)
   STAGED_LOOP_BEGIN(PF_COMP)
   const int nu = it_.ncell + it_.nch;
   int4* sV = smem + swz_chunks<4>(nu);
@@ -991,7 +930,7 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   // ---- Gibbs remainder over the extended faces (a maximum: any order)
   double vv2 = 0.0, cfl = 0.0;
   for (long long k = b + lane; k < e; k += G) {
-    const double4 qj = smem_Q(smem, __ldg(m.lidx + k) & 0x7fff);
+    const double4 qj = smem_Q(smem, __ldg(m.lidx + k));
     const double dp = qj.y - qi.y;
     const double v_avg = 0.5 * (qi.z + qj.z);
     const double beta = 0.5 * (qi.w + qj.w);
@@ -1280,22 +1219,22 @@ __global__ void k_field_in(int N, const int* __restrict__ perm, const double* __
   for (int c = 0; c < 5; ++c) field[size_t(c) * N + i] = src[5 * size_t(o) + c];
 }
 
-// Geometry planes from the per-face records: record r of the extended-face
-// geometry is face rfid[r] (bit 31: seen from the face's second cell, normal
-// negated); compact entry q = qoff[i] + t mirrors extended entry off[i] + t
-// (eofq[q]), whose face is fid[eofq[q]].  One thread per record / entry.
-__global__ void k_expand_entries(long long R, long long Q, const int* __restrict__ rfid,
-                                 const int* __restrict__ fid, const EFRec* __restrict__ ef,
-                                 const CFRec* __restrict__ cf, const long long* __restrict__ eofq,
-                                 double* __restrict__ en, double* __restrict__ qg) {
+// Per-entry geometry planes from the per-face records: entry k of the
+// extended CSR reads face fid[k] (bit 31: the cell is the face's second cell,
+// normal negated); compact entry q = qoff[i] + t mirrors extended entry
+// off[i] + t (eofq[q]).  One thread per entry.
+__global__ void k_expand_entries(long long E, long long Q, const int* __restrict__ fid,
+                                 const EFRec* __restrict__ ef, const CFRec* __restrict__ cf,
+                                 const long long* __restrict__ eofq, double* __restrict__ en,
+                                 double* __restrict__ qg) {
   const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (k < R) {
-    const int f = rfid[k];
+  if (k < E) {
+    const int f = fid[k];
     const EFRec r = ef[f & kFidMask];
     const double sg = (f < 0) ? -1.0 : 1.0;
     for (int d = 0; d < 3; ++d) {
-      en[d * R + k] = sg * r.n[d];
-      en[(3 + d) * R + k] = r.c[d];
+      en[d * E + k] = sg * r.n[d];
+      en[(3 + d) * E + k] = r.c[d];
     }
   }
   if (k < Q) {
@@ -2547,89 +2486,8 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     if (hcell.empty()) hcell.push_back(0);
     if (chcell.empty()) chcell.push_back(0);
     PT.mark("items and halos");
-    // ---- extended-face geometry records.  An internal face whose two cells
-    // lie in one work item gets one record, in the orientation of its first
-    // reader (the lower cell); the second reader's entry refers back to it
-    // (bit 15 of its local index set, n negated when read).  Every other
-    // entry has a record of its own.  A cell's own records follow its entries
-    // in order, from roff[i]; its back-references' targets are
-    // bref[boff[i] + t] (the t-th back-reference, record offset within the
-    // item's records).
-    std::vector<unsigned char> face_internal;
-    {
-      face_internal.assign(std::max(nef, 1), 0);
-#pragma omp parallel for schedule(static)
-      for (int f = 0; f < nef; ++f) face_internal[fnew[f]] = (d->cvoef[2 * size_t(f) + 1] < N) ? 1 : 0;
-    }
-    std::vector<long long> roff(size_t(N) + 1, 0);
-    std::vector<int> boff(size_t(N) + 1, 0);
-    std::vector<int> item_of_cell(N);
-    for (size_t t = 0; t < items.size(); ++t)
-      for (int i = items[t].cell0; i < items[t].cell0 + items[t].ncell; ++i) item_of_cell[i] = int(t);
-    auto is_backref = [&](int i, long long k) {
-      const int f = e_fid[k] & kFidMask;
-      const int j = e_nbr[k];
-      if (!face_internal[f] || j >= i) return false;
-      const Item& it = items[item_of_cell[i]];
-      return j >= it.cell0;
-    };
-    // pass 1: records and back-references per cell
-#pragma omp parallel for schedule(dynamic, 4096)
-    for (int i = 0; i < N; ++i) {
-      int nb = 0;
-      for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) nb += is_backref(i, k) ? 1 : 0;
-      roff[size_t(i) + 1] = (cell_off[i + 1] - cell_off[i]) - nb;
-      boff[size_t(i) + 1] = nb;
-    }
-    for (int i = 0; i < N; ++i) {
-      roff[size_t(i) + 1] += roff[size_t(i)];
-      boff[size_t(i) + 1] += boff[size_t(i)];
-    }
-    const long long Rn = roff[N];
-    uvec<long long> rec_of_entry(std::max(cell_off[N], 1LL));
-    uvec<int> rec_fid(std::max(Rn, 1LL));
-    std::vector<unsigned short> bref(std::max(boff[N], 1), 0);
-    int bad_ref = 0;
-    // pass 2, per item (cells in order, so a first reader's record exists
-    // before its second reader refers to it)
-#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad_ref)
-    for (long long t = 0; t < (long long)items.size(); ++t) {
-      const Item& it = items[size_t(t)];
-      const long long base = roff[it.cell0];
-      for (int i = it.cell0; i < it.cell0 + it.ncell; ++i) {
-        long long r = roff[i];
-        int bq = boff[i];
-        for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
-          if (!is_backref(i, k)) {
-            rec_of_entry[k] = r;
-            rec_fid[r] = e_fid[k];
-            ++r;
-            continue;
-          }
-          // the first reader's entry of the same face (its entries are
-          // ordered by face id)
-          const int f = e_fid[k] & kFidMask, j = e_nbr[k];
-          long long lo = cell_off[j], hi = cell_off[j + 1];
-          while (lo < hi) {
-            const long long mid = (lo + hi) / 2;
-            if ((e_fid[mid] & kFidMask) < f) lo = mid + 1; else hi = mid;
-          }
-          const long long tgt = (lo < cell_off[j + 1] && (e_fid[lo] & kFidMask) == f) ? rec_of_entry[lo] - base : -1;
-          if (tgt < 0 || tgt > 0xffff || lidx[k] >= 0x8000) {
-            bad_ref = 1;
-            continue;
-          }
-          rec_of_entry[k] = base + tgt;
-          bref[bq++] = (unsigned short)tgt;
-          lidx[k] = (unsigned short)(lidx[k] | 0x8000);
-        }
-      }
-    }
-    if (bad_ref) return bail(fail(CGX_E_ARG, "cgx_mesh_create: a work item's geometry records exceed 16-bit offsets"));
-    uvec<long long>().swap(rec_of_entry);
-    PT.mark("geometry records");
     // ---- upload; the per-face records are expanded on the device into the
-    // record planes and then released
+    // per-entry planes and then released
     size_t* acc = &M->bytes;
     int rc;
     const long long E = cell_off[N];
@@ -2668,12 +2526,6 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     UP(d_ivol, inv_vol);
     UP(d_cc, cc);
     UP(M->d_perm, perm);
-    long long* d_roff;
-    int* d_boff;
-    unsigned short* d_bref;
-    UP(d_roff, roff);
-    UP(d_boff, boff);
-    UP(d_bref, bref);
     int *d_bfc = nullptr, *d_bcell = nullptr, *d_bfz = nullptr;
     double *d_bfn = nullptr, *d_bfa = nullptr;
     if (nbf > 0) {
@@ -2684,7 +2536,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       UP(d_bfa, bf_aod);
     }
 #undef UP
-    if ((rc = dalloc(&d_en, 6 * size_t(std::max(Rn, 1LL)), acc))) return bail(rc);
+    if ((rc = dalloc(&d_en, 6 * size_t(std::max(E, 1LL)), acc))) return bail(rc);
     M->allocs.push_back(d_en);
     if ((rc = dalloc(&d_qg, 6 * size_t(std::max(Qn, 1LL)), acc))) return bail(rc);
     M->allocs.push_back(d_qg);
@@ -2693,26 +2545,23 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       for (int i = 0; i < N; ++i)
         for (int t = 0; t < ncomp[i]; ++t) eofq[qoff[i] + t] = cell_off[i] + t;
       int* t_fid = nullptr;
-      int* t_rfid = nullptr;
       EFRec* t_ef = nullptr;
       CFRec* t_cf = nullptr;
       long long* t_eofq = nullptr;
       auto free_tmp = [&] {
         cudaFree(t_fid);
-        cudaFree(t_rfid);
         cudaFree(t_ef);
         cudaFree(t_cf);
         cudaFree(t_eofq);
       };
-      if ((rc = dupload(&t_fid, e_fid, nullptr, &stage)) || (rc = dupload(&t_rfid, rec_fid, nullptr, &stage)) ||
-          (rc = dupload(&t_ef, efr, nullptr, &stage)) || (rc = dupload(&t_cf, cfr, nullptr, &stage)) ||
-          (rc = dupload(&t_eofq, eofq, nullptr, &stage))) {
+      if ((rc = dupload(&t_fid, e_fid, nullptr, &stage)) || (rc = dupload(&t_ef, efr, nullptr, &stage)) ||
+          (rc = dupload(&t_cf, cfr, nullptr, &stage)) || (rc = dupload(&t_eofq, eofq, nullptr, &stage))) {
         free_tmp();
         return bail(rc);
       }
-      const long long nmax = std::max(Rn, Qn);
+      const long long nmax = std::max(E, Qn);
       if (nmax > 0)
-        k_expand_entries<<<int((nmax + 255) / 256), 256>>>(Rn, Qn, t_rfid, t_fid, t_ef, t_cf, t_eofq, d_en, d_qg);
+        k_expand_entries<<<int((nmax + 255) / 256), 256>>>(E, Qn, t_fid, t_ef, t_cf, t_eofq, d_en, d_qg);
       const cudaError_t ke = cudaGetLastError();
       const cudaError_t se = cudaDeviceSynchronize();
       free_tmp();
@@ -2725,11 +2574,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     md.N = N;
     md.nitems = int(items.size());
     md.E = E;
-    md.R = Rn;
     md.Q = Qn;
-    md.roff = d_roff;
-    md.boff = d_boff;
-    md.bref = d_bref;
     md.items = d_items;
     md.hcell = d_hcell;
     md.chcell = d_chcell;
@@ -2767,7 +2612,6 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     M->stats.ncv = N;
     M->stats.n_ef_dir = n_ef_dir;
     M->stats.n_cf_dir = n_cf_dir;
-    M->stats.n_ef_records = Rn;
     int nef_i = 0, nfa_i = 0;
     for (int f = 0; f < nef; ++f) nef_i += (d->cvoef[2 * size_t(f) + 1] < N);
     for (int f = 0; f < nfa; ++f) nfa_i += (d->cvofa[2 * size_t(f) + 1] < N);
@@ -2863,7 +2707,7 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
       float *en32, *qg32, *gx32, *gy32, *gz32;
       size_t* mb = &m->bytes;
       const MeshDev& md = m->md;
-      if ((rc = dalloc(&en32, 6 * size_t(std::max(md.R, 1LL)), mb))) return bail(rc);
+      if ((rc = dalloc(&en32, 6 * size_t(std::max(md.E, 1LL)), mb))) return bail(rc);
       m->allocs.push_back(en32);
       if ((rc = dalloc(&qg32, 6 * size_t(std::max(md.Q, 1LL)), mb))) return bail(rc);
       m->allocs.push_back(qg32);
@@ -2873,8 +2717,8 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
       m->allocs.push_back(gy32);
       if ((rc = dalloc(&gz32, m->nc_dir, mb))) return bail(rc);
       m->allocs.push_back(gz32);
-      const long long nmax = std::max(6 * md.R, std::max(6 * md.Q, m->nc_dir));
-      k_geom32<<<int((nmax + 255) / 256), 256, 0, s->stream>>>(6 * md.R, 6 * md.Q, m->nc_dir, md.en, md.qg,
+      const long long nmax = std::max(6 * md.E, std::max(6 * md.Q, m->nc_dir));
+      k_geom32<<<int((nmax + 255) / 256), 256, 0, s->stream>>>(6 * md.E, 6 * md.Q, m->nc_dir, md.en, md.qg,
                                                                md.gcx, md.gcy, md.gcz, en32, qg32, gx32,
                                                                gy32, gz32);
       if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s->stream) != cudaSuccess)
@@ -3673,7 +3517,7 @@ size_t solver_bytes(long long N, long long nitems, cgx_precision prec) {
 }
 
 size_t mesh32_bytes(const cgx_mesh* m) {
-  return 6 * size_t(std::max(m->md.R, 1LL)) * sizeof(float) + 6 * size_t(std::max(m->md.Q, 1LL)) * sizeof(float) +
+  return 6 * size_t(std::max(m->md.E, 1LL)) * sizeof(float) + 6 * size_t(std::max(m->md.Q, 1LL)) * sizeof(float) +
          size_t(m->nc_dir) * 3 * sizeof(float);
 }
 
@@ -3754,6 +3598,10 @@ int batch_rebuild(cgx_batch* b) {
     CK(cudaMalloc(&b->d_items, size_t(cap) * sizeof(Item)));
     CK(cudaMallocHost(&b->h_items, size_t(cap) * sizeof(Item)));
     b->item_cap = cap;
+    // one CTA per slot of the list, as the single-case path launches one per
+    // item: CTAs past the current item count return at once, and the grid
+    // changes only with the capacity, when the graph is captured again
+    b->run.grid = std::max(b->grid, cap);
     batch_free_graph(b);  // the graph holds the old work-list pointer
   }
   CK(cudaEventSynchronize(b->staged));  // previous staging copy done

@@ -18,13 +18,10 @@
 //   first, then the halo in list order).
 //   Extended-face entries: a CSR over cells (off[N+1]) of directed entries,
 //   one per (cell, face) pair, a cell's compact faces first.  Per entry: the
-//   local index lidx[k] and the global neighbour nbr[k].  Their geometry is
-//   in records of six FP64 planes en[d*R + r] {normal (n[3]) along the
-//   record's reader, the halved c vector (c[3])}: an internal face whose two
-//   cells share a work item has one record, read by its first cell in
-//   stream order and by its second through a back-reference (bit 15 of
-//   lidx, normal negated); every other entry has its own record.  A cell's
-//   own records are consecutive from roff[i], so its G lanes stream them.
+//   local index lidx[k], the global neighbour nbr[k] and six FP64 planes
+//   en[d*E + k] {normal along the entry (n[3], negated for the face's second
+//   cell), the halved c vector (c[3])}, streamed contiguously by the cell's G
+//   lanes.
 //   Compact-face entries: the first ncomp(i) = qoff[i+1]-qoff[i] extended
 //   entries of each cell; their local indices in the compact union clidx[q]
 //   and six FP64 planes qg[d*Q + q] {unit normal along the entry (3), area,
@@ -149,7 +146,6 @@ struct MeshDev {
   int N;                        // owned cells
   int nitems;                   // work items (mesh order)
   long long E;                  // directed extended entries
-  long long R;                  // extended-face geometry records (en plane stride)
   long long Q;                  // directed compact entries
   const Item* items;            // [nitems]
   const int* hcell;             // extended-face halos
@@ -157,13 +153,9 @@ struct MeshDev {
   const long long* off;         // [N+1] extended-entry CSR
   const long long* qoff;        // [N+1] compact-entry CSR
   const int* nbr;               // [E] neighbour (new numbering, ghosts -> owner)
-  const unsigned short* lidx;   // [E] neighbour in the item's extended union (bits 0-14);
-                                // bit 15: the entry refers back to another's record
-  const long long* roff;        // [N+1] each cell's own geometry records
-  const int* boff;              // [N+1] each cell's back-references in bref
-  const unsigned short* bref;   // record of each back-reference, within its item's records
+  const unsigned short* lidx;   // [E] neighbour in the item's extended union
   const unsigned short* clidx;  // [Q] neighbour in the item's compact union
-  const double* en;             // [6][R] n (along the record's first reader), c/2
+  const double* en;             // [6][E] n (along the entry), c/2
   const double* qg;             // [6][Q] unit normal, area, aod, delta
   const long long* coff;        // [N+1] gradient CSR (cvocv without the diagonal)
   const int* cnbr;              // [C_dir]
@@ -183,7 +175,7 @@ struct MeshDev {
   const double* bf_aod;         // [nbf] area_over_delta_bf
   const int* bf_zone;           // [nbf]
   // FP32 copies for the mixed-precision form (null until a mixed solver exists)
-  const float* en32;            // [6][R]
+  const float* en32;            // [6][E]
   const float* qg32;            // [6][Q]
   const float* gcx32;
   const float* gcy32;

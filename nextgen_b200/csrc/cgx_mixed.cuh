@@ -169,11 +169,11 @@ __device__ __forceinline__ void compact_flux_add_f(FluxF& F, const float un_[3],
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
   extern __shared__ int4 smem[];
-#define PF_EXTF(it, mm, r) prefetch_ext_round(mm, mm.en32, it, r, 256 / G)
+#define PF_EXTF(it, mm, r) prefetch_round<false>(mm, mm.en32, it, r, 256 / G)
   STAGED_LOOP_BEGIN(PF_EXTF)
   stage_records<2>(smem, s.LF, it_, m.hcell + it_.hoff, it_.nh);
   stage_wait();
-  const long long R = m.R;
+  const long long E = m.E;
   const double h_ref = CASE_PH.h_ref;
   STAGED_ROUNDS_BEGIN(G, PF_EXTF)
   long long b = 0, e = 0;
@@ -183,22 +183,14 @@ __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
     e = m.off[i + 1];
     smem_LF(smem, loc_, Li);
   }
-  RecWalk<G> rw(m, it_.cell0, valid, i);
-  const int nsweep = __reduce_max_sync(0xffffffffu, int((e - b + G - 1) / G));
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int sw = 0; sw < nsweep; ++sw) {
-    const long long k = b + (long long)sw * G + lane;
-    const bool active = k < e;
-    const unsigned w = active ? __ldg(m.lidx + k) : 0u;
-    bool back;
-    const long long r = rw.next(m, w, active, back);
-    if (!active) continue;
-    const float* g = m.en32 + r;
-    const float sn = back ? -1.0f : 1.0f;  // a back-reference reads its record from the other side
-    const float n[3] = {sn * __ldg(g), sn * __ldg(g + R), sn * __ldg(g + 2 * R)};
-    const float c[3] = {__ldg(g + 3 * R), __ldg(g + 4 * R), __ldg(g + 5 * R)};
+  for (long long k = b + lane; k < e; k += G) {
+    const int jl = __ldg(m.lidx + k);
+    const float* g = m.en32 + k;
+    const float n[3] = {__ldg(g), __ldg(g + E), __ldg(g + 2 * E)};
+    const float c[3] = {__ldg(g + 3 * E), __ldg(g + 4 * E), __ldg(g + 5 * E)};
     LRecF Lj;
-    smem_LF(smem, int(w & 0x7fffu), Lj);
+    smem_LF(smem, jl, Lj);
     float F[5];
     ext_flux_f(F, n, c, Li, Lj);
     if (s.mf) s.mf[k] = double(F[0]);  // mass flux for calcRhsScalars
@@ -222,7 +214,7 @@ __global__ void __launch_bounds__(256, 4) k_rhs_ext_f(CASE_ARGS, int stage) {
 template <int G, bool DIRECT>
 __global__ void __launch_bounds__(256, 3) k_rhs_comp_f(CASE_ARGS, int stage) {
   extern __shared__ int4 smem[];
-#define PF_COMPF(it, mm, r) prefetch_comp_round(mm, mm.qg32, it, r, 256 / G)
+#define PF_COMPF(it, mm, r) prefetch_round<true>(mm, mm.qg32, it, r, 256 / G)
   STAGED_LOOP_BEGIN(PF_COMPF)
   const int nu = it_.ncell + it_.nch;
   int4* sV = smem + swz_chunks<2>(nu);
@@ -423,7 +415,7 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   float vv2 = 0.0f;
   double cfl = 0.0;
   for (long long k = b + lane; k < e; k += G) {
-    const float4 qj = reinterpret_cast<const float4*>(smem)[__ldg(m.lidx + k) & 0x7fff];
+    const float4 qj = reinterpret_cast<const float4*>(smem)[__ldg(m.lidx + k)];
     const float dp = qj.y - qi.y;
     const float v_avg = 0.5f * (qi.z + qj.z);
     const float beta = 0.5f * (qi.w + qj.w);
