@@ -89,6 +89,9 @@ typedef struct cgx_params {
   int    dt_mode;          /* CGX_DT_* */
   double dt_data[2];       /* DT: {dt}; CFL: {cfl}; CFL_DT: {cfl, dt_max} */
   int    check_interval;   /* CHECK_INTERVAL (NaN store cadence) */
+  int    limit_asgs;       /* LIMIT_ASGS: cap a_sgs at 1/(4 dt fax sos^2), fax = 1/(gamma-1) +
+                              |u|^2/(2 sos^2), once dt > 0 (limitAsgs,
+                              IdealGasSolverSgs.cpp:4-48); 0 = off, the default */
 } cgx_params;
 
 /* Fill with the reference's defaults (P_REF, RHO_REF, T_REF, MU_REF = 1). */

@@ -43,6 +43,7 @@ class Params(ctypes.Structure):
         ("coeff_p", ctypes.c_double), ("coeff_h", ctypes.c_double), ("gr_nrm", ctypes.c_double),
         ("diss_mode", ctypes.c_int), ("dt_mode", ctypes.c_int),
         ("dt_data", ctypes.c_double * 2), ("check_interval", ctypes.c_int),
+        ("limit_asgs", ctypes.c_int),
     ]
 
     def __init__(self, **kw):
@@ -70,6 +71,7 @@ class Params(ctypes.Structure):
         self.dt_data[0] = 0.8
         self.dt_data[1] = 0.0
         self.check_interval = 1
+        self.limit_asgs = 0
         for k, v in kw.items():
             setattr(self, k, v)
 

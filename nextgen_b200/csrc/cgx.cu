@@ -796,6 +796,7 @@ __device__ __noinline__ void finalize_ctl(Ctl* ctl, const double* red, int dt_mo
     if (fin_nan[0]) c->nan = 1;
     if (mode & 1) {
       c->dt_last = c->dt;
+      c->dt_sgs = c->dt;
       c->time += c->dt;
       c->step += 1;
     }
@@ -814,10 +815,11 @@ __device__ __noinline__ void finalize_ctl(Ctl* ctl, const double* red, int dt_mo
 }
 
 // computeSgsVreman + calcSgsAndMaterialProperties + setFgrCvs for cell i
-// (its packed state Li, its Gibbs maximum vv2); writes the cell's lagged
-// properties and returns whether rho, p or T is NaN.
+// (its packed state Li, its Gibbs maximum vv2; dt the solver's dt for
+// limitAsgs); writes the cell's lagged properties and returns whether rho,
+// p or T is NaN.
 __device__ __forceinline__ int cell_props(const Phys& ph, const MeshDev& m, const StateDev& s, int i,
-                                          const LRec& Li, double vv2) {
+                                          const LRec& Li, double vv2, double dt) {
   double g[9];
   load_Vg(s.V, i, g);
   // {dx, dx2_approx, dcmag_hat, sa_to_vol}
@@ -856,6 +858,15 @@ __device__ __forceinline__ int cell_props(const Phys& ph, const MeshDev& m, cons
       a_sgs += ph.a_sgs_coeff2 * cc23.y * fmin(Masq, 10.0) * sos;
     }
     a_sgs *= inv_sos2;
+    // limitAsgs (IdealGasSolverSgs.cpp:4-48): with LIMIT_ASGS and dt > 0, a
+    // ceiling that keeps the acoustic SGS term inside the explicit viscous
+    // stability limit (cfl_visc = 1)
+    if (ph.limit_asgs && dt > 0.0) {
+      const double usq = Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2];
+      const double fax = ph.invgm1 + 0.5 * usq * inv_sos2;
+      const double ceil_a = 1.0 / (dt * fax * 4.0) * inv_sos2;
+      if (a_sgs > ceil_a) a_sgs = ceil_a;
+    }
     loc_sgs = ph.lambda_dil_coeff * rho * fabs(dil) * dx2;
     loc_sgs += mu_sgs * (1.0 / ph.Pr_t);
   }
@@ -913,6 +924,8 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   stage_records<4>(sL, s.L, it_, m.chcell + it_.choff, it_.nch);
   stage_wait();
   const long long Q = m.Q;
+  // limitAsgs's dt: this step's, or outside a step the control block's
+  const double dt_sgs = (mode & 1) ? s.ctl->dt : s.ctl->dt_sgs;
   double cmax = 0.0;
   int anynan = 0;
   STAGED_ROUNDS_BEGIN(G, PF_END)
@@ -952,7 +965,7 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   vv2 = group_max<G>(vv2);
   cfl = group_sum<G>(cfl);
   if (valid && lane == 0) {
-    anynan |= cell_props(ph, m, s, i, Li, vv2);
+    anynan |= cell_props(ph, m, s, i, Li, vv2, dt_sgs);
     cfl += cfl_bf(m, i, Li.u[0], Li.u[1], Li.u[2], Li.sos);
     cmax = fmax(cmax, cfl * (0.5 * 1.0 * __ldg(m.inv_vol + i)));
   }
@@ -2055,6 +2068,7 @@ extern "C" void cgx_params_default(cgx_params* p) {
   p->dt_data[0] = 0.8;
   p->dt_data[1] = 0.0;
   p->check_interval = 1;
+  p->limit_asgs = 0;
 }
 
 extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** out) {
@@ -2673,6 +2687,8 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   ph.dt_mode = p->dt_mode;
   ph.dt_max = p->dt_data[1];
   ph.h_ref = ph.R * p->gamma / (p->gamma - 1.0) * p->T_ref;
+  ph.limit_asgs = p->limit_asgs;
+  ph.invgm1 = 1.0 / (p->gamma - 1.0);
   const size_t N = m->N;
   s->nblocks = int((N + kBlock - 1) / kBlock);
   s->nitems = m->md.nitems;

@@ -113,6 +113,8 @@ struct Phys {
   int dt_mode;
   double dt_max;  // CFL_DT
   double h_ref;   // R gamma/(gamma-1) T_ref (mixed-precision offsets)
+  int limit_asgs; // LIMIT_ASGS
+  double invgm1;  // 1/(gamma-1)
 };
 
 // Device-resident control block (one per solver).
@@ -122,6 +124,9 @@ struct Ctl {
   double time;
   double dt_data0;   // DT value or CFL target
   double cfl_max;    // last calcCfl(NULL, 1.0)
+  double dt_sgs;     // the reference's `dt` for properties computed outside a
+                     // step: 0 until a step runs, then the last step's dt (kept
+                     // through a restore, as restoreData keeps it)
   int step;
   int nan;           // NaN seen in rho, p or T since last reset
   unsigned int blocks_done;

@@ -316,10 +316,10 @@ __global__ void __launch_bounds__(256) k_grad_f(CASE_ARGS) {
 #undef PF_GRADF
 }
 
-// cell_props in FP32 (SGS, properties and the sensor function); returns
-// whether rho, p or T is NaN.
+// cell_props in FP32 (SGS, properties and the sensor function; dt the
+// solver's dt for limitAsgs); returns whether rho, p or T is NaN.
 __device__ __forceinline__ int cell_props_f(const Phys& ph, const MeshDev& m, const StateDev& s, int i,
-                                            const LRecF& Li, float vv2) {
+                                            const LRecF& Li, float vv2, double dt) {
   float g[9];
   {
     const float* vg = s.VF[i].g;
@@ -361,6 +361,13 @@ __device__ __forceinline__ int cell_props_f(const Phys& ph, const MeshDev& m, co
       a_sgs += float(ph.a_sgs_coeff2) * float(cc23.y) * fminf(Masq, 10.0f) * sos;
     }
     a_sgs *= inv_sos2;
+    // limitAsgs (IdealGasSolverSgs.cpp:4-48)
+    if (ph.limit_asgs && dt > 0.0) {
+      const float usq = Li.u[0] * Li.u[0] + Li.u[1] * Li.u[1] + Li.u[2] * Li.u[2];
+      const float fax = float(ph.invgm1) + 0.5f * usq * inv_sos2;
+      const float ceil_a = 1.0f / (float(dt) * fax * 4.0f) * inv_sos2;
+      if (a_sgs > ceil_a) a_sgs = ceil_a;
+    }
     loc_sgs = float(ph.lambda_dil_coeff) * rho * fabsf(dil) * dx2;
     loc_sgs += mu_sgs * float(1.0 / ph.Pr_t);
   }
@@ -398,6 +405,8 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   stage_records<2>(sL, s.LF, it_, m.chcell + it_.choff, it_.nch);
   stage_wait();
   const long long Q = m.Q;
+  // limitAsgs's dt: this step's, or outside a step the control block's
+  const double dt_sgs = (mode & 1) ? s.ctl->dt : s.ctl->dt_sgs;
   double cmax = 0.0;
   int anynan = 0;
   STAGED_ROUNDS_BEGIN(G, PF_ENDF)
@@ -437,7 +446,7 @@ __global__ void __launch_bounds__(256) k_step_end_f(CASE_ARGS, int mode) {
   for (int o = G / 2; o > 0; o >>= 1) vv2 = fmaxf(vv2, __shfl_xor_sync(0xffffffffu, vv2, o));
   cfl = group_sum<G>(cfl);
   if (valid && lane == 0) {
-    anynan |= cell_props_f(ph, m, s, i, Li, vv2);
+    anynan |= cell_props_f(ph, m, s, i, Li, vv2, dt_sgs);
     cfl += cfl_bf(m, i, double(Li.u[0]), double(Li.u[1]), double(Li.u[2]), double(Li.sos));
     cmax = fmax(cmax, cfl * (0.5 * 1.0 * __ldg(m.inv_vol + i)));
   }
