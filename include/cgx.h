@@ -249,6 +249,33 @@ int cgx_set_source_hook(cgx_solver* s, cgx_source_hook fn, void* user);
 #define CGX_BC_WALL_ADIABATIC  2
 int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
 
+/*
+ * Boundary conditions that take the reference's zone parameters, in the
+ * order its input line gives them after the type name (params may be NULL
+ * when nparams is 0):
+ *   CGX_BC_SLIP             -
+ *   CGX_BC_WALL_ADIABATIC   [u0 u1 u2]   (the TRANSLATE velocity)
+ *   CGX_BC_WALL_ISOTHERMAL  T            WALL_ISOTHERMAL: tau = mu_lam
+ *                           area_over_delta_bf u, q = loc_lam
+ *                           area_over_delta_bf cp (T - T_bc); rhs.rhou -= p n_bf +
+ *                           tau, rhs.rhoE -= q (WallIsothermal, IdealGasSolverBcs.cpp:1480-1510)
+ *   CGX_BC_CBC_UPT          u0 u1 u2 p T (CbcUpt::initData, IdealGasSolverBcs.cpp:3182-3207)
+ *   CGX_BC_CBC_RUNP         rho un p     inflow speed un against n_bf (CbcRunp::initData, :3242-3266)
+ *   CGX_BC_CBC_MPT          mdot p T     mass flow rate into the zone over its whole area
+ *                           (CbcMpt::initData, :3209-3240)
+ * The CBC zones add the HLLC Riemann flux between the cell's state and the
+ * zone's boundary state (Cbc::addBoundaryFlux, IdealGasSolverBcs.cpp:2960-2976;
+ * calcRiemannFlux, IdealGasSolverFlux.hpp:218-306).  CBC zones carry no
+ * transport scalars: cgx_init_complete refuses a solver that has both.
+ * Returns CGX_E_ARG for an unknown kind, a zone out of range or a wrong
+ * parameter count.
+ */
+#define CGX_BC_WALL_ISOTHERMAL 3
+#define CGX_BC_CBC_UPT         4
+#define CGX_BC_CBC_RUNP        5
+#define CGX_BC_CBC_MPT         6
+int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
+
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */
 int cgx_init_complete(cgx_solver* s);

@@ -149,11 +149,15 @@ EXPORTS = [
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
-    "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc",
+    "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params",
 ]
 
 CGX_BC_SLIP = 1
 CGX_BC_WALL_ADIABATIC = 2
+CGX_BC_WALL_ISOTHERMAL = 3
+CGX_BC_CBC_UPT = 4
+CGX_BC_CBC_RUNP = 5
+CGX_BC_CBC_MPT = 6
 
 
 class Source(ctypes.Structure):
@@ -210,6 +214,7 @@ def lib():
         "cgx_set_scalars": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
         "cgx_set_source": (ctypes.c_int, [vp, ctypes.POINTER(Source)]),
         "cgx_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
+        "cgx_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
         "cgx_get_rhs_sc": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
@@ -330,6 +335,13 @@ class Solver:
         CGX_BC_WALL_ADIABATIC (u_wall: the wall velocity, zero if None)."""
         uw = None if u_wall is None else np.ascontiguousarray(u_wall, dtype=np.float64)
         _check(lib().cgx_set_bc(self.h, int(zone), int(kind), _dp(uw)))
+
+    def set_bc_params(self, zone, kind, params=()):
+        """Boundary condition with the reference's zone parameters in input
+        order: WALL_ISOTHERMAL (T), CBC_UPT (u0 u1 u2 p T), CBC_RUNP
+        (rho un p), CBC_MPT (mdot p T); SLIP and WALL_ADIABATIC as set_bc."""
+        a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+        _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))
 
     # -- source terms (addSourceHook) ----------------------------------------
     def set_source(self, A=0.0, g=(0.0, 0.0, 0.0), field=None):

@@ -63,6 +63,9 @@ constexpr int kMaxRounds = 16;  // most rounds per item of a once-per-step kerne
 // staged face kernels: 64 B per extended-face neighbour record, 192 B per
 // compact-face one)
 constexpr int kMaxUnionExt = 3000;
+// most extended entries of one item: the once-per-step kernel stages the
+// item's local indices (2 B each) in shared memory beside its records
+constexpr int kMaxItemEntries = 16384;
 constexpr int kMaxUnionComp = 1100;
 constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) + step_end
 
@@ -184,8 +187,9 @@ __device__ __forceinline__ void prefetch_end(const MeshDev& m, const Item& it, i
   const int t = threadIdx.x;
   if (a >= b || t >= 6) return;
   if (t == 0) {
-    const long long k0 = __ldg(m.off + it.cell0 + a), k1 = __ldg(m.off + it.cell0 + b);
-    prefetch_l2(m.lidx + k0, (k1 - k0) * 2);
+    // the whole item's local indices, staged when the item starts
+    if (sub == 0)
+      prefetch_l2(m.lidx + __ldg(m.off + it.cell0), (__ldg(m.off + it.cell0 + it.ncell) - __ldg(m.off + it.cell0)) * 2);
     return;
   }
   const long long q0 = __ldg(m.qoff + it.cell0 + a), q1 = __ldg(m.qoff + it.cell0 + b);
@@ -193,6 +197,23 @@ __device__ __forceinline__ void prefetch_end(const MeshDev& m, const Item& it, i
     prefetch_l2(m.clidx + q0, (q1 - q0) * 2);
   else
     prefetch_l2(m.qg + (t - 1) * m.Q + q0, (q1 - q0) * 8);
+}
+
+// 16-byte chunks holding the local indices of n consecutive extended entries
+// copied from the 16-byte boundary at or below the first
+__host__ __device__ constexpr int idx_chunks(int n) { return (n + 7) / 8 + 1; }
+
+// Copy an item's extended-entry local indices lidx[e0, e1) into shared
+// memory from the 16-byte boundary ea = e0 & ~7 (the array is padded by 8
+// entries, so the last chunk stays inside it): entry k sits at sidx[k - ea].
+// Asynchronous: complete with stage_wait().
+__device__ __forceinline__ void stage_lidx(int4* sidx, const unsigned short* __restrict__ lidx, long long e0,
+                                           long long e1) {
+  const long long ea = e0 & ~7LL;
+  const int n = int((e1 - ea + 7) >> 3);
+  const int4* src = reinterpret_cast<const int4*>(lidx + ea);
+  for (int x = threadIdx.x; x < n; x += blockDim.x) cp_async16(sidx + x, src + x);
+  asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // the gradient kernel's streams: local indices and three coefficient planes
@@ -910,7 +931,7 @@ __device__ __forceinline__ double cfl_bf(const MeshDev& m, int i, double u0, dou
 // item of a case reduces them in item order and updates the control block.
 // mode bit 0: advance time/step by the dt just used; bit 1: set dt from CFL.
 template <int G, bool DIRECT>
-__global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
+__global__ void __launch_bounds__(256, 3) k_step_end(CASE_ARGS, int mode) {
   extern __shared__ int4 smem[];
   __shared__ double sh_cfl[256];
   __shared__ int sh_nan[256];
@@ -920,8 +941,12 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   const Phys& ph = CASE_PH;
   const int nu = it_.ncell + it_.nh;
   int4* sL = smem + swz_chunks<2>(nu);
+  int4* sI = sL + swz_chunks<4>(it_.ncell + it_.nch);
+  const long long ea = m.off[it_.cell0] & ~7LL;
+  const unsigned short* sIdx = reinterpret_cast<const unsigned short*>(sI);  // entry k at [k - ea]
   stage_records<2>(smem, s.Q, it_, m.hcell + it_.hoff, it_.nh);
   stage_records<4>(sL, s.L, it_, m.chcell + it_.choff, it_.nch);
+  stage_lidx(sI, m.lidx, m.off[it_.cell0], m.off[it_.cell0 + it_.ncell]);
   stage_wait();
   const long long Q = m.Q;
   // limitAsgs's dt: this step's, or outside a step the control block's
@@ -943,7 +968,7 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
   // ---- Gibbs remainder over the extended faces (a maximum: any order)
   double vv2 = 0.0, cfl = 0.0;
   for (long long k = b + lane; k < e; k += G) {
-    const double4 qj = smem_Q(smem, __ldg(m.lidx + k));
+    const double4 qj = smem_Q(smem, sIdx[k - ea]);
     const double dp = qj.y - qi.y;
     const double v_avg = 0.5 * (qi.z + qj.z);
     const double beta = 0.5 * (qi.w + qj.w);
@@ -1000,17 +1025,86 @@ __global__ void __launch_bounds__(256) k_step_end(CASE_ARGS, int mode) {
 
 #include "cgx_mixed.cuh"
 
-// addBoundaryFlux of the boundary zones (IdealGasSolverBcs.cpp:14-48), one
-// thread per cell with boundary faces, added to one stage's rhs after the
-// face sums:
-//   SLIP            rhs.rhou -= p n_bf
+// A state as the boundary Riemann flux reads it (the reference's
+// IdealGasState: velocity, specific volume, pressure, enthalpy)
+struct RiemannState {
+  double u[3], sp_vol, p, h;
+};
+
+// HLLC flux (Toro, Spruce and Speares 1994) through a boundary face of area
+// vector n, from the cell's state a to the boundary state b, with the wave
+// speeds bounded by the Roe averages (Einfeldt 1988, Batten et al. 1997):
+// the flux the reference's calcRiemannFlux forms (IdealGasSolverFlux.hpp:
+// 218-306) with one gamma.  F = {rho, rhou[3], rhoE} times the face area.
+__device__ void hllc_flux(double F[5], const double n[3], const RiemannState& a, const RiemannState& b,
+                          double gamma) {
+  const double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  const double nh[3] = {n[0] / area, n[1] / area, n[2] / area};
+  // each side's normal velocity, |u|^2, sound speed, density and rho E
+  double un[2], uu[2], cs[2], rho[2], E[2];
+  const RiemannState* st[2] = {&a, &b};
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const RiemannState& q = *st[k];
+    un[k] = q.u[0] * nh[0] + q.u[1] * nh[1] + q.u[2] * nh[2];
+    uu[k] = q.u[0] * q.u[0] + q.u[1] * q.u[1] + q.u[2] * q.u[2];
+    cs[k] = sqrt(gamma * q.p * q.sp_vol);
+    rho[k] = 1.0 / q.sp_vol;
+    E[k] = rho[k] * (q.h + 0.5 * uu[k]) - q.p;
+  }
+  // Roe-averaged velocity and sound speed
+  const double w = sqrt(rho[1] / rho[0]);
+  const double iw = 1.0 / (1.0 + w);
+  double ur[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ur[d] = iw * (a.u[d] + b.u[d] * w);
+  const double un_r = ur[0] * nh[0] + ur[1] * nh[1] + ur[2] * nh[2];
+  const double gh = iw * ((gamma * a.p / rho[0] + 0.5 * (gamma - 1.0) * uu[0]) +
+                          (gamma * b.p / rho[1] + 0.5 * (gamma - 1.0) * uu[1]) * w);
+  const double c_r = sqrt(gh - (gamma - 1.0) * 0.5 * (ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2]));
+  const double s0 = fmin(un_r - c_r, un[0] - cs[0]);
+  const double s1 = fmax(un_r + c_r, un[1] + cs[1]);
+  // contact speed and the star pressure
+  const double sm = (a.p - b.p - rho[0] * un[0] * (s0 - un[0]) + rho[1] * un[1] * (s1 - un[1])) /
+                    (rho[1] * (s1 - un[1]) - rho[0] * (s0 - un[0]));
+  const double ps = rho[1] * (un[1] - s1) * (un[1] - sm) + b.p;
+  // the upwind side of the contact: its own flux when the fan lies beyond
+  // it, else its star state's
+  const int k = (sm >= 0.0) ? 0 : 1;
+  const RiemannState& q = *st[k];
+  const double sk = k ? s1 : s0;
+  if (k == 0 ? (s0 > 0.0) : !(s1 >= 0.0)) {
+    F[0] = rho[k] * un[k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[1 + d] = rho[k] * q.u[d] * un[k] + q.p * nh[d];
+    F[4] = (E[k] + q.p) * un[k];
+  } else {
+    const double inv = 1.0 / (sk - sm);
+    const double dk = sk - un[k];
+    F[0] = rho[k] * dk * inv * sm;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[1 + d] = (rho[k] * q.u[d] * dk + (ps - q.p) * nh[d]) * inv * sm + ps * nh[d];
+    F[4] = ((dk * E[k] - q.p * un[k] + ps * sm) * inv + ps) * sm;
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) F[c] *= area;
+}
+
+// addBoundaryFlux of the boundary zones, one thread per cell with boundary
+// faces, added to one stage's rhs after the face sums:
+//   SLIP            rhs.rhou -= p n_bf                (IdealGasSolverBcs.cpp:14-23)
 //   WALL_ADIABATIC  tau = mu_lam aod (u - u_wall); rhs.rhou -= p n_bf + tau;
-//                   rhs.rhoE -= u_wall.tau
-// p from the FP64 state (updateExtendedState's formula), mu_lam from the
-// cell's property record (the last calcSgsAndMaterialProperties).  The
+//                   rhs.rhoE -= u_wall.tau            (:25-48)
+//   WALL_ISOTHERMAL tau = mu_lam aod u; rhs.rhou -= p n_bf + tau;
+//                   rhs.rhoE -= loc_lam aod cp (T - T_bc)  (:1485-1510)
+//   CBC_*           rhs -= HLLC flux between the cell's state and the zone's
+//                   boundary state                    (:2960-2976)
+// p, T and the cell's Riemann state from the FP64 state (updateExtendedState's
+// formulas), mu_lam from the cell's property record (the last
+// calcSgsAndMaterialProperties), loc_lam = mu_lam / Pr_lam.  The
 // mixed-precision face sums leave out p_ref sum(n_ef), which on a cell with
 // boundary faces is -p_ref sum(n_bf) (the extended-face GCL), so its
-// boundary term takes p - p_ref.
+// boundary momentum terms take p_ref n_bf off.
 template <bool MIX>
 __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
   const MeshDev& m = c.m;
@@ -1018,36 +1112,65 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= m.nbc) return;
   const int i = m.bcell[t];
+  const double gamma = c.ph.gamma;
   const double rho = s.rho[i], rhoE = s.rhoE[i];
   const double u[3] = {s.u0[i], s.u1[i], s.u2[i]};
   const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-  const double p = (c.ph.gamma - 1.0) * (rhoE - 0.5 * rho * usq) - (MIX ? c.ph.p_ref : 0.0);
+  const double pf = (gamma - 1.0) * (rhoE - 0.5 * rho * usq);
+  const double p = pf - (MIX ? c.ph.p_ref : 0.0);
+  const double T = pf / (rho * c.ph.R);
   const double mu_lam = MIX ? double(s.VF[i].mu_lam) : s.V[i].mu_lam;
-  double fr[4] = {0.0, 0.0, 0.0, 0.0};
+  double fr[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int f = m.bfc[i]; f < m.bfc[i + 1]; ++f) {
     const double n[3] = {m.bf_n[f], m.bf_n[m.nbf + f], m.bf_n[2 * m.nbf + f]};
-    const double4 bc = s.bc[m.bf_zone[f]];
-    if (int(bc.x) == CGX_BC_WALL_ADIABATIC) {
+    const BcZone& z = s.bc[m.bf_zone[f]];
+    const int kind = z.kind;
+    if (kind == CGX_BC_SLIP) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d];
+    } else if (kind == CGX_BC_WALL_ADIABATIC) {
       const double visc = mu_lam * m.bf_aod[f];
-      const double uw[3] = {bc.y, bc.z, bc.w};
       double work = 0.0;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const double tau = visc * (u[d] - uw[d]);
-        fr[d] -= p * n[d] + tau;
-        work += uw[d] * tau;
+        const double tau = visc * (u[d] - z.a[d]);
+        fr[1 + d] -= p * n[d] + tau;
+        work += z.a[d] * tau;
       }
-      fr[3] -= work;
-    } else {
+      fr[4] -= work;
+    } else if (kind == CGX_BC_WALL_ISOTHERMAL) {
+      const double visc = mu_lam * m.bf_aod[f];
+      const double cp = c.ph.R * gamma / (gamma - 1.0);
+      const double kc = (mu_lam * (1.0 / c.ph.Pr_lam)) * m.bf_aod[f] * cp;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) fr[d] -= p * n[d];
+      for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d] + visc * u[d];
+      fr[4] -= kc * (T - z.a[3]);
+    } else {
+      const double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      RiemannState sc, sb;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        sc.u[d] = u[d];
+        sb.u[d] = z.a[d] + z.a[3] * n[d] / area;
+      }
+      sc.sp_vol = 1.0 / rho;
+      sc.p = pf;
+      sc.h = c.ph.R * gamma * (1.0 / (gamma - 1.0)) * T;
+      sb.p = z.a[4];
+      sb.sp_vol = z.a[5];
+      sb.h = z.a[6];
+      double F[5];
+      hllc_flux(F, n, sc, sb, gamma);
+      fr[0] -= F[0];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) fr[1 + d] -= F[1 + d] - (MIX ? c.ph.p_ref * n[d] : 0.0);
+      fr[4] -= F[4];
     }
   }
   const size_t N = size_t(m.N);
   double* r = s.rhs + size_t(stage) * 5 * N;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) r[(1 + d) * N + i] += fr[d];
-  r[4 * N + i] += fr[3];
+  for (int q = 0; q < 5; ++q) r[q * N + i] += fr[q];
 }
 
 // report() totals: per-block partial sums in a fixed tree, then one block
@@ -1417,7 +1540,9 @@ struct cgx_mesh {
   std::vector<Item> items;  // work items (host copy of md.items)
   int max_union = 0;        // largest extended-face union of an item (records)
   int max_cunion = 0;       // largest compact-face union of an item
+  int max_item_e = 0;       // most extended entries of an item
   int nbf_zones = 0;        // boundary zones (0: periodic)
+  std::vector<double> zone_area;  // sum of |n_bf| over each zone (its area_global)
   std::vector<void*> allocs;
   size_t bytes = 0;
   cgx_mesh_stats stats{};
@@ -1469,6 +1594,7 @@ struct Runner {
   cgx_precision prec = CGX_FP64;
   int max_union = 0;            // staging sizes: largest unions over the cases
   int max_cunion = 0;
+  int max_item_e = 0;           // and most extended entries of an item
   std::atomic<long long>* launches = nullptr;
   SourceCfg* src = nullptr;     // source terms (single-case solvers only)
 };
@@ -1503,7 +1629,7 @@ struct cgx_solver {
   std::unique_ptr<cgx_staging::Staging> staging;  // for pageable caller arrays, made on first use
   std::atomic<long long> launches{0};
   SourceCfg src;
-  std::vector<double4> bc;  // boundary conditions per zone (host copy of sd.bc)
+  std::vector<BcZone> bc;   // boundary conditions per zone (host copy of sd.bc)
 };
 
 namespace {
@@ -1536,8 +1662,9 @@ inline size_t smem_grad(const Runner& R) {
   return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_cunion) : swz_chunks<2>(R.max_cunion)) * 16;
 }
 inline size_t smem_end(const Runner& R) {
-  return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_union) + swz_chunks<2>(R.max_cunion)
-                                    : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) *
+  return size_t((R.prec == CGX_MIXED ? swz_chunks<1>(R.max_union) + swz_chunks<2>(R.max_cunion)
+                                     : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) +
+                idx_chunks(R.max_item_e)) *
          16;
 }
 inline size_t smem_comp(const Runner& R) {
@@ -2396,6 +2523,11 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
         if (bfc[size_t(i) + 1] > bfc[size_t(i)]) bcell.push_back(i);
     }
     M->nbf_zones = nbf > 0 ? d->nbf_zones : 0;
+    M->zone_area.assign(size_t(M->nbf_zones), 0.0);
+    for (int f = 0; f < nbf; ++f) {
+      const double* n = d->n_bf + 3 * size_t(f);
+      M->zone_area[size_t(d->zone_bf[f])] += std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    }
     // ---- work items (runs of consecutive cells) and their halos; an item
     // whose neighbour unions exceed the shared-memory budget is split
     std::vector<Item> items;
@@ -2405,7 +2537,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     for (int i = 0; i < N; ++i) qoff[i + 1] = qoff[i] + ncomp[i];
     clidx.resize(std::max(qoff[N], 1LL));
     std::vector<unsigned short> cglidx(std::max(coff[N], 1LL));
-    int max_u = 0, max_cu = 0;
+    int max_u = 0, max_cu = 0, max_e = 0;
     {
       // Base items of kItemCells cells are independent: each is built in
       // parallel (and split in halves, first half first, while its unions
@@ -2454,13 +2586,14 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
             SubItem si{c0, nc, {}, {}};
             unions(c0, nc, si.halo, si.chalo);
             const int nu = nc + int(si.halo.size()), ncu = nc + int(si.chalo.size());
-            if ((nu > kMaxUnionExt || ncu > kMaxUnionComp) && nc > 1) {
+            const long long ne = cell_off[c0 + nc] - cell_off[c0];
+            if ((nu > kMaxUnionExt || ncu > kMaxUnionComp || ne > kMaxItemEntries) && nc > 1) {
               const int h1 = nc / 2;  // split, first half processed first
               todo.push_back({c0 + h1, nc - h1});
               todo.push_back({c0, h1});
               continue;
             }
-            if (nu > kMaxUnionExt || ncu > kMaxUnionComp) {
+            if (nu > kMaxUnionExt || ncu > kMaxUnionComp || ne > kMaxItemEntries) {
               too_big = 1;
               break;
             }
@@ -2493,6 +2626,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
           items.push_back(it);
           max_u = std::max(max_u, si.nc + nh);
           max_cu = std::max(max_cu, si.nc + nch);
+          max_e = std::max(max_e, int(cell_off[si.c0 + si.nc] - cell_off[si.c0]));
           std::vector<int>().swap(si.halo);
           std::vector<int>().swap(si.chalo);
         }
@@ -2528,6 +2662,9 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     UP(d_off, cell_off);
     UP(d_qoff, qoff);
     UP(d_nbr, e_nbr);
+    // 8 entries of padding: the once-per-step kernel copies an item's local
+    // indices in 16-byte chunks
+    lidx.resize(size_t(std::max(cell_off[N], 1LL)) + 8, 0);
     UP(d_lidx, lidx);
     UP(d_clidx, clidx);
     UP(d_cglidx, cglidx);
@@ -2621,6 +2758,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     M->items = items;
     M->max_union = max_u;
     M->max_cunion = max_cu;
+    M->max_item_e = max_e;
     M->nc_dir = coff[N];
     long long n_ef_dir = cell_off[N], n_cf_dir = qoff[N];
     M->stats.ncv = N;
@@ -2765,11 +2903,11 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
   AL(s->d_store[0], 5 * N);
   AL(s->d_store[1], 5 * N);
   {
-    double4* d_bc = nullptr;
+    BcZone* d_bc = nullptr;
     AL(d_bc, size_t(std::max(m->nbf_zones, 1)));
     sd.bc = d_bc;
-    s->bc.assign(std::max(m->nbf_zones, 1), make_double4(0.0, 0.0, 0.0, 0.0));
-    if (cudaMemcpyAsync(d_bc, s->bc.data(), s->bc.size() * sizeof(double4), cudaMemcpyHostToDevice, s->stream) !=
+    s->bc.assign(std::max(m->nbf_zones, 1), BcZone{});
+    if (cudaMemcpyAsync(d_bc, s->bc.data(), s->bc.size() * sizeof(BcZone), cudaMemcpyHostToDevice, s->stream) !=
         cudaSuccess)
       return bail(fail(CGX_E_CUDA, "boundary condition table upload failed"));
   }
@@ -2805,6 +2943,7 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     R.prec = prec;
     R.max_union = m->max_union;
     R.max_cunion = m->max_cunion;
+    R.max_item_e = m->max_item_e;
     R.launches = &s->launches;
     s->src.N = int(N);
     s->src.perm = m->d_perm;
@@ -2948,6 +3087,10 @@ extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
   if (!s) return fail(CGX_E_ARG, "cgx_set_scalars: null solver");
   if (nsc < 0 || nsc > kMaxScalars) return fail(CGX_E_ARG, "cgx_set_scalars: nsc out of range 0..8");
   if (nsc > 0 && !sc) return fail(CGX_E_ARG, "cgx_set_scalars: null scalars");
+  if (nsc > 0)
+    for (const BcZone& z : s->bc)
+      if (z.kind >= CGX_BC_CBC_UPT)
+        return fail(CGX_E_STATE, "cgx_set_scalars: CBC boundary zones carry no transport scalars");
   CK(cudaSetDevice(s->mesh->device));
   CK(cudaStreamSynchronize(s->stream));
   const size_t N = size_t(s->mesh->N);
@@ -3116,31 +3259,95 @@ extern "C" int cgx_calc_sgs_props(cgx_solver* s) {
   return CGX_OK;
 }
 
-extern "C" int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]) {
+extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams) {
   if (!s) return fail(CGX_E_ARG, "cgx_set_bc: null solver");
   if (zone < 0 || zone >= s->mesh->nbf_zones)
     return fail(CGX_E_ARG, "cgx_set_bc: zone " + std::to_string(zone) + " not in [0, " +
                                std::to_string(s->mesh->nbf_zones) + ")");
-  if (kind != CGX_BC_SLIP && kind != CGX_BC_WALL_ADIABATIC)
-    return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition");
+  if (nparams < 0 || (nparams > 0 && !params)) return fail(CGX_E_ARG, "cgx_set_bc: bad parameter list");
+  // parameters each kind takes (WALL_ADIABATIC: none or its TRANSLATE velocity)
+  int want = -1;
+  switch (kind) {
+    case CGX_BC_SLIP: want = 0; break;
+    case CGX_BC_WALL_ADIABATIC: want = (nparams == 0) ? 0 : 3; break;
+    case CGX_BC_WALL_ISOTHERMAL: want = 1; break;
+    case CGX_BC_CBC_UPT: want = 5; break;
+    case CGX_BC_CBC_RUNP: want = 3; break;
+    case CGX_BC_CBC_MPT: want = 3; break;
+    default: return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition");
+  }
+  if (nparams != want)
+    return fail(CGX_E_ARG, "cgx_set_bc: kind " + std::to_string(kind) + " takes " + std::to_string(want) +
+                               " parameters, got " + std::to_string(nparams));
+  if (kind >= CGX_BC_CBC_UPT && s->sd.nsc > 0)
+    return fail(CGX_E_STATE, "cgx_set_bc: CBC boundary zones carry no transport scalars");
+  const double R = s->ph.R, gamma = s->ph.gamma;
+  BcZone z{};
+  z.kind = kind;
+  switch (kind) {
+    case CGX_BC_WALL_ADIABATIC:
+      for (int d = 0; d < nparams; ++d) z.a[d] = params[d];
+      break;
+    case CGX_BC_WALL_ISOTHERMAL:  // u_bc stays 0 (WallIsothermal's constructor)
+      z.a[3] = params[0];
+      break;
+    case CGX_BC_CBC_UPT: {  // CbcUpt::initData
+      const double T = params[4];
+      for (int d = 0; d < 3; ++d) z.a[d] = params[d];
+      z.a[4] = params[3];
+      z.a[5] = R * T / params[3];
+      z.a[6] = R * T * gamma / (gamma - 1.0);
+      break;
+    }
+    case CGX_BC_CBC_RUNP: {  // CbcRunp::initData: u = -un n/|n|
+      const double rho = params[0], un = params[1], p = params[2];
+      const double T = p / rho / R;
+      z.a[3] = -un;
+      z.a[4] = p;
+      z.a[5] = 1.0 / rho;
+      z.a[6] = R * T * gamma / (gamma - 1.0);
+      break;
+    }
+    case CGX_BC_CBC_MPT: {  // CbcMpt::initData: u = un n/|n|, un = -mdot/(rho area)
+      const double mdot = params[0], p = params[1], T = params[2];
+      const double rho = p / T / R;
+      z.a[3] = -mdot / (rho * s->mesh->zone_area[size_t(zone)]);
+      z.a[4] = p;
+      z.a[5] = 1.0 / rho;
+      z.a[6] = R * T * gamma / (gamma - 1.0);
+      break;
+    }
+    default:
+      break;
+  }
   CK(cudaSetDevice(s->mesh->device));
-  const double uw[3] = {u_wall ? u_wall[0] : 0.0, u_wall ? u_wall[1] : 0.0, u_wall ? u_wall[2] : 0.0};
-  s->bc[size_t(zone)] = make_double4(double(kind), kind == CGX_BC_SLIP ? 0.0 : uw[0],
-                                     kind == CGX_BC_SLIP ? 0.0 : uw[1], kind == CGX_BC_SLIP ? 0.0 : uw[2]);
-  CK(cudaMemcpyAsync(const_cast<double4*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(double4),
+  s->bc[size_t(zone)] = z;
+  CK(cudaMemcpyAsync(const_cast<BcZone*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(BcZone),
                      cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
+}
+
+extern "C" int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]) {
+  if (kind != CGX_BC_SLIP && kind != CGX_BC_WALL_ADIABATIC)
+    return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition (cgx_set_bc_params takes the others)");
+  const bool uw = kind == CGX_BC_WALL_ADIABATIC && u_wall;
+  return cgx_set_bc_params(s, zone, kind, uw ? u_wall : nullptr, uw ? 3 : 0);
 }
 
 // initComplete; `tune`: pick the lane counts (a case prepared for a batch
 // runs with the batch's own lane counts and skips it)
 static int init_complete(cgx_solver* s, bool tune) {
   if (!s) return fail(CGX_E_ARG, "null solver");
-  for (int z = 0; z < s->mesh->nbf_zones; ++z)
-    if (s->bc[size_t(z)].x == 0.0)
+  for (int z = 0; z < s->mesh->nbf_zones; ++z) {
+    const int kind = s->bc[size_t(z)].kind;
+    if (kind == 0)
       return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
                                    " has no boundary condition (cgx_set_bc)");
+    if (kind >= CGX_BC_CBC_UPT && s->sd.nsc > 0)
+      return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
+                                   " is a CBC zone and the solver has transport scalars");
+  }
   int rc = cgx_update_primitive(s);
   if (rc) return rc;
   if ((rc = cgx_calc_sgs_props(s))) return rc;
@@ -3590,13 +3797,14 @@ void batch_free_graph(cgx_batch* b) {
 int batch_rebuild(cgx_batch* b) {
   std::vector<Item> items;
   long long cells = 0;
-  int mu = 0, mcu = 0;
+  int mu = 0, mcu = 0, mie = 0;
   for (size_t k = 0; k < b->slots.size(); ++k) {
     const BatchCase& c = b->slots[k];
     if (!c.s || c.finished) continue;
     cells += c.s->mesh->N;
     mu = std::max(mu, c.s->mesh->max_union);
     mcu = std::max(mcu, c.s->mesh->max_cunion);
+    mie = std::max(mie, c.s->mesh->max_item_e);
     for (const Item& mi : c.s->mesh->items) {
       Item it = mi;
       it.c = int(k);
@@ -3630,9 +3838,10 @@ int batch_rebuild(cgx_batch* b) {
   b->nitems = int(items.size());
   b->active_cells = cells;
   b->run.items = b->d_items;
-  if (mu != b->run.max_union || mcu != b->run.max_cunion) {
+  if (mu != b->run.max_union || mcu != b->run.max_cunion || mie != b->run.max_item_e) {
     b->run.max_union = mu;  // shared-memory sizes of the staged kernels
     b->run.max_cunion = mcu;
+    b->run.max_item_e = mie;
     batch_free_graph(b);
   }
   b->dirty = false;

@@ -118,6 +118,17 @@ struct Phys {
 };
 
 // Device-resident control block (one per solver).
+// A boundary zone's condition: its kind (CGX_BC_*, 0 until set) and its
+// parameters.  Walls: a[0..2] the wall velocity, a[3] T_bc (isothermal).
+// CBC zones: the boundary state of each face, velocity a[0..2] + a[3] n/|n|,
+// p = a[4], sp_vol = a[5], h = a[6], as the reference's initData fills its
+// bf_state from the zone's parameters.
+struct BcZone {
+  int kind;
+  int pad;
+  double a[7];
+};
+
 struct Ctl {
   double dt;         // dt of the next step (read by the RK kernels)
   double dt_last;    // dt of the last completed step (the reference's `dt`)
@@ -208,8 +219,8 @@ struct StateDev {
   double* sc;      // [nsc][N]
   double* rhs_sc;  // [3][nsc][N]
   double* mf;      // [E] mass flux of each extended entry, entry direction
-  // boundary conditions per boundary zone: {kind (CGX_BC_*), u_wall[3]}
-  const double4* bc;
+  // boundary conditions per boundary zone
+  const struct BcZone* bc;
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

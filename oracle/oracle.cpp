@@ -130,11 +130,13 @@ struct orc_solver {
   std::vector<double> sc, rhs_sc[3], scale_sc;
   bool want_scale = false;
   // boundary faces (cvobf, n_bf, area_over_delta_bf, zone) and one boundary
-  // condition per zone {kind, u_wall[3]}
+  // condition per zone {kind, u_wall[3], T_bc}; the boundary state of each
+  // face of a CBC zone (the reference's bf_state)
   int nbf = 0, nbf_zones = 0;
   std::vector<int> cvobf, zone_bf;
   std::vector<double> n_bf, aod_bf;
-  std::vector<std::array<double, 4>> bc;
+  std::vector<std::array<double, 5>> bc;
+  std::vector<IdealGasState> bf_state;
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
@@ -439,10 +441,12 @@ void add_source(orc_solver* o, IdealGasRhs* rhs) {
 
 // addBoundaryFlux of each zone's boundary condition, zone by zone, before
 // the face loops as calcRhsBase calls them (IdealGasSolver.cpp:261-262):
-// SlipWallBc (IdealGasSolverBcs.cpp:14-23) and WallAdiabatic (:25-48)
+// SlipWallBc (IdealGasSolverBcs.cpp:14-23), WallAdiabatic (:25-48),
+// WallIsothermal (:1485-1510) and Cbc (:2960-2976)
 void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
+  const double gamma = o->prm.gamma;
   for (int z = 0; z < o->nbf_zones; ++z) {
-    const std::array<double, 4>& bc = o->bc[z];
+    const std::array<double, 5>& bc = o->bc[z];
     const int kind = int(bc[0]);
     for (int ibf = 0; ibf < o->nbf; ++ibf) {
       if (o->zone_bf[ibf] != z) continue;
@@ -450,6 +454,19 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
       const double* n = &o->n_bf[3 * size_t(ibf)];
       if (kind == CGX_BC_SLIP) {
         for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= o->p[icv] * n[i];
+      } else if (kind == CGX_BC_WALL_ISOTHERMAL) {
+        const double cp = o->R_gas * gamma / (gamma - 1.0);
+        const double visc_coeff = o->mu_lam[icv] * o->aod_bf[ibf];
+        const double k_coeff = o->loc_lam[icv] * o->aod_bf[ibf] * cp;
+        for (int i = 0; i < 3; ++i)
+          rhs[icv].rhou[i] -= o->p[icv] * n[i] + visc_coeff * (o->u[3 * size_t(icv) + i] - 0.0);
+        rhs[icv].rhoE -= k_coeff * (o->T[icv] - bc[4]);
+      } else if (kind >= CGX_BC_CBC_UPT) {
+        IdealGasRhs flux;
+        calcRiemannFlux(flux, n, o->cv_light[icv], o->bf_state[ibf], gamma, gamma);
+        rhs[icv].rho -= flux.rho;
+        for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= flux.rhou[i];
+        rhs[icv].rhoE -= flux.rhoE;
       } else {
         const double visc_coeff = o->mu_lam[icv] * o->aod_bf[ibf];
         double visc_work = 0.0;
@@ -761,7 +778,8 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->zone_bf.assign(m->zone_bf, m->zone_bf + m->nbf);
     o->n_bf.assign(m->n_bf, m->n_bf + 3 * size_t(m->nbf));
     o->aod_bf.assign(m->area_over_delta_bf, m->area_over_delta_bf + m->nbf);
-    o->bc.assign(m->nbf_zones, {0.0, 0.0, 0.0, 0.0});
+    o->bc.assign(m->nbf_zones, {0.0, 0.0, 0.0, 0.0, 0.0});
+    o->bf_state.assign(m->nbf, IdealGasState());
   }
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
@@ -1075,7 +1093,59 @@ extern "C" void orc_get_aux(const orc_solver* o, double* aux) {
 extern "C" int orc_set_bc(orc_solver* o, int zone, int kind, const double u_wall[3]) {
   if (zone < 0 || zone >= o->nbf_zones || (kind != CGX_BC_SLIP && kind != CGX_BC_WALL_ADIABATIC)) return -1;
   o->bc[zone] = {double(kind), kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[0],
-                 kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[1], kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[2]};
+                 kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[1], kind == CGX_BC_SLIP || !u_wall ? 0.0 : u_wall[2],
+                 0.0};
+  return 0;
+}
+
+// The zone parameters of WALL_ISOTHERMAL (WallIsothermal::initData,
+// IdealGasSolverBcs.cpp:1480-1483) and the boundary states the CBC zones
+// build from theirs: CbcUpt (:3182-3207), CbcMpt (:3209-3240), CbcRunp
+// (:3242-3266); area_global is the zone's summed face area.
+extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double* prm, int np) {
+  if (zone < 0 || zone >= o->nbf_zones) return -1;
+  if (kind == CGX_BC_SLIP || kind == CGX_BC_WALL_ADIABATIC)
+    return (np == 0 || (kind == CGX_BC_WALL_ADIABATIC && np == 3)) ? orc_set_bc(o, zone, kind, np ? prm : nullptr) : -1;
+  const int want = kind == CGX_BC_WALL_ISOTHERMAL ? 1 : kind == CGX_BC_CBC_UPT ? 5
+                 : (kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT) ? 3 : -1;
+  if (want < 0 || np != want || !prm) return -1;
+  o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, kind == CGX_BC_WALL_ISOTHERMAL ? prm[0] : 0.0};
+  if (kind == CGX_BC_WALL_ISOTHERMAL) return 0;
+  const double R = o->R_gas, gamma = o->prm.gamma;
+  double area_global = 0.0;
+  for (int ibf = 0; ibf < o->nbf; ++ibf)
+    if (o->zone_bf[ibf] == zone) {
+      const double* n = &o->n_bf[3 * size_t(ibf)];
+      area_global += std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    }
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    if (o->zone_bf[ibf] != zone) continue;
+    const double* n = &o->n_bf[3 * size_t(ibf)];
+    const double bf_area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    IdealGasState& b = o->bf_state[ibf];
+    if (kind == CGX_BC_CBC_UPT) {
+      const double p_bc = prm[3], T_bc = prm[4];
+      for (int i = 0; i < 3; ++i) b.u[i] = prm[i];
+      b.p = p_bc;
+      b.sp_vol = R * T_bc / p_bc;
+      b.h = R * T_bc * gamma / (gamma - 1.0);
+    } else if (kind == CGX_BC_CBC_RUNP) {
+      const double rho_bc = prm[0], un_bc = prm[1], p_bc = prm[2];
+      const double T_bc = p_bc / rho_bc / R;
+      for (int i = 0; i < 3; ++i) b.u[i] = -un_bc * n[i] / bf_area;
+      b.sp_vol = 1.0 / rho_bc;
+      b.p = p_bc;
+      b.h = R * T_bc * gamma / (gamma - 1.0);
+    } else {
+      const double mdot_bc = prm[0], p_bc = prm[1], T_bc = prm[2];
+      const double rho_bc = p_bc / T_bc / R;
+      const double un_bc = -mdot_bc / (rho_bc * area_global);
+      for (int i = 0; i < 3; ++i) b.u[i] = un_bc * n[i] / bf_area;
+      b.sp_vol = 1.0 / rho_bc;
+      b.p = p_bc;
+      b.h = R * T_bc * gamma / (gamma - 1.0);
+    }
+  }
   return 0;
 }
 

@@ -58,6 +58,7 @@ def _load(path):
         "orc_poison": (None, [vp, ctypes.c_int]),
         "orc_set_source": (None, [vp, ctypes.c_double, c_dbl_p, c_dbl_p]),
         "orc_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
+        "orc_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "orc_uses_reference_flux": (ctypes.c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -194,6 +195,14 @@ class Oracle:
         uw = None if u_wall is None else np.ascontiguousarray(u_wall, dtype=np.float64)
         if self.L.orc_set_bc(self.h, int(zone), int(kind), _dp(uw)) != 0:
             raise ValueError("orc_set_bc: bad zone or kind")
+
+    def set_bc_params(self, zone, kind, params=()):
+        """Boundary condition with the reference's zone parameters:
+        WALL_ISOTHERMAL (T) = 3, CBC_UPT (u0 u1 u2 p T) = 4, CBC_RUNP
+        (rho un p) = 5, CBC_MPT (mdot p T) = 6."""
+        a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+        if self.L.orc_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)) != 0:
+            raise ValueError("orc_set_bc_params: bad zone, kind or parameters")
 
     def poison(self, icv):
         self.L.orc_poison(self.h, int(icv))

@@ -1,0 +1,128 @@
+"""WALL_ISOTHERMAL and the characteristic (CBC) boundary zones in the oracle,
+on CPU, on a channel (periodic in x and z, zones at y = 0 and y = Ly).
+
+* The restated HLLC Riemann flux (calcRiemannFlux, IdealGasSolverFlux.hpp:
+  218-306) equals the reference's own header bit for bit: calcRhs with
+  CBC_UPT / CBC_RUNP / CBC_MPT and WALL_ISOTHERMAL zones, liboracle against
+  the oracle built on the reference tree.
+* A uniform flow through the channel is an exact solution (rhs = 0 to
+  round-off) when the inflow zone (CBC_UPT) carries the flow's state and the
+  outflow zone carries its density, normal speed and pressure (CBC_RUNP) or
+  its mass flow rate, pressure and temperature (CBC_MPT).
+* A fluid at rest between isothermal walls at its own temperature stays at
+  rest; a hotter wall heats the cells next to it.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc_mod
+from nextgen_b200 import cases
+from nextgen_b200.meshgen import ChannelMesh
+from oracle import Oracle
+
+UPT, RUNP, MPT, ISO = 4, 5, 6, 3
+need_ref = pytest.mark.skipif(not orc_mod.ref_available(), reason="reference-built oracle absent")
+
+
+@pytest.fixture(scope="module")
+def chan(built):
+    return ChannelMesh(12, 8, 6, L=(3.0, 2.0, 1.5), jitter=0.25, seed=7)
+
+
+def _uniform(m, prm, u=(0.1, 0.25, -0.05)):
+    rho = np.ones(m.ncv)
+    uu = np.tile(np.asarray(u, dtype=np.float64), (m.ncv, 1))
+    p = np.full(m.ncv, prm.p_ref)
+    return rho, uu, p
+
+
+def _zone_area(m, z):
+    return np.linalg.norm(m.n_bf[m.zone_bf == z], axis=1).sum()
+
+
+@pytest.mark.parametrize("outflow", ["runp", "mpt"])
+def test_uniform_flow_through_cbc_zones(chan, outflow):
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    rho, u, p = _uniform(m, prm)
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+    T0 = p[0] / (rho[0] * R)
+    o = Oracle(m, prm)
+    # inflow at y = 0 (outward normal -y), outflow at y = Ly (outward +y)
+    o.set_bc_params(0, UPT, [u[0, 0], u[0, 1], u[0, 2], p[0], T0])
+    if outflow == "runp":
+        o.set_bc_params(1, RUNP, [rho[0], -u[0, 1], p[0]])  # un: inflow speed against n_bf
+    else:
+        o.set_bc_params(1, MPT, [-rho[0] * u[0, 1] * _zone_area(m, 1), p[0], T0])
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    r, scale = o.calc_rhs(1)
+    # rhs against the boundary momentum flux scale of a face
+    ref = (rho[0] * (u[0] ** 2).sum() + p[0]) * np.linalg.norm(m.n_bf, axis=1).max()
+    assert np.abs(r).max() <= 1e-13 * ref
+    o.close()
+
+
+def test_isothermal_walls(chan):
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    rho = np.ones(m.ncv)
+    u = np.zeros((m.ncv, 3))
+    p = np.full(m.ncv, prm.p_ref)
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+    T0 = prm.p_ref / R
+    o = Oracle(m, prm)
+    o.set_bc_params(0, ISO, [T0])
+    o.set_bc_params(1, ISO, [T0])
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    r, _ = o.calc_rhs(1)
+    assert np.abs(r).max() <= 1e-13 * prm.p_ref * np.linalg.norm(m.n_bf, axis=1).max()
+    o.close()
+    o = Oracle(m, prm)
+    o.set_bc_params(0, ISO, [1.5 * T0])
+    o.set_bc_params(1, ISO, [T0])
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    r, _ = o.calc_rhs(1)
+    hot = np.unique(m.cvobf[m.zone_bf == 0])
+    assert np.all(r[hot, 4] > 0.0)
+    rest = np.setdiff1d(np.arange(m.ncv), hot)
+    assert np.abs(r[rest, 4]).max() <= 1e-12 * r[hot, 4].max()
+    o.close()
+
+
+def test_bad_parameters_refused(chan):
+    o = Oracle(chan, cases.tgv_params())
+    with pytest.raises(ValueError):
+        o.set_bc_params(0, UPT, [1.0, 2.0])
+    with pytest.raises(ValueError):
+        o.set_bc_params(0, 9, [])
+    o.close()
+
+
+@need_ref
+@pytest.mark.parametrize("zones", [((UPT, (0.1, 0.4, 0.0, 0.72, 0.9)), (RUNP, (1.05, -0.3, 0.7))),
+                                   ((ISO, (1.2,)), (MPT, (-0.5, 0.71, 1.0)))])
+def test_restated_riemann_flux_bitwise_equals_reference(chan, zones):
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    Lx, Ly, Lz = m.L
+    xs, zs = 2 * np.pi * x / Lx, 2 * np.pi * z / Lz
+    u = np.stack([0.2 * np.cos(zs) + 0.1, 0.3 + 0.05 * np.sin(xs), 0.1 * np.cos(xs)], 1)
+    p = prm.p_ref * (1.0 + 0.02 * np.cos(xs) * np.sin(np.pi * y / Ly))
+    rho = 1.0 + 0.03 * np.sin(zs)
+    out = []
+    for reference in (False, True):
+        o = Oracle(m, prm, reference=reference)
+        for zz, (kind, a) in enumerate(zones):
+            o.set_bc_params(zz, kind, a)
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        out.append(o.calc_rhs(1)[0])
+        assert o.step(2) == 0
+        out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+        o.close()
+    assert np.array_equal(out[0], out[2])
+    assert np.array_equal(out[1], out[3])

@@ -1,0 +1,138 @@
+"""WALL_ISOTHERMAL and the characteristic boundary zones on the GPU against
+the oracle, on a channel (periodic in x and z, zones at y = 0 and y = Ly):
+CBC_UPT, CBC_RUNP and CBC_MPT add the HLLC Riemann flux between the cell
+and the zone's boundary state (Cbc::addBoundaryFlux, IdealGasSolverBcs.cpp:
+2960-2976; calcRiemannFlux, IdealGasSolverFlux.hpp:218-306); WALL_ISOTHERMAL
+adds the wall's viscous and heat fluxes (IdealGasSolverBcs.cpp:1485-1510).
+
+* calcRhs per cell within 1e-12 of the face-sum scale and calcCfl within
+  1e-12, for an inflow/outflow pair of each kind and a hot isothermal wall;
+* 10 RK3 steps: state within 1e-10 of the oracle's;
+* a uniform flow through the channel stays uniform (rhs = 0 to round-off);
+* the mixed-precision form within its flux tolerance of the FP64 path;
+* CBC zones and transport scalars are refused together; wrong parameter
+  counts are refused.
+"""
+import numpy as np
+import pytest
+
+from nextgen_b200 import cases, cgx
+from nextgen_b200.meshgen import ChannelMesh
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+UPT, RUNP, MPT, ISO = cgx.CGX_BC_CBC_UPT, cgx.CGX_BC_CBC_RUNP, cgx.CGX_BC_CBC_MPT, cgx.CGX_BC_WALL_ISOTHERMAL
+ZONES = {
+    "upt_runp": ((UPT, (0.1, 0.4, 0.0, 0.72, 0.9)), (RUNP, (1.05, -0.3, 0.7))),
+    "upt_mpt": ((UPT, (0.0, 0.35, 0.05, 0.71, 1.0)), (MPT, (-0.9, 0.71, 1.0))),
+    "iso_mpt": ((ISO, (1.2,)), (MPT, (-0.5, 0.71, 1.0))),
+}
+
+
+@pytest.fixture(scope="module")
+def chan(built):
+    m = ChannelMesh(16, 12, 8, L=(4.0, 3.0, 2.0), jitter=0.25, seed=11)
+    return m, cgx.Mesh(m, device=0)
+
+
+def _state(m, prm):
+    x, y, z = m.x_cv[: m.ncv].T
+    Lx, Ly, Lz = m.L
+    xs, zs = 2 * np.pi * x / Lx, 2 * np.pi * z / Lz
+    u = np.stack([0.2 * np.cos(zs) + 0.1, 0.3 + 0.05 * np.sin(xs), 0.1 * np.cos(xs)], 1)
+    p = prm.p_ref * (1.0 + 0.02 * np.cos(xs) * np.sin(np.pi * y / Ly))
+    rho = 1.0 + 0.03 * np.sin(zs)
+    return rho, u, p
+
+
+def _make(m, gm, prm, zones, prec=cgx.CGX_FP64, state=None):
+    st = _state(m, prm) if state is None else state
+    s = cgx.Solver(gm, prm, prec)
+    o = Oracle(m, prm)
+    for z, (k, a) in enumerate(zones):
+        s.set_bc_params(z, k, a)
+        o.set_bc_params(z, k, a)
+    s.set_state_primitive(*st)
+    s.initComplete()
+    o.set_state_primitive(*st)
+    o.init_complete()
+    return s, o
+
+
+@pytest.mark.parametrize("name", list(ZONES))
+def test_cbc_rhs_and_cfl_match_oracle(chan, name):
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    s, o = _make(m, gm, prm, ZONES[name])
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    cg, cells = s.calcCfl(0.01, want_cells=True)
+    co, ocells = o.calc_cfl(0.01)
+    assert abs(cg - co) <= 1e-12 * co and (np.abs(cells - ocells) / ocells.max()).max() <= 1e-12
+    s.close()
+    o.close()
+
+
+@pytest.mark.parametrize("name", ["upt_runp", "iso_mpt"])
+def test_cbc_steps_match_oracle(chan, name):
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    s, o = _make(m, gm, prm, ZONES[name])
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    assert abs(s.time()[0] - o.time()[0]) <= 1e-13 * o.time()[0]
+    s.close()
+    o.close()
+
+
+def test_uniform_flow_stays_uniform(chan):
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    u0 = np.array([0.1, 0.25, -0.05])
+    rho = np.ones(m.ncv)
+    u = np.tile(u0, (m.ncv, 1))
+    p = np.full(m.ncv, prm.p_ref)
+    T0 = prm.T_ref
+    zones = ((UPT, (u0[0], u0[1], u0[2], prm.p_ref, T0)), (RUNP, (1.0, -u0[1], prm.p_ref)))
+    s, o = _make(m, gm, prm, zones, state=(rho, u, p))
+    r = s.calcRhs(1)
+    ref = (u0 @ u0 + prm.p_ref) * np.linalg.norm(m.n_bf, axis=1).max()
+    assert np.abs(r).max() <= 1e-12 * ref
+    s.close()
+    o.close()
+
+
+def test_cbc_mixed_close_to_fp64(chan):
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    res = {}
+    for prec in (cgx.CGX_FP64, cgx.CGX_MIXED):
+        s, o = _make(m, gm, prm, ZONES["upt_runp"], prec)
+        o.close()
+        assert s.step(10) == 0
+        res[prec] = s.get_state()
+        s.close()
+    for a64, a32 in zip(res[cgx.CGX_FP64], res[cgx.CGX_MIXED]):
+        assert np.sqrt(((a32 - a64) ** 2).mean() / (a64 ** 2).mean()) <= 1e-5
+
+
+def test_cbc_refusals(chan):
+    m, gm = chan
+    prm = cases.tgv_params()
+    s = cgx.Solver(gm, prm)
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_params(0, UPT, (0.1, 0.2))
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_params(0, 9, ())
+    with pytest.raises(cgx.CgxError):
+        s.set_bc(0, UPT)  # the parameterised kinds go through set_bc_params
+    s.set_bc_params(0, UPT, ZONES["upt_runp"][0][1])
+    s.set_bc_params(1, RUNP, ZONES["upt_runp"][1][1])
+    s.set_state_primitive(*_state(m, prm))
+    s.initComplete()
+    with pytest.raises(cgx.CgxError):
+        s.set_scalars(np.zeros((m.ncv, 1)))
+    s.close()
