@@ -101,9 +101,12 @@ def test_bad_parameters_refused(chan):
     o.close()
 
 
+P0 = cases.tgv_params(Re=400.0).p_ref  # T_ref = rho_ref = 1
+
+
 @need_ref
-@pytest.mark.parametrize("zones", [((UPT, (0.1, 0.4, 0.0, 0.72, 0.9)), (RUNP, (1.05, -0.3, 0.7))),
-                                   ((ISO, (1.2,)), (MPT, (-0.5, 0.71, 1.0)))])
+@pytest.mark.parametrize("zones", [((UPT, (0.1, 0.4, 0.0, 1.01 * P0, 1.02)), (RUNP, (1.0, -0.3, 0.99 * P0))),
+                                   ((ISO, (1.2,)), (MPT, (-1.8, P0, 1.0)))])
 def test_restated_riemann_flux_bitwise_equals_reference(chan, zones):
     m = chan
     prm = cases.tgv_params(Re=400.0)

@@ -23,10 +23,12 @@ from oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 UPT, RUNP, MPT, ISO = cgx.CGX_BC_CBC_UPT, cgx.CGX_BC_CBC_RUNP, cgx.CGX_BC_CBC_MPT, cgx.CGX_BC_WALL_ISOTHERMAL
+P0 = cases.tgv_params(Re=400.0).p_ref  # T_ref = rho_ref = 1
+# inflow at y = 0, outflow through the 4 x 2 zone at y = Ly
 ZONES = {
-    "upt_runp": ((UPT, (0.1, 0.4, 0.0, 0.72, 0.9)), (RUNP, (1.05, -0.3, 0.7))),
-    "upt_mpt": ((UPT, (0.0, 0.35, 0.05, 0.71, 1.0)), (MPT, (-0.9, 0.71, 1.0))),
-    "iso_mpt": ((ISO, (1.2,)), (MPT, (-0.5, 0.71, 1.0))),
+    "upt_runp": ((UPT, (0.1, 0.4, 0.0, 1.01 * P0, 1.02)), (RUNP, (1.0, -0.3, 0.99 * P0))),
+    "upt_mpt": ((UPT, (0.0, 0.35, 0.05, P0, 1.0)), (MPT, (-2.4, P0, 1.0))),
+    "iso_mpt": ((ISO, (1.2,)), (MPT, (-2.4, P0, 1.0))),
 }
 
 

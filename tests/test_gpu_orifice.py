@@ -11,7 +11,9 @@ orifice faces as SLIP, and:
 * 10 RK3 steps match the oracle's within 1e-10; mass and energy (closed
   box, adiabatic walls at rest) are conserved to 1e-13;
 * the state written to a .sles file and read back into a new solver is bit
-  for bit the same, with its step and time."""
+  for bit the same, with its step and time;
+* with a CBC_UPT inlet and a CBC_RUNP outlet (through-flow), calcRhs within
+  1e-12 and 10 steps within 1e-10 of the oracle."""
 import os
 
 import numpy as np
@@ -45,13 +47,19 @@ def orifice(built):
     return m, cgx.Mesh(m, device=0), prm, (rho, u, p), kinds
 
 
-def _pair(orifice):
+def _pair(orifice, through=False):
     m, gm, prm, st, kinds = orifice
     s = cgx.Solver(gm, prm)
     o = Oracle(m, prm)
     for z, k in enumerate(kinds):
         s.set_bc(z, k)
         o.set_bc(z, k)
+    if through:
+        # inflow at the inlet (u p T), outflow at the outlet (rho, speed, p)
+        for z, k, a in ((0, cgx.CGX_BC_CBC_UPT, (0.3, 0.0, 0.0, prm.p_ref, prm.T_ref)),
+                        (1, cgx.CGX_BC_CBC_RUNP, (prm.rho_ref, -0.3, prm.p_ref))):
+            s.set_bc_params(z, k, a)
+            o.set_bc_params(z, k, a)
     s.set_state_primitive(*st)
     s.initComplete()
     o.set_state_primitive(*st)
@@ -87,3 +95,15 @@ def test_orifice_steps_and_sles(orifice, tmp_path):
     assert s2.time()[0] == s.time()[0] and s2.time()[2] == 10
     s.close()
     s2.close()
+
+
+def test_orifice_through_flow_matches_oracle(orifice):
+    s, o = _pair(orifice, through=True)
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
