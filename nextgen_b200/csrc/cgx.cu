@@ -63,9 +63,6 @@ constexpr int kMaxRounds = 16;  // most rounds per item of a once-per-step kerne
 // staged face kernels: 64 B per extended-face neighbour record, 192 B per
 // compact-face one)
 constexpr int kMaxUnionExt = 3000;
-// most extended entries of one item: the once-per-step kernel stages the
-// item's local indices (2 B each) in shared memory beside its records
-constexpr int kMaxItemEntries = 16384;
 constexpr int kMaxUnionComp = 1100;
 constexpr int kLaunchesPerStep = 13;  // 3 x (rhs_ext, rhs_comp, rk_prim, grad) + step_end
 
@@ -187,9 +184,8 @@ __device__ __forceinline__ void prefetch_end(const MeshDev& m, const Item& it, i
   const int t = threadIdx.x;
   if (a >= b || t >= 6) return;
   if (t == 0) {
-    // the whole item's local indices, staged when the item starts
-    if (sub == 0)
-      prefetch_l2(m.lidx + __ldg(m.off + it.cell0), (__ldg(m.off + it.cell0 + it.ncell) - __ldg(m.off + it.cell0)) * 2);
+    const long long k0 = __ldg(m.off + it.cell0 + a), k1 = __ldg(m.off + it.cell0 + b);
+    prefetch_l2(m.lidx + k0, (k1 - k0) * 2);
     return;
   }
   const long long q0 = __ldg(m.qoff + it.cell0 + a), q1 = __ldg(m.qoff + it.cell0 + b);
@@ -197,23 +193,6 @@ __device__ __forceinline__ void prefetch_end(const MeshDev& m, const Item& it, i
     prefetch_l2(m.clidx + q0, (q1 - q0) * 2);
   else
     prefetch_l2(m.qg + (t - 1) * m.Q + q0, (q1 - q0) * 8);
-}
-
-// 16-byte chunks holding the local indices of n consecutive extended entries
-// copied from the 16-byte boundary at or below the first
-__host__ __device__ constexpr int idx_chunks(int n) { return (n + 7) / 8 + 1; }
-
-// Copy an item's extended-entry local indices lidx[e0, e1) into shared
-// memory from the 16-byte boundary ea = e0 & ~7 (the array is padded by 8
-// entries, so the last chunk stays inside it): entry k sits at sidx[k - ea].
-// Asynchronous: complete with stage_wait().
-__device__ __forceinline__ void stage_lidx(int4* sidx, const unsigned short* __restrict__ lidx, long long e0,
-                                           long long e1) {
-  const long long ea = e0 & ~7LL;
-  const int n = int((e1 - ea + 7) >> 3);
-  const int4* src = reinterpret_cast<const int4*>(lidx + ea);
-  for (int x = threadIdx.x; x < n; x += blockDim.x) cp_async16(sidx + x, src + x);
-  asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // the gradient kernel's streams: local indices and three coefficient planes
@@ -941,12 +920,8 @@ __global__ void __launch_bounds__(256, 3) k_step_end(CASE_ARGS, int mode) {
   const Phys& ph = CASE_PH;
   const int nu = it_.ncell + it_.nh;
   int4* sL = smem + swz_chunks<2>(nu);
-  int4* sI = sL + swz_chunks<4>(it_.ncell + it_.nch);
-  const long long ea = m.off[it_.cell0] & ~7LL;
-  const unsigned short* sIdx = reinterpret_cast<const unsigned short*>(sI);  // entry k at [k - ea]
   stage_records<2>(smem, s.Q, it_, m.hcell + it_.hoff, it_.nh);
   stage_records<4>(sL, s.L, it_, m.chcell + it_.choff, it_.nch);
-  stage_lidx(sI, m.lidx, m.off[it_.cell0], m.off[it_.cell0 + it_.ncell]);
   stage_wait();
   const long long Q = m.Q;
   // limitAsgs's dt: this step's, or outside a step the control block's
@@ -968,7 +943,7 @@ __global__ void __launch_bounds__(256, 3) k_step_end(CASE_ARGS, int mode) {
   // ---- Gibbs remainder over the extended faces (a maximum: any order)
   double vv2 = 0.0, cfl = 0.0;
   for (long long k = b + lane; k < e; k += G) {
-    const double4 qj = smem_Q(smem, sIdx[k - ea]);
+    const double4 qj = smem_Q(smem, __ldg(m.lidx + k));
     const double dp = qj.y - qi.y;
     const double v_avg = 0.5 * (qi.z + qj.z);
     const double beta = 0.5 * (qi.w + qj.w);
@@ -1540,7 +1515,6 @@ struct cgx_mesh {
   std::vector<Item> items;  // work items (host copy of md.items)
   int max_union = 0;        // largest extended-face union of an item (records)
   int max_cunion = 0;       // largest compact-face union of an item
-  int max_item_e = 0;       // most extended entries of an item
   int nbf_zones = 0;        // boundary zones (0: periodic)
   std::vector<double> zone_area;  // sum of |n_bf| over each zone (its area_global)
   std::vector<void*> allocs;
@@ -1594,7 +1568,6 @@ struct Runner {
   cgx_precision prec = CGX_FP64;
   int max_union = 0;            // staging sizes: largest unions over the cases
   int max_cunion = 0;
-  int max_item_e = 0;           // and most extended entries of an item
   std::atomic<long long>* launches = nullptr;
   SourceCfg* src = nullptr;     // source terms (single-case solvers only)
 };
@@ -1662,9 +1635,8 @@ inline size_t smem_grad(const Runner& R) {
   return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_cunion) : swz_chunks<2>(R.max_cunion)) * 16;
 }
 inline size_t smem_end(const Runner& R) {
-  return size_t((R.prec == CGX_MIXED ? swz_chunks<1>(R.max_union) + swz_chunks<2>(R.max_cunion)
-                                     : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) +
-                idx_chunks(R.max_item_e)) *
+  return size_t(R.prec == CGX_MIXED ? swz_chunks<1>(R.max_union) + swz_chunks<2>(R.max_cunion)
+                                    : swz_chunks<2>(R.max_union) + swz_chunks<4>(R.max_cunion)) *
          16;
 }
 inline size_t smem_comp(const Runner& R) {
@@ -2537,7 +2509,7 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     for (int i = 0; i < N; ++i) qoff[i + 1] = qoff[i] + ncomp[i];
     clidx.resize(std::max(qoff[N], 1LL));
     std::vector<unsigned short> cglidx(std::max(coff[N], 1LL));
-    int max_u = 0, max_cu = 0, max_e = 0;
+    int max_u = 0, max_cu = 0;
     {
       // Base items of kItemCells cells are independent: each is built in
       // parallel (and split in halves, first half first, while its unions
@@ -2586,14 +2558,13 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
             SubItem si{c0, nc, {}, {}};
             unions(c0, nc, si.halo, si.chalo);
             const int nu = nc + int(si.halo.size()), ncu = nc + int(si.chalo.size());
-            const long long ne = cell_off[c0 + nc] - cell_off[c0];
-            if ((nu > kMaxUnionExt || ncu > kMaxUnionComp || ne > kMaxItemEntries) && nc > 1) {
+            if ((nu > kMaxUnionExt || ncu > kMaxUnionComp) && nc > 1) {
               const int h1 = nc / 2;  // split, first half processed first
               todo.push_back({c0 + h1, nc - h1});
               todo.push_back({c0, h1});
               continue;
             }
-            if (nu > kMaxUnionExt || ncu > kMaxUnionComp || ne > kMaxItemEntries) {
+            if (nu > kMaxUnionExt || ncu > kMaxUnionComp) {
               too_big = 1;
               break;
             }
@@ -2626,7 +2597,6 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
           items.push_back(it);
           max_u = std::max(max_u, si.nc + nh);
           max_cu = std::max(max_cu, si.nc + nch);
-          max_e = std::max(max_e, int(cell_off[si.c0 + si.nc] - cell_off[si.c0]));
           std::vector<int>().swap(si.halo);
           std::vector<int>().swap(si.chalo);
         }
@@ -2662,9 +2632,6 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     UP(d_off, cell_off);
     UP(d_qoff, qoff);
     UP(d_nbr, e_nbr);
-    // 8 entries of padding: the once-per-step kernel copies an item's local
-    // indices in 16-byte chunks
-    lidx.resize(size_t(std::max(cell_off[N], 1LL)) + 8, 0);
     UP(d_lidx, lidx);
     UP(d_clidx, clidx);
     UP(d_cglidx, cglidx);
@@ -2758,7 +2725,6 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     M->items = items;
     M->max_union = max_u;
     M->max_cunion = max_cu;
-    M->max_item_e = max_e;
     M->nc_dir = coff[N];
     long long n_ef_dir = cell_off[N], n_cf_dir = qoff[N];
     M->stats.ncv = N;
@@ -2943,7 +2909,6 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     R.prec = prec;
     R.max_union = m->max_union;
     R.max_cunion = m->max_cunion;
-    R.max_item_e = m->max_item_e;
     R.launches = &s->launches;
     s->src.N = int(N);
     s->src.perm = m->d_perm;
@@ -3797,14 +3762,13 @@ void batch_free_graph(cgx_batch* b) {
 int batch_rebuild(cgx_batch* b) {
   std::vector<Item> items;
   long long cells = 0;
-  int mu = 0, mcu = 0, mie = 0;
+  int mu = 0, mcu = 0;
   for (size_t k = 0; k < b->slots.size(); ++k) {
     const BatchCase& c = b->slots[k];
     if (!c.s || c.finished) continue;
     cells += c.s->mesh->N;
     mu = std::max(mu, c.s->mesh->max_union);
     mcu = std::max(mcu, c.s->mesh->max_cunion);
-    mie = std::max(mie, c.s->mesh->max_item_e);
     for (const Item& mi : c.s->mesh->items) {
       Item it = mi;
       it.c = int(k);
@@ -3838,10 +3802,9 @@ int batch_rebuild(cgx_batch* b) {
   b->nitems = int(items.size());
   b->active_cells = cells;
   b->run.items = b->d_items;
-  if (mu != b->run.max_union || mcu != b->run.max_cunion || mie != b->run.max_item_e) {
+  if (mu != b->run.max_union || mcu != b->run.max_cunion) {
     b->run.max_union = mu;  // shared-memory sizes of the staged kernels
     b->run.max_cunion = mcu;
-    b->run.max_item_e = mie;
     batch_free_graph(b);
   }
   b->dirty = false;

@@ -51,9 +51,8 @@ __device__ __forceinline__ void prefetch_end_f(const MeshDev& m, const Item& it,
   const int t = threadIdx.x;
   if (a >= b || t >= 6) return;
   if (t == 0) {
-    // the whole item's local indices, staged when the item starts
-    if (sub == 0)
-      prefetch_l2(m.lidx + __ldg(m.off + it.cell0), (__ldg(m.off + it.cell0 + it.ncell) - __ldg(m.off + it.cell0)) * 2);
+    const long long k0 = __ldg(m.off + it.cell0 + a), k1 = __ldg(m.off + it.cell0 + b);
+    prefetch_l2(m.lidx + k0, (k1 - k0) * 2);
     return;
   }
   const long long q0 = __ldg(m.qoff + it.cell0 + a), q1 = __ldg(m.qoff + it.cell0 + b);
@@ -402,12 +401,8 @@ __global__ void __launch_bounds__(256, 3) k_step_end_f(CASE_ARGS, int mode) {
   const Phys& ph = CASE_PH;
   const int nu = it_.ncell + it_.nh;
   int4* sL = smem + swz_chunks<1>(nu);
-  int4* sI = sL + swz_chunks<2>(it_.ncell + it_.nch);
-  const long long ea = m.off[it_.cell0] & ~7LL;
-  const unsigned short* sIdx = reinterpret_cast<const unsigned short*>(sI);  // entry k at [k - ea]
   stage_records<1>(smem, s.QF, it_, m.hcell + it_.hoff, it_.nh);
   stage_records<2>(sL, s.LF, it_, m.chcell + it_.choff, it_.nch);
-  stage_lidx(sI, m.lidx, m.off[it_.cell0], m.off[it_.cell0 + it_.ncell]);
   stage_wait();
   const long long Q = m.Q;
   // limitAsgs's dt: this step's, or outside a step the control block's
@@ -429,7 +424,7 @@ __global__ void __launch_bounds__(256, 3) k_step_end_f(CASE_ARGS, int mode) {
   float vv2 = 0.0f;
   double cfl = 0.0;
   for (long long k = b + lane; k < e; k += G) {
-    const float4 qj = reinterpret_cast<const float4*>(smem)[sIdx[k - ea]];
+    const float4 qj = reinterpret_cast<const float4*>(smem)[__ldg(m.lidx + k)];
     const float dp = qj.y - qi.y;
     const float v_avg = 0.5f * (qi.z + qj.z);
     const float beta = 0.5f * (qi.w + qj.w);
