@@ -2374,71 +2374,70 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       }
     }
     PT.mark("face numbering");
-    // ---- directed entries per cell (new numbering): CSR, compact faces first
-    // (filled in parallel in any order: each cell's entries are sorted by
-    // face id below, so the result is deterministic)
+    // ---- directed entries per cell (new numbering): CSR, each cell's entries
+    // by face id, so compact faces (ids < ncf) come first.  A stable counting
+    // sort of the entries, taken in face-id order, by their cell: per chunk of
+    // face ids a count per cell, the chunks' offsets within each cell, then
+    // the chunks scatter in order.  The result does not depend on the chunking.
     std::vector<int> deg(N, 0), ncomp(N, 0);
-#pragma omp parallel for schedule(static)
-    for (int f = 0; f < nef; ++f) {
-      const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
-      const bool comp = cf_of_ef[f] >= 0;
-      const int na = iperm[a];
-#pragma omp atomic
-      ++deg[na];
-      if (comp) {
-#pragma omp atomic
-        ++ncomp[na];
-      }
-      if (b < N) {
-        const int nb = iperm[b];
-#pragma omp atomic
-        ++deg[nb];
-        if (comp) {
-#pragma omp atomic
-          ++ncomp[nb];
-        }
-      }
-    }
     std::vector<long long> cell_off(N + 1, 0);
-    for (int i = 0; i < N; ++i) cell_off[i + 1] = cell_off[i] + deg[i];
-    uvec<int> e_nbr(cell_off[N]), e_fid(cell_off[N]);
+    uvec<int> e_nbr, e_fid;
     {
-      std::vector<long long> fill(cell_off.begin(), cell_off.end() - 1);
+      uvec<int> ef_of_fid(nef);
 #pragma omp parallel for schedule(static)
-      for (int f = 0; f < nef; ++f) {
-        const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
-        const int na = iperm[a];
-        const int nb = nw(b);
-        long long ka;
-#pragma omp atomic capture
-        ka = fill[na]++;
-        e_nbr[ka] = nb;
-        e_fid[ka] = fnew[f];
-        if (b < N) {
-          long long kb;
-#pragma omp atomic capture
-          kb = fill[nb]++;
-          e_nbr[kb] = na;
-          e_fid[kb] = fnew[f] | kRevBit;
+      for (int f = 0; f < nef; ++f) ef_of_fid[fnew[f]] = f;
+      const int nchunk = std::max(1, std::min(omp_get_max_threads(), 32));
+      auto chunk_lo = [&](int c) { return int((long long)nef * c / nchunk); };
+      uvec<int> cnt(size_t(nchunk) * N);
+#pragma omp parallel for schedule(static, 1)
+      for (int c = 0; c < nchunk; ++c) {
+        int* cc = cnt.data() + size_t(c) * N;
+        std::fill(cc, cc + N, 0);
+        for (int fid = chunk_lo(c); fid < chunk_lo(c + 1); ++fid) {
+          const int f = ef_of_fid[fid];
+          const int b = d->cvoef[2 * size_t(f) + 1];
+          ++cc[iperm[d->cvoef[2 * size_t(f)]]];
+          if (b < N) ++cc[iperm[b]];
         }
       }
-    }
-#pragma omp parallel
-    {
-      std::vector<std::pair<int, int>> tmp;
-#pragma omp for schedule(dynamic, 4096)
+      // per cell: the chunks' counts become their offsets within the cell
+#pragma omp parallel for schedule(static)
       for (int i = 0; i < N; ++i) {
-        const long long b = cell_off[i], e = cell_off[i + 1];
-        tmp.clear();
-        for (long long k = b; k < e; ++k) tmp.push_back({e_fid[k], e_nbr[k]});
-        // compact faces (ids < ncf) first, each part by face id
-        std::sort(tmp.begin(), tmp.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
-          return (x.first & kFidMask) < (y.first & kFidMask);
-        });
-        for (long long k = b; k < e; ++k) {
-          e_fid[k] = tmp[k - b].first;
-          e_nbr[k] = tmp[k - b].second;
+        int run = 0;
+        for (int c = 0; c < nchunk; ++c) {
+          int& v = cnt[size_t(c) * N + i];
+          const int n = v;
+          v = run;
+          run += n;
         }
+        deg[i] = run;
+      }
+      for (int i = 0; i < N; ++i) cell_off[i + 1] = cell_off[i] + deg[i];
+      e_nbr.resize(cell_off[N]);
+      e_fid.resize(cell_off[N]);
+#pragma omp parallel for schedule(static, 1)
+      for (int c = 0; c < nchunk; ++c) {
+        int* cc = cnt.data() + size_t(c) * N;
+        for (int fid = chunk_lo(c); fid < chunk_lo(c + 1); ++fid) {
+          const int f = ef_of_fid[fid];
+          const int a = d->cvoef[2 * size_t(f)], b = d->cvoef[2 * size_t(f) + 1];
+          const int na = iperm[a];
+          const int nb = nw(b);
+          const long long ka = cell_off[na] + cc[na]++;
+          e_nbr[ka] = nb;
+          e_fid[ka] = fid;
+          if (b < N) {
+            const long long kb = cell_off[nb] + cc[nb]++;
+            e_nbr[kb] = na;
+            e_fid[kb] = fid | kRevBit;
+          }
+        }
+      }
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < N; ++i) {
+        int n = 0;
+        for (long long k = cell_off[i]; k < cell_off[i + 1] && (e_fid[k] & kFidMask) < ncf; ++k) ++n;
+        ncomp[i] = n;
       }
     }
     PT.mark("entry CSR");
@@ -2504,11 +2503,12 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
     // whose neighbour unions exceed the shared-memory budget is split
     std::vector<Item> items;
     std::vector<int> hcell, chcell;
-    std::vector<unsigned short> lidx(std::max(cell_off[N], 1LL)), clidx;
+    // (every entry of these is written below)
+    uvec<unsigned short> lidx(std::max(cell_off[N], 1LL)), clidx;
     std::vector<long long> qoff(N + 1, 0);
     for (int i = 0; i < N; ++i) qoff[i + 1] = qoff[i] + ncomp[i];
     clidx.resize(std::max(qoff[N], 1LL));
-    std::vector<unsigned short> cglidx(std::max(coff[N], 1LL));
+    uvec<unsigned short> cglidx(std::max(coff[N], 1LL));
     int max_u = 0, max_cu = 0;
     {
       // Base items of kItemCells cells are independent: each is built in
@@ -2524,30 +2524,44 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       int too_big = 0;
 #pragma omp parallel
       {
+        // per thread: the last (sub)item that listed each cell in its
+        // extended / compact halo, and the cell's local index there
+        std::vector<int> seen_h(N, -1), seen_c(N, -1);
+        uvec<unsigned short> loc_h(N), loc_c(N);
+        int tag = 0;
         // halo of [c0, c0+nc): cells outside it reached by its entries; the
-        // gradient stencil (cvocv) reads the compact union too
+        // gradient stencil (cvocv) reads the compact union too.  Each cell is
+        // listed once (the seen marks), the short lists are sorted, and the
+        // local index of each halo cell is left in loc_h / loc_c.
         auto unions = [&](int c0, int nc, std::vector<int>& halo, std::vector<int>& chalo) {
+          ++tag;
           halo.clear();
           chalo.clear();
           for (int i = c0; i < c0 + nc; ++i) {
             for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
               const int j = e_nbr[k];
               if (j >= c0 && j < c0 + nc) continue;
-              halo.push_back(j);
-              if (k < cell_off[i] + ncomp[i]) chalo.push_back(j);
+              if (seen_h[j] != tag) {
+                seen_h[j] = tag;
+                halo.push_back(j);
+              }
+              if (k < cell_off[i] + ncomp[i] && seen_c[j] != tag) {
+                seen_c[j] = tag;
+                chalo.push_back(j);
+              }
             }
             for (long long k = coff[i]; k < coff[i + 1]; ++k) {
               const int j = c_nbr[k];
-              if (j < c0 || j >= c0 + nc) chalo.push_back(j);
+              if ((j < c0 || j >= c0 + nc) && seen_c[j] != tag) {
+                seen_c[j] = tag;
+                chalo.push_back(j);
+              }
             }
           }
           std::sort(halo.begin(), halo.end());
-          halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
           std::sort(chalo.begin(), chalo.end());
-          chalo.erase(std::unique(chalo.begin(), chalo.end()), chalo.end());
-        };
-        auto local = [](const std::vector<int>& h, int nc, int j) {
-          return (unsigned short)(nc + int(std::lower_bound(h.begin(), h.end(), j) - h.begin()));
+          for (size_t t = 0; t < halo.size() && nc + t <= 0xffff; ++t) loc_h[halo[t]] = (unsigned short)(nc + t);
+          for (size_t t = 0; t < chalo.size() && nc + t <= 0xffff; ++t) loc_c[chalo[t]] = (unsigned short)(nc + t);
         };
 #pragma omp for schedule(dynamic, 16) reduction(| : too_big)
         for (int bi = 0; bi < nbase; ++bi) {
@@ -2572,13 +2586,13 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
               for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) {
                 const int j = e_nbr[k];
                 const bool in = j >= c0 && j < c0 + nc;
-                lidx[k] = in ? (unsigned short)(j - c0) : local(si.halo, nc, j);
+                lidx[k] = in ? (unsigned short)(j - c0) : loc_h[j];
                 const long long t = k - cell_off[i];
-                if (t < ncomp[i]) clidx[qoff[i] + t] = in ? (unsigned short)(j - c0) : local(si.chalo, nc, j);
+                if (t < ncomp[i]) clidx[qoff[i] + t] = in ? (unsigned short)(j - c0) : loc_c[j];
               }
               for (long long k = coff[i]; k < coff[i + 1]; ++k) {
                 const int j = c_nbr[k];
-                cglidx[k] = (j >= c0 && j < c0 + nc) ? (unsigned short)(j - c0) : local(si.chalo, nc, j);
+                cglidx[k] = (j >= c0 && j < c0 + nc) ? (unsigned short)(j - c0) : loc_c[j];
               }
             }
             sub[bi].push_back(std::move(si));
@@ -2600,6 +2614,22 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
           std::vector<int>().swap(si.halo);
           std::vector<int>().swap(si.chalo);
         }
+    }
+    // every local index lies inside its item's staged union (the face
+    // kernels read shared memory at these indices without checks)
+    {
+      int bad_local = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad_local)
+      for (int t = 0; t < int(items.size()); ++t) {
+        const Item& it = items[t];
+        const int nu = it.ncell + it.nh, ncu = it.ncell + it.nch;
+        for (int i = it.cell0; i < it.cell0 + it.ncell; ++i) {
+          for (long long k = cell_off[i]; k < cell_off[i + 1]; ++k) bad_local |= (lidx[k] >= nu);
+          for (long long q = qoff[i]; q < qoff[i + 1]; ++q) bad_local |= (clidx[q] >= ncu);
+          for (long long k = coff[i]; k < coff[i + 1]; ++k) bad_local |= (cglidx[k] >= ncu);
+        }
+      }
+      if (bad_local) return bail(fail(CGX_E_ARG, "internal: local index outside its work item's union"));
     }
     if (hcell.empty()) hcell.push_back(0);
     if (chcell.empty()) chcell.push_back(0);
