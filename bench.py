@@ -789,8 +789,11 @@ def main():
                     help="instead of the throughput bench: FP64 GPU vs CPU oracle over many steps")
     ap.add_argument("--validate-n", type=int, default=128)
     ap.add_argument("--validate-steps", type=int, default=200)
-    ap.add_argument("--device-ops", action="store_true",
-                    help="build the bench mesh's operators on the GPU from the compact mesh")
+    ap.add_argument("--device-ops", dest="device_ops", action="store_true", default=True,
+                    help="build the bench mesh's operators on the GPU from the mesher's compact mesh "
+                         "(the default; bit-identical to the host generator's)")
+    ap.add_argument("--host-ops", dest="device_ops", action="store_false",
+                    help="build the bench mesh with the host generator's operators instead")
     ap.add_argument("--opbuild", action="store_true",
                     help="instead of the throughput bench: operator build on the GPU vs the host generator")
     ap.add_argument("--opbuild-n", type=int, default=128)
