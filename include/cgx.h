@@ -274,6 +274,20 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
 #define CGX_BC_CBC_UPT         4
 #define CGX_BC_CBC_RUNP        5
 #define CGX_BC_CBC_MPT         6
+/* Characteristic zones whose boundary state follows the flow, updated in
+ * each step as the reference's rk3Step of the zone does (before the stage's
+ * RK update) and set after cgx_init_complete as initialHookBcs does:
+ *   CGX_BC_CBC_EXTRAPOLATE  -             the boundary state is the cell's,
+ *                           renewed every stage (CbcExtrapolate,
+ *                           IdealGasSolverBcs.cpp:3436-3445, 3504-3576)
+ *   CGX_BC_CBC_TOTAL_PT     p_total T_total t_relax: each face's normal
+ *                           speed relaxes toward its cell's once per step
+ *                           (eps = 1/(t_relax/dt + 1)), the rest from the
+ *                           isentropic relations (CbcTotalPt,
+ *                           IdealGasSolverBcs.cpp:3372-3434, 3447-3564; the
+ *                           USE_AVG and STATIONARY_FRAME options are not built) */
+#define CGX_BC_CBC_EXTRAPOLATE 7
+#define CGX_BC_CBC_TOTAL_PT    8
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,

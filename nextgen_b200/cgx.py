@@ -158,6 +158,8 @@ CGX_BC_WALL_ISOTHERMAL = 3
 CGX_BC_CBC_UPT = 4
 CGX_BC_CBC_RUNP = 5
 CGX_BC_CBC_MPT = 6
+CGX_BC_CBC_EXTRAPOLATE = 7
+CGX_BC_CBC_TOTAL_PT = 8
 
 
 class Source(ctypes.Structure):
@@ -339,7 +341,8 @@ class Solver:
     def set_bc_params(self, zone, kind, params=()):
         """Boundary condition with the reference's zone parameters in input
         order: WALL_ISOTHERMAL (T), CBC_UPT (u0 u1 u2 p T), CBC_RUNP
-        (rho un p), CBC_MPT (mdot p T); SLIP and WALL_ADIABATIC as set_bc."""
+        (rho un p), CBC_MPT (mdot p T), CBC_EXTRAPOLATE (none), CBC_TOTAL_PT
+        (p_total T_total t_relax); SLIP and WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))
 

@@ -1121,19 +1121,27 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
       for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d] + visc * u[d];
       fr[4] -= kc * (T - z.a[3]);
     } else {
-      const double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
       RiemannState sc, sb;
+      if (kind >= CGX_BC_CBC_EXTRAPOLATE) {  // the face's own boundary state
+        const double* q = s.bfs + f;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        sc.u[d] = u[d];
-        sb.u[d] = z.a[d] + z.a[3] * n[d] / area;
+        for (int d = 0; d < 3; ++d) sb.u[d] = q[d * m.nbf];
+        sb.sp_vol = q[3 * m.nbf];
+        sb.p = q[4 * m.nbf];
+        sb.h = q[5 * m.nbf];
+      } else {
+        const double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sb.u[d] = z.a[d] + z.a[3] * n[d] / area;
+        sb.p = z.a[4];
+        sb.sp_vol = z.a[5];
+        sb.h = z.a[6];
       }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) sc.u[d] = u[d];
       sc.sp_vol = 1.0 / rho;
       sc.p = pf;
       sc.h = c.ph.R * gamma * (1.0 / (gamma - 1.0)) * T;
-      sb.p = z.a[4];
-      sb.sp_vol = z.a[5];
-      sb.h = z.a[6];
       double F[5];
       hllc_flux(F, n, sc, sb, gamma);
       fr[0] -= F[0];
@@ -1146,6 +1154,66 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
   double* r = s.rhs + size_t(stage) * 5 * N;
 #pragma unroll
   for (int q = 0; q < 5; ++q) r[q * N + i] += fr[q];
+}
+
+// rk3Step of the zones whose boundary state follows the flow, one thread per
+// cell with boundary faces, on the stage's state before its RK update (the
+// reference calls the zones' rk3Step just before its own):
+//   CBC_EXTRAPOLATE  every stage, the boundary state is the cell's
+//                    (CbcExtrapolate::calcBfState, IdealGasSolverBcs.cpp:3436-3445)
+//   CBC_TOTAL_PT     stage 1: un_bc = (1 - eps) un_bc + eps u.n_hat with
+//                    eps = 1/(t_relax/dt + 1), then T = T_total - un^2/(2 cp),
+//                    rho and p from the isentropic relations and u = un n_hat
+//                    (CbcTotalPt::rk3Step, :3526-3564, and calcBfState, :3414-3434)
+// init: the zones' initialHook after initComplete (:3447-3523): CBC_TOTAL_PT
+// starts from un_bc = u.n_hat.
+__global__ void __launch_bounds__(128) k_bc_stage(const CaseDev c, int stage, int init) {
+  const MeshDev& m = c.m;
+  const StateDev& s = c.s;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.nbc) return;
+  const int i = m.bcell[t];
+  const double gamma = c.ph.gamma, R = c.ph.R;
+  const double rho = s.rho[i], rhoE = s.rhoE[i];
+  const double u[3] = {s.u0[i], s.u1[i], s.u2[i]};
+  const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const double p = (gamma - 1.0) * (rhoE - 0.5 * rho * usq);
+  const double T = p / (rho * R);
+  for (int f = m.bfc[i]; f < m.bfc[i + 1]; ++f) {
+    const BcZone& z = s.bc[m.bf_zone[f]];
+    double* q = s.bfs + f;
+    if (z.kind == CGX_BC_CBC_EXTRAPOLATE) {
+      const double cp = R * gamma / (gamma - 1.0);
+      q[3 * m.nbf] = 1.0 / rho;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) q[d * m.nbf] = u[d];
+      q[4 * m.nbf] = p;
+      q[5 * m.nbf] = cp * T;
+    } else if (z.kind == CGX_BC_CBC_TOTAL_PT && (init || stage == 1)) {
+      const double n[3] = {m.bf_n[f], m.bf_n[m.nbf + f], m.bf_n[2 * m.nbf + f]};
+      const double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      const double nh[3] = {n[0] / area, n[1] / area, n[2] / area};
+      const double un0 = u[0] * nh[0] + u[1] * nh[1] + u[2] * nh[2];
+      double un = un0;
+      if (!init) {
+        const double eps = 1.0 / (z.a[2] / s.ctl->dt + 1.0);
+        un = (1.0 - eps) * s.un_bc[f] + eps * un0;
+      }
+      s.un_bc[f] = un;
+      const double p_tot = z.a[0], t_tot = z.a[1];
+      const double total_rh = p_tot / R / t_tot;
+      const double invgm1 = 1.0 / (gamma - 1.0);
+      const double cp = R * gamma * invgm1;
+      const double T_bc = t_tot - 0.5 * un * un / cp;
+      const double rho_bc = total_rh * pow(T_bc / t_tot, invgm1);
+      const double p_bc = p_tot * pow(T_bc / t_tot, gamma * invgm1);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) q[d * m.nbf] = un * nh[d];
+      q[3 * m.nbf] = 1.0 / rho_bc;
+      q[4 * m.nbf] = p_bc;
+      q[5 * m.nbf] = cp * T_bc;
+    }
+  }
 }
 
 // report() totals: per-block partial sums in a fixed tree, then one block
@@ -1918,6 +1986,14 @@ int enqueue_bf(const Runner& R, int stage0) {
   return launch_check(R, 1);
 }
 
+// the zones' rk3Step at stage `stage` (1..3), or their initial hooks
+int enqueue_bc_stage(const Runner& R, int stage, bool init) {
+  const int nbc = R.dcase.m.nbc;
+  if (!R.direct || nbc == 0 || !R.dcase.s.bc_dyn) return CGX_OK;
+  k_bc_stage<<<(nbc + 127) / 128, 128, 0, R.stream>>>(R.dcase, stage, init ? 1 : 0);
+  return launch_check(R, 1);
+}
+
 int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
   int rc = enqueue_faces(R, stage0);
   if (rc) return rc;
@@ -1930,7 +2006,7 @@ int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
 // zones and sources)
 inline int launches_per_step(const Runner& R) {
   int n = kLaunchesPerStep + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
-          ((R.direct && R.dcase.m.nbc > 0) ? 3 : 0);
+          ((R.direct && R.dcase.m.nbc > 0) ? 3 : 0) + ((R.direct && R.dcase.m.nbc > 0 && R.dcase.s.bc_dyn) ? 3 : 0);
   if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0));
   return n;
 }
@@ -2058,6 +2134,7 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
     } else if ((rc = enqueue_rhs(R, st))) {
       return rc;
     }
+    if ((rc = enqueue_bc_stage(R, st + 1, false))) return rc;
     if ((rc = enqueue_prim(R, st + 1, kRkW[st], -1.0, st == 2))) return rc;
     if ((rc = enqueue_grad(R))) return rc;
   }
@@ -2906,6 +2983,14 @@ extern "C" int cgx_solver_create(cgx_mesh* m, const cgx_params* p, cgx_precision
     if (cudaMemcpyAsync(d_bc, s->bc.data(), s->bc.size() * sizeof(BcZone), cudaMemcpyHostToDevice, s->stream) !=
         cudaSuccess)
       return bail(fail(CGX_E_CUDA, "boundary condition table upload failed"));
+    // per-face boundary states of the zones that follow the flow
+    const size_t nbf = size_t(std::max(m->md.nbf, 1));
+    AL(sd.bfs, 6 * nbf);
+    AL(sd.un_bc, nbf);
+    sd.bc_dyn = 0;
+    if (cudaMemsetAsync(sd.bfs, 0, 6 * nbf * sizeof(double), s->stream) != cudaSuccess ||
+        cudaMemsetAsync(sd.un_bc, 0, nbf * sizeof(double), s->stream) != cudaSuccess)
+      return bail(fail(CGX_E_CUDA, "cudaMemset failed"));
   }
 #undef AL
   const bool zero_ok =
@@ -3269,6 +3354,8 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
     case CGX_BC_CBC_UPT: want = 5; break;
     case CGX_BC_CBC_RUNP: want = 3; break;
     case CGX_BC_CBC_MPT: want = 3; break;
+    case CGX_BC_CBC_EXTRAPOLATE: want = 0; break;
+    case CGX_BC_CBC_TOTAL_PT: want = 3; break;
     default: return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition");
   }
   if (nparams != want)
@@ -3303,6 +3390,9 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
       z.a[6] = R * T * gamma / (gamma - 1.0);
       break;
     }
+    case CGX_BC_CBC_TOTAL_PT:  // CbcTotalPt::initData: p_total, T_total, t_relax
+      for (int d = 0; d < 3; ++d) z.a[d] = params[d];
+      break;
     case CGX_BC_CBC_MPT: {  // CbcMpt::initData: u = un n/|n|, un = -mdot/(rho area)
       const double mdot = params[0], p = params[1], T = params[2];
       const double rho = p / T / R;
@@ -3319,6 +3409,17 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
   s->bc[size_t(zone)] = z;
   CK(cudaMemcpyAsync(const_cast<BcZone*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(BcZone),
                      cudaMemcpyHostToDevice, s->stream));
+  // zones whose state follows the flow add a kernel to each stage
+  int dyn = 0;
+  for (const BcZone& b : s->bc)
+    dyn |= (b.kind == CGX_BC_CBC_EXTRAPOLATE ? 1 : 0) | (b.kind == CGX_BC_CBC_TOTAL_PT ? 2 : 0);
+  if (dyn != s->sd.bc_dyn) {
+    s->sd.bc_dyn = dyn;
+    s->hcase.s = s->sd;
+    s->run.dcase.s = s->sd;
+    CK(cudaMemcpyAsync(s->d_case, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream));
+    drop_graphs(s);
+  }
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
@@ -3353,6 +3454,8 @@ static int init_complete(cgx_solver* s, bool tune) {
     if ((rc = cgx_update_primitive(s))) return rc;
     if ((rc = cgx_calc_sgs_props(s))) return rc;
   }
+  // initialHookBcs
+  if ((rc = enqueue_bc_stage(s->run, 0, true))) return rc;
   s->inited = true;
   s->have_store = false;
   return store_state(s);

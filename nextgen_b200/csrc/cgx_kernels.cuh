@@ -221,6 +221,12 @@ struct StateDev {
   double* mf;      // [E] mass flux of each extended entry, entry direction
   // boundary conditions per boundary zone
   const struct BcZone* bc;
+  // per boundary face: the boundary state of zones whose state follows the
+  // flow ([6][nbf]: u[3], sp_vol, p, h) and CBC_TOTAL_PT's normal speed
+  // ([nbf]); bc_dyn: such zones exist (1 extrapolated, 2 total p/T)
+  double* bfs;
+  double* un_bc;
+  int bc_dyn;
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

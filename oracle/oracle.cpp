@@ -137,6 +137,7 @@ struct orc_solver {
   std::vector<double> n_bf, aod_bf;
   std::vector<std::array<double, 5>> bc;
   std::vector<IdealGasState> bf_state;
+  std::vector<double> un_bc;  // CBC_TOTAL_PT: each face's relaxed normal speed
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
@@ -481,6 +482,64 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
   }
 }
 
+// CbcExtrapolate::calcBfState (IdealGasSolverBcs.cpp:3436-3445) and
+// CbcTotalPt::calcBfState (:3414-3434, no frame rotation)
+void extrapolate_bf_state(orc_solver* o, int ibf) {
+  const double gamma = o->prm.gamma;
+  const double cp = o->R_gas * gamma / (gamma - 1.0);
+  const int icv = o->cvobf[ibf];
+  IdealGasState& b = o->bf_state[ibf];
+  b.sp_vol = 1.0 / o->rho[icv];
+  for (int i = 0; i < 3; ++i) b.u[i] = o->u[3 * size_t(icv) + i];
+  b.p = o->p[icv];
+  b.h = cp * o->T[icv];
+}
+
+void total_pt_bf_state(orc_solver* o, int ibf, const double unit_n[3]) {
+  const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
+  const double total_p = bc[1], total_t = bc[2];
+  const double gamma = o->prm.gamma;
+  IdealGasState& b = o->bf_state[ibf];
+  for (int i = 0; i < 3; ++i) b.u[i] = o->un_bc[ibf] * unit_n[i] + 0.0;
+  const double total_rh = total_p / o->R_gas / total_t;
+  const double invgm1 = 1.0 / (gamma - 1.0);
+  const double cp = o->R_gas * gamma * invgm1;
+  const double T_bc = total_t - 0.5 * o->un_bc[ibf] * o->un_bc[ibf] / cp;
+  const double rho_bc = total_rh * std::pow(T_bc / total_t, invgm1);
+  const double p_bc = total_p * std::pow(T_bc / total_t, gamma * invgm1);
+  b.sp_vol = 1.0 / rho_bc;
+  b.p = p_bc;
+  b.h = cp * T_bc;
+}
+
+// The zones' rk3Step before the solver's own (advanceSolution,
+// IdealGasSolver.hpp:414-594): CbcExtrapolate renews its state every stage
+// (:3566-3576); CbcTotalPt relaxes un_bc at stage 1 (:3526-3564, without
+// USE_AVG).  init: their initialHook after initComplete (:3447-3523).
+void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
+    const int kind = int(bc[0]);
+    if (kind == CGX_BC_CBC_EXTRAPOLATE) {
+      extrapolate_bf_state(o, ibf);
+    } else if (kind == CGX_BC_CBC_TOTAL_PT && (init || rk_stage == 1)) {
+      const double* n = &o->n_bf[3 * size_t(ibf)];
+      const double bf_area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      const double unit_n[3] = {n[0] / bf_area, n[1] / bf_area, n[2] / bf_area};
+      const double* u = &o->u[3 * size_t(o->cvobf[ibf])];
+      const double un0 = u[0] * unit_n[0] + u[1] * unit_n[1] + u[2] * unit_n[2];
+      if (init) {
+        o->un_bc[ibf] = unit_n[0] * u[0] + unit_n[1] * u[1] + unit_n[2] * u[2];
+      } else {
+        const double t_relax = bc[3];
+        const double eps = 1.0 / (t_relax / dt + 1.0);
+        o->un_bc[ibf] = (1.0 - eps) * o->un_bc[ibf] + eps * un0;
+      }
+      total_pt_bf_state(o, ibf, unit_n);
+    }
+  }
+}
+
 void calc_rhs(orc_solver* o, IdealGasRhs* rhs, double* rhs_sc = nullptr) {
   const bool sc = o->nsc > 0 && rhs_sc;
   add_boundary_flux(o, rhs);
@@ -780,6 +839,7 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->aod_bf.assign(m->area_over_delta_bf, m->area_over_delta_bf + m->nbf);
     o->bc.assign(m->nbf_zones, {0.0, 0.0, 0.0, 0.0, 0.0});
     o->bf_state.assign(m->nbf, IdealGasState());
+    o->un_bc.assign(m->nbf, 0.0);
   }
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
@@ -945,6 +1005,7 @@ extern "C" void orc_get_state(const orc_solver* o, double* rho, double* u, doubl
 extern "C" void orc_init_complete(orc_solver* o) {
   update_primitive(o);
   calc_sgs_props(o);
+  bc_rk3_step(o, 0, 0.0, true);  // initialHookBcs
   store_data(o);
 }
 
@@ -1014,14 +1075,17 @@ extern "C" int orc_advance_solution(orc_solver* o) {
   for (int k = 0; k < 3; ++k) zero_rhs(o, k);
   const double dt = o->dt;
   calc_rhs(o, o->rhs[0].data(), o->rhs_sc[0].data());
+  bc_rk3_step(o, 1, dt, false);
   rk3_step(o, erk_wgt3[0], dt);
   o->time += dt;
   update_primitive(o);
   calc_rhs(o, o->rhs[1].data(), o->rhs_sc[1].data());
+  bc_rk3_step(o, 2, dt, false);
   rk3_step(o, erk_wgt3[1], dt);
   o->time -= 0.5 * dt;
   update_primitive(o);
   calc_rhs(o, o->rhs[2].data(), o->rhs_sc[2].data());
+  bc_rk3_step(o, 3, dt, false);
   rk3_step(o, erk_wgt3[2], dt);
   o->time += 0.5 * dt;
   update_primitive(o);
@@ -1107,10 +1171,15 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
   if (kind == CGX_BC_SLIP || kind == CGX_BC_WALL_ADIABATIC)
     return (np == 0 || (kind == CGX_BC_WALL_ADIABATIC && np == 3)) ? orc_set_bc(o, zone, kind, np ? prm : nullptr) : -1;
   const int want = kind == CGX_BC_WALL_ISOTHERMAL ? 1 : kind == CGX_BC_CBC_UPT ? 5
-                 : (kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT) ? 3 : -1;
-  if (want < 0 || np != want || !prm) return -1;
+                 : (kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT || kind == CGX_BC_CBC_TOTAL_PT) ? 3
+                 : kind == CGX_BC_CBC_EXTRAPOLATE ? 0 : -1;
+  if (want < 0 || np != want || (np > 0 && !prm)) return -1;
   o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, kind == CGX_BC_WALL_ISOTHERMAL ? prm[0] : 0.0};
-  if (kind == CGX_BC_WALL_ISOTHERMAL) return 0;
+  if (kind == CGX_BC_WALL_ISOTHERMAL || kind == CGX_BC_CBC_EXTRAPOLATE) return 0;
+  if (kind == CGX_BC_CBC_TOTAL_PT) {  // CbcTotalPt::initData: p_total, T_total, t_relax
+    o->bc[zone] = {double(kind), prm[0], prm[1], prm[2], 0.0};
+    return 0;
+  }
   const double R = o->R_gas, gamma = o->prm.gamma;
   double area_global = 0.0;
   for (int ibf = 0; ibf < o->nbf; ++ibf)

@@ -76,8 +76,9 @@ void orc_set_source(orc_solver* o, double A, const double g[3], const double* fi
 int orc_set_bc(orc_solver* o, int zone, int kind, const double u_wall[3]);
 /* Boundary condition with the reference's zone parameters (the kinds and
  * parameter lists of cgx_set_bc_params): WALL_ISOTHERMAL T, CBC_UPT u p T,
- * CBC_RUNP rho un p, CBC_MPT mdot p T; SLIP and WALL_ADIABATIC as
- * orc_set_bc.  0, or -1 on a bad argument. */
+ * CBC_RUNP rho un p, CBC_MPT mdot p T, CBC_EXTRAPOLATE, CBC_TOTAL_PT p_total
+ * T_total t_relax; SLIP and WALL_ADIABATIC as orc_set_bc.  0, or -1 on a bad
+ * argument. */
 int orc_set_bc_params(orc_solver* o, int zone, int kind, const double* params, int nparams);
 /* write a NaN into rho[icv] (host-side fault injection for the NaN path) */
 void orc_poison(orc_solver* o, int icv);

@@ -20,7 +20,7 @@ from nextgen_b200 import cases
 from nextgen_b200.meshgen import ChannelMesh
 from oracle import Oracle
 
-UPT, RUNP, MPT, ISO = 4, 5, 6, 3
+UPT, RUNP, MPT, ISO, EXTRAP, TOTAL_PT = 4, 5, 6, 3, 7, 8
 need_ref = pytest.mark.skipif(not orc_mod.ref_available(), reason="reference-built oracle absent")
 
 
@@ -63,6 +63,33 @@ def test_uniform_flow_through_cbc_zones(chan, outflow):
     o.close()
 
 
+def test_uniform_flow_through_flow_following_zones(chan):
+    """CBC_TOTAL_PT inflow (the flow's total pressure and temperature, normal
+    to the zone) and CBC_EXTRAPOLATE outflow: a uniform flow stays uniform
+    over RK3 steps, with the total-pressure zone's relaxation active."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    rho, u, p = _uniform(m, prm, u=(0.0, 0.3, 0.0))
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+    gamma = prm.gamma
+    T0 = p[0] / (rho[0] * R)
+    cp = R * gamma / (gamma - 1.0)
+    T_tot = T0 + 0.5 * 0.3 ** 2 / cp
+    p_tot = p[0] * (T_tot / T0) ** (gamma / (gamma - 1.0))
+    o = Oracle(m, prm)
+    o.set_bc_params(0, TOTAL_PT, [p_tot, T_tot, 0.01])
+    o.set_bc_params(1, EXTRAP, [])
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    r, _ = o.calc_rhs(1)
+    ref = (rho[0] * 0.3 ** 2 + p[0]) * np.linalg.norm(m.n_bf, axis=1).max()
+    assert np.abs(r).max() <= 1e-12 * ref
+    assert o.step(5) == 0
+    r2, u2, e2 = o.get_state()
+    assert np.abs(r2 - rho).max() <= 1e-12 and np.abs(u2 - u).max() <= 1e-12
+    o.close()
+
+
 def test_isothermal_walls(chan):
     m = chan
     prm = cases.tgv_params(Re=400.0)
@@ -98,6 +125,8 @@ def test_bad_parameters_refused(chan):
         o.set_bc_params(0, UPT, [1.0, 2.0])
     with pytest.raises(ValueError):
         o.set_bc_params(0, 9, [])
+    with pytest.raises(ValueError):
+        o.set_bc_params(0, EXTRAP, [1.0])
     o.close()
 
 

@@ -7,6 +7,8 @@ adds the wall's viscous and heat fluxes (IdealGasSolverBcs.cpp:1485-1510).
 
 * calcRhs per cell within 1e-12 of the face-sum scale and calcCfl within
   1e-12, for an inflow/outflow pair of each kind and a hot isothermal wall;
+  CBC_TOTAL_PT and CBC_EXTRAPOLATE set their boundary states after
+  initComplete and renew them in each step (rk3Step of the zone);
 * 10 RK3 steps: state within 1e-10 of the oracle's;
 * a uniform flow through the channel stays uniform (rhs = 0 to round-off);
 * the mixed-precision form within its flux tolerance of the FP64 path;
@@ -23,12 +25,15 @@ from oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 UPT, RUNP, MPT, ISO = cgx.CGX_BC_CBC_UPT, cgx.CGX_BC_CBC_RUNP, cgx.CGX_BC_CBC_MPT, cgx.CGX_BC_WALL_ISOTHERMAL
+EXTRAP, TOTAL_PT = cgx.CGX_BC_CBC_EXTRAPOLATE, cgx.CGX_BC_CBC_TOTAL_PT
 P0 = cases.tgv_params(Re=400.0).p_ref  # T_ref = rho_ref = 1
 # inflow at y = 0, outflow through the 4 x 2 zone at y = Ly
 ZONES = {
     "upt_runp": ((UPT, (0.1, 0.4, 0.0, 1.01 * P0, 1.02)), (RUNP, (1.0, -0.3, 0.99 * P0))),
     "upt_mpt": ((UPT, (0.0, 0.35, 0.05, P0, 1.0)), (MPT, (-2.4, P0, 1.0))),
     "iso_mpt": ((ISO, (1.2,)), (MPT, (-2.4, P0, 1.0))),
+    # boundary states that follow the flow: renewed each step / each stage
+    "totalpt_extrap": ((TOTAL_PT, (1.02 * P0, 1.02, 0.05)), (EXTRAP, ())),
 }
 
 
@@ -77,7 +82,7 @@ def test_cbc_rhs_and_cfl_match_oracle(chan, name):
     o.close()
 
 
-@pytest.mark.parametrize("name", ["upt_runp", "iso_mpt"])
+@pytest.mark.parametrize("name", ["upt_runp", "iso_mpt", "totalpt_extrap"])
 def test_cbc_steps_match_oracle(chan, name):
     m, gm = chan
     prm = cases.tgv_params(Re=400.0)
