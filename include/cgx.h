@@ -288,6 +288,18 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *                           USE_AVG and STATIONARY_FRAME options are not built) */
 #define CGX_BC_CBC_EXTRAPOLATE 7
 #define CGX_BC_CBC_TOTAL_PT    8
+/* Navier-Stokes characteristic zones: each face carries its own rho, p, u,
+ * advanced by the zone's characteristic equations with the solver's RK3
+ * weights (Nscbc::rk3Step, IdealGasSolverBcs.cpp:3651-3660), and stored and
+ * restored with the state on a NaN (Nscbc::storeData/restoreData, :3578-3606):
+ *   CGX_BC_NSCBC_MT        mdot T       subsonic inflow at a fixed mass flow
+ *                          rate and static temperature (NscbcMt, :3722-3844;
+ *                          the T_TOTAL form is not built)
+ *   CGX_BC_NSCBC_OUTLET_P  p_ref sigma L_ref   partially reflecting pressure
+ *                          outlet (NscbcOutletP, :3846-4092; sigma < 0: constant
+ *                          pressure; the MDOT form is not built) */
+#define CGX_BC_NSCBC_MT        9
+#define CGX_BC_NSCBC_OUTLET_P  10
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
@@ -361,6 +373,12 @@ long long cgx_launch_count(const cgx_solver* s);
  * reference, which divides in IEEE FP64): out[i] = that reciprocal of x[i]
  * for n host values, evaluated on `device`. */
 int cgx_selftest_rcp(int device, const double* x, double* out, int n);
+/* Host threads that the calling thread's later calls run their parallel
+ * host phases on (cgx_mesh_create, cgx_operators_build's host side, the
+ * host generator): n > 0 sets the count, n <= 0 restores all cores.  Other
+ * threads are not affected, so a thread that admits new meshes while others
+ * step can leave cores to them. */
+int cgx_set_host_threads(int n);
 
 /*
  * Batched and served form (no single reference counterpart: the reference

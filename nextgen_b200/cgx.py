@@ -149,7 +149,7 @@ EXPORTS = [
     "cgx_get_time", "cgx_totals", "cgx_get_primitive", "cgx_get_grad", "cgx_get_aux",
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
-    "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params",
+    "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params", "cgx_set_host_threads",
 ]
 
 CGX_BC_SLIP = 1
@@ -160,6 +160,8 @@ CGX_BC_CBC_RUNP = 5
 CGX_BC_CBC_MPT = 6
 CGX_BC_CBC_EXTRAPOLATE = 7
 CGX_BC_CBC_TOTAL_PT = 8
+CGX_BC_NSCBC_MT = 9
+CGX_BC_NSCBC_OUTLET_P = 10
 
 
 class Source(ctypes.Structure):
@@ -217,6 +219,7 @@ def lib():
         "cgx_set_source": (ctypes.c_int, [vp, ctypes.POINTER(Source)]),
         "cgx_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
         "cgx_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "cgx_set_host_threads": (ctypes.c_int, [ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
         "cgx_get_rhs_sc": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p]),
@@ -249,6 +252,12 @@ def _check(rc):
     if rc != 0:
         raise CgxError(rc, lib().cgx_last_error().decode())
     return rc
+
+
+def set_host_threads(n):
+    """Host threads for the calling thread's later parallel host phases
+    (mesh set-up); n <= 0 restores all cores.  Other threads are unaffected."""
+    _check(lib().cgx_set_host_threads(int(n)))
 
 
 def _out(n, *shape):
@@ -342,7 +351,8 @@ class Solver:
         """Boundary condition with the reference's zone parameters in input
         order: WALL_ISOTHERMAL (T), CBC_UPT (u0 u1 u2 p T), CBC_RUNP
         (rho un p), CBC_MPT (mdot p T), CBC_EXTRAPOLATE (none), CBC_TOTAL_PT
-        (p_total T_total t_relax); SLIP and WALL_ADIABATIC as set_bc."""
+        (p_total T_total t_relax), NSCBC_MT (mdot T), NSCBC_OUTLET_P
+        (p_ref sigma L_ref); SLIP and WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))
 

@@ -226,7 +226,10 @@ struct StateDev {
   // ([nbf]); bc_dyn: such zones exist (1 extrapolated, 2 total p/T)
   double* bfs;
   double* un_bc;
-  int bc_dyn;
+  // NSCBC zones, per boundary face ([20][nbf]): rho_bc, p_bc, u_bc[3], then
+  // the characteristic rhs of stages 1..3 (5 each)
+  double* nsb;
+  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

@@ -13,6 +13,7 @@ advances all resident cases together one graph replay per step
 latency) and aggregate throughput; `run_sequential()` runs the same cases
 one at a time on the plain FP64 path for comparison.
 """
+import os
 import queue
 import threading
 import time
@@ -103,6 +104,8 @@ def serve(requests, hbm_budget=96 << 30, chunk=8, max_cases=256, device=0, keep_
 
     def prepare_all():
         try:
+            # leave host cores to the stepping threads while meshes are set up
+            cgx.set_host_threads(max(1, (os.cpu_count() or 1) - 4))
             for r in order:
                 while not stop.is_set() and now() < r.arrival:
                     time.sleep(min(0.005, max(0.0, r.arrival - now())))

@@ -138,6 +138,9 @@ struct orc_solver {
   std::vector<std::array<double, 5>> bc;
   std::vector<IdealGasState> bf_state;
   std::vector<double> un_bc;  // CBC_TOTAL_PT: each face's relaxed normal speed
+  // NSCBC zones: each face's rho, p, u and the characteristic rhs of the
+  // three stages (Nscbc::initData, IdealGasSolverBcs.cpp:3615-3628)
+  std::vector<double> ns_rho, ns_p, ns_u, ns_rhs;
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
@@ -462,6 +465,19 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         for (int i = 0; i < 3; ++i)
           rhs[icv].rhou[i] -= o->p[icv] * n[i] + visc_coeff * (o->u[3 * size_t(icv) + i] - 0.0);
         rhs[icv].rhoE -= k_coeff * (o->T[icv] - bc[4]);
+      } else if (kind == CGX_BC_NSCBC_MT || kind == CGX_BC_NSCBC_OUTLET_P) {
+        // Nscbc::addBoundaryFlux (IdealGasSolverBcs.cpp:3662-3693)
+        const double gogm1 = gamma / (gamma - 1.0);
+        IdealGasState bs;
+        for (int i = 0; i < 3; ++i) bs.u[i] = o->ns_u[3 * size_t(ibf) + i];
+        bs.sp_vol = 1.0 / o->ns_rho[ibf];
+        bs.p = o->ns_p[ibf];
+        bs.h = gogm1 * o->ns_p[ibf] * (1.0 / o->ns_rho[ibf]);
+        IdealGasRhs flux;
+        calcRiemannFlux(flux, n, o->cv_light[icv], bs, gamma, gamma);
+        rhs[icv].rho -= flux.rho;
+        for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= flux.rhou[i];
+        rhs[icv].rhoE -= flux.rhoE;
       } else if (kind >= CGX_BC_CBC_UPT) {
         IdealGasRhs flux;
         calcRiemannFlux(flux, n, o->cv_light[icv], o->bf_state[ibf], gamma, gamma);
@@ -478,6 +494,84 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         }
         rhs[icv].rhoE -= visc_work;
       }
+    }
+  }
+}
+
+// The NSCBC characteristic rhs (src/charles/BcCommon.hpp:312-470): the
+// subsonic inflow at fixed mass flux and temperature (rhs[0] only; nothing
+// when the outgoing acoustic speed is negative) and the partially
+// reflecting outlet (rhs[0..4]: rho, p, u).
+void nscbc_inlet_rhs(double* rhs, const double unit_n[3], double delta, double rho_bc, const double u_bc[3],
+                     double p_bc, const double u_cv[3], double p_cv, double gamma) {
+  const double u0 = u_cv[0] * unit_n[0] + u_cv[1] * unit_n[1] + u_cv[2] * unit_n[2];
+  const double un_bc = u_bc[0] * unit_n[0] + u_bc[1] * unit_n[1] + u_bc[2] * unit_n[2];
+  const double dudn = (un_bc - u0) / delta;
+  const double dpdn = (p_bc - p_cv) / delta;
+  const double sos_bc = std::sqrt(gamma * p_bc / rho_bc);
+  const double lam5 = u0 + sos_bc;
+  if (lam5 < 0.0) return;
+  const double L5 = lam5 * (dpdn + rho_bc * sos_bc * dudn);
+  const double Ma = un_bc / sos_bc;
+  double L1 = -(1.0 + Ma * gamma) / (Ma - 1.0) * L5;
+  L1 /= (1.0 + Ma / (Ma - 1.0) * (gamma - 1.0));
+  const double L2 = 0.5 * (gamma - 1.0) * (L5 + L1);
+  rhs[0] = -(L2 + 0.5 * (L5 + L1)) / sos_bc / sos_bc;
+}
+
+void nscbc_outlet_rhs(double* rhs, const double unit_n[3], double delta, double rho_bc, const double u_bc[3],
+                      double p_bc, double rho_cv, const double u_cv[3], double p_cv, double gamma, double L_ref,
+                      double sigma, double p_ref) {
+  const double un_bc = std::max(0.0, u_bc[0] * unit_n[0] + u_bc[1] * unit_n[1] + u_bc[2] * unit_n[2]);
+  const double u0 = std::max(0.0, u_cv[0] * unit_n[0] + u_cv[1] * unit_n[1] + u_cv[2] * unit_n[2]);
+  const double sos_bc = std::sqrt(gamma * p_bc / rho_bc);
+  const double Ma = un_bc / sos_bc;
+  const double dudn = (un_bc - u0) / delta;
+  const double dpdn = (p_bc - p_cv) / delta;
+  const double L5 = (un_bc + sos_bc) * (dpdn + rho_bc * sos_bc * dudn);
+  double dudn_[3];
+  for (int i = 0; i < 3; ++i) dudn_[i] = (u_bc[i] - u_cv[i]) / delta;
+  double L1;
+  if (sigma >= 0.0)
+    L1 = sigma * (1.0 - Ma * Ma) * sos_bc / L_ref * (p_bc - p_ref);
+  else
+    L1 = -L5;
+  const double drhodn = (rho_bc - rho_cv) / delta;
+  const double L2 = un_bc * (sos_bc * sos_bc * drhodn - dpdn);
+  if (Ma >= 1.0) L1 = sos_bc * (Ma - 1.0) * (dpdn - rho_bc * sos_bc * dudn);
+  rhs[0] = -(L2 + 0.5 * (L5 + L1)) / sos_bc / sos_bc;
+  rhs[1] = -0.5 * (L5 + L1);
+  for (int i = 0; i < 3; ++i)
+    rhs[2 + i] = -(rho_bc * un_bc * dudn_[i] + 0.5 * rho_bc * sos_bc * (1.0 - Ma) * dudn * unit_n[i]) / rho_bc -
+                 0.5 * (1.0 + Ma) * dpdn * unit_n[i] / rho_bc + 0.5 * L1 * unit_n[i] / sos_bc / rho_bc;
+}
+
+// The NSCBC zones' calcRhs at stage rk_stage, before the solver's:
+// NscbcMt::calcRhs (IdealGasSolverBcs.cpp:3777-3844, static T) and
+// NscbcOutletP::calcRhsPressure (:4009-4056), without frame rotation.
+void bc_calc_rhs(orc_solver* o, int rk_stage) {
+  const double gamma = o->prm.gamma;
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
+    const int kind = int(bc[0]);
+    if (kind != CGX_BC_NSCBC_MT && kind != CGX_BC_NSCBC_OUTLET_P) continue;
+    const double* n = &o->n_bf[3 * size_t(ibf)];
+    const double bf_area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const double unit_n[3] = {n[0] / bf_area, n[1] / bf_area, n[2] / bf_area};
+    const int icv = o->cvobf[ibf];
+    const double delta = bf_area / o->aod_bf[ibf];
+    double* u_bc = &o->ns_u[3 * size_t(ibf)];
+    double* rhs = &o->ns_rhs[15 * size_t(ibf) + 5 * size_t(rk_stage - 1)];
+    if (kind == CGX_BC_NSCBC_MT) {
+      const double rhoun_bc = bc[1], RT_bc = bc[2] * o->R_gas;
+      const double ut[3] = {0.0, 0.0, 0.0};
+      for (int i = 0; i < 3; ++i) u_bc[i] = (rhoun_bc * unit_n[i] + o->ns_rho[ibf] * ut[i]) / o->ns_rho[ibf];
+      o->ns_p[ibf] = o->ns_rho[ibf] * RT_bc;
+      nscbc_inlet_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], &o->u[3 * size_t(icv)], o->p[icv],
+                      gamma);
+    } else {
+      nscbc_outlet_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], o->rho[icv], &o->u[3 * size_t(icv)],
+                       o->p[icv], gamma, bc[3], bc[2], bc[1]);
     }
   }
 }
@@ -522,6 +616,22 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
     const int kind = int(bc[0]);
     if (kind == CGX_BC_CBC_EXTRAPOLATE) {
       extrapolate_bf_state(o, ibf);
+    } else if (kind == CGX_BC_NSCBC_MT || kind == CGX_BC_NSCBC_OUTLET_P) {
+      // Nscbc::initialHook (:3630-3649) and Nscbc::rk3Step (:3651-3660)
+      const int icv = o->cvobf[ibf];
+      if (init) {
+        o->ns_rho[ibf] = o->rho[icv];
+        o->ns_p[ibf] = o->p[icv];
+        for (int i = 0; i < 3; ++i) o->ns_u[3 * size_t(ibf) + i] = o->u[3 * size_t(icv) + i];
+      } else {
+        const double* w = RkWeights::erk_wgt3[rk_stage - 1];
+        for (int i = 0; i < rk_stage; ++i) {
+          const double* r = &o->ns_rhs[15 * size_t(ibf) + 5 * size_t(i)];
+          o->ns_rho[ibf] += w[i] * dt * r[0];
+          o->ns_p[ibf] += w[i] * dt * r[1];
+          for (int j = 0; j < 3; ++j) o->ns_u[3 * size_t(ibf) + j] += w[i] * dt * r[2 + j];
+        }
+      }
     } else if (kind == CGX_BC_CBC_TOTAL_PT && (init || rk_stage == 1)) {
       const double* n = &o->n_bf[3 * size_t(ibf)];
       const double bf_area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
@@ -755,6 +865,13 @@ void store_data(orc_solver* o) {
   for (int i = 0; i < n; ++i)
     for (int k = 0; k < 3; ++k) o->store_recent[c++] = o->u[3 * size_t(i) + k];
   for (int i = 0; i < n; ++i) o->store_recent[c++] = o->rhoE[i];
+  // Nscbc::storeData (IdealGasSolverBcs.cpp:3578-3592): rho, p, u per face
+  o->store_recent.resize(c + 5 * size_t(o->nbf));
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    o->store_recent[c++] = o->ns_rho[ibf];
+    o->store_recent[c++] = o->ns_p[ibf];
+    for (int k = 0; k < 3; ++k) o->store_recent[c++] = o->ns_u[3 * size_t(ibf) + k];
+  }
   if (o->store_old.empty()) {
     o->store_old = o->store_recent;
     o->store_step_old = o->store_step_recent;
@@ -771,6 +888,11 @@ void restore_data(orc_solver* o) {
   for (int i = 0; i < n; ++i)
     for (int k = 0; k < 3; ++k) o->u[3 * size_t(i) + k] = o->store_old[c++];
   for (int i = 0; i < n; ++i) o->rhoE[i] = o->store_old[c++];
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {  // Nscbc::restoreData (:3594-3606)
+    o->ns_rho[ibf] = o->store_old[c++];
+    o->ns_p[ibf] = o->store_old[c++];
+    for (int k = 0; k < 3; ++k) o->ns_u[3 * size_t(ibf) + k] = o->store_old[c++];
+  }
   update_primitive(o);
   calc_sgs_props(o);
   o->dt_data0 *= 0.8;
@@ -840,6 +962,10 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->bc.assign(m->nbf_zones, {0.0, 0.0, 0.0, 0.0, 0.0});
     o->bf_state.assign(m->nbf, IdealGasState());
     o->un_bc.assign(m->nbf, 0.0);
+    o->ns_rho.assign(m->nbf, 0.0);
+    o->ns_p.assign(m->nbf, 0.0);
+    o->ns_u.assign(3 * size_t(m->nbf), 0.0);
+    o->ns_rhs.assign(15 * size_t(m->nbf), 0.0);
   }
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
@@ -1074,16 +1200,19 @@ extern "C" int orc_advance_solution(orc_solver* o) {
   using RkWeights::erk_wgt3;
   for (int k = 0; k < 3; ++k) zero_rhs(o, k);
   const double dt = o->dt;
+  bc_calc_rhs(o, 1);
   calc_rhs(o, o->rhs[0].data(), o->rhs_sc[0].data());
   bc_rk3_step(o, 1, dt, false);
   rk3_step(o, erk_wgt3[0], dt);
   o->time += dt;
   update_primitive(o);
+  bc_calc_rhs(o, 2);
   calc_rhs(o, o->rhs[1].data(), o->rhs_sc[1].data());
   bc_rk3_step(o, 2, dt, false);
   rk3_step(o, erk_wgt3[1], dt);
   o->time -= 0.5 * dt;
   update_primitive(o);
+  bc_calc_rhs(o, 3);
   calc_rhs(o, o->rhs[2].data(), o->rhs_sc[2].data());
   bc_rk3_step(o, 3, dt, false);
   rk3_step(o, erk_wgt3[2], dt);
@@ -1172,12 +1301,24 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
     return (np == 0 || (kind == CGX_BC_WALL_ADIABATIC && np == 3)) ? orc_set_bc(o, zone, kind, np ? prm : nullptr) : -1;
   const int want = kind == CGX_BC_WALL_ISOTHERMAL ? 1 : kind == CGX_BC_CBC_UPT ? 5
                  : (kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT || kind == CGX_BC_CBC_TOTAL_PT) ? 3
-                 : kind == CGX_BC_CBC_EXTRAPOLATE ? 0 : -1;
+                 : kind == CGX_BC_CBC_EXTRAPOLATE ? 0 : kind == CGX_BC_NSCBC_MT ? 2
+                 : kind == CGX_BC_NSCBC_OUTLET_P ? 3 : -1;
   if (want < 0 || np != want || (np > 0 && !prm)) return -1;
   o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, kind == CGX_BC_WALL_ISOTHERMAL ? prm[0] : 0.0};
   if (kind == CGX_BC_WALL_ISOTHERMAL || kind == CGX_BC_CBC_EXTRAPOLATE) return 0;
-  if (kind == CGX_BC_CBC_TOTAL_PT) {  // CbcTotalPt::initData: p_total, T_total, t_relax
+  if (kind == CGX_BC_CBC_TOTAL_PT || kind == CGX_BC_NSCBC_OUTLET_P) {
+    // CbcTotalPt: p_total, T_total, t_relax; NscbcOutletP: p_ref, sigma, L_ref
     o->bc[zone] = {double(kind), prm[0], prm[1], prm[2], 0.0};
+    return 0;
+  }
+  if (kind == CGX_BC_NSCBC_MT) {  // NscbcMt::initData: rhoun_bc = -mdot / area, static T
+    double area = 0.0;
+    for (int ibf = 0; ibf < o->nbf; ++ibf)
+      if (o->zone_bf[ibf] == zone) {
+        const double* n = &o->n_bf[3 * size_t(ibf)];
+        area += std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      }
+    o->bc[zone] = {double(kind), -prm[0] / area, prm[1], 0.0, 0.0};
     return 0;
   }
   const double R = o->R_gas, gamma = o->prm.gamma;

@@ -158,3 +158,27 @@ def test_restated_riemann_flux_bitwise_equals_reference(chan, zones):
         o.close()
     assert np.array_equal(out[0], out[2])
     assert np.array_equal(out[1], out[3])
+
+
+NSCBC_MT, NSCBC_OUT = 9, 10
+
+
+def test_uniform_flow_through_nscbc_zones(chan):
+    """NSCBC_MT inflow carrying the flow's mass flux and temperature and an
+    NSCBC_OUTLET_P outlet at the flow's pressure: a uniform flow normal to
+    the zones stays uniform over RK3 steps, the faces' own states included."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    rho, u, p = _uniform(m, prm, u=(0.0, 0.3, 0.0))
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+    T0 = p[0] / (rho[0] * R)
+    mdot = rho[0] * 0.3 * _zone_area(m, 0)  # into the domain through y = 0
+    o = Oracle(m, prm)
+    o.set_bc_params(0, NSCBC_MT, [mdot, T0])
+    o.set_bc_params(1, NSCBC_OUT, [p[0], 0.25, 2.0])
+    o.set_state_primitive(rho, u, p)
+    o.init_complete()
+    assert o.step(5) == 0
+    r2, u2, e2 = o.get_state()
+    assert np.abs(r2 - rho).max() <= 1e-12 and np.abs(u2 - u).max() <= 1e-12
+    o.close()

@@ -143,3 +143,36 @@ def test_cbc_refusals(chan):
     with pytest.raises(cgx.CgxError):
         s.set_scalars(np.zeros((m.ncv, 1)))
     s.close()
+
+
+NSCBC_MT, NSCBC_OUT = cgx.CGX_BC_NSCBC_MT, cgx.CGX_BC_NSCBC_OUTLET_P
+
+
+def test_nscbc_steps_and_restore_match_oracle(chan):
+    """NSCBC_MT inflow and a partially reflecting NSCBC_OUTLET_P outlet: the
+    faces' own rho, p, u advance with the zones' characteristic equations;
+    10 steps match the oracle to 1e-10, and a NaN restores the state and the
+    faces' states (Nscbc::storeData/restoreData) as the oracle does."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    zones = ((NSCBC_MT, (2.4, 1.0)), (NSCBC_OUT, (P0, 0.25, 3.0)))
+    s, o = _make(m, gm, prm, zones)
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    # a NaN: both restore the stored state (step 0) with the faces' states
+    o.set_dt()
+    bad = [a.copy() for a in s.get_state()]
+    bad[0][5] = np.nan
+    s.set_state(*bad)
+    s.updateConservativeAndPrimitiveData()
+    o.poison(5)
+    assert s.advanceSolution() == -1 and o.advance_solution() == -1
+    assert s.step(3) == 0 and o.step(3) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
