@@ -13,11 +13,9 @@ advances all resident cases together one graph replay per step
 latency) and aggregate throughput; `run_sequential()` runs the same cases
 one at a time on the plain FP64 path for comparison.
 """
-import os
 import queue
 import threading
 import time
-from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -83,29 +81,38 @@ def serve(requests, hbm_budget=96 << 30, chunk=8, max_cases=256, device=0, keep_
     arrived it builds the request's device mesh if needed and its case
     (cgx_batch_prepare: solver, state, initComplete on the case's own
     stream), at most `prepare_ahead` cases ahead of admission, while the
-    batches step.  The stepping loop joins prepared cases between steps
+    batches step.  Each precision's batch (on its own CUDA stream) has its
+    own stepping thread: it joins its prepared cases between steps
     (cgx_batch_admit, in arrival order, while the HBM budget allows),
-    advances the resident cases `chunk` steps (a case stops at its own step
-    count) and retires the finished ones.  With `concurrent`, the FP64 and
-    the mixed-precision batches (each on its own CUDA stream) are stepped
-    from two host threads at once.  Returns a summary dict; requests are
-    updated in place."""
+    advances its resident cases `chunk` steps (a case stops at its own step
+    count) and retires the finished ones, without waiting for the other
+    batch.  Without `concurrent` one thread steps the batches in turn.
+    Returns a summary dict; requests are updated in place."""
     order = sorted(requests, key=lambda r: r.arrival)
-    batches = {prec: cgx.Batch(device, prec, max_cases=max_cases, hbm_budget=hbm_budget)
-               for prec in sorted(set(r.precision for r in order))}
-    ready = queue.Queue()
+    precs = sorted(set(r.precision for r in order))
+    batches = {prec: cgx.Batch(device, prec, max_cases=max_cases, hbm_budget=hbm_budget) for prec in precs}
+    ready = {prec: queue.Queue() for prec in precs}
+    total = {prec: sum(1 for r in order if r.precision == prec) for prec in precs}
     slots = threading.Semaphore(prepare_ahead)
     stop = threading.Event()
     failure = []
+    lock = threading.Lock()
+    busy = [0.0, 0, 0.0]  # wall time with a batch stepping; steppers active; since
     t0 = time.perf_counter()
 
     def now():
         return time.perf_counter() - t0
 
+    def mark(delta):
+        with lock:
+            t = time.perf_counter()
+            if busy[1] > 0:
+                busy[0] += t - busy[2]
+            busy[1] += delta
+            busy[2] = t
+
     def prepare_all():
         try:
-            # leave host cores to the stepping threads while meshes are set up
-            cgx.set_host_threads(max(1, (os.cpu_count() or 1) - 4))
             for r in order:
                 while not stop.is_set() and now() < r.arrival:
                     time.sleep(min(0.005, max(0.0, r.arrival - now())))
@@ -115,74 +122,99 @@ def serve(requests, hbm_budget=96 << 30, chunk=8, max_cases=256, device=0, keep_
                     return
                 r._dev_mesh, r._own_mesh = device_mesh(r, device)
                 r._prepared = batches[r.precision].prepare(r._dev_mesh, r.params, r.rho, r.u, r.p, r.nsteps)
-                ready.put(r)
-        except Exception as e:  # reported by the stepping loop
+                ready[r.precision].put(r)
+        except Exception as e:  # reported by the stepping threads
             failure.append(e)
 
-    prep = threading.Thread(target=prepare_all, daemon=True)
-    prep.start()
-    pool = ThreadPoolExecutor(max_workers=2) if concurrent and len(batches) > 1 else None
-    busy = 0.0  # wall time with at least one batch stepping
-    waiting, resident, n_done = [], {}, 0
-    try:
-        while n_done < len(order):
-            if failure:
-                raise failure[0]
+    class Lane:
+        """One precision's stepping state."""
+
+        def __init__(self, prec):
+            self.prec, self.b = prec, batches[prec]
+            self.waiting, self.resident, self.n_done = [], {}, 0
+
+        def turn(self):
+            """Admit, step `chunk` steps, retire; False if nothing is resident."""
             while True:
                 try:
-                    waiting.append(ready.get_nowait())
+                    self.waiting.append(ready[self.prec].get_nowait())
                 except queue.Empty:
                     break
             still = []
-            for r in sorted(waiting, key=lambda q: q.arrival):
-                cid = batches[r.precision].admit(r._prepared)
+            for r in sorted(self.waiting, key=lambda q: q.arrival):
+                cid = self.b.admit(r._prepared)
                 if cid is None:
                     still.append(r)
                     continue
                 slots.release()
                 r.case_id = cid
                 r.admitted = now()
-                resident[(r.precision, cid)] = r
-            waiting = still
-            if not resident:
-                time.sleep(0.002)
-                continue
-            active = [b for prec, b in batches.items() if any(k[0] == prec for k in resident)]
-            tb = time.perf_counter()
-            if pool is not None and len(active) > 1:
-                for f in [pool.submit(b.step, chunk) for b in active]:
-                    f.result()
-            else:
-                for b in active:
-                    b.step(chunk)
-            busy += time.perf_counter() - tb
-            for prec, b in batches.items():
-                for cid in b.done():
-                    r = resident.pop((prec, cid))
-                    if keep_state:
-                        r.state = b.get_state(cid)
-                    r.finished = now()
-                    b.remove(cid)
-                    if r._own_mesh:
-                        r._dev_mesh.close()
-                    r._dev_mesh = r._prepared = None
-                    n_done += 1
+                self.resident[cid] = r
+            self.waiting = still
+            if not self.resident:
+                return False
+            mark(1)
+            try:
+                self.b.step(chunk)
+            finally:
+                mark(-1)
+            for cid in self.b.done():
+                r = self.resident.pop(cid)
+                if keep_state:
+                    r.state = self.b.get_state(cid)
+                r.finished = now()
+                self.b.remove(cid)
+                if r._own_mesh:
+                    r._dev_mesh.close()
+                r._dev_mesh = r._prepared = None
+                self.n_done += 1
+            return True
+
+    lanes = [Lane(prec) for prec in precs]
+
+    def run(ls):
+        try:
+            while not stop.is_set() and any(l.n_done < total[l.prec] for l in ls):
+                if failure:
+                    return
+                stepped = False
+                for l in ls:
+                    if l.n_done < total[l.prec]:
+                        stepped |= l.turn()
+                if not stepped:
+                    time.sleep(0.002)
+        except Exception as e:
+            failure.append(e)
+
+    prep = threading.Thread(target=prepare_all, daemon=True)
+    prep.start()
+    groups = [[l] for l in lanes] if concurrent else [lanes]
+    steppers = [threading.Thread(target=run, args=(g,)) for g in groups]
+    try:
+        for t in steppers:
+            t.start()
+        for t in steppers:
+            t.join()
+        if failure:
+            raise failure[0]
         makespan = now()
     finally:
         stop.set()
+        for t in steppers:
+            t.join()
         prep.join()
-        if pool is not None:
-            pool.shutdown()
-        for r in waiting:
-            r._prepared.release()
+        for l in lanes:
+            for r in l.waiting:
+                r._prepared.release()
         for b in batches.values():
             b.close()
     lat = np.array([r.finished - r.arrival for r in requests])
     cs = float(sum(r.cell_steps for r in requests))
     return {"requests": len(requests), "makespan_s": makespan, "solves_per_s": len(requests) / makespan,
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-            "cell_steps_per_s": cs / makespan, "cell_steps": cs, "stepping_s": busy,
-            "concurrent_precisions": pool is not None, "admission": "preparer thread, overlapped with stepping"}
+            "cell_steps_per_s": cs / makespan, "cell_steps": cs, "stepping_s": busy[0],
+            "concurrent_precisions": bool(concurrent and len(lanes) > 1),
+            "admission": "preparer thread, overlapped with stepping"}
 
 
 def run_sequential(requests, precision=cgx.CGX_FP64, keep_state=False, device=0):
