@@ -300,6 +300,15 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *                          pressure; the MDOT form is not built) */
 #define CGX_BC_NSCBC_MT        9
 #define CGX_BC_NSCBC_OUTLET_P  10
+/*   CGX_BC_NSCBC_OUTLET_MDOT  mdot t_relax  outlet driving the zone's mean mass
+ *                          flux toward mdot / area (NscbcOutletP, NSCBC_OUTLET_MDOT:
+ *                          calcRhsMdot, IdealGasSolverBcs.cpp:3934-4007)
+ * Zone-wide forms: CBC_TOTAL_PT takes an optional fourth parameter, 1 for
+ * USE_AVG (one normal speed for the whole zone, relaxed toward its
+ * density-weighted mean); NSCBC_MT with T < 0 takes -T as the total
+ * temperature (T_TOTAL: the static temperature from the zone's mean Mach
+ * number each stage).  Zone means are summed in a fixed order. */
+#define CGX_BC_NSCBC_OUTLET_MDOT 11
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,

@@ -162,6 +162,7 @@ CGX_BC_CBC_EXTRAPOLATE = 7
 CGX_BC_CBC_TOTAL_PT = 8
 CGX_BC_NSCBC_MT = 9
 CGX_BC_NSCBC_OUTLET_P = 10
+CGX_BC_NSCBC_OUTLET_MDOT = 11
 
 
 class Source(ctypes.Structure):
@@ -351,8 +352,9 @@ class Solver:
         """Boundary condition with the reference's zone parameters in input
         order: WALL_ISOTHERMAL (T), CBC_UPT (u0 u1 u2 p T), CBC_RUNP
         (rho un p), CBC_MPT (mdot p T), CBC_EXTRAPOLATE (none), CBC_TOTAL_PT
-        (p_total T_total t_relax), NSCBC_MT (mdot T), NSCBC_OUTLET_P
-        (p_ref sigma L_ref); SLIP and WALL_ADIABATIC as set_bc."""
+        (p_total T_total t_relax [use_avg]), NSCBC_MT (mdot T; T < 0: the
+        total temperature -T), NSCBC_OUTLET_P (p_ref sigma L_ref),
+        NSCBC_OUTLET_MDOT (mdot t_relax); SLIP and WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))
 

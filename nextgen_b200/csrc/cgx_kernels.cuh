@@ -184,6 +184,7 @@ struct MeshDev {
   const double4* cc;            // {pow(vol,1/3), pow(vol,2/3), dcmag_hat, sa_to_vol}
   // boundary faces, ordered by cell (none: nbf = 0, pointers null)
   int nbf;
+  int nzones;  // boundary zones
   int nbc;                      // cells with boundary faces
   const int* bfc;               // [N+1] each cell's faces in the bf arrays
   const int* bcell;             // [nbc] the cells with boundary faces, ascending
@@ -229,7 +230,10 @@ struct StateDev {
   // NSCBC zones, per boundary face ([20][nbf]): rho_bc, p_bc, u_bc[3], then
   // the characteristic rhs of stages 1..3 (5 each)
   double* nsb;
-  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones
+  // per zone [8]: the zone sums of this stage (0..3) and the zone's own
+  // state (4: CBC_TOTAL_PT USE_AVG's relaxed mean normal speed)
+  double* zst;
+  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones, 8 zone sums
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

@@ -141,6 +141,7 @@ struct orc_solver {
   // NSCBC zones: each face's rho, p, u and the characteristic rhs of the
   // three stages (Nscbc::initData, IdealGasSolverBcs.cpp:3615-3628)
   std::vector<double> ns_rho, ns_p, ns_u, ns_rhs;
+  std::vector<double> un_bc_avg;  // CBC_TOTAL_PT USE_AVG: per zone
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
@@ -465,7 +466,7 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         for (int i = 0; i < 3; ++i)
           rhs[icv].rhou[i] -= o->p[icv] * n[i] + visc_coeff * (o->u[3 * size_t(icv) + i] - 0.0);
         rhs[icv].rhoE -= k_coeff * (o->T[icv] - bc[4]);
-      } else if (kind == CGX_BC_NSCBC_MT || kind == CGX_BC_NSCBC_OUTLET_P) {
+      } else if (kind == CGX_BC_NSCBC_MT || kind == CGX_BC_NSCBC_OUTLET_P || kind == CGX_BC_NSCBC_OUTLET_MDOT) {
         // Nscbc::addBoundaryFlux (IdealGasSolverBcs.cpp:3662-3693)
         const double gogm1 = gamma / (gamma - 1.0);
         IdealGasState bs;
@@ -546,15 +547,63 @@ void nscbc_outlet_rhs(double* rhs, const double unit_n[3], double delta, double 
                  0.5 * (1.0 + Ma) * dpdn * unit_n[i] / rho_bc + 0.5 * L1 * unit_n[i] / sos_bc / rho_bc;
 }
 
+// calcNscbcIgOutletMdotWeakRhs (src/charles/BcCommon.hpp): the outlet form
+// with L1 = -c (rhou_avg - rhou_target) / T_relax
+void nscbc_outlet_mdot_rhs(double* rhs, const double unit_n[3], double delta, double rho_bc, const double u_bc[3],
+                           double p_bc, double rho_cv, const double u_cv[3], double p_cv, double gamma,
+                           double rhou_avg, double rhou_target, double T_relax) {
+  const double un_bc = std::max(0.0, u_bc[0] * unit_n[0] + u_bc[1] * unit_n[1] + u_bc[2] * unit_n[2]);
+  const double u0 = std::max(0.0, u_cv[0] * unit_n[0] + u_cv[1] * unit_n[1] + u_cv[2] * unit_n[2]);
+  const double sos_bc = std::sqrt(gamma * p_bc / rho_bc);
+  const double Ma = un_bc / sos_bc;
+  const double dudn = (un_bc - u0) / delta;
+  const double dpdn = (p_bc - p_cv) / delta;
+  const double L5 = (un_bc + sos_bc) * (dpdn + rho_bc * sos_bc * dudn);
+  double dudn_[3];
+  for (int i = 0; i < 3; ++i) dudn_[i] = (u_bc[i] - u_cv[i]) / delta;
+  double L1 = -sos_bc * (rhou_avg - rhou_target) / T_relax;
+  const double drhodn = (rho_bc - rho_cv) / delta;
+  const double L2 = un_bc * (sos_bc * sos_bc * drhodn - dpdn);
+  if (Ma >= 1.0) L1 = sos_bc * (Ma - 1.0) * (dpdn - rho_bc * sos_bc * dudn);
+  rhs[0] = -(L2 + 0.5 * (L5 + L1)) / sos_bc / sos_bc;
+  rhs[1] = -0.5 * (L5 + L1);
+  for (int i = 0; i < 3; ++i)
+    rhs[2 + i] = -(rho_bc * un_bc * dudn_[i] + 0.5 * rho_bc * sos_bc * (1.0 - Ma) * dudn * unit_n[i]) / rho_bc -
+                 0.5 * (1.0 + Ma) * dpdn * unit_n[i] / rho_bc + 0.5 * L1 * unit_n[i] / sos_bc / rho_bc;
+}
+
 // The NSCBC zones' calcRhs at stage rk_stage, before the solver's:
 // NscbcMt::calcRhs (IdealGasSolverBcs.cpp:3777-3844, static T) and
 // NscbcOutletP::calcRhsPressure (:4009-4056), without frame rotation.
 void bc_calc_rhs(orc_solver* o, int rk_stage) {
   const double gamma = o->prm.gamma;
+  // zone sums: NSCBC_MT T_TOTAL (:3781-3805), NSCBC_OUTLET_MDOT (:3934-3954)
+  std::vector<std::array<double, 3>> zs(o->nbf_zones, {0.0, 0.0, 0.0});
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    const int z = o->zone_bf[ibf];
+    const std::array<double, 5>& bc = o->bc[z];
+    const int kind = int(bc[0]);
+    const double* n = &o->n_bf[3 * size_t(ibf)];
+    const double bf_area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const int icv = o->cvobf[ibf];
+    if (kind == CGX_BC_NSCBC_MT && bc[2] < 0.0) {
+      const double un_bc = bc[1] / o->rho[icv];
+      const double Ma = un_bc / o->sos[icv];
+      zs[z][0] += bf_area * Ma * Ma;
+      zs[z][1] += bf_area;
+    } else if (kind == CGX_BC_NSCBC_OUTLET_MDOT) {
+      const double* u = &o->ns_u[3 * size_t(ibf)];
+      const double un_dA = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+      zs[z][0] += bf_area;
+      zs[z][1] += o->ns_rho[ibf] * un_dA;
+      zs[z][2] += un_dA;
+    }
+  }
   for (int ibf = 0; ibf < o->nbf; ++ibf) {
     const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
     const int kind = int(bc[0]);
-    if (kind != CGX_BC_NSCBC_MT && kind != CGX_BC_NSCBC_OUTLET_P) continue;
+    if (kind != CGX_BC_NSCBC_MT && kind != CGX_BC_NSCBC_OUTLET_P && kind != CGX_BC_NSCBC_OUTLET_MDOT) continue;
+    const std::array<double, 3>& zz = zs[o->zone_bf[ibf]];
     const double* n = &o->n_bf[3 * size_t(ibf)];
     const double bf_area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
     const double unit_n[3] = {n[0] / bf_area, n[1] / bf_area, n[2] / bf_area};
@@ -563,15 +612,20 @@ void bc_calc_rhs(orc_solver* o, int rk_stage) {
     double* u_bc = &o->ns_u[3 * size_t(ibf)];
     double* rhs = &o->ns_rhs[15 * size_t(ibf) + 5 * size_t(rk_stage - 1)];
     if (kind == CGX_BC_NSCBC_MT) {
-      const double rhoun_bc = bc[1], RT_bc = bc[2] * o->R_gas;
+      double static_T_bc = bc[2];
+      if (bc[2] < 0.0) static_T_bc = -bc[2] / (1.0 + 0.5 * (gamma - 1.0) * (zz[0] / zz[1]));
+      const double rhoun_bc = bc[1], RT_bc = static_T_bc * o->R_gas;
       const double ut[3] = {0.0, 0.0, 0.0};
       for (int i = 0; i < 3; ++i) u_bc[i] = (rhoun_bc * unit_n[i] + o->ns_rho[ibf] * ut[i]) / o->ns_rho[ibf];
       o->ns_p[ibf] = o->ns_rho[ibf] * RT_bc;
       nscbc_inlet_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], &o->u[3 * size_t(icv)], o->p[icv],
                       gamma);
-    } else {
+    } else if (kind == CGX_BC_NSCBC_OUTLET_P) {
       nscbc_outlet_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], o->rho[icv], &o->u[3 * size_t(icv)],
                        o->p[icv], gamma, bc[3], bc[2], bc[1]);
+    } else {
+      nscbc_outlet_mdot_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], o->rho[icv],
+                            &o->u[3 * size_t(icv)], o->p[icv], gamma, zz[1] / zz[0], bc[1], bc[2]);
     }
   }
 }
@@ -611,12 +665,37 @@ void total_pt_bf_state(orc_solver* o, int ibf, const double unit_n[3]) {
 // (:3566-3576); CbcTotalPt relaxes un_bc at stage 1 (:3526-3564, without
 // USE_AVG).  init: their initialHook after initComplete (:3447-3523).
 void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
+  // CBC_TOTAL_PT USE_AVG (:3447-3461, 3526-3545): the zone's relaxed mean
+  if (init || rk_stage == 1) {
+    std::vector<std::array<double, 2>> zs(o->nbf_zones, {0.0, 0.0});
+    for (int ibf = 0; ibf < o->nbf; ++ibf) {
+      const int z = o->zone_bf[ibf];
+      const std::array<double, 5>& bc = o->bc[z];
+      if (int(bc[0]) != CGX_BC_CBC_TOTAL_PT || bc[4] == 0.0) continue;
+      const int icv = o->cvobf[ibf];
+      const double* n = &o->n_bf[3 * size_t(ibf)];
+      const double* u = &o->u[3 * size_t(icv)];
+      zs[z][0] += o->rho[icv] * std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      zs[z][1] += o->rho[icv] * (u[0] * n[0] + u[1] * n[1] + u[2] * n[2]);
+    }
+    for (int z = 0; z < o->nbf_zones; ++z) {
+      const std::array<double, 5>& bc = o->bc[z];
+      if (int(bc[0]) != CGX_BC_CBC_TOTAL_PT || bc[4] == 0.0) continue;
+      const double avg0 = zs[z][1] / zs[z][0];
+      if (init) {
+        o->un_bc_avg[z] = avg0;
+      } else {
+        const double eps = 1.0 / (bc[3] / dt + 1.0);
+        o->un_bc_avg[z] = (1.0 - eps) * o->un_bc_avg[z] + eps * avg0;
+      }
+    }
+  }
   for (int ibf = 0; ibf < o->nbf; ++ibf) {
     const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
     const int kind = int(bc[0]);
     if (kind == CGX_BC_CBC_EXTRAPOLATE) {
       extrapolate_bf_state(o, ibf);
-    } else if (kind == CGX_BC_NSCBC_MT || kind == CGX_BC_NSCBC_OUTLET_P) {
+    } else if (kind == CGX_BC_NSCBC_MT || kind == CGX_BC_NSCBC_OUTLET_P || kind == CGX_BC_NSCBC_OUTLET_MDOT) {
       // Nscbc::initialHook (:3630-3649) and Nscbc::rk3Step (:3651-3660)
       const int icv = o->cvobf[ibf];
       if (init) {
@@ -638,7 +717,9 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
       const double unit_n[3] = {n[0] / bf_area, n[1] / bf_area, n[2] / bf_area};
       const double* u = &o->u[3 * size_t(o->cvobf[ibf])];
       const double un0 = u[0] * unit_n[0] + u[1] * unit_n[1] + u[2] * unit_n[2];
-      if (init) {
+      if (bc[4] != 0.0) {
+        o->un_bc[ibf] = o->un_bc_avg[o->zone_bf[ibf]];
+      } else if (init) {
         o->un_bc[ibf] = unit_n[0] * u[0] + unit_n[1] * u[1] + unit_n[2] * u[2];
       } else {
         const double t_relax = bc[3];
@@ -966,6 +1047,7 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->ns_p.assign(m->nbf, 0.0);
     o->ns_u.assign(3 * size_t(m->nbf), 0.0);
     o->ns_rhs.assign(15 * size_t(m->nbf), 0.0);
+    o->un_bc_avg.assign(std::max(m->nbf_zones, 1), 0.0);
   }
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
@@ -1302,13 +1384,24 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
   const int want = kind == CGX_BC_WALL_ISOTHERMAL ? 1 : kind == CGX_BC_CBC_UPT ? 5
                  : (kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT || kind == CGX_BC_CBC_TOTAL_PT) ? 3
                  : kind == CGX_BC_CBC_EXTRAPOLATE ? 0 : kind == CGX_BC_NSCBC_MT ? 2
-                 : kind == CGX_BC_NSCBC_OUTLET_P ? 3 : -1;
-  if (want < 0 || np != want || (np > 0 && !prm)) return -1;
+                 : kind == CGX_BC_NSCBC_OUTLET_P ? 3 : kind == CGX_BC_NSCBC_OUTLET_MDOT ? 2 : -1;
+  const bool use_avg = kind == CGX_BC_CBC_TOTAL_PT && np == 4;
+  if (want < 0 || (np != want && !use_avg) || (np > 0 && !prm)) return -1;
   o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, kind == CGX_BC_WALL_ISOTHERMAL ? prm[0] : 0.0};
   if (kind == CGX_BC_WALL_ISOTHERMAL || kind == CGX_BC_CBC_EXTRAPOLATE) return 0;
   if (kind == CGX_BC_CBC_TOTAL_PT || kind == CGX_BC_NSCBC_OUTLET_P) {
-    // CbcTotalPt: p_total, T_total, t_relax; NscbcOutletP: p_ref, sigma, L_ref
-    o->bc[zone] = {double(kind), prm[0], prm[1], prm[2], 0.0};
+    // CbcTotalPt: p_total, T_total, t_relax [, USE_AVG]; NscbcOutletP: p_ref, sigma, L_ref
+    o->bc[zone] = {double(kind), prm[0], prm[1], prm[2], (use_avg && prm[3] != 0.0) ? 1.0 : 0.0};
+    return 0;
+  }
+  if (kind == CGX_BC_NSCBC_OUTLET_MDOT) {  // rhou_target = mdot / area_global, T_relax
+    double area = 0.0;
+    for (int ibf = 0; ibf < o->nbf; ++ibf)
+      if (o->zone_bf[ibf] == zone) {
+        const double* n = &o->n_bf[3 * size_t(ibf)];
+        area += std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      }
+    o->bc[zone] = {double(kind), prm[0] / area, prm[1], 0.0, 0.0};
     return 0;
   }
   if (kind == CGX_BC_NSCBC_MT) {  // NscbcMt::initData: rhoun_bc = -mdot / area, static T

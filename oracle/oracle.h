@@ -77,8 +77,9 @@ int orc_set_bc(orc_solver* o, int zone, int kind, const double u_wall[3]);
 /* Boundary condition with the reference's zone parameters (the kinds and
  * parameter lists of cgx_set_bc_params): WALL_ISOTHERMAL T, CBC_UPT u p T,
  * CBC_RUNP rho un p, CBC_MPT mdot p T, CBC_EXTRAPOLATE, CBC_TOTAL_PT p_total
- * T_total t_relax, NSCBC_MT mdot T, NSCBC_OUTLET_P p_ref sigma L_ref; SLIP
- * and WALL_ADIABATIC as orc_set_bc.  0, or -1 on a bad argument. */
+ * T_total t_relax [use_avg], NSCBC_MT mdot T (T < 0: total temperature -T),
+ * NSCBC_OUTLET_P p_ref sigma L_ref, NSCBC_OUTLET_MDOT mdot t_relax; SLIP and
+ * WALL_ADIABATIC as orc_set_bc.  0, or -1 on a bad argument. */
 int orc_set_bc_params(orc_solver* o, int zone, int kind, const double* params, int nparams);
 /* write a NaN into rho[icv] (host-side fault injection for the NaN path) */
 void orc_poison(orc_solver* o, int icv);

@@ -182,3 +182,34 @@ def test_uniform_flow_through_nscbc_zones(chan):
     r2, u2, e2 = o.get_state()
     assert np.abs(r2 - rho).max() <= 1e-12 and np.abs(u2 - u).max() <= 1e-12
     o.close()
+
+
+NSCBC_MDOT = 11
+
+
+def test_uniform_flow_through_zone_wide_forms(chan):
+    """The zone-wide forms keep a uniform flow uniform over RK3 steps:
+    CBC_TOTAL_PT with USE_AVG inflow against CBC_EXTRAPOLATE, and NSCBC_MT
+    with a total temperature (T_TOTAL) against NSCBC_OUTLET_MDOT at the
+    flow's mass flux."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    rho, u, p = _uniform(m, prm, u=(0.0, 0.3, 0.0))
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+    gamma = prm.gamma
+    T0 = p[0] / (rho[0] * R)
+    cp = R * gamma / (gamma - 1.0)
+    T_tot = T0 + 0.5 * 0.3 ** 2 / cp
+    p_tot = p[0] * (T_tot / T0) ** (gamma / (gamma - 1.0))
+    mdot = rho[0] * 0.3 * _zone_area(m, 0)
+    for zones in (((TOTAL_PT, [p_tot, T_tot, 0.01, 1.0]), (EXTRAP, [])),
+                  ((NSCBC_MT, [mdot, -T_tot]), (NSCBC_MDOT, [rho[0] * 0.3 * _zone_area(m, 1), 0.05]))):
+        o = Oracle(m, prm)
+        for z, (k, a) in enumerate(zones):
+            o.set_bc_params(z, k, a)
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        assert o.step(5) == 0
+        r2, u2, e2 = o.get_state()
+        assert np.abs(r2 - rho).max() <= 1e-11 and np.abs(u2 - u).max() <= 1e-11, zones
+        o.close()

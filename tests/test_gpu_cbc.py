@@ -176,3 +176,25 @@ def test_nscbc_steps_and_restore_match_oracle(chan):
         assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
     s.close()
     o.close()
+
+
+NSCBC_MDOT = cgx.CGX_BC_NSCBC_OUTLET_MDOT
+
+
+@pytest.mark.parametrize("zones", [((TOTAL_PT, (1.02 * P0, 1.02, 0.05, 1.0)), (EXTRAP, ())),
+                                   ((NSCBC_MT, (2.4, -1.05)), (NSCBC_MDOT, (2.3, 0.05)))],
+                         ids=["totalpt_use_avg", "mt_ttotal_outlet_mdot"])
+def test_zone_wide_forms_match_oracle(chan, zones):
+    """Zone means summed on the device in a fixed order: CBC_TOTAL_PT USE_AVG,
+    NSCBC_MT T_TOTAL and NSCBC_OUTLET_MDOT over 10 steps against the oracle."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    s, o = _make(m, gm, prm, zones)
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
