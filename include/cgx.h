@@ -309,6 +309,14 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  * temperature (T_TOTAL: the static temperature from the zone's mean Mach
  * number each stage).  Zone means are summed in a fixed order. */
 #define CGX_BC_NSCBC_OUTLET_MDOT 11
+/*   CGX_BC_CBC_RUP          rho u0 u1 u2 p  a fixed boundary state (CbcRup::initData,
+ *                           IdealGasSolverBcs.cpp:3268-3333, without STATIONARY_FRAME)
+ *   CGX_BC_WALL_CONDUCTIVE  T_end [L_1 k_1 L_2 k_2 ...]  a wall at rest behind
+ *                           layers of thickness L_i and conductivity k_i ending at
+ *                           T_end: q = (T - T_end) / (sum L_i/k_i / A + delta /
+ *                           (loc_lam cp A)) / A (WallConductive, :2699-2743) */
+#define CGX_BC_CBC_RUP         12
+#define CGX_BC_WALL_CONDUCTIVE 13
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,

@@ -163,6 +163,8 @@ CGX_BC_CBC_TOTAL_PT = 8
 CGX_BC_NSCBC_MT = 9
 CGX_BC_NSCBC_OUTLET_P = 10
 CGX_BC_NSCBC_OUTLET_MDOT = 11
+CGX_BC_CBC_RUP = 12
+CGX_BC_WALL_CONDUCTIVE = 13
 
 
 class Source(ctypes.Structure):

@@ -1000,6 +1000,15 @@ __global__ void __launch_bounds__(256, 3) k_step_end(CASE_ARGS, int mode) {
 
 #include "cgx_mixed.cuh"
 
+// the characteristic zone kinds (a Riemann flux against a boundary state)
+__host__ __device__ inline bool bc_is_nscbc(int k) {
+  return k == CGX_BC_NSCBC_MT || k == CGX_BC_NSCBC_OUTLET_P || k == CGX_BC_NSCBC_OUTLET_MDOT;
+}
+__host__ __device__ inline bool bc_is_cbc(int k) {
+  return k == CGX_BC_CBC_UPT || k == CGX_BC_CBC_RUNP || k == CGX_BC_CBC_MPT || k == CGX_BC_CBC_RUP ||
+         k == CGX_BC_CBC_EXTRAPOLATE || k == CGX_BC_CBC_TOTAL_PT || bc_is_nscbc(k);
+}
+
 // A state as the boundary Riemann flux reads it (the reference's
 // IdealGasState: velocity, specific volume, pressure, enthalpy)
 struct RiemannState {
@@ -1120,9 +1129,22 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d] + visc * u[d];
       fr[4] -= kc * (T - z.a[3]);
+    } else if (kind == CGX_BC_WALL_CONDUCTIVE) {
+      // the wall's heat flux through the cell's half and the layers
+      const double cp = c.ph.R * gamma / (gamma - 1.0);
+      const double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      const double L_cv = area / m.bf_aod[f];
+      const double k_cv = (mu_lam * (1.0 / c.ph.Pr_lam)) * cp;
+      const double r_cv = L_cv / k_cv / area;
+      const double r_all = z.a[1] / area + r_cv;
+      const double q_wall = (T - z.a[0]) / r_all / area;
+      const double visc = mu_lam * m.bf_aod[f];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d] + visc * u[d];
+      fr[4] -= q_wall * area;
     } else {
       RiemannState sc, sb;
-      if (kind >= CGX_BC_NSCBC_MT) {  // Nscbc::addBoundaryFlux (:3662-3693)
+      if (bc_is_nscbc(kind)) {  // Nscbc::addBoundaryFlux (:3662-3693)
         const double* q = s.nsb + f;
         const double rb = q[0], pb = q[m.nbf];
 #pragma unroll
@@ -1130,7 +1152,7 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
         sb.sp_vol = 1.0 / rb;
         sb.p = pb;
         sb.h = gamma / (gamma - 1.0) * pb * (1.0 / rb);
-      } else if (kind >= CGX_BC_CBC_EXTRAPOLATE) {  // the face's own boundary state
+      } else if (kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT) {  // the face's own state
         const double* q = s.bfs + f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) sb.u[d] = q[d * m.nbf];
@@ -3453,7 +3475,7 @@ extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
   if (nsc > 0 && !sc) return fail(CGX_E_ARG, "cgx_set_scalars: null scalars");
   if (nsc > 0)
     for (const BcZone& z : s->bc)
-      if (z.kind >= CGX_BC_CBC_UPT)
+      if (bc_is_cbc(z.kind))
         return fail(CGX_E_STATE, "cgx_set_scalars: CBC boundary zones carry no transport scalars");
   CK(cudaSetDevice(s->mesh->device));
   CK(cudaStreamSynchronize(s->stream));
@@ -3643,12 +3665,14 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
     case CGX_BC_NSCBC_MT: want = 2; break;
     case CGX_BC_NSCBC_OUTLET_P: want = 3; break;
     case CGX_BC_NSCBC_OUTLET_MDOT: want = 2; break;
+    case CGX_BC_CBC_RUP: want = 5; break;
+    case CGX_BC_WALL_CONDUCTIVE: want = (nparams >= 1 && nparams % 2 == 1) ? nparams : 1; break;
     default: return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition");
   }
   if (nparams != want)
     return fail(CGX_E_ARG, "cgx_set_bc: kind " + std::to_string(kind) + " takes " + std::to_string(want) +
                                " parameters, got " + std::to_string(nparams));
-  if (kind >= CGX_BC_CBC_UPT && s->sd.nsc > 0)
+  if (bc_is_cbc(kind) && s->sd.nsc > 0)
     return fail(CGX_E_STATE, "cgx_set_bc: CBC boundary zones carry no transport scalars");
   const double R = s->ph.R, gamma = s->ph.gamma;
   BcZone z{};
@@ -3681,6 +3705,22 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
       for (int d = 0; d < 3; ++d) z.a[d] = params[d];
       z.a[3] = (nparams == 4 && params[3] != 0.0) ? 1.0 : 0.0;
       break;
+    case CGX_BC_CBC_RUP: {  // CbcRup::initData: rho, u, p
+      const double rho = params[0], p = params[4];
+      const double T = p / rho / R;
+      for (int d = 0; d < 3; ++d) z.a[d] = params[1 + d];
+      z.a[4] = p;
+      z.a[5] = 1.0 / rho;
+      z.a[6] = R * T * gamma / (gamma - 1.0);
+      break;
+    }
+    case CGX_BC_WALL_CONDUCTIVE: {  // WallConductive::initData: T_end, sum of L_i / k_i
+      double r = 0.0;
+      for (int i = 1; i + 1 < nparams; i += 2) r += params[i] / params[i + 1];
+      z.a[0] = params[0];
+      z.a[1] = r;
+      break;
+    }
     case CGX_BC_NSCBC_OUTLET_MDOT:  // NscbcOutletP (MDOT): rhou_target = mdot / area, T_relax
       z.a[0] = params[0] / s->mesh->zone_area[size_t(zone)];
       z.a[1] = params[1];
@@ -3742,7 +3782,7 @@ static int init_complete(cgx_solver* s, bool tune) {
     if (kind == 0)
       return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
                                    " has no boundary condition (cgx_set_bc)");
-    if (kind >= CGX_BC_CBC_UPT && s->sd.nsc > 0)
+    if (bc_is_cbc(kind) && s->sd.nsc > 0)
       return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
                                    " is a CBC zone and the solver has transport scalars");
   }

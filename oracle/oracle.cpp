@@ -479,7 +479,21 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         rhs[icv].rho -= flux.rho;
         for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= flux.rhou[i];
         rhs[icv].rhoE -= flux.rhoE;
-      } else if (kind >= CGX_BC_CBC_UPT) {
+      } else if (kind == CGX_BC_WALL_CONDUCTIVE) {
+        // WallConductive::addBoundaryFlux (IdealGasSolverBcs.cpp:2715-2743)
+        const double cp = o->R_gas * gamma / (gamma - 1.0);
+        const double area_bf = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        const double L_cv = area_bf / o->aod_bf[ibf];
+        const double k_cv = o->loc_lam[icv] * cp;
+        const double thermal_resistance_cv = L_cv / k_cv / area_bf;
+        const double thermal_resistance_overall = bc[2] / area_bf + thermal_resistance_cv;
+        const double q_wall = (o->T[icv] - bc[1]) / thermal_resistance_overall / area_bf;
+        const double visc_coeff = o->mu_lam[icv] * o->aod_bf[ibf];
+        for (int i = 0; i < 3; ++i)
+          rhs[icv].rhou[i] -= o->p[icv] * n[i] + visc_coeff * (o->u[3 * size_t(icv) + i] - 0.0);
+        rhs[icv].rhoE -= q_wall * area_bf;
+      } else if (kind == CGX_BC_CBC_UPT || kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT ||
+                 kind == CGX_BC_CBC_RUP || kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT) {
         IdealGasRhs flux;
         calcRiemannFlux(flux, n, o->cv_light[icv], o->bf_state[ibf], gamma, gamma);
         rhs[icv].rho -= flux.rho;
@@ -1384,11 +1398,18 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
   const int want = kind == CGX_BC_WALL_ISOTHERMAL ? 1 : kind == CGX_BC_CBC_UPT ? 5
                  : (kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT || kind == CGX_BC_CBC_TOTAL_PT) ? 3
                  : kind == CGX_BC_CBC_EXTRAPOLATE ? 0 : kind == CGX_BC_NSCBC_MT ? 2
-                 : kind == CGX_BC_NSCBC_OUTLET_P ? 3 : kind == CGX_BC_NSCBC_OUTLET_MDOT ? 2 : -1;
+                 : kind == CGX_BC_NSCBC_OUTLET_P ? 3 : kind == CGX_BC_NSCBC_OUTLET_MDOT ? 2
+                 : kind == CGX_BC_CBC_RUP ? 5 : (kind == CGX_BC_WALL_CONDUCTIVE && np >= 1 && np % 2 == 1) ? np : -1;
   const bool use_avg = kind == CGX_BC_CBC_TOTAL_PT && np == 4;
   if (want < 0 || (np != want && !use_avg) || (np > 0 && !prm)) return -1;
   o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, kind == CGX_BC_WALL_ISOTHERMAL ? prm[0] : 0.0};
   if (kind == CGX_BC_WALL_ISOTHERMAL || kind == CGX_BC_CBC_EXTRAPOLATE) return 0;
+  if (kind == CGX_BC_WALL_CONDUCTIVE) {  // WallConductive::initData: T_end, sum of L_i / k_i
+    double r = 0.0;
+    for (int i = 1; i + 1 < np; i += 2) r += prm[i] / prm[i + 1];
+    o->bc[zone] = {double(kind), prm[0], r, 0.0, 0.0};
+    return 0;
+  }
   if (kind == CGX_BC_CBC_TOTAL_PT || kind == CGX_BC_NSCBC_OUTLET_P) {
     // CbcTotalPt: p_total, T_total, t_relax [, USE_AVG]; NscbcOutletP: p_ref, sigma, L_ref
     o->bc[zone] = {double(kind), prm[0], prm[1], prm[2], (use_avg && prm[3] != 0.0) ? 1.0 : 0.0};
@@ -1431,6 +1452,13 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
       for (int i = 0; i < 3; ++i) b.u[i] = prm[i];
       b.p = p_bc;
       b.sp_vol = R * T_bc / p_bc;
+      b.h = R * T_bc * gamma / (gamma - 1.0);
+    } else if (kind == CGX_BC_CBC_RUP) {  // CbcRup::initData (:3268-3299)
+      const double rho_bc = prm[0], p_bc = prm[4];
+      const double T_bc = p_bc / rho_bc / R;
+      for (int i = 0; i < 3; ++i) b.u[i] = prm[1 + i];
+      b.sp_vol = 1.0 / rho_bc;
+      b.p = p_bc;
       b.h = R * T_bc * gamma / (gamma - 1.0);
     } else if (kind == CGX_BC_CBC_RUNP) {
       const double rho_bc = prm[0], un_bc = prm[1], p_bc = prm[2];

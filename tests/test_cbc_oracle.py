@@ -213,3 +213,46 @@ def test_uniform_flow_through_zone_wide_forms(chan):
         r2, u2, e2 = o.get_state()
         assert np.abs(r2 - rho).max() <= 1e-11 and np.abs(u2 - u).max() <= 1e-11, zones
         o.close()
+
+
+RUP, COND = 12, 13
+
+
+def test_rup_and_conductive_limits(chan):
+    """CBC_RUP with a state's rho, u, p gives CBC_UPT's flux with its u, p and
+    T = p/(rho R); WALL_CONDUCTIVE without layers is WALL_ISOTHERMAL at T_end
+    (the layers add a series resistance, which lowers the heat flux)."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.3 + 0.0 * y, 0.02 * np.cos(2 * np.pi * z / m.L[2])], 1)
+    rho = np.ones(m.ncv)
+    p = np.full(m.ncv, prm.p_ref)
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+
+    def rhs(zones):
+        o = Oracle(m, prm)
+        for zz, (k, a) in enumerate(zones):
+            o.set_bc_params(zz, k, a)
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        r, sc = o.calc_rhs(1)
+        o.close()
+        return r, sc
+
+    rb, pb = 1.02, 1.01 * prm.p_ref
+    a, sa = rhs(((RUP, [rb, 0.1, 0.35, 0.0, pb]), (UPT, [0.0, 0.3, 0.0, prm.p_ref, 1.0])))
+    b, _ = rhs(((UPT, [0.1, 0.35, 0.0, pb, pb / rb / R]), (UPT, [0.0, 0.3, 0.0, prm.p_ref, 1.0])))
+    assert (np.abs(a - b) / np.maximum(np.abs(b), sa)).max() <= 1e-13
+    c, sc = rhs(((COND, [1.3]), (COND, [0.8])))
+    d, _ = rhs(((ISO, [1.3]), (ISO, [0.8])))
+    assert (np.abs(c - d) / np.maximum(np.abs(d), sc)).max() <= 1e-13
+    e, _ = rhs(((COND, [1.3, 0.01, 0.5, 0.02, 1.0]), (COND, [0.8])))
+    # the hot wall (T_end 1.3 above the fluid's 1.0) heats its cells less
+    # through the layers; the other cells do not see them
+    hot = np.unique(m.cvobf[m.zone_bf == 0])
+    assert np.all(c[hot, 4] - e[hot, 4] > 0.0)
+    rest = np.setdiff1d(np.arange(m.ncv), hot)
+    assert np.array_equal(c[rest], e[rest])
+    with pytest.raises(ValueError):
+        Oracle(m, prm).set_bc_params(0, COND, [1.0, 0.1])  # layers come in pairs

@@ -198,3 +198,25 @@ def test_zone_wide_forms_match_oracle(chan, zones):
         assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
     s.close()
     o.close()
+
+
+RUP, COND = cgx.CGX_BC_CBC_RUP, cgx.CGX_BC_WALL_CONDUCTIVE
+
+
+def test_rup_and_conductive_match_oracle(chan):
+    """CBC_RUP inflow and a WALL_CONDUCTIVE wall behind two layers: calcRhs to
+    1e-12 of the face-sum scale and 10 steps to 1e-10 against the oracle."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    zones = ((RUP, (1.0, 0.1, 0.4, 0.0, 1.01 * P0)), (COND, (1.1, 0.01, 0.5, 0.02, 1.0)))
+    s, o = _make(m, gm, prm, zones)
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_params(1, COND, (1.0, 0.1))
+    s.close()
+    o.close()
