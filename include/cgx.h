@@ -317,6 +317,19 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *                           (loc_lam cp A)) / A (WallConductive, :2699-2743) */
 #define CGX_BC_CBC_RUP         12
 #define CGX_BC_WALL_CONDUCTIVE 13
+/*   CGX_BC_SPONGE  type strength t_relax length p_sponge L_max
+ *     a sponge layer (Sponge, IdealGasSolverBcs.cpp:4094-4363): each cell
+ *     keeps a sponge state (T_sponge, u_sponge) that relaxes toward its own
+ *     once per step (eps = 1/(t_relax/dt + 1)) and starts from it after
+ *     cgx_init_complete; the zone's faces take the HLLC flux against their
+ *     cell's sponge state at p_sponge, and the cells whose distance s along
+ *     the layer's direction exceeds L_max - length are pulled toward it with
+ *     strength ((s - L_max + length) / length)^2 per unit volume.  type: 0, 1,
+ *     2 for x, y, z; 3 for the radius about the x axis, 4 about the z axis.
+ *     L_max is the domain's largest extent in that direction (the reference
+ *     takes it from the mesh nodes).  The sponge state is stored and restored
+ *     with the flow state.  One sponge zone per solver; the mesh needs x_cv. */
+#define CGX_BC_SPONGE          14
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,

@@ -165,6 +165,7 @@ CGX_BC_NSCBC_OUTLET_P = 10
 CGX_BC_NSCBC_OUTLET_MDOT = 11
 CGX_BC_CBC_RUP = 12
 CGX_BC_WALL_CONDUCTIVE = 13
+CGX_BC_SPONGE = 14
 
 
 class Source(ctypes.Structure):
@@ -356,7 +357,10 @@ class Solver:
         (rho un p), CBC_MPT (mdot p T), CBC_EXTRAPOLATE (none), CBC_TOTAL_PT
         (p_total T_total t_relax [use_avg]), NSCBC_MT (mdot T; T < 0: the
         total temperature -T), NSCBC_OUTLET_P (p_ref sigma L_ref),
-        NSCBC_OUTLET_MDOT (mdot t_relax); SLIP and WALL_ADIABATIC as set_bc."""
+        NSCBC_OUTLET_MDOT (mdot t_relax), CBC_RUP (rho u0 u1 u2 p),
+        WALL_CONDUCTIVE (T_end [L k]...), SPONGE (type strength t_relax
+        length p_sponge L_max; the mesh needs x_cv); SLIP and
+        WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))
 

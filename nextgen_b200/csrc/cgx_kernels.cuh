@@ -233,7 +233,15 @@ struct StateDev {
   // per zone [8]: the zone sums of this stage (0..3) and the zone's own
   // state (4: CBC_TOTAL_PT USE_AVG's relaxed mean normal speed)
   double* zst;
-  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones, 8 zone sums
+  // a sponge zone: each cell's sponge state [4][N] (T, u), and the cells of
+  // the layer with their strength ((s - L_max + length)/length)^2 times the
+  // zone's strength
+  double* spg;
+  const int* spc;
+  const double* spw;
+  int nsp;
+  double sp_p, sp_relax;  // the sponge's pressure and relaxation time
+  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones, 8 zone sums, 16 a sponge
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

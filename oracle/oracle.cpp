@@ -142,6 +142,11 @@ struct orc_solver {
   // three stages (Nscbc::initData, IdealGasSolverBcs.cpp:3615-3628)
   std::vector<double> ns_rho, ns_p, ns_u, ns_rhs;
   std::vector<double> un_bc_avg;  // CBC_TOTAL_PT USE_AVG: per zone
+  // a SPONGE zone (Sponge, IdealGasSolverBcs.cpp:4080-4092): its parameters,
+  // each cell's T_sponge and u_sponge, and the cell centroids
+  int sp_zone = -1, sp_type = 0;
+  double sp_strength = 0.0, sp_relax = 0.0, sp_length = 0.0, sp_p = 0.0, sp_Lmax = 0.0;
+  std::vector<double> T_sponge, u_sponge, x_cv;
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
@@ -444,6 +449,35 @@ void add_source(orc_solver* o, IdealGasRhs* rhs) {
     }
 }
 
+// The sponge layer's volume term (Sponge::addBoundaryFlux,
+// IdealGasSolverBcs.cpp:4196-4283): the cells whose distance along the
+// layer's direction exceeds L_max - length, with the quadratic profile.
+void sponge_volume(orc_solver* o, IdealGasRhs* rhs) {
+  const double gm1 = o->prm.gamma - 1.0;
+  const double Lmax = o->sp_Lmax, len = o->sp_length;
+  for (int icv = 0; icv < o->ncv; ++icv) {
+    const double* x = &o->x_cv[3 * size_t(icv)];
+    double s;
+    if (o->sp_type <= 2)
+      s = x[o->sp_type];
+    else if (o->sp_type == 3)
+      s = std::sqrt(x[1] * x[1] + x[2] * x[2]);
+    else
+      s = std::sqrt(x[0] * x[0] + x[1] * x[1]);
+    if (!(s > Lmax - len)) continue;
+    const double x_sp = (s - (Lmax - len)) / len;
+    const double coeff = o->sp_strength * x_sp * x_sp;
+    const double rho_sp = o->sp_p / (o->T_sponge[icv] * o->R_gas);
+    const double* us = &o->u_sponge[3 * size_t(icv)];
+    const double* u = &o->u[3 * size_t(icv)];
+    const double v = o->vol_cv[icv];
+    rhs[icv].rho -= v * coeff * (o->rho[icv] - rho_sp);
+    for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= v * coeff * (o->rho[icv] * u[i] - rho_sp * us[i]);
+    const double rhoE_sp = o->sp_p / gm1 + 0.5 * rho_sp * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
+    rhs[icv].rhoE -= v * coeff * (o->rhoE[icv] - rhoE_sp);
+  }
+}
+
 // addBoundaryFlux of each zone's boundary condition, zone by zone, before
 // the face loops as calcRhsBase calls them (IdealGasSolver.cpp:261-262):
 // SlipWallBc (IdealGasSolverBcs.cpp:14-23), WallAdiabatic (:25-48),
@@ -474,6 +508,19 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         bs.sp_vol = 1.0 / o->ns_rho[ibf];
         bs.p = o->ns_p[ibf];
         bs.h = gogm1 * o->ns_p[ibf] * (1.0 / o->ns_rho[ibf]);
+        IdealGasRhs flux;
+        calcRiemannFlux(flux, n, o->cv_light[icv], bs, gamma, gamma);
+        rhs[icv].rho -= flux.rho;
+        for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= flux.rhou[i];
+        rhs[icv].rhoE -= flux.rhoE;
+      } else if (kind == CGX_BC_SPONGE) {
+        // Sponge::addBoundaryFlux (IdealGasSolverBcs.cpp:4166-4194): the
+        // face's state from its cell's sponge state at the sponge pressure
+        IdealGasState bs;
+        bs.sp_vol = o->T_sponge[icv] * o->R_gas / o->sp_p;
+        for (int i = 0; i < 3; ++i) bs.u[i] = o->u_sponge[3 * size_t(icv) + i];
+        bs.p = o->sp_p;
+        bs.h = o->R_gas * gamma * (1.0 / (gamma - 1.0)) * o->T_sponge[icv];
         IdealGasRhs flux;
         calcRiemannFlux(flux, n, o->cv_light[icv], bs, gamma, gamma);
         rhs[icv].rho -= flux.rho;
@@ -510,6 +557,7 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         rhs[icv].rhoE -= visc_work;
       }
     }
+    if (kind == CGX_BC_SPONGE) sponge_volume(o, rhs);
   }
 }
 
@@ -702,6 +750,22 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
         const double eps = 1.0 / (bc[3] / dt + 1.0);
         o->un_bc_avg[z] = (1.0 - eps) * o->un_bc_avg[z] + eps * avg0;
       }
+    }
+  }
+  // Sponge::rk3Step (IdealGasSolverBcs.cpp:4289-4309): relax toward the
+  // state at the beginning of the step; Sponge::initialHook (:4311-4346):
+  // start from it
+  if (o->sp_zone >= 0 && (init || rk_stage == 1)) {
+    const double eps = init ? 1.0 : 1.0 / (o->sp_relax / dt + 1.0);
+    for (int icv = 0; icv < o->ncv; ++icv) {
+      if (init) {
+        o->T_sponge[icv] = o->T[icv];
+        for (int i = 0; i < 3; ++i) o->u_sponge[3 * size_t(icv) + i] = o->u[3 * size_t(icv) + i];
+        continue;
+      }
+      o->T_sponge[icv] += eps * (o->T[icv] - o->T_sponge[icv]);
+      for (int i = 0; i < 3; ++i)
+        o->u_sponge[3 * size_t(icv) + i] += eps * (o->u[3 * size_t(icv) + i] - o->u_sponge[3 * size_t(icv) + i]);
     }
   }
   for (int ibf = 0; ibf < o->nbf; ++ibf) {
@@ -967,6 +1031,14 @@ void store_data(orc_solver* o) {
     o->store_recent[c++] = o->ns_p[ibf];
     for (int k = 0; k < 3; ++k) o->store_recent[c++] = o->ns_u[3 * size_t(ibf) + k];
   }
+  // Sponge::storeData (IdealGasSolverBcs.cpp:4130-4145): T, u per cell
+  if (o->sp_zone >= 0) {
+    o->store_recent.resize(c + 4 * size_t(n));
+    for (int i = 0; i < n; ++i) {
+      o->store_recent[c++] = o->T_sponge[i];
+      for (int k = 0; k < 3; ++k) o->store_recent[c++] = o->u_sponge[3 * size_t(i) + k];
+    }
+  }
   if (o->store_old.empty()) {
     o->store_old = o->store_recent;
     o->store_step_old = o->store_step_recent;
@@ -987,6 +1059,12 @@ void restore_data(orc_solver* o) {
     o->ns_rho[ibf] = o->store_old[c++];
     o->ns_p[ibf] = o->store_old[c++];
     for (int k = 0; k < 3; ++k) o->ns_u[3 * size_t(ibf) + k] = o->store_old[c++];
+  }
+  if (o->sp_zone >= 0 && o->store_old.size() >= c + 4 * size_t(n)) {  // Sponge::restoreData (:4147-4159)
+    for (int i = 0; i < n; ++i) {
+      o->T_sponge[i] = o->store_old[c++];
+      for (int k = 0; k < 3; ++k) o->u_sponge[3 * size_t(i) + k] = o->store_old[c++];
+    }
   }
   update_primitive(o);
   calc_sgs_props(o);
@@ -1062,6 +1140,7 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->ns_u.assign(3 * size_t(m->nbf), 0.0);
     o->ns_rhs.assign(15 * size_t(m->nbf), 0.0);
     o->un_bc_avg.assign(std::max(m->nbf_zones, 1), 0.0);
+    if (m->x_cv) o->x_cv.assign(m->x_cv, m->x_cv + 3 * size_t(ncv));
   }
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
@@ -1400,6 +1479,26 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
                  : kind == CGX_BC_CBC_EXTRAPOLATE ? 0 : kind == CGX_BC_NSCBC_MT ? 2
                  : kind == CGX_BC_NSCBC_OUTLET_P ? 3 : kind == CGX_BC_NSCBC_OUTLET_MDOT ? 2
                  : kind == CGX_BC_CBC_RUP ? 5 : (kind == CGX_BC_WALL_CONDUCTIVE && np >= 1 && np % 2 == 1) ? np : -1;
+  if (kind == CGX_BC_SPONGE) {
+    // Sponge::initData (IdealGasSolverBcs.cpp:4094-4128): type strength
+    // t_relax length p_sponge, and L_max in place of the nodes' extent
+    if (np != 6 || !prm || o->x_cv.empty() || (o->sp_zone >= 0 && o->sp_zone != zone)) return -1;
+    if (prm[0] < 0.0 || prm[0] > 4.0 || double(int(prm[0])) != prm[0] || !(prm[3] > 0.0) || !(prm[1] >= 0.0) ||
+        !(prm[2] > 0.0) || !(prm[4] > 0.0))
+      return -1;
+    o->sp_zone = zone;
+    o->sp_type = int(prm[0]);
+    o->sp_strength = prm[1];
+    o->sp_relax = prm[2];
+    o->sp_length = prm[3];
+    o->sp_p = prm[4];
+    o->sp_Lmax = prm[5];
+    o->T_sponge.assign(o->ncv, 0.0);
+    o->u_sponge.assign(3 * size_t(o->ncv), 0.0);
+    o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, 0.0};
+    return 0;
+  }
+  if (zone == o->sp_zone) o->sp_zone = -1;
   const bool use_avg = kind == CGX_BC_CBC_TOTAL_PT && np == 4;
   if (want < 0 || (np != want && !use_avg) || (np > 0 && !prm)) return -1;
   o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, kind == CGX_BC_WALL_ISOTHERMAL ? prm[0] : 0.0};

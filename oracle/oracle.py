@@ -80,7 +80,7 @@ class Oracle:
         if not os.path.exists(path):
             raise OSError("%s not built (make -C oracle%s)" % (path, " ref" if reference else ""))
         self.L = _load(path)
-        self.desc = mesh_desc(mesh, with_x=False)
+        self.desc = mesh_desc(mesh)  # x_cv: for a sponge layer's cells
         self.params = params
         self.ncv = mesh.ncv
         self.h = self.L.orc_create(ctypes.byref(self.desc), ctypes.byref(params), int(nparts))

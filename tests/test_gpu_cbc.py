@@ -220,3 +220,72 @@ def test_rup_and_conductive_match_oracle(chan):
         s.set_bc_params(1, COND, (1.0, 0.1))
     s.close()
     o.close()
+
+
+SPONGE = cgx.CGX_BC_SPONGE
+
+
+@pytest.mark.parametrize("kind", [1, 3], ids=["y", "rx"])
+def test_sponge_matches_oracle(chan, kind):
+    """SPONGE (Sponge, IdealGasSolverBcs.cpp:4080-4346) at y = Ly behind a
+    CBC_UPT inflow: the flow set to a second state after initComplete so
+    that the layer's volume term is live; calcRhs to 1e-12 of the face-sum
+    scale, 10 steps (the sponge state relaxing at stage 1) to 1e-10, and a
+    NaN restores the sponge state with the flow's, as the oracle does."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    dist = (x, y, z, np.sqrt(y * y + z * z), np.sqrt(x * x + y * y))[kind]
+    Lmax = dist.max() + 0.05
+    length = 0.45 * (Lmax - dist.min())
+    zones = ((UPT, (0.1, 0.4, 0.0, 1.01 * P0, 1.02)), (SPONGE, (kind, 3.0, 0.05, length, 1.01 * P0, Lmax)))
+    s, o = _make(m, gm, prm, zones)
+    rho, u, p = _state(m, prm)
+    B = (2.0 - rho, u[:, [1, 2, 0]], prm.p_ref + 0.5 * (p - prm.p_ref))
+    s.set_state_primitive(*B)
+    s.updateConservativeAndPrimitiveData()
+    s.calcSgsAndMaterialProperties()
+    o.set_state_primitive(*B)
+    o.update_primitive()
+    o.calc_sgs_props()
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    o.set_dt()
+    bad = [a.copy() for a in s.get_state()]
+    bad[0][5] = np.nan
+    s.set_state(*bad)
+    s.updateConservativeAndPrimitiveData()
+    o.poison(5)
+    assert s.advanceSolution() == -1 and o.advance_solution() == -1
+    assert s.step(3) == 0 and o.step(3) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
+
+
+def test_sponge_refusals(chan, built):
+    m, gm = chan
+    prm = cases.tgv_params()
+    good = (1, 2.0, 0.5, 0.8, prm.p_ref, m.L[1])
+    s = cgx.Solver(gm, prm)
+    for bad in ((5,) + good[1:], (1.5,) + good[1:], good[:3] + (0.0,) + good[4:], good[:5]):
+        with pytest.raises(cgx.CgxError):
+            s.set_bc_params(1, SPONGE, bad)
+    s.set_bc_params(1, SPONGE, good)
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_params(0, SPONGE, good)  # one sponge zone
+    with pytest.raises(cgx.CgxError):
+        s.set_scalars(np.zeros((m.ncv, 1)))  # no transport scalars with CBC zones
+    s.close()
+    # the layer's cells come from the mesh's x_cv
+    gm2 = cgx.Mesh(m, device=0, sfc=False)
+    s2 = cgx.Solver(gm2, prm)
+    with pytest.raises(cgx.CgxError):
+        s2.set_bc_params(1, SPONGE, good)
+    s2.close()
+    gm2.close()
