@@ -166,6 +166,8 @@ CGX_BC_NSCBC_OUTLET_MDOT = 11
 CGX_BC_CBC_RUP = 12
 CGX_BC_WALL_CONDUCTIVE = 13
 CGX_BC_SPONGE = 14
+CGX_BC_WM_ALG_ADIABATIC = 15
+CGX_BC_WM_ALG_ISOTHERMAL = 16
 
 
 class Source(ctypes.Structure):
@@ -359,7 +361,8 @@ class Solver:
         total temperature -T), NSCBC_OUTLET_P (p_ref sigma L_ref),
         NSCBC_OUTLET_MDOT (mdot t_relax), CBC_RUP (rho u0 u1 u2 p),
         WALL_CONDUCTIVE (T_end [L k]...), SPONGE (type strength t_relax
-        length p_sponge L_max; the mesh needs x_cv); SLIP and
+        length p_sponge L_max; the mesh needs x_cv), WM_ALG_ADIABATIC
+        ([u_wall]), WM_ALG_ISOTHERMAL (T); SLIP and
         WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))

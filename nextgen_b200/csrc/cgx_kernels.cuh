@@ -228,7 +228,8 @@ struct StateDev {
   double* bfs;
   double* un_bc;
   // NSCBC zones, per boundary face ([20][nbf]): rho_bc, p_bc, u_bc[3], then
-  // the characteristic rhs of stages 1..3 (5 each)
+  // the characteristic rhs of stages 1..3 (5 each); wall-model faces keep
+  // tau_wall and q_wall in rows 0 and 1 (stored and restored with rows 0-4)
   double* nsb;
   // per zone [8]: the zone sums of this stage (0..3) and the zone's own
   // state (4: CBC_TOTAL_PT USE_AVG's relaxed mean normal speed)
@@ -241,7 +242,7 @@ struct StateDev {
   const double* spw;
   int nsp;
   double sp_p, sp_relax;  // the sponge's pressure and relaxation time
-  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones, 8 zone sums, 16 a sponge
+  int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones, 8 zone sums, 16 a sponge, 32 wall models
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

@@ -60,6 +60,8 @@ def _load(path):
         "orc_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
         "orc_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "orc_uses_reference_flux": (ctypes.c_int, []),
+        "orc_wm_solve_tau": (ctypes.c_double, [ctypes.c_double] * 5),
+        "orc_wm_q_wall": (ctypes.c_double, [ctypes.c_double] * 8),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -67,6 +69,17 @@ def _load(path):
         f.argtypes = args
     _libs[path] = L
     return L
+
+
+def wm_solve_tau(u1, y1, rho, mu, ut_guess=-1.0, reference=False):
+    """The algebraic wall model's tau_wall (AlgebraicWM::solve_tau): the
+    restatement, or the reference header's own with reference=True."""
+    return _load(REF_LIB_PATH if reference else LIB_PATH).orc_wm_solve_tau(u1, y1, rho, mu, ut_guess)
+
+
+def wm_q_wall(T1, Tw, tau, rho, mu, locp, cp, y1, reference=False):
+    """The algebraic wall model's wall heat flux (compute_q_wall_approx)."""
+    return _load(REF_LIB_PATH if reference else LIB_PATH).orc_wm_q_wall(T1, Tw, tau, rho, mu, locp, cp, y1)
 
 
 def _dp(a):

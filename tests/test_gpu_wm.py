@@ -1,0 +1,101 @@
+"""The algebraic wall-model zones on the GPU against the oracle, on a channel
+(periodic in x and z, walls at y = 0 and y = Ly): WM_ALG_ADIABATIC with a
+moving wall and WM_ALG_ISOTHERMAL (WmAdiabatic, WmIsothermal,
+IdealGasSolverBcs.cpp:996-1478, 2054-2262).
+
+* calcRhs after initComplete (the laminar wall stress) within 1e-12 of the
+  face-sum scale;
+* 10 RK3 steps, each solving the law of the wall for every face at its first
+  stage from the last step's tau_wall: state within 1e-10 of the oracle's;
+* a NaN restores tau_wall with the state, and 3 more steps still match;
+* the mixed-precision form within its flux tolerance of the FP64 path.
+"""
+import numpy as np
+import pytest
+
+from nextgen_b200 import cases, cgx
+from nextgen_b200.meshgen import ChannelMesh
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+WM_AD, WM_ISO = cgx.CGX_BC_WM_ALG_ADIABATIC, cgx.CGX_BC_WM_ALG_ISOTHERMAL
+ZONES = ((WM_AD, (0.0, 0.0, 0.05)), (WM_ISO, (1.2,)))
+
+
+@pytest.fixture(scope="module")
+def chan(built):
+    m = ChannelMesh(16, 12, 8, L=(4.0, 3.0, 2.0), jitter=0.25, seed=11)
+    return m, cgx.Mesh(m, device=0)
+
+
+def _state(m, prm):
+    x, y, z = m.x_cv[: m.ncv].T
+    Lx, Ly, Lz = m.L
+    u = np.stack([0.3 + 0.1 * np.cos(2 * np.pi * z / Lz), 0.02 * np.sin(2 * np.pi * x / Lx),
+                  0.05 * np.sin(np.pi * y / Ly)], 1)
+    rho = 1.0 + 0.02 * np.cos(2 * np.pi * x / Lx)
+    p = prm.p_ref * (1.0 + 0.01 * np.sin(2 * np.pi * z / Lz))
+    return rho, u, p
+
+
+def _make(m, gm, prm, prec=cgx.CGX_FP64):
+    s = cgx.Solver(gm, prm, prec)
+    o = Oracle(m, prm)
+    for z, (k, a) in enumerate(ZONES):
+        s.set_bc_params(z, k, a)
+        o.set_bc_params(z, k, a)
+    st = _state(m, prm)
+    s.set_state_primitive(*st)
+    s.initComplete()
+    o.set_state_primitive(*st)
+    o.init_complete()
+    return s, o
+
+
+def test_wall_models_match_oracle(chan):
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    s, o = _make(m, gm, prm)
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    # a NaN: both restore the stored state with its tau_wall
+    o.set_dt()
+    bad = [a.copy() for a in s.get_state()]
+    bad[0][5] = np.nan
+    s.set_state(*bad)
+    s.updateConservativeAndPrimitiveData()
+    o.poison(5)
+    assert s.advanceSolution() == -1 and o.advance_solution() == -1
+    assert s.step(3) == 0 and o.step(3) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
+
+
+def test_wall_models_mixed_close_to_fp64(chan):
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    res = {}
+    for prec in (cgx.CGX_FP64, cgx.CGX_MIXED):
+        s, o = _make(m, gm, prm, prec)
+        o.close()
+        assert s.step(10) == 0
+        res[prec] = s.get_state()
+        s.close()
+    for a64, a32 in zip(res[cgx.CGX_FP64], res[cgx.CGX_MIXED]):
+        assert np.sqrt(((a32 - a64) ** 2).mean() / (a64 ** 2).mean()) <= 1e-5
+
+
+def test_wall_model_refusals(chan):
+    m, gm = chan
+    s = cgx.Solver(gm, cases.tgv_params())
+    for kind, bad in ((WM_AD, (0.1,)), (WM_ISO, ()), (WM_ISO, (1.0, 2.0))):
+        with pytest.raises(cgx.CgxError):
+            s.set_bc_params(0, kind, bad)
+    s.close()
