@@ -345,6 +345,13 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *     Y_PLUS0 and TOL belong to the equilibrium (WM_EQ_*) forms, not built. */
 #define CGX_BC_WM_ALG_ADIABATIC  15
 #define CGX_BC_WM_ALG_ISOTHERMAL 16
+/*   CGX_BC_WM_ALG_CONDUCTIVE  T_end [L_1 k_1 [L_2 k_2 ...]]   (WM_ALG_CONDUCTIVE
+ *     T_end L_1 k_1 ... END) the algebraic wall model behind conducting
+ *     layers (WmAlgConductive, IdealGasSolverBcs.cpp:2411-2560): tau_wall as
+ *     WM_ALG_ISOTHERMAL, and the wall heat flux through the model's near-wall
+ *     resistance (AlgebraicWM::compute_R_approx) in series with the layers'
+ *     sum of L_i / k_i, toward T_end; no heat flux until the first step. */
+#define CGX_BC_WM_ALG_CONDUCTIVE 17
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,

@@ -168,6 +168,7 @@ CGX_BC_WALL_CONDUCTIVE = 13
 CGX_BC_SPONGE = 14
 CGX_BC_WM_ALG_ADIABATIC = 15
 CGX_BC_WM_ALG_ISOTHERMAL = 16
+CGX_BC_WM_ALG_CONDUCTIVE = 17
 
 
 class Source(ctypes.Structure):
@@ -362,7 +363,8 @@ class Solver:
         NSCBC_OUTLET_MDOT (mdot t_relax), CBC_RUP (rho u0 u1 u2 p),
         WALL_CONDUCTIVE (T_end [L k]...), SPONGE (type strength t_relax
         length p_sponge L_max; the mesh needs x_cv), WM_ALG_ADIABATIC
-        ([u_wall]), WM_ALG_ISOTHERMAL (T); SLIP and
+        ([u_wall]), WM_ALG_ISOTHERMAL (T), WM_ALG_CONDUCTIVE (T_end [L k]...);
+        SLIP and
         WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))

@@ -224,12 +224,38 @@ double wm_q_wall(double T1, double Tw, double tau, double rho, double mu, double
   }
   return num / (1.0 + kappa_t * Ts);
 }
+
+// compute_R_approx (AlgebraicWM.hpp:220-268), restated
+double wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1) {
+  const double Pr_t = 0.85, kappa_t = kWmKappa / Pr_t, C_t = 3.9, ys = 8.28314;
+  const double ut = std::sqrt(tau / rho);
+  const double mu_t = rho * kWmKappa * ut * y1;
+  const double l_t = mu_t * cp / Pr_t;
+  const double l_tot = locp * cp + l_t;
+  const double num = l_tot / y1;
+  const double re = ut * rho * y1 / mu;
+  double Ts;
+  if (re <= ys) {
+    Ts = 0.5 * re;
+  } else {
+    Ts = 0.5 * ys * ys / re;
+    Ts += C_t * (1.0 - ys / re);
+    double t = std::log(re) - 1.0;
+    t -= ys / re * (std::log(ys) - 1.0);
+    t /= kappa_t;
+    Ts += t;
+  }
+  return (1.0 + kappa_t * Ts) / num;
+}
 #else
 double wm_solve_tau(double u1, double y1, double rho, double mu, double ut_guess) {
   return AlgebraicWM::solve_tau(u1, y1, rho, mu, ut_guess);
 }
 double wm_q_wall(double T1, double Tw, double tau, double rho, double mu, double locp, double cp, double y1) {
   return AlgebraicWM::compute_q_wall_approx(T1, Tw, tau, rho, mu, locp, cp, y1);
+}
+double wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1) {
+  return AlgebraicWM::compute_R_approx(tau, rho, mu, locp, cp, y1);
 }
 #endif
 
@@ -607,8 +633,9 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
         } else {
           for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= o->p[icv] * n[i];
         }
-      } else if (kind == CGX_BC_WM_ALG_ISOTHERMAL) {
-        // WmIsothermal::addBoundaryFlux (IdealGasSolverBcs.cpp:2218-2262)
+      } else if (kind == CGX_BC_WM_ALG_ISOTHERMAL || kind == CGX_BC_WM_ALG_CONDUCTIVE) {
+        // WmIsothermal::addBoundaryFlux (IdealGasSolverBcs.cpp:2218-2262) and
+        // WmAlgConductive::addBoundaryFlux (:2562-2595), the same
         const double* u = &o->u[3 * size_t(icv)];
         const double area = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
         double u_mag = 0.0;
@@ -754,7 +781,8 @@ void bc_calc_rhs(orc_solver* o, int rk_stage) {
   for (int ibf = 0; ibf < o->nbf && rk_stage == 1; ++ibf) {
     const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
     const int kind = int(bc[0]);
-    if (kind != CGX_BC_WM_ALG_ADIABATIC && kind != CGX_BC_WM_ALG_ISOTHERMAL) continue;
+    if (kind != CGX_BC_WM_ALG_ADIABATIC && kind != CGX_BC_WM_ALG_ISOTHERMAL && kind != CGX_BC_WM_ALG_CONDUCTIVE)
+      continue;
     const int icv = o->cvobf[ibf];
     const double* n = &o->n_bf[3 * size_t(ibf)];
     const double* u = &o->u[3 * size_t(icv)];
@@ -785,6 +813,11 @@ void bc_calc_rhs(orc_solver* o, int rk_stage) {
     if (kind == CGX_BC_WM_ALG_ISOTHERMAL) {
       const double cp = o->R_gas * gamma / (gamma - 1.0);
       o->wm_q[ibf] = wm_q_wall(o->T[icv], bc[4], o->wm_tau[ibf], o->rho[icv], o->mu_lam[icv], o->loc_lam[icv], cp, y1);
+    } else if (kind == CGX_BC_WM_ALG_CONDUCTIVE) {  // WmAlgConductive::calcRhs (:2495-2560)
+      const double cp = o->R_gas * gamma / (gamma - 1.0);
+      const double r_cv = wm_r_approx(o->wm_tau[ibf], o->rho[icv], o->mu_lam[icv], o->loc_lam[icv], cp, y1);
+      const double r_all = bc[2] / area + r_cv;
+      o->wm_q[ibf] = (o->T[icv] - bc[1]) / r_all / area;
     }
   }
   // zone sums: NSCBC_MT T_TOTAL (:3781-3805), NSCBC_OUTLET_MDOT (:3934-3954)
@@ -919,7 +952,8 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
   for (int ibf = 0; ibf < o->nbf; ++ibf) {
     const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
     const int kind = int(bc[0]);
-    if (init && (kind == CGX_BC_WM_ALG_ADIABATIC || kind == CGX_BC_WM_ALG_ISOTHERMAL)) {
+    if (init && (kind == CGX_BC_WM_ALG_ADIABATIC || kind == CGX_BC_WM_ALG_ISOTHERMAL ||
+                 kind == CGX_BC_WM_ALG_CONDUCTIVE)) {
       // WmAdiabatic::initialHook (:1078-1122), WmIsothermal::initialHook (:2089-2113)
       const int icv = o->cvobf[ibf];
       const double* n = &o->n_bf[3 * size_t(ibf)];
@@ -932,11 +966,13 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
           double d[3];
           for (int i = 0; i < 3; ++i) d[i] = u[i] - bc[1 + i];
           o->wm_tau[ibf] = o->mu_lam[icv] * std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / y1;
-        } else {
+        } else if (kind == CGX_BC_WM_ALG_ISOTHERMAL) {
           const double cp = o->R_gas * o->prm.gamma / (o->prm.gamma - 1.0);
           const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
           o->wm_tau[ibf] = o->mu_lam[icv] * std::sqrt(usq) / y1;
           o->wm_q[ibf] = o->mu_lam[icv] * (cp * o->T[icv] + 0.5 * usq - cp * bc[4]) / y1;
+        } else {  // WmAlgConductive::initialHook (:2432-2457)
+          o->wm_tau[ibf] = o->mu_lam[icv] * std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) / y1;
         }
       }
       continue;
@@ -1680,6 +1716,13 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
     o->bc[zone] = {double(kind), np ? prm[0] : 0.0, np ? prm[1] : 0.0, np ? prm[2] : 0.0, 0.0};
     return 0;
   }
+  if (kind == CGX_BC_WM_ALG_CONDUCTIVE) {  // T_end [L_i k_i]...: T_end, sum of L_i / k_i
+    if (np < 1 || np % 2 != 1 || !prm) return -1;
+    double r = 0.0;
+    for (int i = 1; i + 1 < np; i += 2) r += prm[i] / prm[i + 1];
+    o->bc[zone] = {double(kind), prm[0], r, 0.0, 0.0};
+    return 0;
+  }
   if (kind == CGX_BC_WM_ALG_ISOTHERMAL) {  // T
     if (np != 1 || !prm) return -1;
     o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, prm[0]};
@@ -1786,4 +1829,7 @@ extern "C" double orc_wm_solve_tau(double u1, double y1, double rho, double mu, 
 extern "C" double orc_wm_q_wall(double T1, double Tw, double tau, double rho, double mu, double locp, double cp,
                                 double y1) {
   return wm_q_wall(T1, Tw, tau, rho, mu, locp, cp, y1);
+}
+extern "C" double orc_wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1) {
+  return wm_r_approx(tau, rho, mu, locp, cp, y1);
 }

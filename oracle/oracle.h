@@ -90,6 +90,7 @@ int orc_uses_reference_flux(void);
 /* The algebraic wall model's tau_wall and wall heat flux on their own. */
 double orc_wm_solve_tau(double u1, double y1, double rho, double mu, double ut_guess);
 double orc_wm_q_wall(double T1, double Tw, double tau, double rho, double mu, double locp, double cp, double y1);
+double orc_wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1);
 
 #ifdef __cplusplus
 }

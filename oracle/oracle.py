@@ -62,6 +62,7 @@ def _load(path):
         "orc_uses_reference_flux": (ctypes.c_int, []),
         "orc_wm_solve_tau": (ctypes.c_double, [ctypes.c_double] * 5),
         "orc_wm_q_wall": (ctypes.c_double, [ctypes.c_double] * 8),
+        "orc_wm_r_approx": (ctypes.c_double, [ctypes.c_double] * 6),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -80,6 +81,11 @@ def wm_solve_tau(u1, y1, rho, mu, ut_guess=-1.0, reference=False):
 def wm_q_wall(T1, Tw, tau, rho, mu, locp, cp, y1, reference=False):
     """The algebraic wall model's wall heat flux (compute_q_wall_approx)."""
     return _load(REF_LIB_PATH if reference else LIB_PATH).orc_wm_q_wall(T1, Tw, tau, rho, mu, locp, cp, y1)
+
+
+def wm_r_approx(tau, rho, mu, locp, cp, y1, reference=False):
+    """The algebraic wall model's near-wall thermal resistance (compute_R_approx)."""
+    return _load(REF_LIB_PATH if reference else LIB_PATH).orc_wm_r_approx(tau, rho, mu, locp, cp, y1)
 
 
 def _dp(a):

@@ -1,7 +1,8 @@
 """The algebraic wall-model zones on the GPU against the oracle, on a channel
 (periodic in x and z, walls at y = 0 and y = Ly): WM_ALG_ADIABATIC with a
-moving wall and WM_ALG_ISOTHERMAL (WmAdiabatic, WmIsothermal,
-IdealGasSolverBcs.cpp:996-1478, 2054-2262).
+moving wall, WM_ALG_ISOTHERMAL, and WM_ALG_CONDUCTIVE behind two layers
+(WmAdiabatic, WmIsothermal, WmAlgConductive, IdealGasSolverBcs.cpp:996-1478,
+2054-2262, 2411-2595).
 
 * calcRhs after initComplete (the laminar wall stress) within 1e-12 of the
   face-sum scale;
@@ -20,7 +21,9 @@ from oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 WM_AD, WM_ISO = cgx.CGX_BC_WM_ALG_ADIABATIC, cgx.CGX_BC_WM_ALG_ISOTHERMAL
+WM_COND = cgx.CGX_BC_WM_ALG_CONDUCTIVE
 ZONES = ((WM_AD, (0.0, 0.0, 0.05)), (WM_ISO, (1.2,)))
+ZONES_COND = ((WM_COND, (1.3, 0.01, 0.5, 0.02, 1.0)), (WM_AD, ()))
 
 
 @pytest.fixture(scope="module")
@@ -39,10 +42,10 @@ def _state(m, prm):
     return rho, u, p
 
 
-def _make(m, gm, prm, prec=cgx.CGX_FP64):
+def _make(m, gm, prm, prec=cgx.CGX_FP64, zones=ZONES):
     s = cgx.Solver(gm, prm, prec)
     o = Oracle(m, prm)
-    for z, (k, a) in enumerate(ZONES):
+    for z, (k, a) in enumerate(zones):
         s.set_bc_params(z, k, a)
         o.set_bc_params(z, k, a)
     st = _state(m, prm)
@@ -53,10 +56,11 @@ def _make(m, gm, prm, prec=cgx.CGX_FP64):
     return s, o
 
 
-def test_wall_models_match_oracle(chan):
+@pytest.mark.parametrize("zones", [ZONES, ZONES_COND], ids=["adiabatic_isothermal", "conductive"])
+def test_wall_models_match_oracle(chan, zones):
     m, gm = chan
     prm = cases.tgv_params(Re=400.0)
-    s, o = _make(m, gm, prm)
+    s, o = _make(m, gm, prm, zones=zones)
     r = s.calcRhs(1)
     ref, scale = o.calc_rhs(1)
     assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
@@ -95,7 +99,7 @@ def test_wall_models_mixed_close_to_fp64(chan):
 def test_wall_model_refusals(chan):
     m, gm = chan
     s = cgx.Solver(gm, cases.tgv_params())
-    for kind, bad in ((WM_AD, (0.1,)), (WM_ISO, ()), (WM_ISO, (1.0, 2.0))):
+    for kind, bad in ((WM_AD, (0.1,)), (WM_ISO, ()), (WM_ISO, (1.0, 2.0)), (WM_COND, (1.0, 0.1))):
         with pytest.raises(cgx.CgxError):
             s.set_bc_params(0, kind, bad)
     s.close()

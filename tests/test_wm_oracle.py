@@ -1,13 +1,17 @@
-"""The algebraic wall-model zones WM_ALG_ADIABATIC and WM_ALG_ISOTHERMAL in
-the oracle, on CPU (WmAdiabatic, WmIsothermal, IdealGasSolverBcs.cpp:
-996-1478, 2054-2262; AlgebraicWM.hpp).
+"""The algebraic wall-model zones WM_ALG_ADIABATIC, WM_ALG_ISOTHERMAL and
+WM_ALG_CONDUCTIVE in the oracle, on CPU (WmAdiabatic, WmIsothermal,
+WmAlgConductive, IdealGasSolverBcs.cpp:996-1478, 2054-2262, 2411-2595;
+AlgebraicWM.hpp).
 
 * The restated law-of-the-wall solve recovers u_tau = 0.123 to 1e-7 at the
   y+ values of the reference's own known-answer test
   (src/charles/tests/wm_test.cpp:49-87), and 0 at a separation point.
-* The restated tau_wall and wall heat flux equal the reference header's own
+* The restated tau_wall, wall heat flux and near-wall resistance equal the
+  reference header's own
   (AlgebraicWM.hpp compiled where it lies) bit for bit over random inputs,
   and so do whole solver runs with wall-model zones.
+* WM_ALG_CONDUCTIVE starts without a heat flux, and behind layers lets in
+  less heat than without them.
 * After initComplete the wall stress is the laminar estimate mu |u| / y1, so
   for a flow along the walls WM_ALG_ADIABATIC gives WALL_ADIABATIC's rhs (a
   moving wall included), and WM_ALG_ISOTHERMAL gives WALL_ISOTHERMAL's
@@ -22,7 +26,7 @@ from nextgen_b200 import cases
 from nextgen_b200.meshgen import ChannelMesh
 from oracle import Oracle
 
-WALL, ISO, WM_AD, WM_ISO = 2, 3, 15, 16
+WALL, ISO, WM_AD, WM_ISO, WM_COND = 2, 3, 15, 16, 17
 need_ref = pytest.mark.skipif(not orc_mod.ref_available(), reason="reference-built oracle absent")
 
 KAPPA, B, YSTAR = 0.41, 5.2, 23.3244
@@ -59,6 +63,8 @@ def test_restated_wall_model_bitwise_equals_reference(built):
         assert a == orc_mod.wm_solve_tau(u1, y1, rho, mu, g, reference=True)
         args = (float(rng.uniform(0.8, 1.5)), float(rng.uniform(0.8, 1.5)), a, rho, mu, mu / 0.7, 3.5, y1)
         assert orc_mod.wm_q_wall(*args) == orc_mod.wm_q_wall(*args, reference=True)
+        args = (a, rho, mu, mu / 0.7, 3.5, y1)
+        assert orc_mod.wm_r_approx(*args) == orc_mod.wm_r_approx(*args, reference=True)
 
 
 @pytest.fixture(scope="module")
@@ -117,9 +123,35 @@ def test_initial_isothermal_wall_model(chan):
     assert (np.abs(a[:, 4] - want) / np.maximum(np.abs(want), sa[:, 4])).max() <= 1e-12
 
 
+def test_conductive_wall_model(chan):
+    """WM_ALG_CONDUCTIVE: no heat flux before the first step (its initial
+    hook), so for a flow along the walls its first rhs is WALL_ADIABATIC's;
+    over a step with hot walls the heat that enters is less behind layers
+    than without them (series resistance), and positive."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    st = _along(m, prm)
+    a, sa, _ = _rhs(m, prm, ((WM_COND, [1.3, 0.01, 0.5]), (WM_COND, [1.2])), st)
+    b, _, _ = _rhs(m, prm, ((WALL, []), (WALL, [])), st)
+    assert (np.abs(a - b) / np.maximum(np.abs(b), sa)).max() <= 1e-12
+    E = []
+    for zones in (((WM_COND, [1.3, 0.05, 0.2]), (WM_COND, [1.3, 0.05, 0.2])), ((WM_COND, [1.3]), (WM_COND, [1.3]))):
+        o = Oracle(m, prm)
+        for z, (k, p) in enumerate(zones):
+            o.set_bc_params(z, k, p)
+        o.set_state_primitive(*st)
+        o.init_complete()
+        E0 = o.totals()[4]
+        assert o.step(2) == 0
+        E.append(o.totals()[4] - E0)
+        o.close()
+    assert 0.0 < E[0] < E[1]
+
+
 def test_wall_model_refusals(chan):
     o = Oracle(chan, cases.tgv_params())
-    for kind, bad in ((WM_AD, [0.1]), (WM_AD, [0.1, 0.2]), (WM_ISO, []), (WM_ISO, [1.0, 2.0])):
+    for kind, bad in ((WM_AD, [0.1]), (WM_AD, [0.1, 0.2]), (WM_ISO, []), (WM_ISO, [1.0, 2.0]), (WM_COND, []),
+                      (WM_COND, [1.0, 0.1])):
         with pytest.raises(ValueError):
             o.set_bc_params(0, kind, bad)
     o.close()
@@ -143,7 +175,16 @@ def test_wall_model_solver_bitwise_equals_reference(chan):
         o.init_complete()
         assert o.step(4) == 0
         out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+        o.close()
+        o = Oracle(m, prm, reference=reference)
+        o.set_bc_params(0, WM_COND, [1.3, 0.01, 0.5])
+        o.set_bc_params(1, WM_ISO, [0.9])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        assert o.step(4) == 0
+        out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
         out.append(o.calc_rhs(1)[0])
         o.close()
-    assert np.array_equal(out[0], out[2])
-    assert np.array_equal(out[1], out[3])
+    assert np.array_equal(out[0], out[3])
+    assert np.array_equal(out[1], out[4])
+    assert np.array_equal(out[2], out[5])
