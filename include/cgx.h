@@ -352,7 +352,21 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *     resistance (AlgebraicWM::compute_R_approx) in series with the layers'
  *     sum of L_i / k_i, toward T_end; no heat flux until the first step. */
 #define CGX_BC_WM_ALG_CONDUCTIVE 17
+/*   CGX_BC_CBC_PROFILE  (set with cgx_set_bc_profile)  CBC_PROFILE and
+ *     CBC_PROFILE_SIMPLE (CbcProfile, CbcProfileSimple, IdealGasSolverBcs.cpp:
+ *     3024-3180, 5339-5375): a characteristic zone whose boundary state is
+ *     given face by face; the HLLC Riemann flux as the other CBC zones. */
+#define CGX_BC_CBC_PROFILE       18
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
+
+/* A CBC_PROFILE zone from the boundary states of its faces: bf_state
+ * [nbf_zone][6] = u[0], u[1], u[2], sp_vol, p, h of each face (the members of
+ * the reference's IdealGasState that Cbc::addBoundaryFlux reads), the zone's
+ * faces in the order the mesh description lists them.  The reference reads a
+ * profile file and interpolates it to the faces in CbcProfile::initData; the
+ * caller passes the interpolated states (INTEGRATION shows the forwarding).
+ * nbf_zone must be the zone's face count. */
+int cgx_set_bc_profile(cgx_solver* s, int zone, const double* bf_state, int nbf_zone);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */

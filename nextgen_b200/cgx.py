@@ -150,6 +150,7 @@ EXPORTS = [
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
     "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params", "cgx_set_host_threads",
+    "cgx_set_bc_profile",
 ]
 
 CGX_BC_SLIP = 1
@@ -169,6 +170,7 @@ CGX_BC_SPONGE = 14
 CGX_BC_WM_ALG_ADIABATIC = 15
 CGX_BC_WM_ALG_ISOTHERMAL = 16
 CGX_BC_WM_ALG_CONDUCTIVE = 17
+CGX_BC_CBC_PROFILE = 18
 
 
 class Source(ctypes.Structure):
@@ -226,6 +228,7 @@ def lib():
         "cgx_set_source": (ctypes.c_int, [vp, ctypes.POINTER(Source)]),
         "cgx_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
         "cgx_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "cgx_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_host_threads": (ctypes.c_int, [ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
@@ -368,6 +371,13 @@ class Solver:
         WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         _check(lib().cgx_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)))
+
+    def set_bc_profile(self, zone, states):
+        """CBC_PROFILE zone: states[nz][6] = u0 u1 u2 sp_vol p h of each of the
+        zone's faces, in the order the mesh lists them (the reference's
+        bf_state after CbcProfile::initData)."""
+        a = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6)
+        _check(lib().cgx_set_bc_profile(self.h, int(zone), _dp(a), int(a.shape[0])))
 
     # -- source terms (addSourceHook) ----------------------------------------
     def set_source(self, A=0.0, g=(0.0, 0.0, 0.0), field=None):

@@ -1096,7 +1096,8 @@ __host__ __device__ inline double wm_r_approx(double tau, double rho, double mu,
 
 __host__ __device__ inline bool bc_is_cbc(int k) {
   return k == CGX_BC_CBC_UPT || k == CGX_BC_CBC_RUNP || k == CGX_BC_CBC_MPT || k == CGX_BC_CBC_RUP ||
-         k == CGX_BC_CBC_EXTRAPOLATE || k == CGX_BC_CBC_TOTAL_PT || k == CGX_BC_SPONGE || bc_is_nscbc(k);
+         k == CGX_BC_CBC_EXTRAPOLATE || k == CGX_BC_CBC_TOTAL_PT || k == CGX_BC_SPONGE || k == CGX_BC_CBC_PROFILE ||
+         bc_is_nscbc(k);
 }
 
 // A state as the boundary Riemann flux reads it (the reference's
@@ -1285,7 +1286,8 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
         sb.sp_vol = 1.0 / rb;
         sb.p = pb;
         sb.h = gamma / (gamma - 1.0) * pb * (1.0 / rb);
-      } else if (kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT) {  // the face's own state
+      } else if (kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT ||
+                 kind == CGX_BC_CBC_PROFILE) {  // the face's own state
         const double* q = s.bfs + f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) sb.u[d] = q[d * m.nbf];
@@ -2087,6 +2089,7 @@ struct cgx_mesh {
   int nbf_zones = 0;        // boundary zones (0: periodic)
   std::vector<double> zone_area;  // sum of |n_bf| over each zone (its area_global)
   std::vector<double> x_cv;       // [N][3] cell centroids in the mesh's order (when given)
+  std::vector<std::vector<int>> zone_faces;  // per zone: its faces' positions, in description order
   std::vector<void*> allocs;
   size_t bytes = 0;
   cgx_mesh_stats stats{};
@@ -3148,6 +3151,10 @@ extern "C" int cgx_mesh_create(const cgx_mesh_desc* d, int device, cgx_mesh** ou
       std::vector<int> fill(bfc.begin(), bfc.end() - 1);
       for (int f = 0; f < nbf; ++f) {
         const int k = fill[size_t(iperm[d->cvobf[f]])]++;
+        if (d->zone_bf[f] >= 0 && d->zone_bf[f] < d->nbf_zones) {
+          if (M->zone_faces.size() < size_t(d->nbf_zones)) M->zone_faces.resize(size_t(d->nbf_zones));
+          M->zone_faces[size_t(d->zone_bf[f])].push_back(k);
+        }
         for (int c = 0; c < 3; ++c) bf_n[size_t(c) * nbf + k] = d->n_bf[3 * size_t(f) + c];
         bf_aod[k] = d->area_over_delta_bf[f];
         bf_zone[k] = d->zone_bf[f];
@@ -4010,7 +4017,37 @@ static int set_sponge(cgx_solver* s, int zone, const double* a) {
   return CGX_OK;
 }
 
+static int set_bc_impl(cgx_solver* s, int zone, int kind, const double* params, int nparams, bool profile);
+
 extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams) {
+  return set_bc_impl(s, zone, kind, params, nparams, false);
+}
+
+// CbcProfile::initData's result (IdealGasSolverBcs.cpp:3024-3180): the
+// zone's faces take the given states in the per-face boundary-state rows.
+extern "C" int cgx_set_bc_profile(cgx_solver* s, int zone, const double* st, int nbf_zone) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_bc_profile: null solver");
+  if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_profile: bad zone");
+  const std::vector<int>& faces = s->mesh->zone_faces[size_t(zone)];
+  if (nbf_zone != int(faces.size()) || (nbf_zone > 0 && !st))
+    return fail(CGX_E_ARG, "cgx_set_bc_profile: zone " + std::to_string(zone) + " has " +
+                               std::to_string(faces.size()) + " faces, got " + std::to_string(nbf_zone));
+  if (s->sd.nsc > 0) return fail(CGX_E_STATE, "cgx_set_bc: CBC boundary zones carry no transport scalars");
+  for (int j = 0; j < 6 * nbf_zone; ++j)
+    if (!std::isfinite(st[j])) return fail(CGX_E_ARG, "cgx_set_bc_profile: a boundary state is not finite");
+  const size_t nbf = size_t(s->mesh->md.nbf);
+  CK(cudaSetDevice(s->mesh->device));
+  std::vector<double> h(6 * nbf);
+  CK(cudaMemcpyAsync(h.data(), s->sd.bfs, 6 * nbf * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (int j = 0; j < nbf_zone; ++j)
+    for (int r = 0; r < 6; ++r) h[size_t(r) * nbf + size_t(faces[size_t(j)])] = st[6 * size_t(j) + r];
+  CK(cudaMemcpyAsync(s->sd.bfs, h.data(), 6 * nbf * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return set_bc_impl(s, zone, CGX_BC_CBC_PROFILE, nullptr, 0, true);
+}
+
+static int set_bc_impl(cgx_solver* s, int zone, int kind, const double* params, int nparams, bool profile) {
   if (!s) return fail(CGX_E_ARG, "cgx_set_bc: null solver");
   if (zone < 0 || zone >= s->mesh->nbf_zones)
     return fail(CGX_E_ARG, "cgx_set_bc: zone " + std::to_string(zone) + " not in [0, " +
@@ -4036,6 +4073,10 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
     case CGX_BC_WM_ALG_ADIABATIC: want = (nparams == 0) ? 0 : 3; break;
     case CGX_BC_WM_ALG_ISOTHERMAL: want = 1; break;
     case CGX_BC_WM_ALG_CONDUCTIVE: want = (nparams >= 1 && nparams % 2 == 1) ? nparams : 1; break;
+    case CGX_BC_CBC_PROFILE:
+      if (!profile) return fail(CGX_E_ARG, "cgx_set_bc: CBC_PROFILE zones are set with cgx_set_bc_profile");
+      want = 0;
+      break;
     default: return fail(CGX_E_ARG, "cgx_set_bc: unknown boundary condition");
   }
   if (nparams != want)

@@ -677,7 +677,8 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
           rhs[icv].rhou[i] -= o->p[icv] * n[i] + visc_coeff * (o->u[3 * size_t(icv) + i] - 0.0);
         rhs[icv].rhoE -= q_wall * area_bf;
       } else if (kind == CGX_BC_CBC_UPT || kind == CGX_BC_CBC_RUNP || kind == CGX_BC_CBC_MPT ||
-                 kind == CGX_BC_CBC_RUP || kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT) {
+                 kind == CGX_BC_CBC_RUP || kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT ||
+                 kind == CGX_BC_CBC_PROFILE) {
         IdealGasRhs flux;
         calcRiemannFlux(flux, n, o->cv_light[icv], o->bf_state[ibf], gamma, gamma);
         rhs[icv].rho -= flux.rho;
@@ -1832,4 +1833,26 @@ extern "C" double orc_wm_q_wall(double T1, double Tw, double tau, double rho, do
 }
 extern "C" double orc_wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1) {
   return wm_r_approx(tau, rho, mu, locp, cp, y1);
+}
+
+// CBC_PROFILE (CbcProfile::initData, IdealGasSolverBcs.cpp:3024-3180): the
+// zone's faces, in their order, take the given u[3], sp_vol, p, h.
+extern "C" int orc_set_bc_profile(orc_solver* o, int zone, const double* st, int nz) {
+  if (zone < 0 || zone >= o->nbf_zones) return -1;
+  int n = 0;
+  for (int ibf = 0; ibf < o->nbf; ++ibf) n += (o->zone_bf[ibf] == zone);
+  if (n != nz || (nz > 0 && !st)) return -1;
+  if (zone == o->sp_zone) o->sp_zone = -1;
+  int j = 0;
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    if (o->zone_bf[ibf] != zone) continue;
+    IdealGasState& b = o->bf_state[ibf];
+    for (int i = 0; i < 3; ++i) b.u[i] = st[6 * size_t(j) + i];
+    b.sp_vol = st[6 * size_t(j) + 3];
+    b.p = st[6 * size_t(j) + 4];
+    b.h = st[6 * size_t(j) + 5];
+    ++j;
+  }
+  o->bc[zone] = {double(CGX_BC_CBC_PROFILE), 0.0, 0.0, 0.0, 0.0};
+  return 0;
 }

@@ -91,6 +91,8 @@ int orc_uses_reference_flux(void);
 double orc_wm_solve_tau(double u1, double y1, double rho, double mu, double ut_guess);
 double orc_wm_q_wall(double T1, double Tw, double tau, double rho, double mu, double locp, double cp, double y1);
 double orc_wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1);
+/* CBC_PROFILE: the zone's faces (in face order) take bf_state[nz][6] = u[3], sp_vol, p, h. */
+int orc_set_bc_profile(orc_solver* o, int zone, const double* bf_state, int nz);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,7 @@ def _load(path):
         "orc_wm_solve_tau": (ctypes.c_double, [ctypes.c_double] * 5),
         "orc_wm_q_wall": (ctypes.c_double, [ctypes.c_double] * 8),
         "orc_wm_r_approx": (ctypes.c_double, [ctypes.c_double] * 6),
+        "orc_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -222,6 +223,12 @@ class Oracle:
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
         if self.L.orc_set_bc_params(self.h, int(zone), int(kind), _dp(a) if a.size else None, int(a.size)) != 0:
             raise ValueError("orc_set_bc_params: bad zone, kind or parameters")
+
+    def set_bc_profile(self, zone, states):
+        """CBC_PROFILE: states[nz][6] = u0 u1 u2 sp_vol p h of the zone's faces."""
+        a = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6)
+        if self.L.orc_set_bc_profile(self.h, int(zone), _dp(a), int(a.shape[0])) != 0:
+            raise ValueError("orc_set_bc_profile: bad zone or face count")
 
     def poison(self, icv):
         self.L.orc_poison(self.h, int(icv))

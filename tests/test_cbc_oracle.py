@@ -256,3 +256,75 @@ def test_rup_and_conductive_limits(chan):
     assert np.array_equal(c[rest], e[rest])
     with pytest.raises(ValueError):
         Oracle(m, prm).set_bc_params(0, COND, [1.0, 0.1])  # layers come in pairs
+
+
+PROFILE = 18
+
+
+def _profile(m, prm, zone, u_of_x):
+    """Per-face (u, sp_vol, p, h) of a zone, as CbcProfile::initData builds
+    them from interpolated u, p and T (TYPE UPT)."""
+    R = prm.p_ref / prm.rho_ref / prm.T_ref
+    g = prm.gamma
+    faces = np.flatnonzero(m.zone_bf == zone)
+    xf = m.x_cv[m.cvobf[faces]]
+    st = np.empty((faces.size, 6))
+    for j in range(faces.size):
+        u, p, T = u_of_x(xf[j])
+        st[j, :3] = u
+        st[j, 3] = R * T / p
+        st[j, 4] = p
+        st[j, 5] = R * T * g / (g - 1.0)
+    return st
+
+
+def test_profile_zone(chan):
+    """CBC_PROFILE: a profile that is CBC_UPT's state everywhere gives CBC_UPT's
+    rhs bit for bit; a wrong face count is refused."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.3 + 0.0 * y, 0.02 * np.cos(2 * np.pi * z / m.L[2])], 1)
+    rho, p = np.ones(m.ncv), np.full(m.ncv, prm.p_ref)
+    upt = [0.1, 0.35, 0.0, 1.01 * prm.p_ref, 1.02]
+    out = []
+    for use_profile in (False, True):
+        o = Oracle(m, prm)
+        if use_profile:
+            o.set_bc_profile(0, _profile(m, prm, 0, lambda xf: (upt[:3], upt[3], upt[4])))
+        else:
+            o.set_bc_params(0, UPT, upt)
+        o.set_bc_params(1, RUNP, [1.0, -0.3, prm.p_ref])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        out.append(o.calc_rhs(1)[0])
+        o.close()
+    assert np.array_equal(out[0], out[1])
+    o = Oracle(m, prm)
+    with pytest.raises(ValueError):
+        o.set_bc_profile(0, np.zeros((3, 6)))
+    o.close()
+
+
+@need_ref
+def test_profile_zone_bitwise_equals_reference(chan):
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.3 + 0.0 * y, 0.02 * np.cos(2 * np.pi * z / m.L[2])], 1)
+    rho, p = np.ones(m.ncv), np.full(m.ncv, prm.p_ref)
+    st = _profile(m, prm, 0, lambda xf: ((0.05 * np.cos(xf[2]), 0.4 * (1.0 - ((xf[0] - 1.5) / 1.5) ** 2), 0.0),
+                                          prm.p_ref * (1.0 + 0.01 * xf[0]), 1.0 + 0.02 * xf[2]))
+    out = []
+    for reference in (False, True):
+        o = Oracle(m, prm, reference=reference)
+        o.set_bc_profile(0, st)
+        o.set_bc_params(1, RUNP, [1.0, -0.3, prm.p_ref])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        out.append(o.calc_rhs(1)[0])
+        assert o.step(3) == 0
+        out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+        o.close()
+    assert np.array_equal(out[0], out[2])
+    assert np.array_equal(out[1], out[3])

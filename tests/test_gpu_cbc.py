@@ -289,3 +289,43 @@ def test_sponge_refusals(chan, built):
         s2.set_bc_params(1, SPONGE, good)
     s2.close()
     gm2.close()
+
+
+def test_profile_zone_matches_oracle(chan):
+    """CBC_PROFILE (CbcProfile, IdealGasSolverBcs.cpp:3024-3180): an inflow
+    whose state varies face by face (a parabolic normal speed, p and T
+    varying along the zone) behind a CBC_RUNP outflow; calcRhs to 1e-12 and
+    10 steps to 1e-10 against the oracle.  The kind is refused through
+    cgx_set_bc_params and with a wrong face count."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    R, g = prm.p_ref / prm.rho_ref / prm.T_ref, prm.gamma
+    faces = np.flatnonzero(m.zone_bf == 0)
+    xf = m.x_cv[m.cvobf[faces]]
+    T = 1.0 + 0.02 * xf[:, 2]
+    p = P0 * (1.0 + 0.01 * xf[:, 0])
+    st = np.column_stack([0.05 * np.cos(xf[:, 2]), 0.4 * (1.0 - ((xf[:, 0] - 2.0) / 2.0) ** 2), 0.0 * T,
+                          R * T / p, p, R * T * g / (g - 1.0)])
+    s = cgx.Solver(gm, prm)
+    o = Oracle(m, prm)
+    s.set_bc_profile(0, st)
+    o.set_bc_profile(0, st)
+    for h in (s, o):
+        h.set_bc_params(1, RUNP, (1.0, -0.3, 0.99 * P0))
+    st0 = _state(m, prm)
+    s.set_state_primitive(*st0)
+    s.initComplete()
+    o.set_state_primitive(*st0)
+    o.init_complete()
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_params(0, cgx.CGX_BC_CBC_PROFILE, ())
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_profile(0, st[:-1])
+    s.close()
+    o.close()
