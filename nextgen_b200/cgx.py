@@ -171,6 +171,8 @@ CGX_BC_WM_ALG_ADIABATIC = 15
 CGX_BC_WM_ALG_ISOTHERMAL = 16
 CGX_BC_WM_ALG_CONDUCTIVE = 17
 CGX_BC_CBC_PROFILE = 18
+CGX_BC_WM_EQ_ADIABATIC = 19
+CGX_BC_WM_EQ_ISOTHERMAL = 20
 
 
 class Source(ctypes.Structure):
@@ -366,7 +368,9 @@ class Solver:
         NSCBC_OUTLET_MDOT (mdot t_relax), CBC_RUP (rho u0 u1 u2 p),
         WALL_CONDUCTIVE (T_end [L k]...), SPONGE (type strength t_relax
         length p_sponge L_max; the mesh needs x_cv), WM_ALG_ADIABATIC
-        ([u_wall]), WM_ALG_ISOTHERMAL (T), WM_ALG_CONDUCTIVE (T_end [L k]...);
+        ([u_wall]), WM_ALG_ISOTHERMAL (T), WM_ALG_CONDUCTIVE (T_end [L k]...),
+        WM_EQ_ADIABATIC ([u_wall [relax y_plus0 tol]]), WM_EQ_ISOTHERMAL (T
+        [relax y_plus0 tol]);
         SLIP and
         WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)

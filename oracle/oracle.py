@@ -64,6 +64,7 @@ def _load(path):
         "orc_wm_q_wall": (ctypes.c_double, [ctypes.c_double] * 8),
         "orc_wm_r_approx": (ctypes.c_double, [ctypes.c_double] * 6),
         "orc_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "orc_wm_eq_solve": (ctypes.c_int, [c_dbl_p] + [ctypes.c_double] * 10),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -87,6 +88,16 @@ def wm_q_wall(T1, Tw, tau, rho, mu, locp, cp, y1, reference=False):
 def wm_r_approx(tau, rho, mu, locp, cp, y1, reference=False):
     """The algebraic wall model's near-wall thermal resistance (compute_R_approx)."""
     return _load(REF_LIB_PATH if reference else LIB_PATH).orc_wm_r_approx(tau, rho, mu, locp, cp, y1)
+
+
+def wm_eq_solve(tau, q, T_w, u1, T1, rho1, y1, mu1, Pr_lam, cp, relax=0.7, y_plus0=1.0, tol=1e-4,
+                reference=False):
+    """The equilibrium wall model (EquilibriumWM::solve_qt with its guesses):
+    returns (status, tau, q, T_w); T_w < 0 asks for the adiabatic form."""
+    a = np.array([tau, q, T_w], dtype=np.float64)
+    rc = _load(REF_LIB_PATH if reference else LIB_PATH).orc_wm_eq_solve(
+        _dp(a), u1, T1, rho1, y1, mu1, Pr_lam, cp, relax, y_plus0, tol)
+    return rc, a[0], a[1], a[2]
 
 
 def _dp(a):

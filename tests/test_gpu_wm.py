@@ -1,8 +1,9 @@
 """The algebraic wall-model zones on the GPU against the oracle, on a channel
 (periodic in x and z, walls at y = 0 and y = Ly): WM_ALG_ADIABATIC with a
-moving wall, WM_ALG_ISOTHERMAL, and WM_ALG_CONDUCTIVE behind two layers
-(WmAdiabatic, WmIsothermal, WmAlgConductive, IdealGasSolverBcs.cpp:996-1478,
-2054-2262, 2411-2595).
+moving wall, WM_ALG_ISOTHERMAL, WM_ALG_CONDUCTIVE behind two layers, and the
+equilibrium WM_EQ_ADIABATIC and WM_EQ_ISOTHERMAL (WmAdiabatic, WmIsothermal,
+WmAlgConductive, IdealGasSolverBcs.cpp:996-1478, 2054-2262, 2411-2595;
+EquilibriumWM.hpp).
 
 * calcRhs after initComplete (the laminar wall stress) within 1e-12 of the
   face-sum scale;
@@ -24,6 +25,8 @@ WM_AD, WM_ISO = cgx.CGX_BC_WM_ALG_ADIABATIC, cgx.CGX_BC_WM_ALG_ISOTHERMAL
 WM_COND = cgx.CGX_BC_WM_ALG_CONDUCTIVE
 ZONES = ((WM_AD, (0.0, 0.0, 0.05)), (WM_ISO, (1.2,)))
 ZONES_COND = ((WM_COND, (1.3, 0.01, 0.5, 0.02, 1.0)), (WM_AD, ()))
+WM_EQ_AD, WM_EQ_ISO = cgx.CGX_BC_WM_EQ_ADIABATIC, cgx.CGX_BC_WM_EQ_ISOTHERMAL
+ZONES_EQ = ((WM_EQ_AD, (0.0, 0.0, 0.05)), (WM_EQ_ISO, (1.2, 0.7, 1.0, 1e-5)))
 
 
 @pytest.fixture(scope="module")
@@ -56,7 +59,8 @@ def _make(m, gm, prm, prec=cgx.CGX_FP64, zones=ZONES):
     return s, o
 
 
-@pytest.mark.parametrize("zones", [ZONES, ZONES_COND], ids=["adiabatic_isothermal", "conductive"])
+@pytest.mark.parametrize("zones", [ZONES, ZONES_COND, ZONES_EQ], ids=["adiabatic_isothermal", "conductive",
+                                                                     "equilibrium"])
 def test_wall_models_match_oracle(chan, zones):
     m, gm = chan
     prm = cases.tgv_params(Re=400.0)
@@ -67,13 +71,17 @@ def test_wall_models_match_oracle(chan, zones):
     assert s.step(10) == 0 and o.step(10) == 0
     for a, b in zip(s.get_state(), o.get_state()):
         assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
-    # a NaN: both restore the stored state with its tau_wall
+    # a NaN in a cell on the zone-0 wall: both restore the stored state with
+    # its tau_wall (the equilibrium isothermal zone 1 keeps its own, so the
+    # NaN stays away from it)
     o.set_dt()
+    icv = int(m.cvobf[m.zone_bf == 0][0])
+    assert icv not in set(m.cvobf[m.zone_bf == 1].tolist())
     bad = [a.copy() for a in s.get_state()]
-    bad[0][5] = np.nan
+    bad[0][icv] = np.nan
     s.set_state(*bad)
     s.updateConservativeAndPrimitiveData()
-    o.poison(5)
+    o.poison(icv)
     assert s.advanceSolution() == -1 and o.advance_solution() == -1
     assert s.step(3) == 0 and o.step(3) == 0
     for a, b in zip(s.get_state(), o.get_state()):
@@ -99,7 +107,8 @@ def test_wall_models_mixed_close_to_fp64(chan):
 def test_wall_model_refusals(chan):
     m, gm = chan
     s = cgx.Solver(gm, cases.tgv_params())
-    for kind, bad in ((WM_AD, (0.1,)), (WM_ISO, ()), (WM_ISO, (1.0, 2.0)), (WM_COND, (1.0, 0.1))):
+    for kind, bad in ((WM_AD, (0.1,)), (WM_ISO, ()), (WM_ISO, (1.0, 2.0)), (WM_COND, (1.0, 0.1)),
+                      (WM_EQ_AD, (0.1,)), (WM_EQ_ISO, (1.0, 0.7))):
         with pytest.raises(cgx.CgxError):
             s.set_bc_params(0, kind, bad)
     s.close()

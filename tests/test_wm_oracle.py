@@ -1,7 +1,8 @@
-"""The algebraic wall-model zones WM_ALG_ADIABATIC, WM_ALG_ISOTHERMAL and
-WM_ALG_CONDUCTIVE in the oracle, on CPU (WmAdiabatic, WmIsothermal,
-WmAlgConductive, IdealGasSolverBcs.cpp:996-1478, 2054-2262, 2411-2595;
-AlgebraicWM.hpp).
+"""The wall-model zones in the oracle, on CPU: the algebraic WM_ALG_ADIABATIC,
+WM_ALG_ISOTHERMAL and WM_ALG_CONDUCTIVE and the equilibrium WM_EQ_ADIABATIC
+and WM_EQ_ISOTHERMAL (WmAdiabatic, WmIsothermal, WmAlgConductive,
+IdealGasSolverBcs.cpp:996-1478, 2054-2262, 2411-2595; AlgebraicWM.hpp,
+EquilibriumWM.hpp).
 
 * The restated law-of-the-wall solve recovers u_tau = 0.123 to 1e-7 at the
   y+ values of the reference's own known-answer test
@@ -10,6 +11,8 @@ AlgebraicWM.hpp).
   reference header's own
   (AlgebraicWM.hpp compiled where it lies) bit for bit over random inputs,
   and so do whole solver runs with wall-model zones.
+* The restated equilibrium solve equals EquilibriumWM::solve_qt bit for bit
+  (status included), and gives the laminar stress in the viscous sublayer.
 * WM_ALG_CONDUCTIVE starts without a heat flux, and behind layers lets in
   less heat than without them.
 * After initComplete the wall stress is the laminar estimate mu |u| / y1, so
@@ -26,7 +29,7 @@ from nextgen_b200 import cases
 from nextgen_b200.meshgen import ChannelMesh
 from oracle import Oracle
 
-WALL, ISO, WM_AD, WM_ISO, WM_COND = 2, 3, 15, 16, 17
+WALL, ISO, WM_AD, WM_ISO, WM_COND, WM_EQ_AD, WM_EQ_ISO = 2, 3, 15, 16, 17, 19, 20
 need_ref = pytest.mark.skipif(not orc_mod.ref_available(), reason="reference-built oracle absent")
 
 KAPPA, B, YSTAR = 0.41, 5.2, 23.3244
@@ -65,6 +68,46 @@ def test_restated_wall_model_bitwise_equals_reference(built):
         assert orc_mod.wm_q_wall(*args) == orc_mod.wm_q_wall(*args, reference=True)
         args = (a, rho, mu, mu / 0.7, 3.5, y1)
         assert orc_mod.wm_r_approx(*args) == orc_mod.wm_r_approx(*args, reference=True)
+
+
+@need_ref
+def test_restated_equilibrium_model_bitwise_equals_reference(built):
+    """EquilibriumWM::solve_qt restated: the same tau_w, q_w, wall
+    temperature as the reference header's own, isothermal and adiabatic,
+    from guesses as the zones pass them (over the inputs where the solve
+    converges: on a diverging one the header's own assert stops the
+    process)."""
+    rng = np.random.default_rng(9)
+    cp, Pr = 3.5, 0.7
+    converged = 0
+    for k in range(120):
+        u1 = float(10.0 ** rng.uniform(-2, 0.5))
+        y1 = float(10.0 ** rng.uniform(-4, -1))
+        rho = float(rng.uniform(0.7, 1.5))
+        mu = float(10.0 ** rng.uniform(-6, -3.5))
+        T1 = float(rng.uniform(0.8, 1.3))
+        tau0 = mu * u1 / y1 * float(rng.uniform(0.3, 3.0))
+        Tw = float(rng.uniform(0.7, 1.6)) if k % 2 else -(T1 + 0.5 * u1 * u1 / cp)
+        q0 = 0.0 if Tw < 0 else mu * cp * (T1 - Tw) / y1
+        a = orc_mod.wm_eq_solve(tau0, q0, Tw, u1, T1, rho, y1, mu, Pr, cp)
+        if a[0] != 0 or not np.isfinite(a[1:]).all():
+            # diverged (a NaN march): the reference header asserts on it
+            continue
+        converged += 1
+        assert a == orc_mod.wm_eq_solve(tau0, q0, Tw, u1, T1, rho, y1, mu, Pr, cp, reference=True)
+        assert a[1] > 0.0
+    assert converged >= 90
+
+
+def test_equilibrium_model_laminar_limit(built):
+    """Deep in the viscous sublayer (y+ about 0.45, little eddy viscosity left by
+    the damping) the adiabatic equilibrium model gives the laminar stress
+    mu u1 / y1 to within the model's own tolerance."""
+    cp, Pr, rho, mu, T1, u1 = 3.5, 0.7, 1.0, 1e-3, 1.0, 0.01
+    y1 = 0.02  # y+ = y1 sqrt(rho mu u1 / y1) / mu, about 0.45
+    rc, tau, q, Tw = orc_mod.wm_eq_solve(mu * u1 / y1, 0.0, -(T1 + 0.5 * u1 * u1 / cp), u1, T1, rho, y1, mu, Pr, cp)
+    assert rc == 0 and q == 0.0 and Tw < 0.0
+    assert abs(tau / (mu * u1 / y1) - 1.0) < 1e-3
 
 
 @pytest.fixture(scope="module")
@@ -151,7 +194,8 @@ def test_conductive_wall_model(chan):
 def test_wall_model_refusals(chan):
     o = Oracle(chan, cases.tgv_params())
     for kind, bad in ((WM_AD, [0.1]), (WM_AD, [0.1, 0.2]), (WM_ISO, []), (WM_ISO, [1.0, 2.0]), (WM_COND, []),
-                      (WM_COND, [1.0, 0.1])):
+                      (WM_COND, [1.0, 0.1]), (WM_EQ_AD, [0.1]), (WM_EQ_AD, [0.0] * 4), (WM_EQ_ISO, []),
+                      (WM_EQ_ISO, [1.0, 0.7])):
         with pytest.raises(ValueError):
             o.set_bc_params(0, kind, bad)
     o.close()
@@ -177,6 +221,14 @@ def test_wall_model_solver_bitwise_equals_reference(chan):
         out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
         o.close()
         o = Oracle(m, prm, reference=reference)
+        o.set_bc_params(0, WM_EQ_AD, [0.0, 0.0, 0.05])
+        o.set_bc_params(1, WM_EQ_ISO, [1.2, 0.7, 1.0, 1e-5])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        assert o.step(3) == 0
+        out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+        o.close()
+        o = Oracle(m, prm, reference=reference)
         o.set_bc_params(0, WM_COND, [1.3, 0.01, 0.5])
         o.set_bc_params(1, WM_ISO, [0.9])
         o.set_state_primitive(rho, u, p)
@@ -185,6 +237,7 @@ def test_wall_model_solver_bitwise_equals_reference(chan):
         out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
         out.append(o.calc_rhs(1)[0])
         o.close()
-    assert np.array_equal(out[0], out[3])
-    assert np.array_equal(out[1], out[4])
-    assert np.array_equal(out[2], out[5])
+    assert np.array_equal(out[0], out[4])
+    assert np.array_equal(out[1], out[5])
+    assert np.array_equal(out[2], out[6])
+    assert np.array_equal(out[3], out[7])
