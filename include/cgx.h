@@ -373,6 +373,13 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *     reference has no bound; a face that needs more is degenerate). */
 #define CGX_BC_WM_EQ_ADIABATIC   19
 #define CGX_BC_WM_EQ_ISOTHERMAL  20
+/*   CGX_BC_HOOK  (no parameters)  HOOK (initHookBc, IdealGasSolver.hpp:221,
+ *     251): a zone whose condition is the caller's own code.  Its faces add
+ *     nothing on the device; the caller's addBoundaryFlux (and calcRhs,
+ *     rk3Step) run in the host hook of cgx_set_source_hook, which adds to the
+ *     stage's rhs of the zone's cells.  Transport scalars are refused with
+ *     it, as with the CBC zones. */
+#define CGX_BC_HOOK              21
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* A CBC_PROFILE zone from the boundary states of its faces: bf_state

@@ -173,6 +173,7 @@ CGX_BC_WM_ALG_CONDUCTIVE = 17
 CGX_BC_CBC_PROFILE = 18
 CGX_BC_WM_EQ_ADIABATIC = 19
 CGX_BC_WM_EQ_ISOTHERMAL = 20
+CGX_BC_HOOK = 21
 
 
 class Source(ctypes.Structure):
@@ -370,7 +371,8 @@ class Solver:
         length p_sponge L_max; the mesh needs x_cv), WM_ALG_ADIABATIC
         ([u_wall]), WM_ALG_ISOTHERMAL (T), WM_ALG_CONDUCTIVE (T_end [L k]...),
         WM_EQ_ADIABATIC ([u_wall [relax y_plus0 tol]]), WM_EQ_ISOTHERMAL (T
-        [relax y_plus0 tol]);
+        [relax y_plus0 tol]), HOOK (none: the flux comes from the source
+        hook);
         SLIP and
         WALL_ADIABATIC as set_bc."""
         a = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)

@@ -1179,6 +1179,9 @@ __host__ __device__ inline bool bc_is_cbc(int k) {
          k == CGX_BC_CBC_EXTRAPOLATE || k == CGX_BC_CBC_TOTAL_PT || k == CGX_BC_SPONGE || k == CGX_BC_CBC_PROFILE ||
          bc_is_nscbc(k);
 }
+// zones whose scalar boundary flux is not built (the CBC zones' upwinded
+// scalar flux, a hook zone's own): transport scalars are refused with them
+__host__ __device__ inline bool bc_no_scalars(int k) { return bc_is_cbc(k) || k == CGX_BC_HOOK; }
 
 // A state as the boundary Riemann flux reads it (the reference's
 // IdealGasState: velocity, specific volume, pressure, enthalpy)
@@ -1338,6 +1341,8 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d] + ((um > 0.0) ? tau * u[d] / um * area : 0.0);
       fr[4] -= qw * area;
+    } else if (kind == CGX_BC_HOOK) {
+      // nothing here: the caller's hook adds the zone's flux on the host
     } else if (kind == CGX_BC_WALL_CONDUCTIVE) {
       // the wall's heat flux through the cell's half and the layers
       const double cp = c.ph.R * gamma / (gamma - 1.0);
@@ -3881,8 +3886,8 @@ extern "C" int cgx_set_scalars(cgx_solver* s, int nsc, const double* sc) {
   if (nsc > 0 && !sc) return fail(CGX_E_ARG, "cgx_set_scalars: null scalars");
   if (nsc > 0)
     for (const BcZone& z : s->bc)
-      if (bc_is_cbc(z.kind))
-        return fail(CGX_E_STATE, "cgx_set_scalars: CBC boundary zones carry no transport scalars");
+      if (bc_no_scalars(z.kind))
+        return fail(CGX_E_STATE, "cgx_set_scalars: CBC and HOOK boundary zones carry no transport scalars");
   CK(cudaSetDevice(s->mesh->device));
   CK(cudaStreamSynchronize(s->stream));
   const size_t N = size_t(s->mesh->N);
@@ -4140,7 +4145,7 @@ extern "C" int cgx_set_bc_profile(cgx_solver* s, int zone, const double* st, int
   if (nbf_zone != int(faces.size()) || (nbf_zone > 0 && !st))
     return fail(CGX_E_ARG, "cgx_set_bc_profile: zone " + std::to_string(zone) + " has " +
                                std::to_string(faces.size()) + " faces, got " + std::to_string(nbf_zone));
-  if (s->sd.nsc > 0) return fail(CGX_E_STATE, "cgx_set_bc: CBC boundary zones carry no transport scalars");
+  if (s->sd.nsc > 0) return fail(CGX_E_STATE, "cgx_set_bc: CBC and HOOK boundary zones carry no transport scalars");
   for (int j = 0; j < 6 * nbf_zone; ++j)
     if (!std::isfinite(st[j])) return fail(CGX_E_ARG, "cgx_set_bc_profile: a boundary state is not finite");
   const size_t nbf = size_t(s->mesh->md.nbf);
@@ -4182,6 +4187,7 @@ static int set_bc_impl(cgx_solver* s, int zone, int kind, const double* params, 
     case CGX_BC_WM_ALG_ISOTHERMAL: want = 1; break;
     case CGX_BC_WM_ALG_CONDUCTIVE: want = (nparams >= 1 && nparams % 2 == 1) ? nparams : 1; break;
     case CGX_BC_WM_EQ_ADIABATIC: want = (nparams == 0 || nparams == 3) ? nparams : 6; break;
+    case CGX_BC_HOOK: want = 0; break;
     case CGX_BC_WM_EQ_ISOTHERMAL: want = (nparams == 1) ? 1 : 4; break;
     case CGX_BC_CBC_PROFILE:
       if (!profile) return fail(CGX_E_ARG, "cgx_set_bc: CBC_PROFILE zones are set with cgx_set_bc_profile");
@@ -4192,8 +4198,8 @@ static int set_bc_impl(cgx_solver* s, int zone, int kind, const double* params, 
   if (nparams != want)
     return fail(CGX_E_ARG, "cgx_set_bc: kind " + std::to_string(kind) + " takes " + std::to_string(want) +
                                " parameters, got " + std::to_string(nparams));
-  if (bc_is_cbc(kind) && s->sd.nsc > 0)
-    return fail(CGX_E_STATE, "cgx_set_bc: CBC boundary zones carry no transport scalars");
+  if (bc_no_scalars(kind) && s->sd.nsc > 0)
+    return fail(CGX_E_STATE, "cgx_set_bc: CBC and HOOK boundary zones carry no transport scalars");
   const double R = s->ph.R, gamma = s->ph.gamma;
   BcZone z{};
   z.kind = kind;
@@ -4328,9 +4334,9 @@ static int init_complete(cgx_solver* s, bool tune) {
     if (kind == 0)
       return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
                                    " has no boundary condition (cgx_set_bc)");
-    if (bc_is_cbc(kind) && s->sd.nsc > 0)
+    if (bc_no_scalars(kind) && s->sd.nsc > 0)
       return fail(CGX_E_STATE, "cgx_init_complete: boundary zone " + std::to_string(z) +
-                                   " is a CBC zone and the solver has transport scalars");
+                                   " is a CBC or HOOK zone and the solver has transport scalars");
   }
   int rc = cgx_update_primitive(s);
   if (rc) return rc;

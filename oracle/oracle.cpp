@@ -730,6 +730,8 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
           for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= o->p[icv] * n[i];
         }
         rhs[icv].rhoE -= o->wm_q[ibf] * area;
+      } else if (kind == CGX_BC_HOOK) {
+        // a hook zone: its flux is the caller's (a source term here)
       } else if (kind == CGX_BC_SPONGE) {
         // Sponge::addBoundaryFlux (IdealGasSolverBcs.cpp:4166-4194): the
         // face's state from its cell's sponge state at the sponge pressure
@@ -1825,6 +1827,11 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
   if (kind == CGX_BC_WM_ALG_ADIABATIC) {  // [TRANSLATE u]
     if ((np != 0 && np != 3) || (np > 0 && !prm)) return -1;
     o->bc[zone] = {double(kind), np ? prm[0] : 0.0, np ? prm[1] : 0.0, np ? prm[2] : 0.0, 0.0};
+    return 0;
+  }
+  if (kind == CGX_BC_HOOK) {
+    if (np != 0) return -1;
+    o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, 0.0};
     return 0;
   }
   if (kind == CGX_BC_WM_EQ_ADIABATIC) {  // [u_wall [relax y_plus0 tol]]

@@ -328,3 +328,30 @@ def test_profile_zone_bitwise_equals_reference(chan):
         o.close()
     assert np.array_equal(out[0], out[2])
     assert np.array_equal(out[1], out[3])
+
+
+def test_hook_zone_adds_nothing(chan):
+    """A HOOK zone adds no flux of its own: with SlipWallBc's -p n_bf given as
+    a source on the zone's cells it is the SLIP zone."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.02 * np.cos(2 * np.pi * z / m.L[2]), 0.0 * y], 1)
+    rho = 1.0 + 0.01 * np.cos(2 * np.pi * x / m.L[0])
+    p = np.full(m.ncv, prm.p_ref) * (1.0 + 0.01 * np.sin(2 * np.pi * z / m.L[2]))
+    faces = np.flatnonzero(m.zone_bf == 0)
+    field = np.zeros((m.ncv, 5))
+    np.subtract.at(field[:, 1:4], m.cvobf[faces], p[m.cvobf[faces], None] * m.n_bf[faces])
+    out = []
+    for hook in (True, False):
+        o = Oracle(m, prm)
+        o.set_bc_params(0, 21 if hook else 1, [])
+        o.set_bc_params(1, 1, [])
+        if hook:
+            o.set_source(field=field)
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        out.append(o.calc_rhs(1))
+        o.close()
+    (a, sa), (b, _) = out
+    assert (np.abs(a - b) / np.maximum(np.abs(b), sa)).max() <= 1e-13

@@ -329,3 +329,41 @@ def test_profile_zone_matches_oracle(chan):
         s.set_bc_profile(0, st[:-1])
     s.close()
     o.close()
+
+
+def test_hook_zone_through_the_source_hook(chan):
+    """HOOK (initHookBc): a zone whose flux is the caller's own code, added by
+    the host hook of cgx_set_source_hook.  A hook that adds SlipWallBc's
+    -p n_bf (IdealGasSolverBcs.cpp:14-23) to the zone's cells reproduces a
+    SLIP zone: calcRhs within 1e-12 and 5 steps within 1e-10.  Transport
+    scalars are refused with the hook zone."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    g = prm.gamma
+    faces = np.flatnonzero(m.zone_bf == 0)
+    cells, nb = m.cvobf[faces], m.n_bf[faces]
+
+    def slip(rho, u, rhoE, rhs, time, stage):
+        p = (g - 1.0) * (rhoE - 0.5 * rho * (u * u).sum(1))
+        np.subtract.at(rhs[:, 1:4], cells, p[cells, None] * nb)
+
+    st = _state(m, prm)
+    out = []
+    for hook in (True, False):
+        s = cgx.Solver(gm, prm)
+        s.set_bc_params(0, cgx.CGX_BC_HOOK if hook else cgx.CGX_BC_SLIP, ())
+        s.set_bc_params(1, cgx.CGX_BC_SLIP, ())
+        if hook:
+            s.set_source_hook(slip)
+        s.set_state_primitive(*st)
+        s.initComplete()
+        out.append(s.calcRhs(1))
+        assert s.step(5) == 0
+        out.append(np.concatenate([a.reshape(m.ncv, -1) for a in s.get_state()], 1))
+        if hook:
+            with pytest.raises(cgx.CgxError):
+                s.set_scalars(np.zeros((m.ncv, 1)))
+        s.close()
+    scale = np.abs(out[2]).max(0)
+    assert (np.abs(out[0] - out[2]) / scale).max() <= 1e-12
+    assert np.abs(out[1] - out[3]).max() / np.abs(out[3]).max() <= 1e-10
