@@ -367,3 +367,25 @@ def test_hook_zone_through_the_source_hook(chan):
     scale = np.abs(out[2]).max(0)
     assert (np.abs(out[0] - out[2]) / scale).max() <= 1e-12
     assert np.abs(out[1] - out[3]).max() / np.abs(out[3]).max() <= 1e-10
+
+
+@pytest.mark.parametrize("zones", [
+    ((NSCBC_MT, (2.4, 1.0)), (NSCBC_OUT, (P0, 0.25, 3.0))),
+    ((RUP, (1.0, 0.1, 0.4, 0.0, 1.01 * P0)), (COND, (1.1, 0.01, 0.5, 0.02, 1.0))),
+    ((UPT, (0.1, 0.4, 0.0, 1.01 * P0, 1.02)), (SPONGE, (1, 3.0, 0.05, 1.5, 1.01 * P0, 3.0))),
+], ids=["nscbc", "rup_conductive", "sponge"])
+def test_zone_kinds_mixed_close_to_fp64(chan, zones):
+    """The mixed-precision form with the zones that keep their own state (the
+    NSCBC faces, the sponge state) and the other flux forms: 10 steps within
+    the form's flux tolerance of the FP64 path."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    res = {}
+    for prec in (cgx.CGX_FP64, cgx.CGX_MIXED):
+        s, o = _make(m, gm, prm, zones, prec)
+        o.close()
+        assert s.step(10) == 0
+        res[prec] = s.get_state()
+        s.close()
+    for a64, a32 in zip(res[cgx.CGX_FP64], res[cgx.CGX_MIXED]):
+        assert np.sqrt(((a32 - a64) ** 2).mean() / (a64 ** 2).mean()) <= 1e-5
