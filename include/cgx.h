@@ -231,6 +231,17 @@ typedef void (*cgx_source_hook)(void* user, int ncv, const double* rho, const do
 int cgx_set_source_hook(cgx_solver* s, cgx_source_hook fn, void* user);
 
 /*
+ * cgx_set_frame_rotation: ROTATING_REFERENCE_FRAME wx wy wz (revolutions per
+ * unit time; IdealGasSolver.hpp:126-142 turns them into radians, as here).
+ * Each stage's rhs then takes addRotationSourceTerms (IdealGasSolver.cpp:
+ * 695-733), after the source terms: the centrifugal -rho vol w x (w x x_cv)
+ * and the Coriolis -2 rho vol w x u into rhs.rhou, and their dot product
+ * with u into rhs.rhoE.  x_cv[ncv][3] are the cell centroids in reference
+ * order.  A zero rate removes it.
+ */
+int cgx_set_frame_rotation(cgx_solver* s, const double rev_per_time[3], const double* x_cv);
+
+/*
  * Boundary conditions of a mesh's boundary zones (registerBoundaryConditions,
  * IdealGasSolver.hpp:170-231).  Their fluxes enter each stage's rhs as
  * addBoundaryFlux does (IdealGasSolver.cpp:261-262) and their faces enter

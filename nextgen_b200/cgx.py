@@ -150,7 +150,7 @@ EXPORTS = [
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
     "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params", "cgx_set_host_threads",
-    "cgx_set_bc_profile",
+    "cgx_set_bc_profile", "cgx_set_frame_rotation",
 ]
 
 CGX_BC_SLIP = 1
@@ -232,6 +232,7 @@ def lib():
         "cgx_set_bc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p]),
         "cgx_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "cgx_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p]),
         "cgx_set_host_threads": (ctypes.c_int, [ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
@@ -384,6 +385,13 @@ class Solver:
         bf_state after CbcProfile::initData)."""
         a = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6)
         _check(lib().cgx_set_bc_profile(self.h, int(zone), _dp(a), int(a.shape[0])))
+
+    def set_frame_rotation(self, rev, x_cv):
+        """ROTATING_REFERENCE_FRAME: rev[3] in revolutions per unit time, the
+        cell centroids x_cv[ncv][3] in reference order; zeros remove it."""
+        r = np.ascontiguousarray(rev, dtype=np.float64).reshape(3)
+        x = np.ascontiguousarray(np.asarray(x_cv)[: self.ncv], dtype=np.float64).reshape(self.ncv, 3)
+        _check(lib().cgx_set_frame_rotation(self.h, _dp(r), _dp(x)))
 
     # -- source terms (addSourceHook) ----------------------------------------
     def set_source(self, A=0.0, g=(0.0, 0.0, 0.0), field=None):

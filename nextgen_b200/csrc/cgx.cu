@@ -1995,6 +1995,41 @@ __global__ void k_source(int N, double* __restrict__ rhs, StateDev s, const doub
     for (int c = 0; c < 5; ++c) rhs[c * n + i] += field[c * n + i];
 }
 
+// addRotationSourceTerms (IdealGasSolver.cpp:695-733), one thread per cell:
+// msource = -rho vol (w x (w x x) + 2 w x u) into rhs.rhou, msource.u into
+// rhs.rhoE.
+__global__ void k_rotation(int N, double* __restrict__ rhs, StateDev s, const double* __restrict__ vol,
+                           const double* __restrict__ xcv, double w0, double w1, double w2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const size_t n = size_t(N);
+  const double x[3] = {xcv[i], xcv[n + i], xcv[2 * n + i]};
+  const double u[3] = {s.u0[i], s.u1[i], s.u2[i]};
+  const double rv = s.rho[i] * vol[i];
+  // w x x, then the centrifugal -rho vol w x (w x x)
+  const double a0 = w1 * x[2] - w2 * x[1], a1 = w2 * x[0] - w0 * x[2], a2 = w0 * x[1] - w1 * x[0];
+  double m0 = -rv * (w1 * a2 - w2 * a1);
+  double m1 = -rv * (w2 * a0 - w0 * a2);
+  double m2 = -rv * (w0 * a1 - w1 * a0);
+  // the Coriolis -2 rho vol w x u
+  m0 -= 2.0 * rv * (w1 * u[2] - w2 * u[1]);
+  m1 -= 2.0 * rv * (w2 * u[0] - w0 * u[2]);
+  m2 -= 2.0 * rv * (w0 * u[1] - w1 * u[0]);
+  rhs[n + i] += m0;
+  rhs[2 * n + i] += m1;
+  rhs[3 * n + i] += m2;
+  rhs[4 * n + i] += m0 * u[0] + m1 * u[1] + m2 * u[2];
+}
+
+// [ncv][3] reference order -> [3][N] cell order
+__global__ void k_vec3_in(int N, const int* __restrict__ perm, const double* __restrict__ src,
+                          double* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int o = perm[i];
+  for (int c = 0; c < 3; ++c) dst[size_t(c) * N + i] = src[3 * size_t(o) + c];
+}
+
 // a host hook's source [ncv][5] (reference order, in the staging buffer)
 // added to one stage's rhs
 __global__ void k_source_ref(int N, const int* __restrict__ perm, const double* __restrict__ src,
@@ -2234,8 +2269,13 @@ struct SourceCfg {
     bool explicit_time;
     double time;
   } ctx[4] = {};
+  // ROTATING_REFERENCE_FRAME: the rate in radians per unit time and the
+  // cell centroids [3][N] in cell order
+  bool rot = false;
+  double om[3] = {0.0, 0.0, 0.0};
+  double* xcv = nullptr;
   bool device_form() const { return force || field; }
-  bool any() const { return force || field || fn; }
+  bool any() const { return force || field || fn || rot; }
 };
 
 // What a launch needs: the case table and work list on the device, the grid,
@@ -2593,6 +2633,11 @@ int enqueue_source(const Runner& R, int stage0, const double* time) {
     k_source_ref<<<(N + 255) / 256, 256, 0, R.stream>>>(N, c->perm, c->d_stage, rhs);
     if ((rc = launch_check(R, 1))) return rc;
   }
+  if (c->rot) {  // addRotationSourceTerms, after addSourceHook (IdealGasSolver.hpp:702-703)
+    k_rotation<<<(N + 255) / 256, 256, 0, R.stream>>>(N, rhs, s, R.dcase.m.vol, c->xcv, c->om[0], c->om[1],
+                                                       c->om[2]);
+    if ((rc = launch_check(R, 1))) return rc;
+  }
   return CGX_OK;
 }
 
@@ -2686,7 +2731,7 @@ inline int launches_per_step(const Runner& R) {
            : (R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & 32)) ? 1 : 0) +
           ((R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & 8)) ? 4 : 0) +
           ((R.direct && (R.dcase.s.bc_dyn & 16)) ? (R.dcase.s.nsp > 0 ? 4 : 1) : 0);
-  if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0));
+  if (R.src) n += 3 * ((R.src->device_form() ? 1 : 0) + (R.src->fn ? 2 : 0) + (R.src->rot ? 1 : 0));
   return n;
 }
 
@@ -3975,6 +4020,35 @@ static void drop_graphs(cgx_solver* s) {
     cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
   }
+}
+
+extern "C" int cgx_set_frame_rotation(cgx_solver* s, const double rev[3], const double* x_cv) {
+  if (!s || !rev) return fail(CGX_E_ARG, "cgx_set_frame_rotation: null argument");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(rev[k])) return fail(CGX_E_ARG, "cgx_set_frame_rotation: the rate must be finite");
+  SourceCfg& c = s->src;
+  const bool on = rev[0] != 0.0 || rev[1] != 0.0 || rev[2] != 0.0;
+  if (on && !x_cv) return fail(CGX_E_ARG, "cgx_set_frame_rotation: the cell centroids are needed");
+  CK(cudaSetDevice(s->mesh->device));
+  CK(cudaStreamSynchronize(s->stream));
+  const size_t N = size_t(s->mesh->N);
+  if (on) {
+    if (!c.xcv) {
+      int rc = dalloc(&c.xcv, 3 * N, &s->bytes);
+      if (rc) return rc;
+      s->allocs.push_back(c.xcv);
+    }
+    int rc = host_to_device(s, s->d_stage, x_cv, 3 * N * sizeof(double));
+    if (rc) return rc;
+    k_vec3_in<<<int((N + 255) / 256), 256, 0, s->stream>>>(int(N), s->mesh->d_perm, s->d_stage, c.xcv);
+    if ((rc = launch_check(s->run, 1))) return rc;
+  }
+  // IdealGasSolver.hpp:141: revolutions to radians per unit time
+  for (int k = 0; k < 3; ++k) c.om[k] = rev[k] * (2.0 * M_PI);
+  c.rot = on;
+  drop_graphs(s);
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
 }
 
 extern "C" int cgx_set_source(cgx_solver* s, const cgx_source* src) {

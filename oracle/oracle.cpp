@@ -160,6 +160,8 @@ struct orc_solver {
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
   std::vector<double> src_field;  // [ncv][5] or empty
+  double frame_rotation[3] = {0.0, 0.0, 0.0};  // ROTATING_REFERENCE_FRAME, radians per unit time
+  bool rotating = false;
   // time
   int step = 0;
   double time = 0.0, dt = 0.0;
@@ -623,6 +625,30 @@ void add_source(orc_solver* o, IdealGasRhs* rhs) {
       for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] += f[1 + i];
       rhs[icv].rhoE += f[4];
     }
+}
+
+// addRotationSourceTerms (IdealGasSolver.cpp:695-733): the centrifugal and
+// Coriolis forces of the rotating frame into rhou, their work into rhoE
+void add_rotation(orc_solver* o, IdealGasRhs* rhs) {
+  if (!o->rotating) return;
+  const double* w = o->frame_rotation;
+  for (int icv = 0; icv < o->ncv; ++icv) {
+    const double* x = &o->x_cv[3 * size_t(icv)];
+    const double* u = &o->u[3 * size_t(icv)];
+    double coeff[3];
+    coeff[0] = w[1] * x[2] - w[2] * x[1];
+    coeff[1] = w[2] * x[0] - w[0] * x[2];
+    coeff[2] = w[0] * x[1] - w[1] * x[0];
+    double msource[3];
+    msource[0] = -o->rho[icv] * o->vol_cv[icv] * (w[1] * coeff[2] - w[2] * coeff[1]);
+    msource[1] = -o->rho[icv] * o->vol_cv[icv] * (w[2] * coeff[0] - w[0] * coeff[2]);
+    msource[2] = -o->rho[icv] * o->vol_cv[icv] * (w[0] * coeff[1] - w[1] * coeff[0]);
+    msource[0] -= 2.0 * o->rho[icv] * o->vol_cv[icv] * (w[1] * u[2] - w[2] * u[1]);
+    msource[1] -= 2.0 * o->rho[icv] * o->vol_cv[icv] * (w[2] * u[0] - w[0] * u[2]);
+    msource[2] -= 2.0 * o->rho[icv] * o->vol_cv[icv] * (w[0] * u[1] - w[1] * u[0]);
+    for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] += msource[i];
+    rhs[icv].rhoE += msource[0] * u[0] + msource[1] * u[1] + msource[2] * u[2];
+  }
 }
 
 // The sponge layer's volume term (Sponge::addBoundaryFlux,
@@ -1136,6 +1162,7 @@ void calc_rhs(orc_solver* o, IdealGasRhs* rhs, double* rhs_sc = nullptr) {
     }
   }
   add_source(o, rhs);
+  add_rotation(o, rhs);
 }
 
 // computeSgsVreman (IdealGasSolverSgs.cpp:207-296) over [b, e)
@@ -1465,8 +1492,8 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->ns_u.assign(3 * size_t(m->nbf), 0.0);
     o->ns_rhs.assign(15 * size_t(m->nbf), 0.0);
     o->un_bc_avg.assign(std::max(m->nbf_zones, 1), 0.0);
-    if (m->x_cv) o->x_cv.assign(m->x_cv, m->x_cv + 3 * size_t(ncv));
   }
+  if (m->x_cv) o->x_cv.assign(m->x_cv, m->x_cv + 3 * size_t(ncv));
   // level-1 ghosts: those reachable through a compact face
   int ncv_g = ncv;
   for (int ifa = 0; ifa < nfa; ++ifa) ncv_g = std::max(ncv_g, m->cvofa[2 * size_t(ifa) + 1] + 1);
@@ -1945,6 +1972,15 @@ extern "C" void orc_set_source(orc_solver* o, double A, const double g[3], const
     o->src_field.assign(field, field + 5 * size_t(o->ncv));
   else
     o->src_field.clear();
+}
+
+// ROTATING_REFERENCE_FRAME in revolutions per unit time (IdealGasSolver.hpp:
+// 126-142); needs the mesh's x_cv
+extern "C" int orc_set_frame_rotation(orc_solver* o, const double rev[3]) {
+  o->rotating = rev[0] != 0.0 || rev[1] != 0.0 || rev[2] != 0.0;
+  if (o->rotating && o->x_cv.size() != 3 * size_t(o->ncv)) return -1;
+  for (int i = 0; i < 3; ++i) o->frame_rotation[i] = rev[i] * (2.0 * M_PI);
+  return 0;
 }
 
 extern "C" void orc_poison(orc_solver* o, int icv) {

@@ -93,6 +93,8 @@ double orc_wm_q_wall(double T1, double Tw, double tau, double rho, double mu, do
 double orc_wm_r_approx(double tau, double rho, double mu, double locp, double cp, double y1);
 /* CBC_PROFILE: the zone's faces (in face order) take bf_state[nz][6] = u[3], sp_vol, p, h. */
 int orc_set_bc_profile(orc_solver* o, int zone, const double* bf_state, int nz);
+/* ROTATING_REFERENCE_FRAME (revolutions per unit time); needs the mesh's x_cv. */
+int orc_set_frame_rotation(orc_solver* o, const double rev[3]);
 /* The equilibrium wall model's solve: tqT = {tau_w, q_w, T_w} in and out. */
 int orc_wm_eq_solve(double* tqT, double u1, double T1, double rho1, double y1, double mu1, double Pr_lam, double cp,
                     double relax, double y_plus0, double tol);

@@ -65,6 +65,7 @@ def _load(path):
         "orc_wm_r_approx": (ctypes.c_double, [ctypes.c_double] * 6),
         "orc_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "orc_wm_eq_solve": (ctypes.c_int, [c_dbl_p] + [ctypes.c_double] * 10),
+        "orc_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -240,6 +241,12 @@ class Oracle:
         a = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6)
         if self.L.orc_set_bc_profile(self.h, int(zone), _dp(a), int(a.shape[0])) != 0:
             raise ValueError("orc_set_bc_profile: bad zone or face count")
+
+    def set_frame_rotation(self, rev):
+        """ROTATING_REFERENCE_FRAME: the rate in revolutions per unit time."""
+        a = np.ascontiguousarray(rev, dtype=np.float64).reshape(3)
+        if self.L.orc_set_frame_rotation(self.h, _dp(a)) != 0:
+            raise ValueError("orc_set_frame_rotation: the mesh's x_cv is needed")
 
     def poison(self, icv):
         self.L.orc_poison(self.h, int(icv))
