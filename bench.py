@@ -7,7 +7,8 @@ one replica per GPU.
 Prints one JSON line (rank 0).  value = whole-job cell-steps/s from CUDA
 events on the solver's stream around K graph-replayed steps (max over ranks);
 e2e = the same metric through the C ABI with host buffers (pinned host state
-copied in and read back every step); roofline = the face-flux kernel pair's
+copied in and read back every step, cgx_set_state + cgx_step_out);
+roofline = the face-flux kernel pair's
 algorithmic bytes per launch over its launch time, timed by CUDA events
 recorded around the two kernels inside the timed steps, against the
 measured HBM copy bandwidth; cpu_baseline = the CPU oracle on the host cores
@@ -405,8 +406,7 @@ def run_cgx(args):
     t0 = time.perf_counter()
     for _ in range(ke):
         s.set_state_ptr(r_h.data_ptr(), u_h.data_ptr(), e_h.data_ptr())
-        s.step(1)
-        s.get_state_ptr(r_h.data_ptr(), u_h.data_ptr(), e_h.data_ptr())
+        s.step_out_ptr(1, r_h.data_ptr(), u_h.data_ptr(), e_h.data_ptr())
     el = time.perf_counter() - t0
     el = dist.max_over_ranks(el)
     e2e = world * N * ke / el
@@ -418,8 +418,7 @@ def run_cgx(args):
     t0 = time.perf_counter()
     for _ in range(ke):
         s.set_state_ptr(r_p.ctypes.data, u_p.ctypes.data, e_p.ctypes.data)
-        s.step(1)
-        s.get_state_ptr(r_p.ctypes.data, u_p.ctypes.data, e_p.ctypes.data)
+        s.step_out_ptr(1, r_p.ctypes.data, u_p.ctypes.data, e_p.ctypes.data)
     el_p = dist.max_over_ranks(time.perf_counter() - t0)
     e2e_pageable = world * N * ke / el_p
 
@@ -458,8 +457,9 @@ def run_cgx(args):
                   "mesh_operators": "gpu (cgx_operators_build)" if args.device_ops else "host generator"},
         "e2e_pageable_host_arrays": {"value": e2e_pageable, "unit": UNIT},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 40 * N, "d2h_bytes_per_step": 40 * N,
-                "steps": ke, "how": "per step: cgx_set_state (pinned host -> device), cgx_step(1), "
-                                    "cgx_get_state (device -> pinned host); host wall clock"},
+                "steps": ke, "how": "per step: cgx_set_state (pinned host -> device), then cgx_step_out(1) "
+                                    "(the step, its new state copied device -> pinned host beside the step's "
+                                    "last gradient and step-end kernels); host wall clock"},
         "gpu_launches": res["fp64"]["launches"],
         "clocks": res["fp64"]["clocks"],
         "roofline": {"bound": "hbm", "kernel": "k_rhs_ext + k_rhs_comp (calcRhsBase)", "achieved": achieved, "peak": peak,

@@ -150,7 +150,7 @@ EXPORTS = [
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
     "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params", "cgx_set_host_threads",
-    "cgx_set_bc_profile", "cgx_set_frame_rotation",
+    "cgx_set_bc_profile", "cgx_set_frame_rotation", "cgx_step_out",
 ]
 
 CGX_BC_SLIP = 1
@@ -233,6 +233,7 @@ def lib():
         "cgx_set_bc_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p]),
+        "cgx_step_out": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]),
         "cgx_set_host_threads": (ctypes.c_int, [ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
@@ -547,6 +548,17 @@ class Solver:
     def get_state_ptr(self, rho_ptr, u_ptr, rhoE_ptr):
         _check(lib().cgx_get_state(self.h, ctypes.cast(rho_ptr, c_dbl_p), ctypes.cast(u_ptr, c_dbl_p),
                                    ctypes.cast(rhoE_ptr, c_dbl_p)))
+
+    def step_out_ptr(self, nsteps, rho_ptr, u_ptr, rhoE_ptr):
+        """cgx_step_out: nsteps, then the state into the host arrays at these
+        addresses (its copy beside the step's last kernels when they are
+        page-locked).  Returns 0, or -1 after a NaN (state restored)."""
+        rc = lib().cgx_step_out(self.h, int(nsteps), ctypes.cast(rho_ptr, c_dbl_p), ctypes.cast(u_ptr, c_dbl_p),
+                                ctypes.cast(rhoE_ptr, c_dbl_p))
+        if rc == -4:
+            return -1
+        _check(rc)
+        return 0
 
     def synchronize(self):
         _check(lib().cgx_synchronize(self.h))

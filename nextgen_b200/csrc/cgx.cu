@@ -2327,6 +2327,11 @@ struct cgx_solver {
   bool inited = false;
   cudaGraphExec_t graph = nullptr;
   cudaGraphExec_t pgraph = nullptr;  // the step with face-kernel timing events (cgx_step_profiled)
+  // the step in two parts for cgx_step_out: up to the last RK update, and the
+  // rest (gradient and step end), with the copy-out stream and its event
+  cudaGraphExec_t hgraph = nullptr, tgraph = nullptr;
+  cudaStream_t ostream = nullptr;
+  cudaEvent_t oev = nullptr;
   cudaEvent_t pev[9] = {};
   std::unique_ptr<cgx_staging::Staging> staging;  // for pageable caller arrays, made on first use
   std::atomic<long long> launches{0};
@@ -2842,9 +2847,11 @@ const double kRkW[3][3] = {{1.0, 0.0, 0.0}, {-0.75, 0.25, 0.0}, {-1.0 / 12.0, -1
 // between it and the compact-closure kernel (marks[3*st+1]) and after the
 // closures (marks[3*st+2]), so that the face kernels can be timed inside the
 // step.
-int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
+// part: 0 the whole step; 1 up to the last stage's RK update; 2 the rest
+// (the last gradient and the step end)
+int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr, int part = 0) {
   int rc;
-  for (int st = 0; st < 3; ++st) {
+  for (int st = 0; st < 3 && part != 2; ++st) {
     if ((rc = enqueue_bc_calc(R, st + 1))) return rc;
     if (marks) {
       // external records: captured into a graph they become event-record nodes
@@ -2864,8 +2871,10 @@ int enqueue_step(const Runner& R, const cudaEvent_t* marks = nullptr) {
     if (st == 0 && (rc = enqueue_zone_keep(R, false))) return rc;
     if (st == 0 && (rc = enqueue_sponge_relax(R, false))) return rc;
     if ((rc = enqueue_prim(R, st + 1, kRkW[st], -1.0, st == 2))) return rc;
+    if (st == 2 && part == 1) return CGX_OK;
     if ((rc = enqueue_grad(R))) return rc;
   }
+  if (part == 2 && (rc = enqueue_grad(R))) return rc;
   return enqueue_step_end(R, 3);
 }
 
@@ -3808,6 +3817,13 @@ extern "C" int cgx_solver_destroy(cgx_solver* s) {
   cudaSetDevice(s->mesh->device);
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->pgraph) cudaGraphExecDestroy(s->pgraph);
+  if (s->hgraph) cudaGraphExecDestroy(s->hgraph);
+  if (s->tgraph) cudaGraphExecDestroy(s->tgraph);
+  if (s->ostream) {
+    cudaStreamSynchronize(s->ostream);
+    cudaStreamDestroy(s->ostream);
+  }
+  if (s->oev) cudaEventDestroy(s->oev);
   for (cudaEvent_t e : s->pev)
     if (e) cudaEventDestroy(e);
   if (s->stream) cudaStreamSynchronize(s->stream);
@@ -4012,6 +4028,11 @@ extern "C" int cgx_get_rhs_sc(cgx_solver* s, int rk_stage, double* rhs_sc) {
 
 // a new source configuration changes what the step graphs hold
 static void drop_graphs(cgx_solver* s) {
+  for (cudaGraphExec_t* g : {&s->hgraph, &s->tgraph})
+    if (*g) {
+      cudaGraphExecDestroy(*g);
+      *g = nullptr;
+    }
   if (s->pgraph) {
     cudaGraphExecDestroy(s->pgraph);
     s->pgraph = nullptr;
@@ -4567,6 +4588,76 @@ static int ensure_graph(cgx_solver* s) {
   ec = cudaGraphInstantiate(&s->graph, g, 0);
   cudaGraphDestroy(g);
   if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec));
+  return CGX_OK;
+}
+
+// one part of the step captured into its own graph (see enqueue_step)
+static int capture_part(cgx_solver* s, int part, cudaGraphExec_t* out) {
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  const long long before = s->launches.load();
+  int rc = enqueue_step(s->run, nullptr, part);
+  cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
+  s->launches = before;
+  if (rc || ec != cudaSuccess) cudaGetLastError();
+  if (rc) {
+    if (ec == cudaSuccess) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+  ec = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (ec != cudaSuccess) return fail(CGX_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec));
+  return CGX_OK;
+}
+
+extern "C" int cgx_step_out(cgx_solver* s, int nsteps, double* rho, double* u, double* rhoE) {
+  if (!s || !rho || !u || !rhoE) return fail(CGX_E_ARG, "cgx_step_out: null argument");
+  if (!s->inited) return fail(CGX_E_STATE, "cgx_init_complete not called");
+  if (nsteps < 1) return fail(CGX_E_ARG, "nsteps < 1");
+  CK(cudaSetDevice(s->mesh->device));
+  int rc;
+  if (nsteps > 1 && (rc = cgx_step(s, nsteps - 1))) {
+    if (rc == CGX_E_NAN) cgx_get_state(s, rho, u, rhoE);
+    return rc == CGX_E_NAN ? fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8") : rc;
+  }
+  if (!page_locked(rho) || !page_locked(u) || !page_locked(rhoE)) {
+    rc = cgx_step(s, 1);
+    if (rc && rc != CGX_E_NAN) return rc;
+    const int rg = cgx_get_state(s, rho, u, rhoE);
+    if (rc) return fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8");
+    return rg;
+  }
+  if (!s->ostream) {
+    if (cudaStreamCreateWithFlags(&s->ostream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->oev, cudaEventDisableTiming) != cudaSuccess)
+      return fail(CGX_E_CUDA, "cgx_step_out: stream or event creation failed");
+  }
+  if (!s->hgraph && (rc = capture_part(s, 1, &s->hgraph))) return rc;
+  if (!s->tgraph && (rc = capture_part(s, 2, &s->tgraph))) return rc;
+  const int N = s->mesh->N;
+  CK(cudaGraphLaunch(s->hgraph, s->stream));
+  CK(cudaEventRecord(s->oev, s->stream));
+  CK(cudaGraphLaunch(s->tgraph, s->stream));
+  s->launches += launches_per_step(s->run);
+  // the new state, gathered to reference order and copied while the
+  // gradient and the step end run (neither writes rho, u, rhoE)
+  CK(cudaStreamWaitEvent(s->ostream, s->oev, 0));
+  k_state_out<<<(N + 255) / 256, 256, 0, s->ostream>>>(N, s->mesh->d_perm, s->d_stage, s->sd);
+  if ((rc = launch_check(s->run, 1))) return rc;
+  CK(cudaMemcpyAsync(rho, s->d_stage, N * sizeof(double), cudaMemcpyDeviceToHost, s->ostream));
+  CK(cudaMemcpyAsync(u, s->d_stage + N, 3 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->ostream));
+  CK(cudaMemcpyAsync(rhoE, s->d_stage + 4 * size_t(N), N * sizeof(double), cudaMemcpyDeviceToHost, s->ostream));
+  CK(cudaStreamSynchronize(s->ostream));
+  Ctl c;
+  if ((rc = read_ctl(s, &c))) return rc;
+  if (c.nan) {
+    if ((rc = restore_state(s))) return rc;
+    if ((rc = cgx_get_state(s, rho, u, rhoE))) return rc;
+    return fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8");
+  }
+  const int ci = std::max(1, s->prm.check_interval);
+  if (c.step % (ci * 20) == 0 && (rc = store_state(s))) return rc;
   return CGX_OK;
 }
 
