@@ -1174,6 +1174,14 @@ __host__ __device__ inline int wm_eq_solve(double& tau_w, double& q_w, double u1
   return 0;
 }
 
+// The wall velocity of an adiabatic wall zone's face: the zone's own
+// (TRANSLATE), or the face's (flag 1 in BcZone::pad, rows 0-2 of bfs, set by
+// cgx_set_bc_wall_velocity)
+__device__ __forceinline__ void wall_velocity(const StateDev& s, const BcZone& z, int f, int nbf, double ub[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ub[d] = (z.pad & 1) ? s.bfs[size_t(d) * nbf + f] : z.a[d];
+}
+
 __host__ __device__ inline bool bc_is_cbc(int k) {
   return k == CGX_BC_CBC_UPT || k == CGX_BC_CBC_RUNP || k == CGX_BC_CBC_MPT || k == CGX_BC_CBC_RUP ||
          k == CGX_BC_CBC_EXTRAPOLATE || k == CGX_BC_CBC_TOTAL_PT || k == CGX_BC_SPONGE || k == CGX_BC_CBC_PROFILE ||
@@ -1288,12 +1296,14 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
       for (int d = 0; d < 3; ++d) fr[1 + d] -= p * n[d];
     } else if (kind == CGX_BC_WALL_ADIABATIC) {
       const double visc = mu_lam * m.bf_aod[f];
+      double ub[3];
+      wall_velocity(s, z, f, m.nbf, ub);
       double work = 0.0;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const double tau = visc * (u[d] - z.a[d]);
+        const double tau = visc * (u[d] - ub[d]);
         fr[1 + d] -= p * n[d] + tau;
-        work += z.a[d] * tau;
+        work += ub[d] * tau;
       }
       fr[4] -= work;
     } else if (kind == CGX_BC_WALL_ISOTHERMAL) {
@@ -1313,9 +1323,10 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
         for (int d = 0; d < 3; ++d) nh[d] = n[d] / area;
       }
       const double un = u[0] * nh[0] + u[1] * nh[1] + u[2] * nh[2];
-      double up[3];
+      double ub[3], up[3];
+      wall_velocity(s, z, f, m.nbf, ub);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) up[d] = u[d] - un * nh[d] - z.a[d];
+      for (int d = 0; d < 3; ++d) up[d] = u[d] - un * nh[d] - ub[d];
       const double um = sqrt(up[0] * up[0] + up[1] * up[1] + up[2] * up[2]);
       if (um > 0.0) {
         const double tau = s.nsb[f];
@@ -1324,7 +1335,7 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
         for (int d = 0; d < 3; ++d) {
           const double force = tau * up[d] / um * area;
           fr[1 + d] -= p * n[d] + force;
-          work += force * z.a[d];
+          work += force * ub[d];
         }
         fr[4] -= work;
       } else {
@@ -1643,15 +1654,16 @@ __global__ void __launch_bounds__(128) k_bc_calc(const CaseDev c, int stage) {
       const double mu = s.VF ? double(s.VF[i].mu_lam) : s.V[i].mu_lam;
       double um;
       if (z.kind == CGX_BC_WM_ALG_ADIABATIC || z.kind == CGX_BC_WM_EQ_ADIABATIC) {
-        double up[3];
+        double ub[3], up[3];
+        wall_velocity(s, z, f, nbf, ub);
         if (area > 0.0) {
           const double nh[3] = {n[0] / area, n[1] / area, n[2] / area};
           const double un = u[0] * nh[0] + u[1] * nh[1] + u[2] * nh[2];
 #pragma unroll
-          for (int d = 0; d < 3; ++d) up[d] = u[d] - un * nh[d] - z.a[d];
+          for (int d = 0; d < 3; ++d) up[d] = u[d] - un * nh[d] - ub[d];
         } else {
 #pragma unroll
-          for (int d = 0; d < 3; ++d) up[d] = u[d] - z.a[d];
+          for (int d = 0; d < 3; ++d) up[d] = u[d] - ub[d];
         }
         um = sqrt(up[0] * up[0] + up[1] * up[1] + up[2] * up[2]);
       } else {
@@ -1783,7 +1795,9 @@ __global__ void __launch_bounds__(128) k_bc_stage(const CaseDev c, int stage, in
         const double y1 = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) / aod;
         const double mu = s.VF ? double(s.VF[i].mu_lam) : s.V[i].mu_lam;
         if (adiabatic) {
-          const double du[3] = {u[0] - z.a[0], u[1] - z.a[1], u[2] - z.a[2]};
+          double ub[3];
+          wall_velocity(s, z, f, m.nbf, ub);
+          const double du[3] = {u[0] - ub[0], u[1] - ub[1], u[2] - ub[2]};
           u1 = sqrt(du[0] * du[0] + du[1] * du[1] + du[2] * du[2]);
           tau = mu * u1 / y1;
         } else if (z.kind == CGX_BC_WM_ALG_ISOTHERMAL || z.kind == CGX_BC_WM_EQ_ISOTHERMAL) {
@@ -4233,25 +4247,47 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
 
 // CbcProfile::initData's result (IdealGasSolverBcs.cpp:3024-3180): the
 // zone's faces take the given states in the per-face boundary-state rows.
-extern "C" int cgx_set_bc_profile(cgx_solver* s, int zone, const double* st, int nbf_zone) {
-  if (!s) return fail(CGX_E_ARG, "cgx_set_bc_profile: null solver");
-  if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_profile: bad zone");
+// rows 0-2 of the per-face boundary-state array for the zone's faces
+static int write_bfs_rows(cgx_solver* s, int zone, const double* v, int width, int nbf_zone) {
   const std::vector<int>& faces = s->mesh->zone_faces[size_t(zone)];
-  if (nbf_zone != int(faces.size()) || (nbf_zone > 0 && !st))
-    return fail(CGX_E_ARG, "cgx_set_bc_profile: zone " + std::to_string(zone) + " has " +
-                               std::to_string(faces.size()) + " faces, got " + std::to_string(nbf_zone));
-  if (s->sd.nsc > 0) return fail(CGX_E_STATE, "cgx_set_bc: CBC and HOOK boundary zones carry no transport scalars");
-  for (int j = 0; j < 6 * nbf_zone; ++j)
-    if (!std::isfinite(st[j])) return fail(CGX_E_ARG, "cgx_set_bc_profile: a boundary state is not finite");
+  if (nbf_zone != int(faces.size()) || (nbf_zone > 0 && !v))
+    return fail(CGX_E_ARG, "zone " + std::to_string(zone) + " has " + std::to_string(faces.size()) +
+                               " faces, got " + std::to_string(nbf_zone));
+  for (int j = 0; j < width * nbf_zone; ++j)
+    if (!std::isfinite(v[j])) return fail(CGX_E_ARG, "a per-face value is not finite");
   const size_t nbf = size_t(s->mesh->md.nbf);
   CK(cudaSetDevice(s->mesh->device));
   std::vector<double> h(6 * nbf);
   CK(cudaMemcpyAsync(h.data(), s->sd.bfs, 6 * nbf * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   for (int j = 0; j < nbf_zone; ++j)
-    for (int r = 0; r < 6; ++r) h[size_t(r) * nbf + size_t(faces[size_t(j)])] = st[6 * size_t(j) + r];
+    for (int r = 0; r < width; ++r) h[size_t(r) * nbf + size_t(faces[size_t(j)])] = v[width * size_t(j) + r];
   CK(cudaMemcpyAsync(s->sd.bfs, h.data(), 6 * nbf * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
+extern "C" int cgx_set_bc_wall_velocity(cgx_solver* s, int zone, const double* u_bf, int nbf_zone) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_bc_wall_velocity: null solver");
+  if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_wall_velocity: bad zone");
+  BcZone& z = s->bc[size_t(zone)];
+  if (z.kind != CGX_BC_WALL_ADIABATIC && z.kind != CGX_BC_WM_ALG_ADIABATIC && z.kind != CGX_BC_WM_EQ_ADIABATIC)
+    return fail(CGX_E_STATE, "cgx_set_bc_wall_velocity: the zone is not an adiabatic wall");
+  int rc = write_bfs_rows(s, zone, u_bf, 3, nbf_zone);
+  if (rc) return rc;
+  z.pad = 1;
+  CK(cudaMemcpyAsync(const_cast<BcZone*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(BcZone),
+                     cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return CGX_OK;
+}
+
+extern "C" int cgx_set_bc_profile(cgx_solver* s, int zone, const double* st, int nbf_zone) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_bc_profile: null solver");
+  if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_profile: bad zone");
+  if (s->sd.nsc > 0) return fail(CGX_E_STATE, "cgx_set_bc: CBC and HOOK boundary zones carry no transport scalars");
+  const int rc = write_bfs_rows(s, zone, st, 6, nbf_zone);
+  if (rc) return rc;
   return set_bc_impl(s, zone, CGX_BC_CBC_PROFILE, nullptr, 0, true);
 }
 

@@ -355,3 +355,36 @@ def test_hook_zone_adds_nothing(chan):
         o.close()
     (a, sa), (b, _) = out
     assert (np.abs(a - b) / np.maximum(np.abs(b), sa)).max() <= 1e-13
+
+
+def test_wall_velocity_per_face(chan):
+    """An adiabatic wall's velocity given face by face (the zone's u_bc after
+    initData): the same velocity on every face is TRANSLATE, bit for bit; a
+    wall-model zone takes it too; the other kinds refuse it."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.02 * np.cos(2 * np.pi * z / m.L[2]), 0.0 * y], 1)
+    rho, p = np.ones(m.ncv), np.full(m.ncv, prm.p_ref)
+    uw = np.array([0.05, 0.0, -0.1])
+    nz = int((m.zone_bf == 0).sum())
+    for kind in (2, 15):
+        out = []
+        for per_face in (False, True):
+            o = Oracle(m, prm)
+            o.set_bc_params(0, kind, [] if per_face else list(uw))
+            if per_face:
+                o.set_bc_wall_velocity(0, np.tile(uw, (nz, 1)))
+            o.set_bc_params(1, 1, [])
+            o.set_state_primitive(rho, u, p)
+            o.init_complete()
+            out.append(o.calc_rhs(1)[0])
+            assert o.step(2) == 0
+            out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+            o.close()
+        assert np.array_equal(out[0], out[2]) and np.array_equal(out[1], out[3])
+    o = Oracle(m, prm)
+    o.set_bc_params(0, 3, [1.0])
+    with pytest.raises(ValueError):
+        o.set_bc_wall_velocity(0, np.zeros((nz, 3)))
+    o.close()
