@@ -436,12 +436,12 @@ int cgx_advance_solution(cgx_solver* s);
  * (IdealGasSolver.hpp:807-811; CGX_E_NAN as above). */
 int cgx_step(cgx_solver* s, int nsteps);
 /* cgx_step, then the state in the caller's host arrays (cgx_get_state's
- * layout), for a host solver that keeps its arrays on the host.  With
- * page-locked arrays the copy of the last step's state starts as soon as its
- * last RK update is done and runs beside the step's remaining kernels (the
- * gradient and the once-per-step properties, which do not change the
- * state); pageable arrays are copied after the step.  On CGX_E_NAN the
- * arrays hold the restored state. */
+ * layout), for a host solver that keeps its arrays on the host.  The copy of
+ * the last step's state starts as soon as its last RK update is done and runs
+ * beside the step's remaining kernels (the gradient and the once-per-step
+ * properties, which do not change the state); pageable arrays go through the
+ * library's pinned chunks on that copy.  On CGX_E_NAN the arrays hold the
+ * restored state. */
 int cgx_step_out(cgx_solver* s, int nsteps, double* rho, double* u, double* rhoE);
 
 /* time, dt of the last completed step (0 before the first) and step count */

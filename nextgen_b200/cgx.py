@@ -559,8 +559,9 @@ class Solver:
 
     def step_out_ptr(self, nsteps, rho_ptr, u_ptr, rhoE_ptr):
         """cgx_step_out: nsteps, then the state into the host arrays at these
-        addresses (its copy beside the step's last kernels when they are
-        page-locked).  Returns 0, or -1 after a NaN (state restored)."""
+        addresses, its copy beside the step's last kernels (pageable arrays
+        through the library's pinned chunks).  Returns 0, or -1 after a NaN
+        (state restored)."""
         rc = lib().cgx_step_out(self.h, int(nsteps), ctypes.cast(rho_ptr, c_dbl_p), ctypes.cast(u_ptr, c_dbl_p),
                                 ctypes.cast(rhoE_ptr, c_dbl_p))
         if rc == -4:

@@ -4657,13 +4657,6 @@ extern "C" int cgx_step_out(cgx_solver* s, int nsteps, double* rho, double* u, d
     if (rc == CGX_E_NAN) cgx_get_state(s, rho, u, rhoE);
     return rc == CGX_E_NAN ? fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8") : rc;
   }
-  if (!page_locked(rho) || !page_locked(u) || !page_locked(rhoE)) {
-    rc = cgx_step(s, 1);
-    if (rc && rc != CGX_E_NAN) return rc;
-    const int rg = cgx_get_state(s, rho, u, rhoE);
-    if (rc) return fail(CGX_E_NAN, "NaN detected; state restored and dt_data[0] scaled by 0.8");
-    return rg;
-  }
   if (!s->ostream) {
     if (cudaStreamCreateWithFlags(&s->ostream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->oev, cudaEventDisableTiming) != cudaSuccess)
@@ -4681,9 +4674,18 @@ extern "C" int cgx_step_out(cgx_solver* s, int nsteps, double* rho, double* u, d
   CK(cudaStreamWaitEvent(s->ostream, s->oev, 0));
   k_state_out<<<(N + 255) / 256, 256, 0, s->ostream>>>(N, s->mesh->d_perm, s->d_stage, s->sd);
   if ((rc = launch_check(s->run, 1))) return rc;
-  CK(cudaMemcpyAsync(rho, s->d_stage, N * sizeof(double), cudaMemcpyDeviceToHost, s->ostream));
-  CK(cudaMemcpyAsync(u, s->d_stage + N, 3 * size_t(N) * sizeof(double), cudaMemcpyDeviceToHost, s->ostream));
-  CK(cudaMemcpyAsync(rhoE, s->d_stage + 4 * size_t(N), N * sizeof(double), cudaMemcpyDeviceToHost, s->ostream));
+  double* dst[3] = {rho, u, rhoE};
+  const size_t off[3] = {0, size_t(N), 4 * size_t(N)}, len[3] = {size_t(N), 3 * size_t(N), size_t(N)};
+  for (int a = 0; a < 3; ++a) {
+    const size_t bytes = len[a] * sizeof(double);
+    if (bytes < (size_t(4) << 20) || page_locked(dst[a])) {
+      CK(cudaMemcpyAsync(dst[a], s->d_stage + off[a], bytes, cudaMemcpyDeviceToHost, s->ostream));
+    } else {  // pageable: through the pinned chunks, on the copy-out stream
+      cgx_staging::Staging* st;
+      if ((rc = staging_of(s, &st))) return rc;
+      CK(st->get(dst[a], s->d_stage + off[a], bytes, s->ostream));
+    }
+  }
   CK(cudaStreamSynchronize(s->ostream));
   Ctl c;
   if ((rc = read_ctl(s, &c))) return rc;

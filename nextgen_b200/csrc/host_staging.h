@@ -67,15 +67,17 @@ class Staging {
     return cudaSuccess;
   }
 
-  // device -> host, complete on return
-  cudaError_t get(void* dst, const void* src, size_t bytes) {
+  // device -> host, complete on return; on `st` instead of the object's
+  // stream when given (the copies then follow st's earlier work)
+  cudaError_t get(void* dst, const void* src, size_t bytes, cudaStream_t st = nullptr) {
+    cudaStream_t q = st ? st : s_;
     const size_t nch = (bytes + kChunk - 1) / kChunk;
     for (size_t c = 0; c < nch; ++c) {
       const size_t off = c * kChunk, len = std::min(kChunk, bytes - off);
       cudaError_t e = cudaMemcpyAsync(pin_[c & 1], static_cast<const char*>(src) + off, len,
-                                      cudaMemcpyDeviceToHost, s_);
+                                      cudaMemcpyDeviceToHost, q);
       if (e != cudaSuccess) return e;
-      e = cudaEventRecord(done_[c & 1], s_);
+      e = cudaEventRecord(done_[c & 1], q);
       if (e != cudaSuccess) return e;
       if (c > 0 && (e = drain(static_cast<char*>(dst), c - 1, bytes)) != cudaSuccess) return e;
     }
