@@ -398,7 +398,7 @@ int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, i
  * the reference's IdealGasState that Cbc::addBoundaryFlux reads), the zone's
  * faces in the order the mesh description lists them.  The reference reads a
  * profile file and interpolates it to the faces in CbcProfile::initData; the
- * caller passes the interpolated states (INTEGRATION shows the forwarding).
+ * caller passes the interpolated states.
  * nbf_zone must be the zone's face count. */
 int cgx_set_bc_profile(cgx_solver* s, int zone, const double* bf_state, int nbf_zone);
 
