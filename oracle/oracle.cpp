@@ -456,7 +456,7 @@ void rhs_part(orc_solver* o, int ip, IdealGasRhs* rhs) {
   // [n_c__i, n_ec_i): internal, with c, extended only
   for (const FRec& r : P.A) {
     FaNC g;
-    FaCompact cg;
+    FaCompact cg{};
     geom_of(o, r, g, cg);
     IdealGasRhs flux;
     double u_avg[3], inv_v_avg, p_avg, h_stag;
@@ -480,7 +480,7 @@ void rhs_part(orc_solver* o, int ip, IdealGasRhs* rhs) {
   // [n_ec_i, n_cc_i): internal, with c, compact
   for (const FRec& r : P.B) {
     FaNC g;
-    FaCompact cg;
+    FaCompact cg{};
     geom_of(o, r, g, cg);
     IdealGasRhs flux;
     double u_avg[3], inv_v_avg, p_avg, h_stag;
@@ -506,7 +506,7 @@ void rhs_part(orc_solver* o, int ip, IdealGasRhs* rhs) {
   // [n_c__b, n_ec_b): boundary, with c, extended only (icv0 only)
   for (const FRec& r : P.C) {
     FaNC g;
-    FaCompact cg;
+    FaCompact cg{};
     geom_of(o, r, g, cg);
     IdealGasRhs flux;
     double u_avg[3], inv_v_avg, p_avg, h_stag;
@@ -528,7 +528,7 @@ void rhs_part(orc_solver* o, int ip, IdealGasRhs* rhs) {
   // [n_ec_b, n_cc_b): boundary, with c, compact (icv0 only)
   for (const FRec& r : P.D) {
     FaNC g;
-    FaCompact cg;
+    FaCompact cg{};
     geom_of(o, r, g, cg);
     IdealGasRhs flux;
     double u_avg[3], inv_v_avg, p_avg, h_stag;
