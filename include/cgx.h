@@ -402,14 +402,19 @@ int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, i
  * nbf_zone must be the zone's face count. */
 int cgx_set_bc_profile(cgx_solver* s, int zone, const double* bf_state, int nbf_zone);
 
-/* The wall velocity face by face for a WALL_ADIABATIC, WM_ALG_ADIABATIC or
- * WM_EQ_ADIABATIC zone: u_bf[nbf_zone][3], the zone's faces in the order the
- * mesh description lists them.  It is the zones' u_bc after their initData
- * (IdealGasSolverBcs.cpp:450-497, 996-1041): TRANSLATE gives every face the
- * same velocity, STATIONARY_FRAME in a rotating frame gives each face
- * -w x x_bf.  Set the zone's kind first (cgx_set_bc_params); setting the
- * kind again returns the zone to its one velocity. */
-int cgx_set_bc_wall_velocity(cgx_solver* s, int zone, const double* u_bf, int nbf_zone);
+/* A velocity face by face, u_bf[nbf_zone][3], the zone's faces in the order
+ * the mesh description lists them:
+ *   WALL_ADIABATIC, WM_ALG_ADIABATIC, WM_EQ_ADIABATIC: the wall's velocity,
+ *     the zones' u_bc after their initData (IdealGasSolverBcs.cpp:450-497,
+ *     996-1041): TRANSLATE gives every face the same velocity,
+ *     STATIONARY_FRAME in a rotating frame gives each face -w x x_bf;
+ *   CBC_TOTAL_PT: the frame velocity u_fr of STATIONARY_FRAME (-w x x_bf,
+ *     CbcTotalPt::initData, :3372-3405), whose part along the face enters
+ *     the boundary state beside the relaxed normal speed (calcBfState,
+ *     :3413-3434).
+ * Set the zone's kind first (cgx_set_bc_params); setting the kind again
+ * returns the zone to its one velocity (or to no frame velocity). */
+int cgx_set_bc_face_velocity(cgx_solver* s, int zone, const double* u_bf, int nbf_zone);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */

@@ -150,7 +150,7 @@ EXPORTS = [
     "cgx_synchronize", "cgx_launch_count", "cgx_last_error", "cgx_step_timed", "cgx_kernel_times", "cgx_get_tuning",
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
     "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params", "cgx_set_host_threads",
-    "cgx_set_bc_profile", "cgx_set_frame_rotation", "cgx_step_out", "cgx_set_bc_wall_velocity",
+    "cgx_set_bc_profile", "cgx_set_frame_rotation", "cgx_step_out", "cgx_set_bc_face_velocity",
 ]
 
 CGX_BC_SLIP = 1
@@ -234,7 +234,7 @@ def lib():
         "cgx_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p]),
         "cgx_step_out": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]),
-        "cgx_set_bc_wall_velocity": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "cgx_set_bc_face_velocity": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "cgx_set_host_threads": (ctypes.c_int, [ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
@@ -388,12 +388,12 @@ class Solver:
         a = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6)
         _check(lib().cgx_set_bc_profile(self.h, int(zone), _dp(a), int(a.shape[0])))
 
-    def set_bc_wall_velocity(self, zone, u):
-        """An adiabatic wall zone's velocity face by face: u[nz][3], the
-        zone's faces in the order the mesh lists them (STATIONARY_FRAME:
-        -w x x_bf)."""
+    def set_bc_face_velocity(self, zone, u):
+        """A velocity face by face, u[nz][3], the zone's faces in the order
+        the mesh lists them: an adiabatic wall's velocity, or CBC_TOTAL_PT's
+        frame velocity (STATIONARY_FRAME: -w x x_bf)."""
         a = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
-        _check(lib().cgx_set_bc_wall_velocity(self.h, int(zone), _dp(a), int(a.shape[0])))
+        _check(lib().cgx_set_bc_face_velocity(self.h, int(zone), _dp(a), int(a.shape[0])))
 
     def set_frame_rotation(self, rev, x_cv):
         """ROTATING_REFERENCE_FRAME: rev[3] in revolutions per unit time, the

@@ -1176,7 +1176,7 @@ __host__ __device__ inline int wm_eq_solve(double& tau_w, double& q_w, double u1
 
 // The wall velocity of an adiabatic wall zone's face: the zone's own
 // (TRANSLATE), or the face's (flag 1 in BcZone::pad, rows 0-2 of bfs, set by
-// cgx_set_bc_wall_velocity)
+// cgx_set_bc_face_velocity)
 __device__ __forceinline__ void wall_velocity(const StateDev& s, const BcZone& z, int f, int nbf, double ub[3]) {
 #pragma unroll
   for (int d = 0; d < 3; ++d) ub[d] = (z.pad & 1) ? s.bfs[size_t(d) * nbf + f] : z.a[d];
@@ -1837,8 +1837,18 @@ __global__ void __launch_bounds__(128) k_bc_stage(const CaseDev c, int stage, in
       const double T_bc = t_tot - 0.5 * un * un / cp;
       const double rho_bc = total_rh * pow(T_bc / t_tot, invgm1);
       const double p_bc = p_tot * pow(T_bc / t_tot, gamma * invgm1);
+      // STATIONARY_FRAME (flag 1): the frame velocity's part along the face
+      // (CbcTotalPt::calcBfState, :3413-3421), from rows 5-7 of nsb
+      double ut[3] = {0.0, 0.0, 0.0};
+      if (z.pad & 1) {
+        const double* fr = s.nsb + 5 * size_t(m.nbf) + f;
+        const double uf[3] = {fr[0], fr[m.nbf], fr[2 * size_t(m.nbf)]};
+        const double ufn = uf[0] * nh[0] + uf[1] * nh[1] + uf[2] * nh[2];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) q[d * m.nbf] = un * nh[d];
+        for (int d = 0; d < 3; ++d) ut[d] = uf[d] - ufn * nh[d];
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) q[d * m.nbf] = un * nh[d] + ut[d];
       q[3 * m.nbf] = 1.0 / rho_bc;
       q[4 * m.nbf] = p_bc;
       q[5 * m.nbf] = cp * T_bc;
@@ -4247,8 +4257,10 @@ extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double
 
 // CbcProfile::initData's result (IdealGasSolverBcs.cpp:3024-3180): the
 // zone's faces take the given states in the per-face boundary-state rows.
-// rows 0-2 of the per-face boundary-state array for the zone's faces
-static int write_bfs_rows(cgx_solver* s, int zone, const double* v, int width, int nbf_zone) {
+// the first `width` rows of a [rows][nbf] per-face device array for the
+// zone's faces (v: [nbf_zone][width])
+static int write_face_rows(cgx_solver* s, int zone, const double* v, int width, int nbf_zone, double* arr,
+                           int rows) {
   const std::vector<int>& faces = s->mesh->zone_faces[size_t(zone)];
   if (nbf_zone != int(faces.size()) || (nbf_zone > 0 && !v))
     return fail(CGX_E_ARG, "zone " + std::to_string(zone) + " has " + std::to_string(faces.size()) +
@@ -4257,23 +4269,33 @@ static int write_bfs_rows(cgx_solver* s, int zone, const double* v, int width, i
     if (!std::isfinite(v[j])) return fail(CGX_E_ARG, "a per-face value is not finite");
   const size_t nbf = size_t(s->mesh->md.nbf);
   CK(cudaSetDevice(s->mesh->device));
-  std::vector<double> h(6 * nbf);
-  CK(cudaMemcpyAsync(h.data(), s->sd.bfs, 6 * nbf * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  std::vector<double> h(size_t(rows) * nbf);
+  CK(cudaMemcpyAsync(h.data(), arr, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   for (int j = 0; j < nbf_zone; ++j)
     for (int r = 0; r < width; ++r) h[size_t(r) * nbf + size_t(faces[size_t(j)])] = v[width * size_t(j) + r];
-  CK(cudaMemcpyAsync(s->sd.bfs, h.data(), 6 * nbf * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(arr, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }
 
-extern "C" int cgx_set_bc_wall_velocity(cgx_solver* s, int zone, const double* u_bf, int nbf_zone) {
-  if (!s) return fail(CGX_E_ARG, "cgx_set_bc_wall_velocity: null solver");
-  if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_wall_velocity: bad zone");
+// rows of the per-face boundary-state array [6][nbf]
+static int write_bfs_rows(cgx_solver* s, int zone, const double* v, int width, int nbf_zone) {
+  return write_face_rows(s, zone, v, width, nbf_zone, s->sd.bfs, 6);
+}
+
+extern "C" int cgx_set_bc_face_velocity(cgx_solver* s, int zone, const double* u_bf, int nbf_zone) {
+  if (!s) return fail(CGX_E_ARG, "cgx_set_bc_face_velocity: null solver");
+  if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_face_velocity: bad zone");
   BcZone& z = s->bc[size_t(zone)];
-  if (z.kind != CGX_BC_WALL_ADIABATIC && z.kind != CGX_BC_WM_ALG_ADIABATIC && z.kind != CGX_BC_WM_EQ_ADIABATIC)
-    return fail(CGX_E_STATE, "cgx_set_bc_wall_velocity: the zone is not an adiabatic wall");
-  int rc = write_bfs_rows(s, zone, u_bf, 3, nbf_zone);
+  const bool frame = z.kind == CGX_BC_CBC_TOTAL_PT;
+  if (z.kind != CGX_BC_WALL_ADIABATIC && z.kind != CGX_BC_WM_ALG_ADIABATIC && z.kind != CGX_BC_WM_EQ_ADIABATIC &&
+      !frame)
+    return fail(CGX_E_STATE, "cgx_set_bc_face_velocity: the zone is not an adiabatic wall or CBC_TOTAL_PT");
+  // walls: rows 0-2 of the per-face boundary state; CBC_TOTAL_PT (whose
+  // boundary state those rows hold): rows 5-7 of the NSCBC array
+  int rc = frame ? write_face_rows(s, zone, u_bf, 3, nbf_zone, s->sd.nsb + 5 * size_t(s->mesh->md.nbf), 3)
+                 : write_bfs_rows(s, zone, u_bf, 3, nbf_zone);
   if (rc) return rc;
   z.pad = 1;
   CK(cudaMemcpyAsync(const_cast<BcZone*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(BcZone),

@@ -1029,7 +1029,14 @@ void total_pt_bf_state(orc_solver* o, int ibf, const double unit_n[3]) {
   const double total_p = bc[1], total_t = bc[2];
   const double gamma = o->prm.gamma;
   IdealGasState& b = o->bf_state[ibf];
-  for (int i = 0; i < 3; ++i) b.u[i] = o->un_bc[ibf] * unit_n[i] + 0.0;
+  // the frame velocity's part along the face (STATIONARY_FRAME, :3413-3421)
+  double ut[3] = {0.0, 0.0, 0.0};
+  if (o->zone_u_face[size_t(o->zone_bf[ibf])]) {
+    const double* u_fr = &o->u_bf[3 * size_t(ibf)];
+    const double ufr_n = u_fr[0] * unit_n[0] + u_fr[1] * unit_n[1] + u_fr[2] * unit_n[2];
+    for (int i = 0; i < 3; ++i) ut[i] = u_fr[i] - ufr_n * unit_n[i];
+  }
+  for (int i = 0; i < 3; ++i) b.u[i] = o->un_bc[ibf] * unit_n[i] + ut[i];
   const double total_rh = total_p / o->R_gas / total_t;
   const double invgm1 = 1.0 / (gamma - 1.0);
   const double cp = o->R_gas * gamma * invgm1;
@@ -2047,13 +2054,15 @@ extern "C" int orc_wm_eq_solve(double* tqT, double u1, double T1, double rho1, d
   return wm_eq_solve(tqT[0], tqT[1], u1, T1, rho1, y1, mu1, Pr_lam, cp, tqT[2], relax, y_plus0, tol);
 }
 
-// an adiabatic wall zone's velocity face by face (the zone's u_bc[ibf] after
-// WallAdiabatic/WmAdiabatic::initData, IdealGasSolverBcs.cpp:450-497,
-// 996-1041): u[nz][3], the zone's faces in face order
-extern "C" int orc_set_bc_wall_velocity(orc_solver* o, int zone, const double* u, int nz) {
+// a velocity face by face, u[nz][3] in face order: an adiabatic wall zone's
+// u_bc (WallAdiabatic/WmAdiabatic::initData, IdealGasSolverBcs.cpp:450-497,
+// 996-1041), or CBC_TOTAL_PT's frame velocity u_fr (:3372-3405)
+extern "C" int orc_set_bc_face_velocity(orc_solver* o, int zone, const double* u, int nz) {
   if (zone < 0 || zone >= o->nbf_zones) return -1;
   const int kind = int(o->bc[size_t(zone)][0]);
-  if (kind != CGX_BC_WALL_ADIABATIC && kind != CGX_BC_WM_ALG_ADIABATIC && kind != CGX_BC_WM_EQ_ADIABATIC) return -1;
+  if (kind != CGX_BC_WALL_ADIABATIC && kind != CGX_BC_WM_ALG_ADIABATIC && kind != CGX_BC_WM_EQ_ADIABATIC &&
+      kind != CGX_BC_CBC_TOTAL_PT)
+    return -1;
   int n = 0;
   for (int ibf = 0; ibf < o->nbf; ++ibf) n += (o->zone_bf[ibf] == zone);
   if (n != nz || (nz > 0 && !u)) return -1;

@@ -95,8 +95,9 @@ double orc_wm_r_approx(double tau, double rho, double mu, double locp, double cp
 int orc_set_bc_profile(orc_solver* o, int zone, const double* bf_state, int nz);
 /* ROTATING_REFERENCE_FRAME (revolutions per unit time); needs the mesh's x_cv. */
 int orc_set_frame_rotation(orc_solver* o, const double rev[3]);
-/* An adiabatic wall zone's velocity face by face: u[nz][3] in face order. */
-int orc_set_bc_wall_velocity(orc_solver* o, int zone, const double* u, int nz);
+/* A velocity face by face, u[nz][3] in face order: an adiabatic wall's u_bc or
+ * CBC_TOTAL_PT's frame velocity. */
+int orc_set_bc_face_velocity(orc_solver* o, int zone, const double* u, int nz);
 /* The equilibrium wall model's solve: tqT = {tau_w, q_w, T_w} in and out. */
 int orc_wm_eq_solve(double* tqT, double u1, double T1, double rho1, double y1, double mu1, double Pr_lam, double cp,
                     double relax, double y_plus0, double tol);

@@ -66,7 +66,7 @@ def _load(path):
         "orc_set_bc_profile": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
         "orc_wm_eq_solve": (ctypes.c_int, [c_dbl_p] + [ctypes.c_double] * 10),
         "orc_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p]),
-        "orc_set_bc_wall_velocity": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "orc_set_bc_face_velocity": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -243,11 +243,12 @@ class Oracle:
         if self.L.orc_set_bc_profile(self.h, int(zone), _dp(a), int(a.shape[0])) != 0:
             raise ValueError("orc_set_bc_profile: bad zone or face count")
 
-    def set_bc_wall_velocity(self, zone, u):
-        """An adiabatic wall zone's velocity face by face: u[nz][3]."""
+    def set_bc_face_velocity(self, zone, u):
+        """A velocity face by face, u[nz][3]: an adiabatic wall's or
+        CBC_TOTAL_PT's frame velocity."""
         a = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
-        if self.L.orc_set_bc_wall_velocity(self.h, int(zone), _dp(a), int(a.shape[0])) != 0:
-            raise ValueError("orc_set_bc_wall_velocity: bad zone, kind or face count")
+        if self.L.orc_set_bc_face_velocity(self.h, int(zone), _dp(a), int(a.shape[0])) != 0:
+            raise ValueError("orc_set_bc_face_velocity: bad zone, kind or face count")
 
     def set_frame_rotation(self, rev):
         """ROTATING_REFERENCE_FRAME: the rate in revolutions per unit time."""

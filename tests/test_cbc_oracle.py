@@ -374,7 +374,7 @@ def test_wall_velocity_per_face(chan):
             o = Oracle(m, prm)
             o.set_bc_params(0, kind, [] if per_face else list(uw))
             if per_face:
-                o.set_bc_wall_velocity(0, np.tile(uw, (nz, 1)))
+                o.set_bc_face_velocity(0, np.tile(uw, (nz, 1)))
             o.set_bc_params(1, 1, [])
             o.set_state_primitive(rho, u, p)
             o.init_complete()
@@ -386,5 +386,31 @@ def test_wall_velocity_per_face(chan):
     o = Oracle(m, prm)
     o.set_bc_params(0, 3, [1.0])
     with pytest.raises(ValueError):
-        o.set_bc_wall_velocity(0, np.zeros((nz, 3)))
+        o.set_bc_face_velocity(0, np.zeros((nz, 3)))
     o.close()
+
+
+def test_total_pt_frame_velocity(chan):
+    """CBC_TOTAL_PT's STATIONARY_FRAME velocity: a frame velocity along each
+    face's normal adds nothing (only its part along the face enters), so the
+    rhs equals the zone's without one, bit for bit."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.3 + 0.0 * y, 0.02 * np.cos(2 * np.pi * z / m.L[2])], 1)
+    rho, p = np.ones(m.ncv), np.full(m.ncv, prm.p_ref)
+    faces = np.flatnonzero(m.zone_bf == 0)
+    nb = m.n_bf[faces]
+    normal = 0.7 * nb / np.linalg.norm(nb, axis=1)[:, None]
+    out = []
+    for ufr in (None, normal):
+        o = Oracle(m, prm)
+        o.set_bc_params(0, TOTAL_PT, [1.02 * prm.p_ref, 1.02, 0.05])
+        if ufr is not None:
+            o.set_bc_face_velocity(0, ufr)
+        o.set_bc_params(1, RUNP, [1.0, -0.3, prm.p_ref])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        out.append(o.calc_rhs(1)[0])
+        o.close()
+    assert (np.abs(out[0] - out[1]) / np.maximum(np.abs(out[1]), 1e-300)).max() <= 1e-13

@@ -407,8 +407,8 @@ def test_stationary_walls_in_a_rotating_frame(chan):
         h.set_bc_params(1, cgx.CGX_BC_WM_ALG_ADIABATIC, ())
     for zone in (0, 1):
         ub = -np.cross(w, m.x_bf[m.zone_bf == zone])
-        s.set_bc_wall_velocity(zone, ub)
-        o.set_bc_wall_velocity(zone, ub)
+        s.set_bc_face_velocity(zone, ub)
+        o.set_bc_face_velocity(zone, ub)
     s.set_frame_rotation(rev, m.x_cv[: m.ncv])
     o.set_frame_rotation(rev)
     st = _state(m, prm)
@@ -423,6 +423,43 @@ def test_stationary_walls_in_a_rotating_frame(chan):
     for a, b in zip(s.get_state(), o.get_state()):
         assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
     with pytest.raises(cgx.CgxError):
-        s.set_bc_wall_velocity(0, np.zeros((3, 3)))  # wrong face count
+        s.set_bc_face_velocity(0, np.zeros((3, 3)))  # wrong face count
+    s.close()
+    o.close()
+
+
+def test_total_pt_inlet_in_a_rotating_frame(chan):
+    """CBC_TOTAL_PT with STATIONARY_FRAME (CbcTotalPt, IdealGasSolverBcs.cpp:
+    3372-3434): the frame velocity -w x x_bf of each face, given face by
+    face, adds its part along the face to the boundary state; with the
+    frame's source terms and an extrapolated outlet, calcRhs within 1e-12 and
+    10 steps within 1e-10 of the oracle."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    rev = np.array([0.02, 0.05, -0.01])
+    w = rev * 2.0 * np.pi
+    s = cgx.Solver(gm, prm)
+    o = Oracle(m, prm)
+    for h in (s, o):
+        h.set_bc_params(0, TOTAL_PT, (1.02 * P0, 1.02, 0.05))
+        h.set_bc_params(1, EXTRAP, ())
+    ufr = -np.cross(w, m.x_bf[m.zone_bf == 0])
+    s.set_bc_face_velocity(0, ufr)
+    o.set_bc_face_velocity(0, ufr)
+    s.set_frame_rotation(rev, m.x_cv[: m.ncv])
+    o.set_frame_rotation(rev)
+    st = _state(m, prm)
+    s.set_state_primitive(*st)
+    s.initComplete()
+    o.set_state_primitive(*st)
+    o.init_complete()
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    with pytest.raises(cgx.CgxError):
+        s.set_bc_face_velocity(1, np.zeros((int((m.zone_bf == 1).sum()), 3)))  # not for EXTRAPOLATE
     s.close()
     o.close()
