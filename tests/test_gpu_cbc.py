@@ -13,7 +13,12 @@ adds the wall's viscous and heat fluxes (IdealGasSolverBcs.cpp:1485-1510).
 * a uniform flow through the channel stays uniform (rhs = 0 to round-off);
 * the mixed-precision form within its flux tolerance of the FP64 path;
 * CBC zones and transport scalars are refused together; wrong parameter
-  counts are refused.
+  counts are refused;
+* the NSCBC zones, the zone-wide forms, CBC_RUP and WALL_CONDUCTIVE, the
+  sponge layer, a profile zone and a HOOK zone against the oracle (or, for
+  the hook, against the zone it reproduces), the mixed form of the zones
+  with their own state, and STATIONARY_FRAME walls and a CBC_TOTAL_PT inlet
+  in a rotating frame.
 """
 import numpy as np
 import pytest
