@@ -1715,9 +1715,18 @@ __global__ void __launch_bounds__(128) k_bc_calc(const CaseDev c, int stage) {
       // T_TOTAL (a negative T): the static temperature from the zone's mean Ma^2
       const double static_T = (z.a[1] > 0.0) ? z.a[1] : -z.a[1] / (1.0 + 0.5 * (gamma - 1.0) * (zs[0] / zs[1]));
       const double rhoun_bc = z.a[0], RT_bc = static_T * c.ph.R;
+      // the frame velocity's part along the face (u_fr, rows 0-2 of bfs when
+      // given; NscbcMt::calcRhs, :3820-3830)
+      double ut[3] = {0.0, 0.0, 0.0};
+      if (z.pad & 1) {
+        const double uf[3] = {s.bfs[f], s.bfs[nbf + f], s.bfs[2 * size_t(nbf) + f]};
+        const double ufn = uf[0] * nh[0] + uf[1] * nh[1] + uf[2] * nh[2];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ut[d] = uf[d] - ufn * nh[d];
+      }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        ub[d] = (rhoun_bc * nh[d] + rb * 0.0) / rb;
+        ub[d] = (rhoun_bc * nh[d] + rb * ut[d]) / rb;
         q[(2 + d) * nbf] = ub[d];
       }
       pb = rb * RT_bc;
@@ -1727,6 +1736,24 @@ __global__ void __launch_bounds__(128) k_bc_calc(const CaseDev c, int stage) {
       nscbc_outlet_rhs(rhs, nbf, nh, delta, rb, ub, pb, rho, u, p, gamma, z.a[2], z.a[1], z.a[0]);
     } else {
       nscbc_outlet_mdot_rhs(rhs, nbf, nh, delta, rb, ub, pb, rho, u, p, gamma, zs[1] / zs[0], z.a[0], z.a[1]);
+    }
+    // an outlet in a rotating frame (NscbcOutletP::calcRhsPressure/Mdot,
+    // :3975-3996, 4027-4052): the centrifugal w x u_fr (= -w x (w x x_bf))
+    // and the Coriolis -2 w x u_bc accelerations join the face's u rhs
+    const double* w = s.frame_om;
+    if (z.kind != CGX_BC_NSCBC_MT && (w[0] != 0.0 || w[1] != 0.0 || w[2] != 0.0)) {
+      double a[3] = {0.0, 0.0, 0.0};
+      if (z.pad & 1) {
+        const double uf[3] = {s.bfs[f], s.bfs[nbf + f], s.bfs[2 * size_t(nbf) + f]};
+        a[0] = w[1] * uf[2] - w[2] * uf[1];
+        a[1] = w[2] * uf[0] - w[0] * uf[2];
+        a[2] = w[0] * uf[1] - w[1] * uf[0];
+      }
+      a[0] -= 2.0 * (w[1] * ub[2] - w[2] * ub[1]);
+      a[1] -= 2.0 * (w[2] * ub[0] - w[0] * ub[2]);
+      a[2] -= 2.0 * (w[0] * ub[1] - w[1] * ub[0]);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) rhs[(2 + d) * nbf] += a[d];
     }
   }
 }
@@ -4091,6 +4118,11 @@ extern "C" int cgx_set_frame_rotation(cgx_solver* s, const double rev[3], const 
   // IdealGasSolver.hpp:141: revolutions to radians per unit time
   for (int k = 0; k < 3; ++k) c.om[k] = rev[k] * (2.0 * M_PI);
   c.rot = on;
+  // the NSCBC outlets' rotating-frame terms read the rate from the state
+  for (int k = 0; k < 3; ++k) s->sd.frame_om[k] = on ? c.om[k] : 0.0;
+  s->hcase.s = s->sd;
+  s->run.dcase.s = s->sd;
+  CK(cudaMemcpyAsync(s->d_case, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream));
   drop_graphs(s);
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
@@ -4290,8 +4322,9 @@ extern "C" int cgx_set_bc_face_velocity(cgx_solver* s, int zone, const double* u
   BcZone& z = s->bc[size_t(zone)];
   const bool frame = z.kind == CGX_BC_CBC_TOTAL_PT;
   if (z.kind != CGX_BC_WALL_ADIABATIC && z.kind != CGX_BC_WM_ALG_ADIABATIC && z.kind != CGX_BC_WM_EQ_ADIABATIC &&
-      !frame)
-    return fail(CGX_E_STATE, "cgx_set_bc_face_velocity: the zone is not an adiabatic wall or CBC_TOTAL_PT");
+      !frame && !bc_is_nscbc(z.kind))
+    return fail(CGX_E_STATE,
+                "cgx_set_bc_face_velocity: the zone is not an adiabatic wall, CBC_TOTAL_PT or an NSCBC zone");
   // walls: rows 0-2 of the per-face boundary state; CBC_TOTAL_PT (whose
   // boundary state those rows hold): rows 5-7 of the NSCBC array
   int rc = frame ? write_face_rows(s, zone, u_bf, 3, nbf_zone, s->sd.nsb + 5 * size_t(s->mesh->md.nbf), 3)

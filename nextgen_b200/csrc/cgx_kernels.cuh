@@ -243,6 +243,7 @@ struct StateDev {
   int nsp;
   double sp_p, sp_relax;  // the sponge's pressure and relaxation time
   int bc_dyn;  // 1 extrapolated, 2 total p/T, 4 NSCBC zones, 8 zone sums, 16 a sponge, 32 wall models
+  double frame_om[3];  // the rotating frame's rate in radians per unit time (0: none)
 };
 
 // One resident case: its mesh, its state and its parameters.  The step

@@ -996,7 +996,13 @@ void bc_calc_rhs(orc_solver* o, int rk_stage) {
       double static_T_bc = bc[2];
       if (bc[2] < 0.0) static_T_bc = -bc[2] / (1.0 + 0.5 * (gamma - 1.0) * (zz[0] / zz[1]));
       const double rhoun_bc = bc[1], RT_bc = static_T_bc * o->R_gas;
-      const double ut[3] = {0.0, 0.0, 0.0};
+      // NscbcMt::calcRhs (:3820-3830): the frame velocity's part along the face
+      double ut[3] = {0.0, 0.0, 0.0};
+      if (o->zone_u_face[size_t(o->zone_bf[ibf])]) {
+        const double* u_fr = &o->u_bf[3 * size_t(ibf)];
+        const double ufr_n = u_fr[0] * unit_n[0] + u_fr[1] * unit_n[1] + u_fr[2] * unit_n[2];
+        for (int i = 0; i < 3; ++i) ut[i] = u_fr[i] - ufr_n * unit_n[i];
+      }
       for (int i = 0; i < 3; ++i) u_bc[i] = (rhoun_bc * unit_n[i] + o->ns_rho[ibf] * ut[i]) / o->ns_rho[ibf];
       o->ns_p[ibf] = o->ns_rho[ibf] * RT_bc;
       nscbc_inlet_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], &o->u[3 * size_t(icv)], o->p[icv],
@@ -1007,6 +1013,22 @@ void bc_calc_rhs(orc_solver* o, int rk_stage) {
     } else {
       nscbc_outlet_mdot_rhs(rhs, unit_n, delta, o->ns_rho[ibf], u_bc, o->ns_p[ibf], o->rho[icv],
                             &o->u[3 * size_t(icv)], o->p[icv], gamma, zz[1] / zz[0], bc[1], bc[2]);
+    }
+    // an outlet in a rotating frame (:3975-3996, 4027-4052): -w x (w x x_bf),
+    // here w x u_fr with u_fr = -w x x_bf (the same numbers), and -2 w x u_bc
+    if (kind != CGX_BC_NSCBC_MT && o->rotating) {
+      const double* w = o->frame_rotation;
+      double rot_accel[3] = {0.0, 0.0, 0.0};
+      if (o->zone_u_face[size_t(o->zone_bf[ibf])]) {
+        const double* u_fr = &o->u_bf[3 * size_t(ibf)];
+        rot_accel[0] = w[1] * u_fr[2] - w[2] * u_fr[1];
+        rot_accel[1] = w[2] * u_fr[0] - w[0] * u_fr[2];
+        rot_accel[2] = w[0] * u_fr[1] - w[1] * u_fr[0];
+      }
+      rot_accel[0] -= 2.0 * (w[1] * u_bc[2] - w[2] * u_bc[1]);
+      rot_accel[1] -= 2.0 * (w[2] * u_bc[0] - w[0] * u_bc[2]);
+      rot_accel[2] -= 2.0 * (w[0] * u_bc[1] - w[1] * u_bc[0]);
+      for (int i = 0; i < 3; ++i) rhs[2 + i] += rot_accel[i];
     }
   }
 }
@@ -2061,7 +2083,8 @@ extern "C" int orc_set_bc_face_velocity(orc_solver* o, int zone, const double* u
   if (zone < 0 || zone >= o->nbf_zones) return -1;
   const int kind = int(o->bc[size_t(zone)][0]);
   if (kind != CGX_BC_WALL_ADIABATIC && kind != CGX_BC_WM_ALG_ADIABATIC && kind != CGX_BC_WM_EQ_ADIABATIC &&
-      kind != CGX_BC_CBC_TOTAL_PT)
+      kind != CGX_BC_CBC_TOTAL_PT && kind != CGX_BC_NSCBC_MT && kind != CGX_BC_NSCBC_OUTLET_P &&
+      kind != CGX_BC_NSCBC_OUTLET_MDOT)
     return -1;
   int n = 0;
   for (int ibf = 0; ibf < o->nbf; ++ibf) n += (o->zone_bf[ibf] == zone);

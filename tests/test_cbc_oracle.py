@@ -414,3 +414,35 @@ def test_total_pt_frame_velocity(chan):
         out.append(o.calc_rhs(1)[0])
         o.close()
     assert (np.abs(out[0] - out[1]) / np.maximum(np.abs(out[1]), 1e-300)).max() <= 1e-13
+
+
+def test_nscbc_rotating_frame_terms(chan):
+    """NSCBC zones in a rotating frame: a frame velocity along the inflow's
+    normals leaves it as it was, and the outlet's rotation terms change the
+    steps (they are live), against the same run without a frame."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.3 + 0.0 * y, 0.02 * np.cos(2 * np.pi * z / m.L[2])], 1)
+    rho, p = np.ones(m.ncv), np.full(m.ncv, prm.p_ref)
+
+    def run(ufr0=None, rev=None):
+        o = Oracle(m, prm)
+        o.set_bc_params(0, NSCBC_MT, [2.4, 1.0])
+        o.set_bc_params(1, NSCBC_OUT, [prm.p_ref, 0.25, 3.0])
+        if ufr0 is not None:
+            o.set_bc_face_velocity(0, ufr0)
+        if rev is not None:
+            o.set_frame_rotation(rev)
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        assert o.step(3) == 0
+        st = np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1)
+        o.close()
+        return st
+
+    base = run()
+    nb = m.n_bf[m.zone_bf == 0]
+    along_n = 0.5 * nb / np.linalg.norm(nb, axis=1)[:, None]
+    assert np.abs(run(ufr0=along_n) - base).max() <= 1e-13 * np.abs(base).max()
+    assert np.abs(run(rev=np.array([0.0, 0.2, 0.0])) - base).max() > 1e-9

@@ -468,3 +468,36 @@ def test_total_pt_inlet_in_a_rotating_frame(chan):
         s.set_bc_face_velocity(1, np.zeros((int((m.zone_bf == 1).sum()), 3)))  # not for EXTRAPOLATE
     s.close()
     o.close()
+
+
+def test_nscbc_zones_in_a_rotating_frame(chan):
+    """NSCBC_MT and NSCBC_OUTLET_P in a rotating frame (NscbcMt::initData and
+    calcRhs, NscbcOutletP::calcRhsPressure, IdealGasSolverBcs.cpp:3752-3830,
+    3975-3996): the inflow's u_bc takes the frame velocity's part along the
+    face and the outlet's u rhs the centrifugal and Coriolis accelerations;
+    10 steps within 1e-10 of the oracle."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    rev = np.array([0.01, 0.04, -0.02])
+    w = rev * 2.0 * np.pi
+    zones = ((NSCBC_MT, (2.4, 1.0)), (NSCBC_OUT, (P0, 0.25, 3.0)))
+    s = cgx.Solver(gm, prm)
+    o = Oracle(m, prm)
+    for z, (k, a) in enumerate(zones):
+        s.set_bc_params(z, k, a)
+        o.set_bc_params(z, k, a)
+        ufr = -np.cross(w, m.x_bf[m.zone_bf == z])
+        s.set_bc_face_velocity(z, ufr)
+        o.set_bc_face_velocity(z, ufr)
+    s.set_frame_rotation(rev, m.x_cv[: m.ncv])
+    o.set_frame_rotation(rev)
+    st = _state(m, prm)
+    s.set_state_primitive(*st)
+    s.initComplete()
+    o.set_state_primitive(*st)
+    o.init_complete()
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
