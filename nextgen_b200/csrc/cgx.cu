@@ -4094,6 +4094,8 @@ static void drop_graphs(cgx_solver* s) {
   }
 }
 
+static int check_frame_velocities(const cgx_solver* s);
+
 extern "C" int cgx_set_frame_rotation(cgx_solver* s, const double rev[3], const double* x_cv) {
   if (!s || !rev) return fail(CGX_E_ARG, "cgx_set_frame_rotation: null argument");
   for (int k = 0; k < 3; ++k)
@@ -4118,6 +4120,12 @@ extern "C" int cgx_set_frame_rotation(cgx_solver* s, const double rev[3], const 
   // IdealGasSolver.hpp:141: revolutions to radians per unit time
   for (int k = 0; k < 3; ++k) c.om[k] = rev[k] * (2.0 * M_PI);
   c.rot = on;
+  if (s->inited) {
+    if (int rc = check_frame_velocities(s)) {
+      c.rot = false;
+      return rc;
+    }
+  }
   // the NSCBC outlets' rotating-frame terms read the rate from the state
   for (int k = 0; k < 3; ++k) s->sd.frame_om[k] = on ? c.om[k] : 0.0;
   s->hcase.s = s->sd;
@@ -4513,8 +4521,23 @@ extern "C" int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall
 
 // initComplete; `tune`: pick the lane counts (a case prepared for a batch
 // runs with the batch's own lane counts and skips it)
+// In a rotating frame the reference forms every NSCBC face's frame velocity
+// from its centroid (NscbcMt/NscbcOutletP::initData); here the caller passes
+// them, and a zone without them is refused rather than run without its
+// centrifugal terms.
+static int check_frame_velocities(const cgx_solver* s) {
+  if (!s->src.rot) return CGX_OK;
+  for (size_t z = 0; z < s->bc.size(); ++z)
+    if (bc_is_nscbc(s->bc[z].kind) && !(s->bc[z].pad & 1))
+      return fail(CGX_E_STATE, "boundary zone " + std::to_string(z) +
+                                   ": an NSCBC zone in a rotating frame needs its faces' frame velocity "
+                                   "(cgx_set_bc_face_velocity)");
+  return CGX_OK;
+}
+
 static int init_complete(cgx_solver* s, bool tune) {
   if (!s) return fail(CGX_E_ARG, "null solver");
+  if (int rc = check_frame_velocities(s)) return rc;
   for (int z = 0; z < s->mesh->nbf_zones; ++z) {
     const int kind = s->bc[size_t(z)].kind;
     if (kind == 0)

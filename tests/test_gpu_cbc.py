@@ -475,7 +475,8 @@ def test_nscbc_zones_in_a_rotating_frame(chan):
     calcRhs, NscbcOutletP::calcRhsPressure, IdealGasSolverBcs.cpp:3752-3830,
     3975-3996): the inflow's u_bc takes the frame velocity's part along the
     face and the outlet's u rhs the centrifugal and Coriolis accelerations;
-    10 steps within 1e-10 of the oracle."""
+    10 steps within 1e-10 of the oracle; without the faces' frame velocities
+    the zones are refused."""
     m, gm = chan
     prm = cases.tgv_params(Re=400.0)
     rev = np.array([0.01, 0.04, -0.02])
@@ -501,3 +502,12 @@ def test_nscbc_zones_in_a_rotating_frame(chan):
         assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
     s.close()
     o.close()
+    # without the faces' frame velocities the zones are refused in a rotating frame
+    s = cgx.Solver(gm, prm)
+    for z, (k, a) in enumerate(zones):
+        s.set_bc_params(z, k, a)
+    s.set_frame_rotation(rev, m.x_cv[: m.ncv])
+    s.set_state_primitive(*st)
+    with pytest.raises(cgx.CgxError, match="frame velocity"):
+        s.initComplete()
+    s.close()
