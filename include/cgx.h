@@ -391,6 +391,18 @@ int cgx_set_bc(cgx_solver* s, int zone, int kind, const double u_wall[3]);
  *     stage's rhs of the zone's cells.  Transport scalars are refused with
  *     it, as with the CBC zones. */
 #define CGX_BC_HOOK              21
+/*   CGX_BC_WM_EXCHANGE_ADIABATIC   [del_exch_ratio]
+ *   CGX_BC_WM_EXCHANGE_ISOTHERMAL  T_wall [del_exch_ratio]
+ *     the algebraic wall model fed from off the wall (WmExchange,
+ *     IdealGasSolverBcs.cpp:500-990): once per step, at the first stage, each
+ *     face's velocity comes from its exchange point x_ex = x_bf - ratio
+ *     delta n_hat (ratio 3 by default), reconstructed in the cell that holds
+ *     it as u + dudx (x_ex - x_cv), and the model is solved at distance ratio
+ *     delta; a face whose point was not located uses its own cell at delta.
+ *     The exchange points' cells and positions are set with
+ *     cgx_set_bc_exchange before cgx_init_complete. */
+#define CGX_BC_WM_EXCHANGE_ADIABATIC  22
+#define CGX_BC_WM_EXCHANGE_ISOTHERMAL 23
 int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams);
 
 /* A CBC_PROFILE zone from the boundary states of its faces: bf_state
@@ -419,6 +431,13 @@ int cgx_set_bc_profile(cgx_solver* s, int zone, const double* bf_state, int nbf_
  * Set the zone's kind first (cgx_set_bc_params); setting the kind again
  * returns the zone to its one velocity (or to no frame velocity). */
 int cgx_set_bc_face_velocity(cgx_solver* s, int zone, const double* u_bf, int nbf_zone);
+
+/* The exchange points of a WM_EXCHANGE zone's faces (WmExchange::initData and
+ * its DataExchanger, IdealGasSolverBcs.cpp:500-575): cv_ex[nbf_zone] the cell
+ * (reference numbering) that holds each face's point, or -1 where the point
+ * was not located, and x_ex[nbf_zone][3] the points, the zone's faces in the
+ * order the mesh description lists them.  The mesh needs x_cv. */
+int cgx_set_bc_exchange(cgx_solver* s, int zone, const int* cv_ex, const double* x_ex, int nbf_zone);
 
 /* initComplete: updateConservativeAndPrimitiveData + calcSgsAndMaterialProperties,
  * then stores the state for NaN recovery (initialHookBcs -> storeData). */

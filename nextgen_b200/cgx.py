@@ -151,6 +151,7 @@ EXPORTS = [
     "cgx_set_scalars", "cgx_get_scalars", "cgx_get_rhs_sc", "cgx_step_profiled", "cgx_set_time",
     "cgx_set_source", "cgx_set_source_hook", "cgx_set_bc", "cgx_set_bc_params", "cgx_set_host_threads",
     "cgx_set_bc_profile", "cgx_set_frame_rotation", "cgx_step_out", "cgx_set_bc_face_velocity",
+    "cgx_set_bc_exchange",
 ]
 
 CGX_BC_SLIP = 1
@@ -174,6 +175,8 @@ CGX_BC_CBC_PROFILE = 18
 CGX_BC_WM_EQ_ADIABATIC = 19
 CGX_BC_WM_EQ_ISOTHERMAL = 20
 CGX_BC_HOOK = 21
+CGX_BC_WM_EXCHANGE_ADIABATIC = 22
+CGX_BC_WM_EXCHANGE_ISOTHERMAL = 23
 
 
 class Source(ctypes.Structure):
@@ -235,6 +238,7 @@ def lib():
         "cgx_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p, c_dbl_p]),
         "cgx_step_out": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]),
         "cgx_set_bc_face_velocity": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "cgx_set_bc_exchange": (ctypes.c_int, [vp, ctypes.c_int, c_int_p, c_dbl_p, ctypes.c_int]),
         "cgx_set_host_threads": (ctypes.c_int, [ctypes.c_int]),
         "cgx_set_source_hook": (ctypes.c_int, [vp, SOURCE_HOOK, vp]),
         "cgx_get_scalars": (ctypes.c_int, [vp, c_dbl_p]),
@@ -394,6 +398,14 @@ class Solver:
         frame velocity (STATIONARY_FRAME: -w x x_bf)."""
         a = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
         _check(lib().cgx_set_bc_face_velocity(self.h, int(zone), _dp(a), int(a.shape[0])))
+
+    def set_bc_exchange(self, zone, cv, x):
+        """A WM_EXCHANGE zone's exchange points: the cells that hold them
+        cv[nz] (reference numbering, -1 where not located) and the points
+        x[nz][3], the zone's faces in the order the mesh lists them."""
+        c = np.ascontiguousarray(cv, dtype=np.int32).reshape(-1)
+        a = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        _check(lib().cgx_set_bc_exchange(self.h, int(zone), c.ctypes.data_as(c_int_p), _dp(a), int(c.size)))
 
     def set_frame_rotation(self, rev, x_cv):
         """ROTATING_REFERENCE_FRAME: rev[3] in revolutions per unit time, the

@@ -160,6 +160,10 @@ struct orc_solver {
   // per zone and the faces' velocities [nbf][3]
   std::vector<char> zone_u_face;
   std::vector<double> u_bf;
+  // WM_EXCHANGE zones: each face's exchange cell (-1: not located) and
+  // x_ex - x_cv of that cell
+  std::vector<int> ex_cv;
+  std::vector<double> ex_dx;
   std::vector<std::array<double, 3>> wm_eq;        // per zone: relax, y_plus0, tol
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
@@ -767,6 +771,26 @@ void add_boundary_flux(orc_solver* o, IdealGasRhs* rhs) {
           for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= o->p[icv] * n[i];
         }
         rhs[icv].rhoE -= o->wm_q[ibf] * area;
+      } else if (kind == CGX_BC_WM_EXCHANGE_ADIABATIC || kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL) {
+        // WmExchange::addBoundaryFlux (IdealGasSolverBcs.cpp:914-953)
+        const double n_mag = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        double unit_n[3] = {0.0, 0.0, 0.0};
+        if (n_mag > 0.0)
+          for (int i = 0; i < 3; ++i) unit_n[i] = n[i] / n_mag;
+        const double* u = &o->u[3 * size_t(icv)];
+        double u_par[3] = {0.0, 0.0, 0.0};
+        const double un = u[0] * unit_n[0] + u[1] * unit_n[1] + u[2] * unit_n[2];
+        for (int i = 0; i < 3; ++i) u_par[i] = u[i] - un * unit_n[i];
+        const double u_mag = std::sqrt(u_par[0] * u_par[0] + u_par[1] * u_par[1] + u_par[2] * u_par[2]);
+        if (u_mag > 0.0) {
+          for (int i = 0; i < 3; ++i) {
+            rhs[icv].rhou[i] -= o->p[icv] * n[i];
+            rhs[icv].rhou[i] -= o->wm_tau[ibf] * u_par[i] / u_mag * n_mag;
+          }
+        } else {
+          for (int i = 0; i < 3; ++i) rhs[icv].rhou[i] -= o->p[icv] * n[i];
+        }
+        rhs[icv].rhoE -= o->wm_q[ibf] * n_mag;
       } else if (kind == CGX_BC_HOOK) {
         // a hook zone: its flux is the caller's (a source term here)
       } else if (kind == CGX_BC_SPONGE) {
@@ -897,6 +921,49 @@ void nscbc_outlet_mdot_rhs(double* rhs, const double unit_n[3], double delta, do
 // NscbcOutletP::calcRhsPressure (:4009-4056), without frame rotation.
 void bc_calc_rhs(orc_solver* o, int rk_stage) {
   const double gamma = o->prm.gamma;
+  // WmExchange::calcRhs (IdealGasSolverBcs.cpp:820-910): the velocity at each
+  // face's exchange point, u + dudx (x_ex - x_cv) in the cell that holds it
+  // (DataExchanger::exchangeCvDataWithGhosts, DataExchanger.hpp:442-501)
+  for (int ibf = 0; ibf < o->nbf && rk_stage == 1; ++ibf) {
+    const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
+    const int kind = int(bc[0]);
+    if (kind != CGX_BC_WM_EXCHANGE_ADIABATIC && kind != CGX_BC_WM_EXCHANGE_ISOTHERMAL) continue;
+    const int icv = o->cvobf[ibf];
+    if (o->aod_bf[ibf] < 0.0) {
+      o->wm_tau[ibf] = 0.0;
+      o->wm_q[ibf] = 0.0;
+      continue;
+    }
+    const double* n = &o->n_bf[3 * size_t(ibf)];
+    const double n_mag = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    double unit_n[3] = {0.0, 0.0, 0.0};
+    if (n_mag > 0.0)
+      for (int i = 0; i < 3; ++i) unit_n[i] = n[i] / n_mag;
+    double u_tmp[3], y1;
+    const int j = o->ex_cv[ibf];
+    if (j >= 0) {
+      const double* dx = &o->ex_dx[3 * size_t(ibf)];
+      const double* g = &o->dudx[9 * size_t(j)];
+      for (int i = 0; i < 3; ++i)
+        u_tmp[i] = o->u[3 * size_t(j) + i] + (g[3 * i] * dx[0] + g[3 * i + 1] * dx[1] + g[3 * i + 2] * dx[2]);
+      y1 = bc[3] * n_mag / o->aod_bf[ibf];
+    } else {
+      for (int i = 0; i < 3; ++i) u_tmp[i] = o->u[3 * size_t(icv) + i];
+      y1 = n_mag / o->aod_bf[ibf];
+    }
+    double u_par[3];
+    const double un = u_tmp[0] * unit_n[0] + u_tmp[1] * unit_n[1] + u_tmp[2] * unit_n[2];
+    for (int i = 0; i < 3; ++i) u_par[i] = u_tmp[i] - un * unit_n[i];
+    const double u1 = std::sqrt(u_par[0] * u_par[0] + u_par[1] * u_par[1] + u_par[2] * u_par[2]);
+    const double u_tau = std::sqrt(o->wm_tau[ibf] / o->rho[icv]);
+    o->wm_tau[ibf] = wm_solve_tau(u1, y1, o->rho[icv], o->mu_lam[icv], u_tau);
+    if (kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL) {
+      const double cp = o->R_gas * gamma / (gamma - 1.0);
+      o->wm_q[ibf] = wm_q_wall(o->T[icv], bc[4], o->wm_tau[ibf], o->rho[icv], o->mu_lam[icv], o->loc_lam[icv], cp, y1);
+    } else {
+      o->wm_q[ibf] = 0.0;
+    }
+  }
   // WmAdiabatic::calcRhs (IdealGasSolverBcs.cpp:1323-1393) and
   // WmIsothermal::calcRhs (:2159-2216): tau_wall (and q_wall) once per step
   for (int ibf = 0; ibf < o->nbf && rk_stage == 1; ++ibf) {
@@ -1119,6 +1186,23 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
   for (int ibf = 0; ibf < o->nbf; ++ibf) {
     const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
     const int kind = int(bc[0]);
+    if (init && (kind == CGX_BC_WM_EXCHANGE_ADIABATIC || kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL)) {
+      // WmExchange::initialHook (:577-632)
+      const int icv = o->cvobf[ibf];
+      const double* n = &o->n_bf[3 * size_t(ibf)];
+      const double* u = &o->u[3 * size_t(icv)];
+      o->wm_tau[ibf] = 0.0;
+      o->wm_q[ibf] = 0.0;
+      if (o->aod_bf[ibf] > 0.0) {
+        const double y1 = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) / o->aod_bf[ibf];
+        o->wm_tau[ibf] = o->mu_lam[icv] * std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) / y1;
+        if (kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL) {
+          const double cp = o->prm.gamma * o->R_gas / (o->prm.gamma - 1.0);
+          o->wm_q[ibf] = cp * o->loc_lam[icv] * (o->T[icv] - bc[4]) / y1;
+        }
+      }
+      continue;
+    }
     if (init && (kind == CGX_BC_WM_ALG_ADIABATIC || kind == CGX_BC_WM_ALG_ISOTHERMAL ||
                  kind == CGX_BC_WM_ALG_CONDUCTIVE || kind == CGX_BC_WM_EQ_ADIABATIC ||
                  kind == CGX_BC_WM_EQ_ISOTHERMAL)) {
@@ -1532,6 +1616,8 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->wm_Tw.assign(m->nbf, 0.0);
     o->zone_u_face.assign(m->nbf_zones, 0);
     o->u_bf.assign(3 * size_t(m->nbf), 0.0);
+    o->ex_cv.assign(m->nbf, -1);
+    o->ex_dx.assign(3 * size_t(m->nbf), 0.0);
     o->wm_eq.assign(m->nbf_zones, {0.7, 1.0, 1.0e-4});
     o->ns_rho.assign(m->nbf, 0.0);
     o->ns_p.assign(m->nbf, 0.0);
@@ -1904,6 +1990,16 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
     o->bc[zone] = {double(kind), np ? prm[0] : 0.0, np ? prm[1] : 0.0, np ? prm[2] : 0.0, 0.0};
     return 0;
   }
+  if (kind == CGX_BC_WM_EXCHANGE_ADIABATIC || kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL) {
+    // WmExchange::initData (:500-533): [del_exch_ratio] or T [del_exch_ratio], ratio 3 by default
+    const bool iso = kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL;
+    if ((iso && np != 1 && np != 2) || (!iso && np != 0 && np != 1) || (np > 0 && !prm)) return -1;
+    const double ratio = (np == (iso ? 2 : 1)) ? prm[np - 1] : 3.0;
+    o->bc[zone] = {double(kind), 0.0, 0.0, ratio, iso ? prm[0] : 0.0};
+    for (int ibf = 0; ibf < o->nbf; ++ibf)
+      if (o->zone_bf[ibf] == zone) o->ex_cv[ibf] = -1;
+    return 0;
+  }
   if (kind == CGX_BC_HOOK) {
     if (np != 0) return -1;
     o->bc[zone] = {double(kind), 0.0, 0.0, 0.0, 0.0};
@@ -2096,5 +2192,27 @@ extern "C" int orc_set_bc_face_velocity(orc_solver* o, int zone, const double* u
       ++j;
     }
   o->zone_u_face[size_t(zone)] = 1;
+  return 0;
+}
+
+// a WM_EXCHANGE zone's exchange points (WmExchange::initData, :535-575):
+// cv[nz] the cell holding each face's point (-1: not located), x[nz][3] the
+// points, the zone's faces in face order
+extern "C" int orc_set_bc_exchange(orc_solver* o, int zone, const int* cv, const double* x, int nz) {
+  if (zone < 0 || zone >= o->nbf_zones) return -1;
+  const int kind = int(o->bc[size_t(zone)][0]);
+  if (kind != CGX_BC_WM_EXCHANGE_ADIABATIC && kind != CGX_BC_WM_EXCHANGE_ISOTHERMAL) return -1;
+  int n = 0;
+  for (int ibf = 0; ibf < o->nbf; ++ibf) n += (o->zone_bf[ibf] == zone);
+  if (n != nz || (nz > 0 && (!cv || !x)) || o->x_cv.size() != 3 * size_t(o->ncv)) return -1;
+  int k = 0;
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    if (o->zone_bf[ibf] != zone) continue;
+    if (cv[k] < -1 || cv[k] >= o->ncv) return -1;
+    o->ex_cv[ibf] = cv[k];
+    for (int i = 0; i < 3; ++i)
+      o->ex_dx[3 * size_t(ibf) + i] = (cv[k] >= 0) ? x[3 * size_t(k) + i] - o->x_cv[3 * size_t(cv[k]) + i] : 0.0;
+    ++k;
+  }
   return 0;
 }

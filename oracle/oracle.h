@@ -98,6 +98,8 @@ int orc_set_frame_rotation(orc_solver* o, const double rev[3]);
 /* A velocity face by face, u[nz][3] in face order: an adiabatic wall's u_bc or
  * CBC_TOTAL_PT's frame velocity. */
 int orc_set_bc_face_velocity(orc_solver* o, int zone, const double* u, int nz);
+/* A WM_EXCHANGE zone's exchange points: cells cv[nz] (-1: not located), points x[nz][3]. */
+int orc_set_bc_exchange(orc_solver* o, int zone, const int* cv, const double* x, int nz);
 /* The equilibrium wall model's solve: tqT = {tau_w, q_w, T_w} in and out. */
 int orc_wm_eq_solve(double* tqT, double u1, double T1, double rho1, double y1, double mu1, double Pr_lam, double cp,
                     double relax, double y_plus0, double tol);

@@ -67,6 +67,7 @@ def _load(path):
         "orc_wm_eq_solve": (ctypes.c_int, [c_dbl_p] + [ctypes.c_double] * 10),
         "orc_set_frame_rotation": (ctypes.c_int, [vp, c_dbl_p]),
         "orc_set_bc_face_velocity": (ctypes.c_int, [vp, ctypes.c_int, c_dbl_p, ctypes.c_int]),
+        "orc_set_bc_exchange": (ctypes.c_int, [vp, ctypes.c_int, c_int_p, c_dbl_p, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -249,6 +250,13 @@ class Oracle:
         a = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
         if self.L.orc_set_bc_face_velocity(self.h, int(zone), _dp(a), int(a.shape[0])) != 0:
             raise ValueError("orc_set_bc_face_velocity: bad zone, kind or face count")
+
+    def set_bc_exchange(self, zone, cv, x):
+        """A WM_EXCHANGE zone's exchange points: cells cv[nz] (-1: not located), points x[nz][3]."""
+        c = np.ascontiguousarray(cv, dtype=np.int32).reshape(-1)
+        a = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        if self.L.orc_set_bc_exchange(self.h, int(zone), c.ctypes.data_as(c_int_p), _dp(a), int(c.size)) != 0:
+            raise ValueError("orc_set_bc_exchange: bad zone, kind, cells or face count")
 
     def set_frame_rotation(self, rev):
         """ROTATING_REFERENCE_FRAME: the rate in revolutions per unit time."""

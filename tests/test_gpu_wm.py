@@ -112,3 +112,68 @@ def test_wall_model_refusals(chan):
         with pytest.raises(cgx.CgxError):
             s.set_bc_params(0, kind, bad)
     s.close()
+
+
+WM_EX_AD, WM_EX_ISO = cgx.CGX_BC_WM_EXCHANGE_ADIABATIC, cgx.CGX_BC_WM_EXCHANGE_ISOTHERMAL
+
+
+def test_exchange_wall_models_match_oracle(chan):
+    """WM_EXCHANGE_ADIABATIC and WM_EXCHANGE_ISOTHERMAL (WmExchange,
+    IdealGasSolverBcs.cpp:500-990): each face's velocity reconstructed at its
+    exchange point x_bf - ratio delta n_hat in a nearby cell (every fifth face
+    left unlocated); calcRhs within 1e-12, 10 steps within 1e-10 of the
+    oracle, and a NaN restores tau_wall; an exchange zone without its points
+    is refused."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    zones = ((WM_EX_AD, ()), (WM_EX_ISO, (1.2, 2.0)))
+    ratios = (3.0, 2.0)
+    xc = m.x_cv[: m.ncv]
+    pts = {}
+    for z in (0, 1):
+        sel = m.zone_bf == z
+        nb, xb = m.n_bf[sel], m.x_bf[sel]
+        area = np.linalg.norm(nb, axis=1)
+        delta = area / m.area_over_delta_bf[sel]
+        xe = xb - ratios[z] * (delta / area)[:, None] * nb
+        cv = np.array([int(np.argmin(((xc - q) ** 2).sum(1))) for q in xe], dtype=np.int32)
+        cv[::5] = -1
+        pts[z] = (cv, xe)
+    s = cgx.Solver(gm, prm)
+    o = Oracle(m, prm)
+    for z, (k, a) in enumerate(zones):
+        s.set_bc_params(z, k, a)
+        o.set_bc_params(z, k, a)
+    s2 = cgx.Solver(gm, prm)
+    for z, (k, a) in enumerate(zones):
+        s2.set_bc_params(z, k, a)
+    for z in (0, 1):
+        s.set_bc_exchange(z, *pts[z])
+        o.set_bc_exchange(z, *pts[z])
+    st = _state(m, prm)
+    for h in (s, o):
+        h.set_state_primitive(*st)
+    s.initComplete()
+    o.init_complete()
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    o.set_dt()
+    icv = int(m.cvobf[m.zone_bf == 0][0])
+    bad = [a.copy() for a in s.get_state()]
+    bad[0][icv] = np.nan
+    s.set_state(*bad)
+    s.updateConservativeAndPrimitiveData()
+    o.poison(icv)
+    assert s.advanceSolution() == -1 and o.advance_solution() == -1
+    assert s.step(3) == 0 and o.step(3) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s2.set_state_primitive(*st)
+    with pytest.raises(cgx.CgxError, match="exchange points"):
+        s2.initComplete()
+    for h in (s, o, s2):
+        h.close()

@@ -241,3 +241,76 @@ def test_wall_model_solver_bitwise_equals_reference(chan):
     assert np.array_equal(out[1], out[5])
     assert np.array_equal(out[2], out[6])
     assert np.array_equal(out[3], out[7])
+
+
+WM_EX_AD, WM_EX_ISO = 22, 23
+
+
+def test_exchange_wall_model_at_its_own_cell(chan):
+    """WM_EXCHANGE_ADIABATIC with each exchange point at its face's own cell
+    centroid and a distance ratio of 1, or with no point located, is the
+    algebraic WM_ALG_ADIABATIC wall, bit for bit (WmExchange,
+    IdealGasSolverBcs.cpp:500-990); an exchange zone refuses points for the
+    wrong face count."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.3 + 0.1 * np.cos(2 * np.pi * z / m.L[2]), 0.02 * np.sin(2 * np.pi * x / m.L[0]),
+                  0.05 * np.sin(np.pi * y / m.L[1])], 1)
+    rho, p = 1.0 + 0.02 * np.cos(2 * np.pi * x / m.L[0]), np.full(m.ncv, prm.p_ref)
+    cells = {zz: m.cvobf[m.zone_bf == zz] for zz in (0, 1)}
+
+    def run(form):
+        o = Oracle(m, prm)
+        for zz in (0, 1):
+            if form == "alg":
+                o.set_bc_params(zz, WM_AD, [])
+            else:
+                o.set_bc_params(zz, WM_EX_AD, [1.0] if form == "own" else [])
+                cv = cells[zz] if form == "own" else -np.ones(cells[zz].size, dtype=np.int32)
+                o.set_bc_exchange(zz, cv, m.x_cv[cells[zz]])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        r = o.calc_rhs(1)[0]
+        assert o.step(3) == 0
+        st = np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1)
+        o.close()
+        return r, st
+
+    a = run("alg")
+    for form in ("own", "unlocated"):
+        b = run(form)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    o = Oracle(m, prm)
+    o.set_bc_params(0, WM_EX_ISO, [1.2, 2.5])
+    with pytest.raises(ValueError):
+        o.set_bc_exchange(0, cells[0][:-1], m.x_cv[cells[0][:-1]])
+    with pytest.raises(ValueError):
+        o.set_bc_params(1, WM_EX_ISO, [])
+    o.close()
+
+
+@need_ref
+def test_exchange_wall_model_bitwise_equals_reference(chan):
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.3 + 0.1 * np.cos(2 * np.pi * z / m.L[2]), 0.02 * np.sin(2 * np.pi * x / m.L[0]),
+                  0.05 * np.sin(np.pi * y / m.L[1])], 1)
+    rho, p = 1.0 + 0.02 * np.cos(2 * np.pi * x / m.L[0]), np.full(m.ncv, prm.p_ref)
+    out = []
+    for reference in (False, True):
+        o = Oracle(m, prm, reference=reference)
+        o.set_bc_params(0, WM_EX_AD, [])
+        o.set_bc_params(1, WM_EX_ISO, [1.2])
+        for zz in (0, 1):
+            c = m.cvobf[m.zone_bf == zz]
+            nb = m.n_bf[m.zone_bf == zz]
+            xe = m.x_cv[c] - 0.3 * nb / np.linalg.norm(nb, axis=1)[:, None]
+            o.set_bc_exchange(zz, c, xe)
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        assert o.step(3) == 0
+        out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+        o.close()
+    assert np.array_equal(out[0], out[1])
