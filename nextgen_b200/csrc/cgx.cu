@@ -1186,6 +1186,35 @@ __device__ __forceinline__ void wall_velocity(const StateDev& s, const BcZone& z
   for (int d = 0; d < 3; ++d) ub[d] = (z.pad & 1) ? s.bfs[size_t(d) * nbf + f] : z.a[d];
 }
 
+// CBC_RUP with STATIONARY_FRAME in a rotating frame (CbcRup::initData and
+// calcBfState, IdealGasSolverBcs.cpp:3297-3348): the inflow velocity u_bc,
+// fixed in the absolute frame, turns by -|w| t about the frame's axis
+// (Rodrigues' formula) unless it lies along the axis, plus the face's frame
+// velocity u_fr (rows 5-7 of nsb)
+__device__ inline void rup_frame_velocity(const StateDev& s, const BcZone& z, int f, int nbf, double t,
+                                          double u[3]) {
+  const double* w = s.frame_om;
+  const double* ub = z.a;
+  const double* fr = s.nsb + 5 * size_t(nbf) + f;
+  const double ufr[3] = {fr[0], fr[nbf], fr[2 * size_t(nbf)]};
+  const double om = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  const double K[3] = {w[0] / om, w[1] / om, w[2] / om};
+  const double mag_ub = sqrt(ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2]);
+  const double c[3] = {(ub[1] * K[2] - ub[2] * K[1]) / mag_ub, (ub[2] * K[0] - ub[0] * K[2]) / mag_ub,
+                       (ub[0] * K[1] - ub[1] * K[0]) / mag_ub};
+  if (!(sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) > 1.0e-12)) {  // along the axis
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[d] = ub[d] + ufr[d];
+    return;
+  }
+  const double th = -om * t;
+  const double kx[3] = {K[1] * ub[2] - K[2] * ub[1], K[2] * ub[0] - K[0] * ub[2], K[0] * ub[1] - K[1] * ub[0]};
+  const double kd = K[0] * ub[0] + K[1] * ub[1] + K[2] * ub[2];
+  const double ct = cos(th), st = sin(th);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) u[d] = ub[d] * ct + kx[d] * st + K[d] * kd * (1.0 - ct) + ufr[d];
+}
+
 __host__ __device__ inline bool bc_is_cbc(int k) {
   return k == CGX_BC_CBC_UPT || k == CGX_BC_CBC_RUNP || k == CGX_BC_CBC_MPT || k == CGX_BC_CBC_RUP ||
          k == CGX_BC_CBC_EXTRAPOLATE || k == CGX_BC_CBC_TOTAL_PT || k == CGX_BC_SPONGE || k == CGX_BC_CBC_PROFILE ||
@@ -1406,8 +1435,8 @@ __global__ void __launch_bounds__(128) k_rhs_bf(const CaseDev c, int stage) {
         sb.sp_vol = 1.0 / rb;
         sb.p = pb;
         sb.h = gamma / (gamma - 1.0) * pb * (1.0 / rb);
-      } else if (kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT ||
-                 kind == CGX_BC_CBC_PROFILE) {  // the face's own state
+      } else if (kind == CGX_BC_CBC_EXTRAPOLATE || kind == CGX_BC_CBC_TOTAL_PT || kind == CGX_BC_CBC_PROFILE ||
+                 (kind == CGX_BC_CBC_RUP && (z.pad & 1))) {  // the face's own state
         const double* q = s.bfs + f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) sb.u[d] = q[d * m.nbf];
@@ -1654,6 +1683,20 @@ __global__ void __launch_bounds__(128) k_bc_calc(const CaseDev c, int stage) {
   const int nbf = m.nbf;
   for (int f = m.bfc[i]; f < m.bfc[i + 1]; ++f) {
     const BcZone& z = s.bc[m.bf_zone[f]];
+    if (z.kind == CGX_BC_CBC_RUP) {
+      // CbcRup::calcRhs (:3350-3358): the face's velocity at the stage's time
+      // (t, t + dt, t + dt - dt/2 as advanceSolution steps it)
+      if (!(z.pad & 1)) continue;
+      const Ctl& k = *s.ctl;
+      double t = k.time;
+      if (stage >= 2) t += k.dt;
+      if (stage == 3) t -= 0.5 * k.dt;
+      double uf[3];
+      rup_frame_velocity(s, z, f, nbf, t, uf);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) s.bfs[size_t(d) * nbf + f] = uf[d];
+      continue;
+    }
     if (bc_is_wm_exchange(z.kind)) {
       // WmExchange::calcRhs (:820-910): the velocity at the exchange point,
       // u + dudx dx in the cell that holds it (rows 0-2 of bfs: dx, row 3:
@@ -1893,6 +1936,12 @@ __global__ void __launch_bounds__(128) k_bc_stage(const CaseDev c, int stage, in
           ns[k * m.nbf] = x;
         }
       }
+    } else if (z.kind == CGX_BC_CBC_RUP && (z.pad & 1) && init) {
+      // CbcRup::initData (:3320-3326): the velocity at the start time
+      double uf[3];
+      rup_frame_velocity(s, z, f, m.nbf, s.ctl->time, uf);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) s.bfs[size_t(d) * m.nbf + f] = uf[d];
     } else if (bc_is_wm_exchange(z.kind) && init) {
       // WmExchange::initialHook (:577-632): mu |u| / y1, and the isothermal
       // form's laminar heat flux
@@ -2827,7 +2876,8 @@ int enqueue_sponge_relax(const Runner& R, bool init) {
 // (w: the stage's RK3 weights, for the NSCBC zones' own integration)
 int enqueue_bc_stage(const Runner& R, int stage, bool init, const double* w = nullptr) {
   const int nbc = R.dcase.m.nbc;
-  if (!R.direct || nbc == 0 || (!(R.dcase.s.bc_dyn & 15) && !(init && (R.dcase.s.bc_dyn & 32)))) return CGX_OK;
+  if (!R.direct || nbc == 0 || (!(R.dcase.s.bc_dyn & 15) && !(init && (R.dcase.s.bc_dyn & (32 | 64)))))
+    return CGX_OK;
   k_bc_stage<<<(nbc + 127) / 128, 128, 0, R.stream>>>(R.dcase, stage, init ? 1 : 0, w ? w[0] : 0.0, w ? w[1] : 0.0,
                                                         w ? w[2] : 0.0);
   return launch_check(R, 1);
@@ -2843,7 +2893,7 @@ int enqueue_bc_calc(const Runner& R, int stage) {
     k_zone_sums<<<R.dcase.m.nzones, 256, 0, R.stream>>>(R.dcase);
     if ((rc = launch_check(R, 1))) return rc;
   }
-  if (!(R.dcase.s.bc_dyn & 4) && !((R.dcase.s.bc_dyn & 32) && stage == 1)) return CGX_OK;
+  if (!(R.dcase.s.bc_dyn & (4 | 64)) && !((R.dcase.s.bc_dyn & 32) && stage == 1)) return CGX_OK;
   k_bc_calc<<<(nbc + 127) / 128, 128, 0, R.stream>>>(R.dcase, stage);
   return launch_check(R, 1);
 }
@@ -2885,7 +2935,7 @@ int enqueue_rhs(const Runner& R, int stage0, const double* time = nullptr) {
 inline int launches_per_step(const Runner& R) {
   int n = kLaunchesPerStep + ((R.direct && R.dcase.s.nsc > 0) ? 3 : 0) +
           ((R.direct && R.dcase.m.nbc > 0) ? 3 : 0) + ((R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & 15)) ? 3 : 0) +
-          ((R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & 4)) ? 3
+          ((R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & (4 | 64))) ? 3
            : (R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & 32)) ? 1 : 0) +
           ((R.direct && R.dcase.m.nbc > 0 && (R.dcase.s.bc_dyn & 8)) ? 4 : 0) +
           ((R.direct && (R.dcase.s.bc_dyn & 16)) ? (R.dcase.s.nsp > 0 ? 4 : 1) : 0);
@@ -4393,6 +4443,26 @@ static int set_sponge(cgx_solver* s, int zone, const double* a) {
 
 static int set_bc_impl(cgx_solver* s, int zone, int kind, const double* params, int nparams, bool profile);
 
+// The zones that add kernels to a step (StateDev::bc_dyn), from the zones'
+// kinds and per-face forms; a change re-records the step graphs.
+static int refresh_bc_dyn(cgx_solver* s, bool force) {
+  int dyn = (s->sp_zone >= 0) ? 16 : 0;
+  for (const BcZone& b : s->bc)
+    dyn |= (b.kind == CGX_BC_CBC_EXTRAPOLATE ? 1 : 0) | (b.kind == CGX_BC_CBC_TOTAL_PT ? 2 : 0) |
+           ((b.kind == CGX_BC_NSCBC_MT || b.kind == CGX_BC_NSCBC_OUTLET_P || b.kind == CGX_BC_NSCBC_OUTLET_MDOT) ? 4 : 0) |
+           (((b.kind == CGX_BC_CBC_TOTAL_PT && b.a[3] != 0.0) || (b.kind == CGX_BC_NSCBC_MT && b.a[1] < 0.0) ||
+             b.kind == CGX_BC_NSCBC_OUTLET_MDOT) ? 8 : 0) |
+           (bc_is_wm(b.kind) ? 32 : 0) | ((b.kind == CGX_BC_CBC_RUP && (b.pad & 1)) ? 64 : 0);
+  if (dyn != s->sd.bc_dyn || force) {
+    s->sd.bc_dyn = dyn;
+    s->hcase.s = s->sd;
+    s->run.dcase.s = s->sd;
+    CK(cudaMemcpyAsync(s->d_case, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream));
+    drop_graphs(s);
+  }
+  return CGX_OK;
+}
+
 extern "C" int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, int nparams) {
   return set_bc_impl(s, zone, kind, params, nparams, false);
 }
@@ -4430,21 +4500,33 @@ extern "C" int cgx_set_bc_face_velocity(cgx_solver* s, int zone, const double* u
   if (!s) return fail(CGX_E_ARG, "cgx_set_bc_face_velocity: null solver");
   if (zone < 0 || zone >= s->mesh->nbf_zones) return fail(CGX_E_ARG, "cgx_set_bc_face_velocity: bad zone");
   BcZone& z = s->bc[size_t(zone)];
-  const bool frame = z.kind == CGX_BC_CBC_TOTAL_PT;
+  const bool frame = z.kind == CGX_BC_CBC_TOTAL_PT || z.kind == CGX_BC_CBC_RUP;
   if (z.kind != CGX_BC_WALL_ADIABATIC && z.kind != CGX_BC_WM_ALG_ADIABATIC && z.kind != CGX_BC_WM_EQ_ADIABATIC &&
       !frame && !bc_is_nscbc(z.kind))
-    return fail(CGX_E_STATE,
-                "cgx_set_bc_face_velocity: the zone is not an adiabatic wall, CBC_TOTAL_PT or an NSCBC zone");
+    return fail(CGX_E_STATE, "cgx_set_bc_face_velocity: the zone is not an adiabatic wall, CBC_TOTAL_PT, "
+                             "CBC_RUP or an NSCBC zone");
   // walls: rows 0-2 of the per-face boundary state; CBC_TOTAL_PT (whose
   // boundary state those rows hold): rows 5-7 of the NSCBC array
   int rc = frame ? write_face_rows(s, zone, u_bf, 3, nbf_zone, s->sd.nsb + 5 * size_t(s->mesh->md.nbf), 3)
                  : write_bfs_rows(s, zone, u_bf, 3, nbf_zone);
   if (rc) return rc;
+  if (z.kind == CGX_BC_CBC_RUP) {
+    // its face state: rows 0-2 follow the frame (k_bc_calc, k_bc_stage),
+    // rows 3-5 keep the zone's sp_vol, p, h
+    std::vector<double> st(6 * size_t(std::max(nbf_zone, 0)));
+    for (int k = 0; k < nbf_zone; ++k) {
+      for (int d = 0; d < 3; ++d) st[6 * size_t(k) + d] = z.a[d] + u_bf[3 * size_t(k) + d];
+      st[6 * size_t(k) + 3] = z.a[5];
+      st[6 * size_t(k) + 4] = z.a[4];
+      st[6 * size_t(k) + 5] = z.a[6];
+    }
+    if ((rc = write_bfs_rows(s, zone, st.data(), 6, nbf_zone))) return rc;
+  }
   z.pad = 1;
   CK(cudaMemcpyAsync(const_cast<BcZone*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(BcZone),
                      cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  return CGX_OK;
+  return refresh_bc_dyn(s, false);
 }
 
 extern "C" int cgx_set_bc_exchange(cgx_solver* s, int zone, const int* cv_ex, const double* x_ex, int nbf_zone) {
@@ -4639,20 +4721,7 @@ static int set_bc_impl(cgx_solver* s, int zone, int kind, const double* params, 
   CK(cudaMemcpyAsync(const_cast<BcZone*>(s->sd.bc), s->bc.data(), s->bc.size() * sizeof(BcZone),
                      cudaMemcpyHostToDevice, s->stream));
   // zones whose state follows the flow add a kernel to each stage
-  int dyn = (s->sp_zone >= 0) ? 16 : 0;
-  for (const BcZone& b : s->bc)
-    dyn |= (b.kind == CGX_BC_CBC_EXTRAPOLATE ? 1 : 0) | (b.kind == CGX_BC_CBC_TOTAL_PT ? 2 : 0) |
-           ((b.kind == CGX_BC_NSCBC_MT || b.kind == CGX_BC_NSCBC_OUTLET_P || b.kind == CGX_BC_NSCBC_OUTLET_MDOT) ? 4 : 0) |
-           (((b.kind == CGX_BC_CBC_TOTAL_PT && b.a[3] != 0.0) || (b.kind == CGX_BC_NSCBC_MT && b.a[1] < 0.0) ||
-             b.kind == CGX_BC_NSCBC_OUTLET_MDOT) ? 8 : 0) |
-           (bc_is_wm(b.kind) ? 32 : 0);
-  if (dyn != s->sd.bc_dyn || kind == CGX_BC_SPONGE) {
-    s->sd.bc_dyn = dyn;
-    s->hcase.s = s->sd;
-    s->run.dcase.s = s->sd;
-    CK(cudaMemcpyAsync(s->d_case, &s->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, s->stream));
-    drop_graphs(s);
-  }
+  if (int rc = refresh_bc_dyn(s, kind == CGX_BC_SPONGE)) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return CGX_OK;
 }

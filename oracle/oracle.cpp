@@ -164,6 +164,8 @@ struct orc_solver {
   // x_ex - x_cv of that cell
   std::vector<int> ex_cv;
   std::vector<double> ex_dx;
+  // CBC_RUP zones: their u_bc (for STATIONARY_FRAME in a rotating frame)
+  std::vector<std::array<double, 3>> rup_u;
   std::vector<std::array<double, 3>> wm_eq;        // per zone: relax, y_plus0, tol
   // source terms (the addSourceHook of a subclass)
   double src_A = 0.0, src_g[3] = {0.0, 0.0, 0.0};
@@ -919,8 +921,45 @@ void nscbc_outlet_mdot_rhs(double* rhs, const double unit_n[3], double delta, do
 // The NSCBC zones' calcRhs at stage rk_stage, before the solver's:
 // NscbcMt::calcRhs (IdealGasSolverBcs.cpp:3777-3844, static T) and
 // NscbcOutletP::calcRhsPressure (:4009-4056), without frame rotation.
+// CbcRup::calcBfState and initData (IdealGasSolverBcs.cpp:3297-3348): a
+// STATIONARY_FRAME inflow's velocity at time t in the rotating frame
+void rup_frame_state(orc_solver* o, int ibf, double t) {
+  const int z = o->zone_bf[ibf];
+  const double* u_bc = o->rup_u[size_t(z)].data();
+  const double* u_fr = &o->u_bf[3 * size_t(ibf)];
+  const double* w = o->frame_rotation;
+  const double omega = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  double rot_axis[3];
+  for (int i = 0; i < 3; ++i) rot_axis[i] = w[i] / omega;
+  double ubc_x_axis[3] = {u_bc[1] * rot_axis[2] - u_bc[2] * rot_axis[1], u_bc[2] * rot_axis[0] - u_bc[0] * rot_axis[2],
+                          u_bc[0] * rot_axis[1] - u_bc[1] * rot_axis[0]};
+  const double mag_ubc = std::sqrt(u_bc[0] * u_bc[0] + u_bc[1] * u_bc[1] + u_bc[2] * u_bc[2]);
+  for (int i = 0; i < 3; ++i) ubc_x_axis[i] /= mag_ubc;
+  const double mag_x = std::sqrt(ubc_x_axis[0] * ubc_x_axis[0] + ubc_x_axis[1] * ubc_x_axis[1] +
+                                 ubc_x_axis[2] * ubc_x_axis[2]);
+  IdealGasState& b = o->bf_state[ibf];
+  if (!(mag_x > 1.0e-12)) {  // aligned: u_bc + u_fr
+    for (int i = 0; i < 3; ++i) b.u[i] = u_bc[i] + u_fr[i];
+    return;
+  }
+  const double theta = -omega * t;
+  const double axis_x_ubc[3] = {rot_axis[1] * u_bc[2] - rot_axis[2] * u_bc[1],
+                                rot_axis[2] * u_bc[0] - rot_axis[0] * u_bc[2],
+                                rot_axis[0] * u_bc[1] - rot_axis[1] * u_bc[0]};
+  const double axis_dot_ubc = rot_axis[0] * u_bc[0] + rot_axis[1] * u_bc[1] + rot_axis[2] * u_bc[2];
+  const double cos_theta = std::cos(theta), sin_theta = std::sin(theta);
+  for (int i = 0; i < 3; ++i)
+    b.u[i] = u_bc[i] * cos_theta + axis_x_ubc[i] * sin_theta + rot_axis[i] * axis_dot_ubc * (1.0 - cos_theta) +
+             u_fr[i];
+}
+
 void bc_calc_rhs(orc_solver* o, int rk_stage) {
   const double gamma = o->prm.gamma;
+  // CbcRup::calcRhs (:3350-3358) at the stage's time
+  for (int ibf = 0; ibf < o->nbf; ++ibf) {
+    const int z = o->zone_bf[ibf];
+    if (int(o->bc[size_t(z)][0]) == CGX_BC_CBC_RUP && o->zone_u_face[size_t(z)]) rup_frame_state(o, ibf, o->time);
+  }
   // WmExchange::calcRhs (IdealGasSolverBcs.cpp:820-910): the velocity at each
   // face's exchange point, u + dudx (x_ex - x_cv) in the cell that holds it
   // (DataExchanger::exchangeCvDataWithGhosts, DataExchanger.hpp:442-501)
@@ -1186,6 +1225,10 @@ void bc_rk3_step(orc_solver* o, int rk_stage, double dt, bool init) {
   for (int ibf = 0; ibf < o->nbf; ++ibf) {
     const std::array<double, 5>& bc = o->bc[o->zone_bf[ibf]];
     const int kind = int(bc[0]);
+    if (init && kind == CGX_BC_CBC_RUP && o->zone_u_face[size_t(o->zone_bf[ibf])]) {
+      rup_frame_state(o, ibf, o->time);  // CbcRup::initData (:3320-3326)
+      continue;
+    }
     if (init && (kind == CGX_BC_WM_EXCHANGE_ADIABATIC || kind == CGX_BC_WM_EXCHANGE_ISOTHERMAL)) {
       // WmExchange::initialHook (:577-632)
       const int icv = o->cvobf[ibf];
@@ -1617,6 +1660,7 @@ extern "C" orc_solver* orc_create(const cgx_mesh_desc* m, const cgx_params* prm,
     o->zone_u_face.assign(m->nbf_zones, 0);
     o->u_bf.assign(3 * size_t(m->nbf), 0.0);
     o->ex_cv.assign(m->nbf, -1);
+    o->rup_u.assign(m->nbf_zones, {0.0, 0.0, 0.0});
     o->ex_dx.assign(3 * size_t(m->nbf), 0.0);
     o->wm_eq.assign(m->nbf_zones, {0.7, 1.0, 1.0e-4});
     o->ns_rho.assign(m->nbf, 0.0);
@@ -2083,6 +2127,7 @@ extern "C" int orc_set_bc_params(orc_solver* o, int zone, int kind, const double
       b.sp_vol = R * T_bc / p_bc;
       b.h = R * T_bc * gamma / (gamma - 1.0);
     } else if (kind == CGX_BC_CBC_RUP) {  // CbcRup::initData (:3268-3299)
+      o->rup_u[size_t(zone)] = {prm[1], prm[2], prm[3]};
       const double rho_bc = prm[0], p_bc = prm[4];
       const double T_bc = p_bc / rho_bc / R;
       for (int i = 0; i < 3; ++i) b.u[i] = prm[1 + i];
@@ -2180,7 +2225,7 @@ extern "C" int orc_set_bc_face_velocity(orc_solver* o, int zone, const double* u
   const int kind = int(o->bc[size_t(zone)][0]);
   if (kind != CGX_BC_WALL_ADIABATIC && kind != CGX_BC_WM_ALG_ADIABATIC && kind != CGX_BC_WM_EQ_ADIABATIC &&
       kind != CGX_BC_CBC_TOTAL_PT && kind != CGX_BC_NSCBC_MT && kind != CGX_BC_NSCBC_OUTLET_P &&
-      kind != CGX_BC_NSCBC_OUTLET_MDOT)
+      kind != CGX_BC_NSCBC_OUTLET_MDOT && kind != CGX_BC_CBC_RUP)
     return -1;
   int n = 0;
   for (int ibf = 0; ibf < o->nbf; ++ibf) n += (o->zone_bf[ibf] == zone);

@@ -446,3 +446,29 @@ def test_nscbc_rotating_frame_terms(chan):
     along_n = 0.5 * nb / np.linalg.norm(nb, axis=1)[:, None]
     assert np.abs(run(ufr0=along_n) - base).max() <= 1e-13 * np.abs(base).max()
     assert np.abs(run(rev=np.array([0.0, 0.2, 0.0])) - base).max() > 1e-9
+
+
+def test_rup_stationary_frame_aligned(chan):
+    """CBC_RUP with STATIONARY_FRAME in a rotating frame, its velocity along
+    the rotation axis and no frame velocity: the inflow stays u_bc, bit for
+    bit the zone without the option (CbcRup::initData, :3297-3328)."""
+    m = chan
+    prm = cases.tgv_params(Re=400.0)
+    x, y, z = m.x_cv[: m.ncv].T
+    u = np.stack([0.1 + 0.05 * np.sin(2 * np.pi * x / m.L[0]), 0.3 + 0.0 * y, 0.02 * np.cos(2 * np.pi * z / m.L[2])], 1)
+    rho, p = np.ones(m.ncv), np.full(m.ncv, prm.p_ref)
+    nz = int((m.zone_bf == 0).sum())
+    out = []
+    for frame in (False, True):
+        o = Oracle(m, prm)
+        o.set_bc_params(0, 12, [1.0, 0.0, 0.4, 0.0, 1.01 * prm.p_ref])
+        if frame:
+            o.set_bc_face_velocity(0, np.zeros((nz, 3)))
+        o.set_bc_params(1, RUNP, [1.0, -0.3, prm.p_ref])
+        o.set_frame_rotation([0.0, 0.03, 0.0])
+        o.set_state_primitive(rho, u, p)
+        o.init_complete()
+        assert o.step(3) == 0
+        out.append(np.concatenate([v.reshape(m.ncv, -1) for v in o.get_state()], 1))
+        o.close()
+    assert np.array_equal(out[0], out[1])

@@ -511,3 +511,37 @@ def test_nscbc_zones_in_a_rotating_frame(chan):
     with pytest.raises(cgx.CgxError, match="frame velocity"):
         s.initComplete()
     s.close()
+
+
+def test_rup_inflow_in_a_rotating_frame(chan):
+    """CBC_RUP with STATIONARY_FRAME (CbcRup, IdealGasSolverBcs.cpp:
+    3297-3358): an inflow velocity off the rotation axis turns by -|w| t
+    each stage (Rodrigues' formula) and adds the face's frame velocity;
+    10 steps within 1e-10 of the oracle."""
+    m, gm = chan
+    prm = cases.tgv_params(Re=400.0)
+    rev = np.array([0.0, 0.05, 0.0])
+    w = rev * 2.0 * np.pi
+    s = cgx.Solver(gm, prm)
+    o = Oracle(m, prm)
+    for h in (s, o):
+        h.set_bc_params(0, RUP, (1.0, 0.1, 0.4, 0.05, 1.01 * P0))
+        h.set_bc_params(1, RUNP, (1.0, -0.3, 0.99 * P0))
+    ufr = -np.cross(w, m.x_bf[m.zone_bf == 0])
+    s.set_bc_face_velocity(0, ufr)
+    o.set_bc_face_velocity(0, ufr)
+    s.set_frame_rotation(rev, m.x_cv[: m.ncv])
+    o.set_frame_rotation(rev)
+    st = _state(m, prm)
+    s.set_state_primitive(*st)
+    s.initComplete()
+    o.set_state_primitive(*st)
+    o.init_complete()
+    r = s.calcRhs(1)
+    ref, scale = o.calc_rhs(1)
+    assert (np.abs(r - ref) / np.maximum(np.abs(ref), scale)).max() <= 1e-12
+    assert s.step(10) == 0 and o.step(10) == 0
+    for a, b in zip(s.get_state(), o.get_state()):
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-10
+    s.close()
+    o.close()
