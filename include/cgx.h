@@ -415,7 +415,9 @@ int cgx_set_bc_params(cgx_solver* s, int zone, int kind, const double* params, i
 int cgx_set_bc_profile(cgx_solver* s, int zone, const double* bf_state, int nbf_zone);
 
 /* A velocity face by face, u_bf[nbf_zone][3], the zone's faces in the order
- * the mesh description lists them (NSCBC zones: the frame velocity u_fr =
+ * the mesh description lists them (CBC_RUP: the STATIONARY_FRAME velocity
+ * u_fr; its u_bc then turns with the frame, CbcRup::calcBfState, :3335-3348;
+ * NSCBC zones: the frame velocity u_fr =
  * -w x x_bf that the reference forms in a rotating frame, NscbcMt::initData,
  * :3752-3770: its part along the face joins NSCBC_MT's u_bc, and the
  * outlets' centrifugal term is w x u_fr; the outlets' Coriolis term needs no
